@@ -1,0 +1,327 @@
+"""Benchmark of the B200 TILD step (particle-steps/s) on the coacervate workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one per GPU; N > 1 runs independent replicas, one per rank -- the step does
+not shard): polyelectrolyte coacervate, 2,097,152 particles (8,000 + 8,000 chains of
+N=32, q = +1/-1, 512,000 counterions, neutral solvent), rho0 = 5, L = 74.85, 192^3 grid,
+pmeorder 3, `potential gaussian all all 5.0 0.7071` + `potential charges 1.0 0.5`,
+harmonic bonds k = 1.5, GJF dt = 0.005, Philox noise.  Synthetic data (numpy seed 2).
+
+value: particle-steps/s of K graph-replayed steps with all state resident in HBM, timed
+with CUDA events on the box's stream, max over ranks.  The per-step working set
+(about 0.8 GB of grids and particle arrays) is larger than the 126 MB L2, so no flush
+is needed between steps.
+e2e: the same metric through the C ABI for one job of S steps: positions uploaded from
+pinned host memory, S steps, positions read back; copies inside the timed region.
+--impl reference: the reference's step restated on the host cores (oracle CpuStep,
+FP32, all threads), same workload and metric, rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "matilda.ft_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "particle-steps/s"
+WORKLOAD = ("c2_coacervate: 2,097,152 particles, 192^3 grid, pmeorder 3, gaussian(all,all) + "
+            "smeared charges (lB 1.0, sigma 0.5), harmonic bonds, GJF dt 0.005")
+STAGES = ["deposit", "fft_x_fwd", "fft_y_fwd", "kspace_z", "fft_y_inv", "fft_x_inv", "particles"]
+KERNEL_NAMES = {"deposit": "k_deposit", "fft_x_fwd": "k_xfwd", "fft_y_fwd": "k_ypass<false>",
+                "kspace_z": "k_kspace_z", "fft_y_inv": "k_ypass<true>", "fft_x_inv": "k_xinv",
+                "particles": "k_particles"}
+KERNELS_PER_STEP = 8   # deposit, xfwd, yfwd, kspace_z, yinv, xinv, particles, tick
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def algorithmic_bytes(spec, nd=2, nfg=2, maxb=2, charged=True):
+    """Compulsory bytes per launch of each kernel: every input read once, every output
+    written once (no re-reads, no atomics read-modify-write)."""
+    N = spec.N
+    nx, ny, nz = (int(v) for v in spec.grid)
+    M = nx * ny * nz
+    hs = nz * ny * (nx // 2 + 1) * 8          # one half-spectrum field, complex64
+    npair = (nd + 1) // 2
+    qb = 4 if charged else 0
+    return {
+        "deposit": N * (12 + 4 + qb) + npair * M * 8,
+        "fft_x_fwd": npair * M * 8 + nd * hs,
+        "fft_y_fwd": 2 * nd * hs,
+        "kspace_z": nd * hs + 3 * nfg * hs,
+        "fft_y_inv": 2 * 3 * nfg * hs,
+        "fft_x_inv": 3 * nfg * hs + nfg * M * 16,
+        # x_t 12, x_{t-1} 12, x_{t+1} 12, noise r/w 24, flags 4, q, ids 4, bonds (nb 1,
+        # partners 4*maxb, types 1*maxb), partner positions assumed cached, records once
+        "particles": N * (12 + 12 + 12 + 24 + 4 + qb + 4 + 1 + 5 * maxb) + nfg * M * 16,
+    }
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            for k, n in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def make_spec(scale):
+    from tild_b200 import synth
+    return synth.config_c2(scale=scale)
+
+
+def cpu_sample(spec, threads, nsteps, warmup=1):
+    """The reference's step on the host cores (oracle CpuStep, FP32).  Returns
+    (particle-steps/s, seconds per step)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    nb, partner, btype = spec.partner_lists(2)
+    sysm = oracle.System(Dim=3, L=spec.L, Nx=spec.grid, order=spec.order, x=spec.x, types=spec.types,
+                         mass=np.ones(len(spec.species), np.float32),
+                         mobility=np.ones(len(spec.species), np.float32), species=spec.species,
+                         charges=spec.charges, nb=nb, partner=partner, btype=btype,
+                         bond_k=np.array([spec.bond_k], np.float32), bond_req=np.array([0.0], np.float32),
+                         bond_style=np.array([0], np.int32), potentials=spec.potentials, delt=spec.delt)
+    cs = oracle.CpuStep(sysm, threads, seed=spec.seed)
+    for _ in range(warmup):
+        cs.step()
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        cs.step()
+    dt = time.perf_counter() - t0
+    return spec.N * nsteps / dt, dt / nsteps
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return world, rank, local, pg
+
+
+def run_reference(args):
+    world, rank, local, _ = (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+                             int(os.environ.get("LOCAL_RANK", "0")), None)
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    # Each step is a bounded sample: a scaled replica of the workload (same density,
+    # chain length, charge fractions and grid spacing) sized so that W + K steps take
+    # about `--ref-budget` seconds on the host cores.
+    probe = make_spec(args.scale / 64.0)
+    _, t_probe = cpu_sample(probe, threads, 1, warmup=1)
+    per_step_full = t_probe * 64.0
+    s = min(1.0, args.ref_budget / max(1, args.steps + args.warmup) / per_step_full)
+    s = max(s, 1.0 / 512.0)
+    spec = make_spec(args.scale * s)
+    value, sec = cpu_sample(spec, threads, args.steps, warmup=args.warmup)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "particles": spec.N, "grid": [int(v) for v in spec.grid]},
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
+                             "sample": "%d steps (after %d warm-up) of a scaled replica of the workload (%d particles, "
+                                       "%s grid, same density and composition) with the reference's algorithm "
+                                       "restated on the host (stencil tables, deposit of every group, FP32 C2C "
+                                       "FFTs); full-size step estimated at %.1f s"
+                                       % (args.steps, args.warmup, spec.N, "x".join(str(int(v)) for v in spec.grid),
+                                          per_step_full)},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import tild_b200
+    world, rank, local, dist = dist_setup(args)
+    torch.cuda.set_device(local)
+    spec = make_spec(args.scale)
+    stream = torch.cuda.Stream(device=local)
+    box = tild_b200.box_from_spec(spec, device=local, options={"write_files": 0})
+    box.set_stream(stream.cuda_stream)
+    box.command("endBox")
+    info = box.info()
+    for _ in range(args.warmup):
+        box.step(1)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        box.step(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = world * spec.N * args.steps / (ms * 1e-3)
+
+    # end to end through the C ABI: pinned host positions -> S steps -> host positions
+    S = args.e2e_steps
+    hx = torch.empty((spec.N, 3), dtype=torch.float32).pin_memory()
+    hx.copy_(torch.from_numpy(box.positions()))
+    hout = torch.empty_like(hx).pin_memory()
+    import ctypes
+    L = tild_b200.lib()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    tild_b200._check(L.tild_box_set_positions(box._h, ctypes.c_void_p(hx.data_ptr())))
+    tild_b200._check(L.tild_box_step(box._h, S))
+    tild_b200._check(L.tild_box_get_positions(box._h, ctypes.c_void_p(hout.data_ptr())))
+    f1.record(stream)
+    torch.cuda.synchronize()
+    ems = f0.elapsed_time(f1)
+    if dist:
+        t = torch.tensor([ems], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ems = float(t.item())
+    e2e = world * spec.N * S / (ems * 1e-3)
+
+    # per-kernel durations: instrumented launches (an event after every kernel)
+    box.set_option("stage_timing", 1)
+    box.step(args.profile_steps)
+    box.set_option("stage_timing", 0)
+    st = np.zeros(8)
+    n = ctypes.c_int()
+    L.tild_box_stage_times(box._h, st.ctypes.data_as(ctypes.c_void_p), 8, ctypes.byref(n))
+    stage_s = dict(zip(STAGES, st[: n.value]))
+    ab = algorithmic_bytes(spec, nd=info.n_density_fields, nfg=info.n_force_groups, charged=True)
+    dom = max(stage_s, key=lambda k: stage_s[k])
+    peak, peak_kind = peaks()
+    achieved = ab[dom] / stage_s[dom] / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "dram_traffic_c2.json")
+    if os.path.exists(tf):
+        traffic = json.load(open(tf)).get(KERNEL_NAMES[dom])
+    step_bytes = sum(ab.values())
+
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            threads = os.cpu_count() or 1
+            cv, csec = cpu_sample(spec, threads, args.cpu_steps, warmup=0)
+            cpu = {"value": cv, "unit": METRIC, "cores": threads, "kind": "port",
+                   "sample": "%d full step(s) of the same workload, reference algorithm restated on the host "
+                             "(oracle CpuStep, FP32, OpenMP + scipy.fft), %.1f s per step" % (args.cpu_steps, csec)}
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (numpy seed 2)",
+            "config": {"workload": WORKLOAD, "particles": spec.N, "grid": [int(v) for v in spec.grid],
+                       "parallelism": "replicas" if world > 1 else "single", "rng": "philox",
+                       "l2": "inputs larger than L2 (%.2f GB moved per step by the kernels' compulsory traffic)"
+                             % (step_bytes / 1e9)},
+            "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": traffic, "algorithmic_bytes": ab[dom],
+                         "kernel_ms": {k: v * 1e3 for k, v in stage_s.items()},
+                         "step_algorithmic_gbs": step_bytes / (ms / args.steps * 1e-3) / 1e9},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e, "unit": METRIC, "steps_per_job": S,
+                    "h2d_bytes_per_step": spec.N * 12 / S, "d2h_bytes_per_step": spec.N * 12 / S},
+            "gpu_launches": KERNELS_PER_STEP * args.steps,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    box.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0, help="workload scale (tests only)")
+    ap.add_argument("--e2e-steps", type=int, default=100)
+    ap.add_argument("--profile-steps", type=int, default=10)
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ref-budget", type=float, default=150.0, help="seconds for the reference arm")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    return run_reference(args) if args.impl == "reference" else run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,180 @@
+/*
+ * tild_b200.h -- C ABI of the B200-native TILD particle-mesh step.
+ *
+ * One opaque box object replaces MATILDA.FT's PS_Box (PS_Box.h:19-212) together with
+ * the objects it owns (PS_Group, PS_Potential and its kinds, Integrator GJF/EM,
+ * PS_Species).  MATILDA.FT has no C ABI or plugin loader: its "API" is the input
+ * script plus those C++ classes.  Each entry point below names the reference member
+ * or code path it replaces (file:line in the MATILDA.FT source tree).
+ *
+ * Conventions
+ *  - Every call returns an int status (TILD_OK == 0); nothing calls exit().  The
+ *    reference dies instead (die.cu:7-20).  tild_last_error() returns the message of
+ *    the last failing call on the calling thread.
+ *  - All pointers are caller-owned HOST buffers; device memory is owned by the box.
+ *  - A box is used from one host thread at a time (thread-compatible, not
+ *    thread-safe) and issues its work on one CUDA stream (tild_box_set_stream).
+ *  - Positions are float[n*Dim] interleaved (x fastest) as in the reference.
+ */
+#ifndef TILD_B200_H
+#define TILD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum tild_status {
+    TILD_OK = 0,
+    TILD_ERR_ARG = 1,         /* bad argument / null pointer / size                  */
+    TILD_ERR_PARSE = 2,       /* script or data-file error (reference: die())        */
+    TILD_ERR_IO = 3,          /* file could not be opened or written                 */
+    TILD_ERR_CUDA = 4,        /* a CUDA runtime call or kernel failed                */
+    TILD_ERR_STATE = 5,       /* call out of order (e.g. step before endBox)         */
+    TILD_ERR_UNSUPPORTED = 6, /* a script feature outside the TILD hot path          */
+    TILD_ERR_DEVICE = 7       /* device-side check failed (error flag set by a kernel)*/
+};
+
+typedef struct tild_box tild_box;
+
+/* Summary of a box after endBox (PS_Box public members used by callers). */
+typedef struct tild_box_info {
+    int64_t nstot;        /* particles                                       */
+    int32_t dim;          /* Dim                                             */
+    int32_t nx[3];        /* grid                                            */
+    float L[3];           /* box lengths                                     */
+    int32_t pmeorder;     /* spline order                                    */
+    int32_t n_groups;     /* psGroup.size()                                  */
+    int32_t n_potentials; /* potentials.size()                               */
+    int32_t n_density_fields; /* distinct density fields the potentials read */
+    int32_t n_force_groups;   /* groups that receive grid forces             */
+    int32_t n_bond_types;
+    int64_t n_bonds;      /* nBondsTot                                       */
+    int64_t step;         /* steps taken so far (totSteps)                   */
+    int64_t device_bytes; /* device memory held by this box                  */
+} tild_box_info;
+
+/* Version / build string of the library. */
+const char *tild_version(void);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *tild_last_error(void);
+
+/* Create an empty PS box on CUDA device `device` (reference: BoxFactory + PS_Box ctor,
+ * Box.cu:491-507, PS_Box.cu:585-589).  Defaults follow PS_Box::readInput
+ * (PS_Box_initialization.cu:36-62). */
+int tild_box_create(int device, tild_box **out);
+
+/* Free every device and host resource of the box (PS_Box::~PS_Box, PS_Box.cu:578). */
+int tild_box_destroy(tild_box *box);
+
+/* Use this CUDA stream (cudaStream_t passed as void*) for all work of the box; NULL
+ * selects a stream the box creates itself.  The reference runs on the legacy default
+ * stream (one host thread, PS_Box.cu:73-207). */
+int tild_box_set_stream(tild_box *box, void *cuda_stream);
+
+/* Set the directory that relative file names in the script (readData, datFileName)
+ * resolve against.  The reference resolves them against the process working dir. */
+int tild_box_set_base_dir(tild_box *box, const char *dir);
+
+/* Feed one line of the `box ps` block, parsed word by word exactly like
+ * PS_Box::readInput (PS_Box_initialization.cu:68-339).  The line "endBox" runs
+ * finishInitialization (PS_Box_initialization.cu:352-569). */
+int tild_box_command(tild_box *box, const char *line);
+
+/* Feed a whole `box ps ... endBox` block (several lines; "box ps" itself optional);
+ * the block must end with endBox (PS_Box::readInput, PS_Box_initialization.cu:32-345). */
+int tild_box_read_input(tild_box *box, const char *text);
+
+/* Particles supplied as arrays instead of `readData` (PS_Box::readDataConfig atoms
+ * section, PS_Box_initialization.cu:858-884).  type is 0-based into the declared
+ * species; mol may be NULL; q may be NULL unless doCharges was given.  Must precede
+ * endBox. */
+int tild_box_set_particles(tild_box *box, int64_t n, const float *x, const int32_t *type,
+                           const int32_t *mol, const float *q);
+
+/* Bonds supplied as arrays (readDataConfig bonds section,
+ * PS_Box_initialization.cu:887-926): pairs[2*nbonds] 0-based particle ids,
+ * btype[nbonds] 0-based bond types (NULL = all type 0).  Must precede endBox. */
+int tild_box_set_bonds(tild_box *box, int64_t nbonds, const int64_t *pairs,
+                       const int32_t *btype);
+
+/* Options outside the reference grammar.  Keys:
+ *   "rng"            0 = Philox4x32-10 (default), 1 = cuRAND XORWOW compatible mode
+ *                    (same curand_init/curand_normal calls as device_utils.cu:465-472,
+ *                    ps_integratorGJF.cu:140)
+ *   "deterministic"  1 = deposit by exact fixed-point sums (bit-reproducible), 0 = fast
+ *   "bspline4_exact" 1 = true quartic B-spline at pmeorder 4 instead of the
+ *                    reference's weights (ps_grid_utils.cu:57)
+ *   "write_files"    0 = do not write ps_data.dat / data files (default 1)
+ *   "sort_interval"  steps between spatial re-sorts of the particle arrays (0 = never)
+ * Must precede endBox except "write_files". */
+int tild_box_set_option(tild_box *box, const char *key, int64_t value);
+
+/* JSON description of the parsed box (species, groups, potentials, integrators, grid,
+ * box lengths) -- the state PS_Box holds after readInput.  Works before endBox and
+ * without a GPU.  Writes at most size bytes including the terminating NUL; *needed
+ * (may be NULL) receives the full size. */
+int tild_box_describe(const tild_box *box, char *buf, int64_t size, int64_t *needed);
+
+/* Box summary (valid after endBox). */
+int tild_box_get_info(const tild_box *box, tild_box_info *out);
+
+/* `run nvt nsteps`: PS_Box::NVT (PS_Box.cu:210-234) -- writeData(-1), nsteps calls of
+ * doTimeStep with thermo logging every logFreq steps to datFileName (PS_Box.cu:339-370),
+ * then the final writeData and final.input.data. */
+int tild_box_run_nvt(tild_box *box, int64_t nsteps);
+
+/* nsteps time steps with no I/O and no thermo (PS_Box::doTimeStep, PS_Box.cu:73-162,
+ * without the I/O branch :168-205).  Runs as replays of a captured CUDA graph. */
+int tild_box_step(tild_box *box, int64_t nsteps);
+
+/* Total force on every particle at the current positions, f[n*Dim] (PS_Box::forces,
+ * PS_Box.cu:240-278, after the deposit of :97-114).  Positions are not changed. */
+int tild_box_forces(tild_box *box, float *f_out);
+
+/* Thermodynamic terms at the current positions (PS_Box::computeThermoProps,
+ * PS_Box.cu:282-317) in FP64: out[0] = Upe, out[1] = Ubond, out[2+i] = energy of
+ * potential i; then, if nout >= 2 + npot + 6, the bond virial sum (6 comps, 3-D).
+ * Returns the number of values written through *nwritten (may be NULL). */
+int tild_box_thermo(tild_box *box, double *out, int nout, int *nwritten);
+
+/* Copy positions device -> host (x_out[n*Dim]) / host -> device.  Setting positions
+ * also resets the GJF old positions to them (GJF::finishInitialization,
+ * ps_integratorGJF.cu:48-51). */
+int tild_box_get_positions(tild_box *box, float *x_out);
+int tild_box_set_positions(tild_box *box, const float *x_in);
+
+/* Density field of group `group` at the current positions (PS_Group::d_rho, or d_rhoq
+ * when charge_channel != 0), rho_out[M] in the reference's x-fastest order. */
+int tild_box_get_density(tild_box *box, const char *group, int charge_channel, float *rho_out);
+
+/* Stencil indices and weights of every particle at the current positions
+ * (d_calcGridWeights, ps_grid_utils.cu:74-204): inds_out/w_out[n*(pmeorder+1)^Dim],
+ * same order and float arithmetic as the reference (weights divided by gvol). */
+int tild_box_grid_weights(tild_box *box, int32_t *inds_out, float *w_out);
+
+/* Energies recorded by the last run (one row per logged step: step, Ubond, pot...)
+ * copied to out[rows*cols]; rows and cols report the shape.  Pass out=NULL to query. */
+int tild_box_get_log(tild_box *box, double *out, int64_t *rows, int32_t *cols);
+
+/* Execute a whole MATILDA.FT input script file (main.cu:21-156): `box ps` blocks,
+ * `run nvt N`, `modify potential remove i`; unknown top-level words are ignored as in
+ * the reference.  Output files are written next to the script. */
+int tild_run_script_file(const char *path, int device);
+
+/* Average device seconds per launch of each kernel during the last tild_box_step call
+ * made with option "stage_timing" = 1 (then the steps run as individual launches with a
+ * CUDA event after every kernel instead of as graph replays):
+ * out[0] zero + deposit, [1] x-axis forward FFT, [2] y-axis forward FFT,
+ * [3] z-axis FFT + k-space multiply + inverse z FFT, [4] y-axis inverse FFT,
+ * [5] x-axis inverse FFT, [6] particle pass.  The reference has no counterpart (it keeps
+ * second-resolution timers only, timing.h:8-12).  *n receives the count written. */
+int tild_box_stage_times(tild_box *box, double *out, int nmax, int *n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TILD_B200_H */

@@ -1,0 +1,314 @@
+// tild_api.cpp -- extern "C" boundary of the B200 TILD library (declared in
+// include/tild_b200.h).  Converts C++ exceptions into status codes; never exits.
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+
+#include "tild_b200.h"
+#include "tild_box.h"
+
+struct tild_box {
+    tild::Box *impl;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &m)
+{
+    g_err = m;
+    return code;
+}
+
+template <typename F>
+int guarded(F &&f)
+{
+    try {
+        f();
+        g_err.clear();
+        return TILD_OK;
+    } catch (const tild::BoxError &e) {
+        return fail(e.code, e.msg);
+    } catch (const std::bad_alloc &) {
+        return fail(TILD_ERR_ARG, "host out of memory");
+    } catch (const std::exception &e) {
+        return fail(TILD_ERR_ARG, e.what());
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *tild_version(void) { return "tild-b200 1.0 (sm_100a)"; }
+
+const char *tild_last_error(void) { return g_err.c_str(); }
+
+int tild_box_create(int device, tild_box **out)
+{
+    if (!out) return fail(TILD_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess) ndev = 0;
+    if (device < 0 || (ndev > 0 && device >= ndev))   // main.cu:63-76
+        return fail(TILD_ERR_ARG, "Device " + std::to_string(device) + " not found; only detecting " +
+                                      std::to_string(ndev) + " devices");
+    // The device is bound at endBox, so scripts can be parsed and checked without a GPU.
+    return guarded([&] { *out = new tild_box{new tild::Box(device)}; });
+}
+
+int tild_box_destroy(tild_box *box)
+{
+    if (!box) return TILD_OK;
+    delete box->impl;
+    delete box;
+    return TILD_OK;
+}
+
+#define NEED_BOX                                                   \
+    if (!box || !box->impl) return fail(TILD_ERR_ARG, "box is NULL")
+
+int tild_box_set_stream(tild_box *box, void *cuda_stream)
+{
+    NEED_BOX;
+    return guarded([&] { box->impl->setStream(reinterpret_cast<cudaStream_t>(cuda_stream)); });
+}
+
+int tild_box_set_base_dir(tild_box *box, const char *dir)
+{
+    NEED_BOX;
+    if (!dir) return fail(TILD_ERR_ARG, "dir is NULL");
+    return guarded([&] { box->impl->setBaseDir(dir); });
+}
+
+int tild_box_command(tild_box *box, const char *line)
+{
+    NEED_BOX;
+    if (!line) return fail(TILD_ERR_ARG, "line is NULL");
+    return guarded([&] { box->impl->command(line); });
+}
+
+int tild_box_read_input(tild_box *box, const char *text)
+{
+    NEED_BOX;
+    if (!text) return fail(TILD_ERR_ARG, "text is NULL");
+    return guarded([&] {
+        std::istringstream in(text);
+        std::string line;
+        bool ended = false;
+        while (std::getline(in, line)) {
+            std::istringstream w(line);
+            std::string first, second;
+            w >> first >> second;
+            if (first == "box") {
+                if (second != "ps") throw tild::BoxError{TILD_ERR_UNSUPPORTED, "box style '" + second + "' (only ps)"};
+                continue;
+            }
+            box->impl->command(line);
+            if (box->impl->initialized()) {
+                ended = true;
+                break;
+            }
+        }
+        if (!ended) throw tild::BoxError{TILD_ERR_PARSE, "input ended before endBox"};
+    });
+}
+
+int tild_box_set_particles(tild_box *box, int64_t n, const float *x, const int32_t *type, const int32_t *mol,
+                           const float *q)
+{
+    NEED_BOX;
+    return guarded([&] { box->impl->setParticles(n, x, type, mol, q); });
+}
+
+int tild_box_set_bonds(tild_box *box, int64_t nbonds, const int64_t *pairs, const int32_t *btype)
+{
+    NEED_BOX;
+    return guarded([&] { box->impl->setBonds(nbonds, pairs, btype); });
+}
+
+int tild_box_set_option(tild_box *box, const char *key, int64_t value)
+{
+    NEED_BOX;
+    if (!key) return fail(TILD_ERR_ARG, "key is NULL");
+    return guarded([&] { box->impl->setOption(key, value); });
+}
+
+int tild_box_get_info(const tild_box *box, tild_box_info *out)
+{
+    NEED_BOX;
+    if (!out) return fail(TILD_ERR_ARG, "out is NULL");
+    const tild::Box &b = *box->impl;
+    std::memset(out, 0, sizeof(*out));
+    out->nstot = b.nstot;
+    out->dim = b.Dim;
+    for (int j = 0; j < 3; j++) {
+        out->nx[j] = b.Nx[j];
+        out->L[j] = b.L[j];
+    }
+    out->pmeorder = b.pmeorder;
+    out->n_groups = (int32_t)b.psGroup.size();
+    out->n_potentials = (int32_t)b.potentials.size();
+    out->n_density_fields = b.nDensityFields();
+    out->n_force_groups = b.nForceGroups();
+    out->n_bond_types = b.nBondTypes;
+    out->n_bonds = b.nBondsTot;
+    out->step = b.totSteps;
+    out->device_bytes = b.deviceBytes();
+    return TILD_OK;
+}
+
+int tild_box_describe(const tild_box *box, char *buf, int64_t size, int64_t *needed)
+{
+    NEED_BOX;
+    const std::string j = box->impl->describe();
+    if (needed) *needed = (int64_t)j.size() + 1;
+    if (buf && size > 0) {
+        const size_t n = std::min<size_t>((size_t)size - 1, j.size());
+        std::memcpy(buf, j.data(), n);
+        buf[n] = '\0';
+    }
+    return TILD_OK;
+}
+
+int tild_box_run_nvt(tild_box *box, int64_t nsteps)
+{
+    NEED_BOX;
+    if (nsteps < 0) return fail(TILD_ERR_ARG, "nsteps < 0");
+    return guarded([&] { box->impl->NVT(nsteps); });
+}
+
+int tild_box_step(tild_box *box, int64_t nsteps)
+{
+    NEED_BOX;
+    if (nsteps < 0) return fail(TILD_ERR_ARG, "nsteps < 0");
+    return guarded([&] { box->impl->steps(nsteps); });
+}
+
+int tild_box_forces(tild_box *box, float *f_out)
+{
+    NEED_BOX;
+    if (!f_out) return fail(TILD_ERR_ARG, "f_out is NULL");
+    return guarded([&] { box->impl->forces(f_out); });
+}
+
+int tild_box_thermo(tild_box *box, double *out, int nout, int *nwritten)
+{
+    NEED_BOX;
+    if (!out && nout > 0) return fail(TILD_ERR_ARG, "out is NULL");
+    return guarded([&] {
+        std::vector<double> t = box->impl->thermo();
+        const int n = std::min<int>(nout, (int)t.size());
+        for (int k = 0; k < n; k++) out[k] = t[k];
+        if (nwritten) *nwritten = n;
+    });
+}
+
+int tild_box_get_positions(tild_box *box, float *x_out)
+{
+    NEED_BOX;
+    if (!x_out) return fail(TILD_ERR_ARG, "x_out is NULL");
+    return guarded([&] { box->impl->getPositions(x_out); });
+}
+
+int tild_box_set_positions(tild_box *box, const float *x_in)
+{
+    NEED_BOX;
+    if (!x_in) return fail(TILD_ERR_ARG, "x_in is NULL");
+    return guarded([&] { box->impl->setPositions(x_in); });
+}
+
+int tild_box_get_density(tild_box *box, const char *group, int charge_channel, float *rho_out)
+{
+    NEED_BOX;
+    if (!group || !rho_out) return fail(TILD_ERR_ARG, "NULL argument");
+    return guarded([&] { box->impl->getDensity(group, charge_channel, rho_out); });
+}
+
+int tild_box_grid_weights(tild_box *box, int32_t *inds_out, float *w_out)
+{
+    NEED_BOX;
+    if (!inds_out || !w_out) return fail(TILD_ERR_ARG, "NULL argument");
+    return guarded([&] { box->impl->gridWeights(inds_out, w_out); });
+}
+
+int tild_box_get_log(tild_box *box, double *out, int64_t *rows, int32_t *cols)
+{
+    NEED_BOX;
+    const auto &L = box->impl->logRows;
+    const int32_t c = 2 + (int32_t)box->impl->potentials.size();
+    if (rows) *rows = (int64_t)L.size();
+    if (cols) *cols = c;
+    if (out)
+        for (size_t r = 0; r < L.size(); r++)
+            for (int32_t k = 0; k < c; k++) out[r * c + k] = k < (int32_t)L[r].size() ? L[r][k] : 0.0;
+    return TILD_OK;
+}
+
+int tild_box_stage_times(tild_box *box, double *out, int nmax, int *n)
+{
+    NEED_BOX;
+    std::vector<double> v;
+    box->impl->stageTimes(v);
+    const int k = std::min<int>(nmax, (int)v.size());
+    for (int i = 0; i < k; i++) out[i] = v[i];
+    if (n) *n = k;
+    return TILD_OK;
+}
+
+// main.cu:21-156: box blocks, run nvt, modify; other top-level words are ignored.
+int tild_run_script_file(const char *path, int device)
+{
+    if (!path) return fail(TILD_ERR_ARG, "path is NULL");
+    std::ifstream in(path);
+    if (!in) return fail(TILD_ERR_IO, std::string("cannot open ") + path);
+    std::string dir = path;
+    const size_t sl = dir.find_last_of('/');
+    dir = (sl == std::string::npos) ? "." : dir.substr(0, sl);
+    tild::Box *box = nullptr;
+    int rc = guarded([&] {
+        std::string line;
+        while (std::getline(in, line)) {
+            if (line.empty() || line[0] == '#') continue;
+            std::istringstream iss(line);
+            std::string word;
+            iss >> word;
+            if (word == "box") {
+                std::string style;
+                iss >> style;
+                if (style == "fts") throw tild::BoxError{TILD_ERR_UNSUPPORTED, "fts boxes are outside the TILD step"};
+                if (style != "ps") throw tild::BoxError{TILD_ERR_PARSE, style + " is not a valid box style yet"};
+                if (box) throw tild::BoxError{TILD_ERR_UNSUPPORTED, "only one box per script"};
+                box = new tild::Box(device);
+                box->setBaseDir(dir);
+                box->echo = true;
+                while (!box->initialized() && std::getline(in, line)) box->command(line);
+                if (!box->initialized()) throw tild::BoxError{TILD_ERR_PARSE, "input ended before endBox"};
+            } else if (word == "run") {
+                std::string kind;
+                iss >> kind;
+                if (!box) throw tild::BoxError{TILD_ERR_STATE, "run before any box"};
+                if (kind == "nvt") {
+                    long long n = 0;
+                    iss >> n;
+                    box->NVT(n);
+                } else if (kind == "vt" || kind == "findspinodal" || kind == "findSpinodal") {
+                    throw tild::BoxError{TILD_ERR_PARSE, "invalid box style trying to run const 'vt' simulation"};
+                } else {
+                    throw tild::BoxError{TILD_ERR_PARSE, kind + " is an invalid global command!"};
+                }
+            } else if (word == "modify") {
+                if (!box) throw tild::BoxError{TILD_ERR_STATE, "modify before any box"};
+                std::string rest;
+                std::getline(iss, rest);
+                box->modifyBox(rest);
+            }
+        }
+    });
+    delete box;
+    return rc;
+}
+
+}  // extern "C"

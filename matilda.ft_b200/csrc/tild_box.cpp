@@ -1,0 +1,1256 @@
+// tild_box.cpp -- PS box host logic: script grammar, data files, plan building and the
+// per-step launch sequence of the B200 TILD pipeline.
+//
+// Reference behaviour restated here (MATILDA.FT source tree):
+//   PS_Box::readInput           PS_Box_initialization.cu:32-345 (word-by-word grammar)
+//   PS_Box::finishInitialization PS_Box_initialization.cu:352-569
+//   PS_Box::createDefaultGroups PS_Box_initialization.cu:573-587
+//   PS_Box::readDataConfig      PS_Box_initialization.cu:787-997
+//   PSPotentialFactory          ps_potential.cu:294-333, kinds' ctors (gaussian/erf2/erfG/charges)
+//   IntegratorFactory / ctor    ps_integrator.cu:18-69
+//   PS_Box::NVT, doTimeStep     PS_Box.cu:73-234; writeData PS_Box.cu:339-370
+//   PS_Box::writeDataConfig     PS_Box.cu:629-748; modifyBox PS_Box.cu:848-870
+#include "tild_box.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <numeric>
+#include <sstream>
+
+#include "tild_b200.h"
+
+namespace tild {
+
+void init_fft_attributes();
+
+namespace {
+
+std::vector<std::string> split(const std::string &line)
+{
+    std::vector<std::string> w;
+    std::istringstream iss(line);
+    std::string s;
+    while (iss >> s) w.push_back(s);
+    return w;
+}
+
+[[noreturn]] void fail(int code, const std::string &msg) { throw BoxError{code, msg}; }
+
+const std::string &need(const std::vector<std::string> &w, size_t &i, const char *what)
+{
+    if (i >= w.size()) fail(TILD_ERR_PARSE, std::string("missing value for ") + what);
+    return w[i++];
+}
+
+double dnum(const std::vector<std::string> &w, size_t &i, const char *what)
+{
+    const std::string &s = need(w, i, what);
+    char *end = nullptr;
+    double v = std::strtod(s.c_str(), &end);
+    if (end == s.c_str() || *end != '\0') fail(TILD_ERR_PARSE, std::string("bad number '") + s + "' for " + what);
+    return v;
+}
+
+float fnum(const std::vector<std::string> &w, size_t &i, const char *what)
+{
+    const std::string &s = need(w, i, what);
+    char *end = nullptr;
+    float v = std::strtof(s.c_str(), &end);
+    if (end == s.c_str() || *end != '\0') fail(TILD_ERR_PARSE, std::string("bad number '") + s + "' for " + what);
+    return v;
+}
+
+long long inum(const std::vector<std::string> &w, size_t &i, const char *what)
+{
+    const std::string &s = need(w, i, what);
+    char *end = nullptr;
+    long long v = std::strtoll(s.c_str(), &end, 10);
+    if (end == s.c_str() || *end != '\0') fail(TILD_ERR_PARSE, std::string("bad integer '") + s + "' for " + what);
+    return v;
+}
+
+}  // namespace
+
+double PS_Potential::T0() const
+{
+    const double PI4 = 12.566370614359172953850573533118;
+    const double v = PI4 * (double)Rp * Rp * Rp / 3.0;
+    if (kind == POT_ERF2) return v * v;
+    if (kind == POT_ERFG) return v;
+    return 1.0;
+}
+
+// =====================================================================================
+Box::Box(int dev) : device(dev)
+{
+    RANDSEED = (long long)time(nullptr);   // idum = RANDSEED = time(0) (:45)
+}
+
+Box::~Box()
+{
+    dropGraphs();
+    freeDevice();
+    if (hKsPinned) cudaFreeHost(hKsPinned);
+    if (ownStream && stream) cudaStreamDestroy(stream);
+}
+
+void Box::ck(cudaError_t e, const char *what) const
+{
+    if (e != cudaSuccess) fail(TILD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+T *Box::dalloc(size_t count)
+{
+    void *p = nullptr;
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    ck(cudaMalloc(&p, bytes), "cudaMalloc");
+    allocs.push_back(p);
+    devBytes += (int64_t)bytes;
+    return reinterpret_cast<T *>(p);
+}
+
+void Box::freeDevice()
+{
+    cudaSetDevice(device);
+    for (void *p : allocs) cudaFree(p);
+    allocs.clear();
+    devBytes = 0;
+}
+
+std::string Box::resolve(const std::string &name) const
+{
+    if (name.empty() || name[0] == '/' || baseDir.empty() || baseDir == ".") return name;
+    return baseDir + "/" + name;
+}
+
+void Box::setStream(cudaStream_t st)
+{
+    if (ownStream && stream) cudaStreamDestroy(stream);
+    ownStream = false;
+    stream = st;
+    dropGraphs();
+}
+
+void Box::setOption(const std::string &key, int64_t v)
+{
+    if (key == "write_files") { writeFiles = (int)v; return; }
+    if (key == "echo") { echo = v != 0; return; }
+    if (key == "stage_timing") { stageTiming = (int)v; return; }
+    if (ready && key != "sort_interval") fail(TILD_ERR_STATE, "option '" + key + "' must be set before endBox");
+    if (key == "rng") rngCompat = (int)v;
+    else if (key == "deterministic") deterministic = (int)v;
+    else if (key == "bspline4_exact") exact4 = (int)v;
+    else if (key == "sort_interval") { /* particle order is kept; accepted for API stability */ }
+    else fail(TILD_ERR_ARG, "unknown option '" + key + "'");
+}
+
+// ---------------------------------------------------------------------------------------
+// Script grammar
+// ---------------------------------------------------------------------------------------
+void Box::command(const std::string &line)
+{
+    if (ready) fail(TILD_ERR_STATE, "box is already initialised (endBox was seen)");
+    if (line.empty() || line[0] == '#') return;   // PS_Box_initialization.cu:71-72
+    std::vector<std::string> w = split(line);
+    size_t i = 0;
+    while (i < w.size()) parseWords(w, i);
+}
+
+void Box::parseWords(std::vector<std::string> &w, size_t &i)
+{
+    const std::string fw = w[i++];
+    if (fw == "endBox") {
+        i = w.size();
+        finishInitialization();
+        return;
+    }
+    if (fw == "angle") {
+        (void)inum(w, i, "angle type");
+        const std::string style = need(w, i, "angle style");
+        (void)dnum(w, i, "angle k");
+        if (style == "harmonic") (void)dnum(w, i, "angle theta");
+        else if (style != "wlc") fail(TILD_ERR_PARSE, "Angle style not supported!");
+    } else if (fw == "blocksize" || fw == "blockSize") {
+        blockSize = (int)inum(w, i, "blockSize");
+    } else if (fw == "bond") {
+        const long long bt = inum(w, i, "bond type");
+        if (bt < 1 || bt > kMaxBondTypes) fail(TILD_ERR_PARSE, "bond type out of range (1.." + std::to_string(kMaxBondTypes) + ")");
+        if ((size_t)bt > bondK.size()) {
+            bondK.resize(bt, 0.f);
+            bondReq.resize(bt, 0.f);
+            bondStyle.resize(bt, 0);
+        }
+        const std::string style = need(w, i, "bond style");
+        bondK[bt - 1] = fnum(w, i, "bond k");
+        bondReq[bt - 1] = fnum(w, i, "bond r_eq");
+        if (style == "harmonic") bondStyle[bt - 1] = 0;
+        else if (style == "fene" || style == "FENE") bondStyle[bt - 1] = 1;
+        else fail(TILD_ERR_PARSE, "Bond type not supported!");
+        nBondTypes = (int)bondK.size();
+    } else if (fw == "boxLengths") {
+        if (!readDimension) fail(TILD_ERR_PARSE, "boxLengths read before Dim was specified");
+        for (int j = 0; j < Dim; j++) L[j] = fnum(w, i, "boxLengths");
+    } else if (fw == "compute") {
+        fail(TILD_ERR_UNSUPPORTED, "compute is outside the TILD step (avg_sk is never initialised in the reference)");
+    } else if (fw == "datFileName" || fw == "dat_file_name") {
+        datFileName = need(w, i, "datFileName");
+    } else if (fw == "Dim") {
+        Dim = (int)inum(w, i, "Dim");
+        if (Dim != 2 && Dim != 3) fail(TILD_ERR_PARSE, "Dim must be 2 or 3");
+        readDimension = true;
+    } else if (fw == "doCharges") {
+        if (!doCharges) {
+            doCharges = true;
+            if (nstot > 0) charges.assign(nstot, 0.f);
+        }
+    } else if (fw == "fieldFreq" || fw == "field_freq" || fw == "gsdFreq" || fw == "gsd_freq") {
+        (void)inum(w, i, fw.c_str());
+        if (i < w.size()) {
+            const std::string t = need(w, i, "logspace");
+            if (t != "logspace" && t != "log_space" && t != "logSpace")
+                fail(TILD_ERR_PARSE, "invalid option to " + fw);
+            (void)dnum(w, i, "log scale");
+        }
+    } else if (fw == "grid") {
+        if (!readDimension) fail(TILD_ERR_PARSE, "Dim must be defined before grid!");
+        for (int j = 0; j < Dim; j++) Nx[j] = (int)inum(w, i, "grid");
+    } else if (fw == "group") {
+        PS_Group g;
+        g.name = need(w, i, "group name");
+        const std::string s1 = need(w, i, "group style");
+        if (s1 != "types") fail(TILD_ERR_UNSUPPORTED, "group style '" + s1 + "' (only 'types')");
+        std::vector<int> tids;
+        while (i < w.size()) tids.push_back(findSpeciesInteger(w[i++]));
+        for (int64_t p = 0; p < nstot; p++)
+            if (std::find(tids.begin(), tids.end(), intSpecies[p]) != tids.end()) g.siteList.push_back((int)p);
+        g.inputCommand = "group " + g.name;
+        psGroup.push_back(g);
+    } else if (fw == "gsdName" || fw == "gsd_name" || fw == "trajFileName") {
+        (void)need(w, i, fw.c_str());
+    } else if (fw == "integrator") {
+        Integrator in;
+        in.groupName = need(w, i, "integrator group");
+        in.name = need(w, i, "integrator name");
+        if (i < w.size()) {
+            const std::string kw = need(w, i, "integrator option");
+            if (kw == "delt") in.delt = fnum(w, i, "delt");
+            else fail(TILD_ERR_PARSE, "Invalid keyword in Integrator command");
+        }
+        if (in.name == "VV") fail(TILD_ERR_UNSUPPORTED, "integrator VV is outside the TILD step (GJF, EM)");
+        if (in.name != "GJF" && in.name != "EM") fail(TILD_ERR_PARSE, in.name + " is not a valid Integrator");
+        integrators.push_back(in);
+    } else if (fw == "initDataFileName") {
+        initDataFileName = need(w, i, "initDataFileName");
+    } else if (fw == "logFreq" || fw == "logfreq") {
+        logFreq = (int)inum(w, i, "logFreq");
+        if (logFreq <= 0) fail(TILD_ERR_PARSE, "logFreq must be positive");
+    } else if (fw == "MAXANGLES") {
+        if (nstot > 0) fail(TILD_ERR_PARSE, "MAXANGLES must be set before defining any molecules");
+        MAXANGLES = (int)inum(w, i, "MAXANGLES");
+    } else if (fw == "MAXBONDS") {
+        if (nstot > 0) fail(TILD_ERR_PARSE, "MAXBONDS must be set before defining any molecules");
+        MAXBONDS = (int)inum(w, i, "MAXBONDS");
+        if (MAXBONDS < 1 || MAXBONDS > 255) fail(TILD_ERR_PARSE, "MAXBONDS out of range");
+    } else if (fw == "molecule") {
+        fail(TILD_ERR_UNSUPPORTED, "molecule builders are outside the TILD step; use readData");
+    } else if (fw == "Nr") {
+        Nr = (int)inum(w, i, "Nr");
+    } else if (fw == "NSEXTRA" || fw == "nsextra") {
+        NSEXTRA = (int)inum(w, i, "NSEXTRA");
+    } else if (fw == "Nx") {
+        Nx[0] = (int)inum(w, i, "Nx");
+    } else if (fw == "Ny") {
+        Nx[1] = (int)inum(w, i, "Ny");
+    } else if (fw == "Nz") {
+        if (Dim != 3) fail(TILD_ERR_PARSE, "Nz supplied in a non-3D simulation!");
+        Nx[2] = (int)inum(w, i, "Nz");
+    } else if (fw == "pmeorder") {
+        pmeorder = (int)inum(w, i, "pmeorder");
+        if (pmeorder < 0 || pmeorder > 4) fail(TILD_ERR_PARSE, "pmeorder must be 0..4");
+    } else if (fw == "potential") {
+        addPotential(w, i);
+    } else if (fw == "neighbor_list") {
+        fail(TILD_ERR_UNSUPPORTED, "neighbor_list is only used by DPD, outside the TILD step");
+    } else if (fw == "randSeed" || fw == "RAND_SEED" || fw == "RANDSEED") {
+        RANDSEED = inum(w, i, "randSeed");
+    } else if (fw == "readData") {
+        readDataConfig(need(w, i, "readData file"));
+    } else if (fw == "rho0") {
+        rho0 = dnum(w, i, "rho0");
+    } else if (fw == "species") {
+        if (i >= w.size()) fail(TILD_ERR_PARSE, "Missing label for species");
+        PS_Species s;
+        s.label = w[i++];
+        while (i < w.size()) {   // ps_species.cu:28-37 consumes the rest of the line
+            const std::string word = w[i++];
+            if (word == "mass" || word == "Mass") s.mass = fnum(w, i, "mass");
+            else if (word == "mobility" || word == "Mobility" || word == "Diffusivity" || word == "diffusivity")
+                s.mobility = fnum(w, i, "mobility");
+        }
+        if ((int)species.size() >= kMaxTypes) fail(TILD_ERR_UNSUPPORTED, "too many species");
+        species.push_back(s);
+    } else if (fw == "trajFreq" || fw == "traj_freq") {
+        (void)inum(w, i, "trajFreq");
+    } else if (fw == "verbose") {
+        verbose = inum(w, i, "verbose") != 0;
+    } else {
+        fail(TILD_ERR_PARSE, "Invalid keyword " + fw + " in PS_Box::readInput()");
+    }
+}
+
+void Box::addPotential(std::vector<std::string> &w, size_t &i)
+{
+    PS_Potential p;
+    p.word = need(w, i, "potential kind");
+    auto ramp_check = [&](PS_Potential &q) {   // ps_potential.cu:253-283
+        if (i >= w.size()) return;
+        const std::string conv = w[i++];
+        if (conv != "ramp") fail(TILD_ERR_PARSE, "Invalid keyword: " + conv);
+        if (i >= w.size()) fail(TILD_ERR_PARSE, "no final prefactor specified");
+        q.ramp = true;
+        q.Ao_final = fnum(w, i, "ramp final prefactor");
+        q.Ao_initial = q.Ao;
+    };
+    if (p.word == "gaussian") {                  // ps_potentialGaussian.cu:14-26
+        p.kind = POT_GAUSSIAN;
+        p.grpI = need(w, i, "grpI");
+        p.grpJ = need(w, i, "grpJ");
+        p.Ao = fnum(w, i, "amplitude");
+        p.sigma = fnum(w, i, "sigma");
+        ramp_check(p);
+    } else if (p.word == "erf2" || p.word == "erfG") {   // ps_potentialErf2.cu:85-96
+        p.kind = p.word == "erf2" ? POT_ERF2 : POT_ERFG;
+        p.grpI = need(w, i, "grpI");
+        p.grpJ = need(w, i, "grpJ");
+        p.Ao = fnum(w, i, "amplitude");
+        p.Rp = fnum(w, i, "Rp");
+        p.sigma = fnum(w, i, "sigma");
+        ramp_check(p);
+    } else if (p.word == "charges") {            // ps_potentialCharges.cu:217-226
+        p.kind = POT_CHARGES;
+        p.grpI = p.grpJ = "charges";
+        p.LB = fnum(w, i, "Bjerrum length");
+        p.sigma = fnum(w, i, "sigma");
+    } else if (p.word == "bias" || p.word == "bias_lc" || p.word == "Langevin" || p.word == "langevin" ||
+               p.word == "dpd" || p.word == "maiersaupe" || p.word == "wall") {
+        fail(TILD_ERR_UNSUPPORTED, "potential " + p.word + " is outside the TILD step");
+    } else {
+        fail(TILD_ERR_PARSE, "ps_potential.cu: " + p.word + " is not a supported potential");
+    }
+    if ((int)potentials.size() >= kMaxPots) fail(TILD_ERR_UNSUPPORTED, "too many potentials");
+    p.amp_eff = p.Ao;
+    potentials.push_back(p);
+}
+
+int Box::findSpeciesInteger(const std::string &name) const
+{
+    for (size_t k = 0; k < species.size(); k++)
+        if (species[k].label == name) return (int)k;
+    fail(TILD_ERR_PARSE, "Species label: " + name + " not found!");
+}
+
+int Box::findGroupInteger(const std::string &name) const
+{
+    for (size_t k = 0; k < psGroup.size(); k++)
+        if (psGroup[k].name == name) return (int)k;
+    fail(TILD_ERR_PARSE, "PS_Box.cu: Group label not found: " + name);
+}
+
+// ---------------------------------------------------------------------------------------
+// Particles and the LAMMPS-style data file
+// ---------------------------------------------------------------------------------------
+void Box::readDataConfig(const std::string &name)
+{
+    if (nstot != 0) fail(TILD_ERR_PARSE, "Must read data file before making additional molecules");
+    if (!readDimension) fail(TILD_ERR_PARSE, "Dim must be defined before readData");
+    std::ifstream in(resolve(name));
+    if (!in) fail(TILD_ERR_IO, "Failed to open " + name);
+    std::vector<std::string> lines;
+    std::string ln;
+    while (std::getline(in, ln)) lines.push_back(ln);
+    int64_t natoms = -1, nbonds = 0, nangles = 0;
+    int ntypes = 0;
+    size_t k = 1;   // first line is the title (PS_Box_initialization.cu:805)
+    auto has = [](const std::string &s, const char *kw) { return s.find(kw) != std::string::npos; };
+    float Lread[3] = {0, 0, 1.0f};
+    for (; k < lines.size(); k++) {
+        const std::string &s = lines[k];
+        std::istringstream iss(s);
+        if (has(s, "xlo xhi") || has(s, "ylo yhi") || has(s, "zlo zhi")) {
+            float lo, hi;
+            iss >> lo >> hi;
+            const int d = has(s, "xlo") ? 0 : has(s, "ylo") ? 1 : 2;
+            Lread[d] = (float)(hi - lo);
+        } else if (has(s, "atom types")) iss >> ntypes;
+        else if (has(s, "bond types")) { int t; iss >> t; }
+        else if (has(s, "angle types")) { int t; iss >> t; }
+        else if (has(s, "atoms")) iss >> natoms;
+        else if (has(s, "bonds")) iss >> nbonds;
+        else if (has(s, "angles")) iss >> nangles;
+        else if (has(s, "Masses") || has(s, "Atoms")) break;
+    }
+    if (natoms <= 0) fail(TILD_ERR_PARSE, "data file " + name + ": no atom count");
+    L[0] = Lread[0];
+    L[1] = Lread[1];
+    L[2] = Dim > 2 ? Lread[2] : 1.0f;
+    auto seek = [&](const char *kw) -> bool {
+        for (; k < lines.size(); k++) {
+            std::string t = lines[k];
+            t.erase(0, t.find_first_not_of(" \t"));
+            if (t.rfind(kw, 0) == 0) { k++; return true; }
+        }
+        return false;
+    };
+    auto next_data = [&]() -> const std::string & {
+        while (k < lines.size() && lines[k].find_first_not_of(" \t\r") == std::string::npos) k++;
+        if (k >= lines.size()) fail(TILD_ERR_PARSE, "Premature end of " + name);
+        return lines[k++];
+    };
+    const size_t kSave = k;
+    if (seek("Masses")) {
+        for (int t = 0; t < ntypes; t++) {
+            std::istringstream iss(next_data());
+            int di;
+            float m;
+            iss >> di >> m;
+            if (di < 1 || di > (int)species.size())
+                fail(TILD_ERR_PARSE, "data file type " + std::to_string(di) + " has no declared species (declare species before readData)");
+            species[di - 1].mass = m;   // :850-853
+        }
+    } else {
+        k = kSave;
+    }
+    if (!seek("Atoms")) fail(TILD_ERR_PARSE, "data file " + name + ": no Atoms section");
+    nstot = natoms;
+    x.assign(nstot * Dim, 0.f);
+    intSpecies.assign(nstot, 0);
+    mID.assign(nstot, 0);
+    if (doCharges) charges.assign(nstot, 0.f);
+    for (int64_t a = 0; a < nstot; a++) {
+        std::istringstream iss(next_data());
+        long long ind, di, ltp;
+        if (!(iss >> ind >> di >> ltp)) fail(TILD_ERR_PARSE, "bad atom line in " + name);
+        ind -= 1;
+        if (ind < 0 || ind >= nstot) fail(TILD_ERR_PARSE, "atom id out of range in " + name);
+        if (ltp < 1 || ltp > (long long)species.size())
+            fail(TILD_ERR_PARSE, "atom type " + std::to_string(ltp) + " has no declared species");
+        mID[ind] = (int)(di - 1);
+        intSpecies[ind] = (int)(ltp - 1);
+        if (doCharges) iss >> charges[ind];
+        for (int j = 0; j < Dim; j++)
+            if (!(iss >> x[ind * Dim + j])) fail(TILD_ERR_PARSE, "bad coordinates in " + name);
+    }
+    nBonds.assign(nstot, 0);
+    bondedTo.assign(nstot * MAXBONDS, 0);
+    bondType.assign(nstot * MAXBONDS, 0);
+    if (nbonds > 0) {
+        if (!seek("Bonds")) fail(TILD_ERR_PARSE, "data file " + name + ": no Bonds section");
+        std::vector<int64_t> pairs(2 * nbonds);
+        std::vector<int32_t> bt(nbonds);
+        for (int64_t b = 0; b < nbonds; b++) {
+            std::istringstream iss(next_data());
+            long long id, t, i1, i2;
+            if (!(iss >> id >> t >> i1 >> i2)) fail(TILD_ERR_PARSE, "bad bond line in " + name);
+            pairs[2 * b] = i1 - 1;
+            pairs[2 * b + 1] = i2 - 1;
+            bt[b] = (int32_t)(t - 1);
+        }
+        setBonds(nbonds, pairs.data(), bt.data());
+    }
+    nAnglesTot = (int)nangles;
+}
+
+void Box::setParticles(int64_t n, const float *xin, const int32_t *type, const int32_t *mol, const float *q)
+{
+    if (ready) fail(TILD_ERR_STATE, "particles must be set before endBox");
+    if (nstot != 0) fail(TILD_ERR_PARSE, "particles were already defined");
+    if (!readDimension) fail(TILD_ERR_PARSE, "Dim must be defined before particles");
+    if (n <= 0 || !xin || !type) fail(TILD_ERR_ARG, "particles need n > 0, x and type");
+    if (doCharges && !q) fail(TILD_ERR_ARG, "doCharges is set: charges are required");
+    nstot = n;
+    x.assign(xin, xin + n * Dim);
+    intSpecies.assign(type, type + n);
+    for (int64_t p = 0; p < n; p++)
+        if (intSpecies[p] < 0 || intSpecies[p] >= (int)species.size())
+            fail(TILD_ERR_ARG, "particle type has no declared species");
+    mID.assign(n, 0);
+    if (mol) mID.assign(mol, mol + n);
+    if (doCharges) charges.assign(q, q + n);
+    nBonds.assign(nstot, 0);
+    bondedTo.assign(nstot * MAXBONDS, 0);
+    bondType.assign(nstot * MAXBONDS, 0);
+}
+
+void Box::setBonds(int64_t nb, const int64_t *pairs, const int32_t *btype)
+{
+    if (ready) fail(TILD_ERR_STATE, "bonds must be set before endBox");
+    if (nstot == 0) fail(TILD_ERR_STATE, "bonds need particles");
+    if (nb < 0 || (nb > 0 && !pairs)) fail(TILD_ERR_ARG, "bad bond arrays");
+    for (int64_t b = 0; b < nb; b++) {   // PS_Box_initialization.cu:897-926
+        int64_t i1 = pairs[2 * b], i2 = pairs[2 * b + 1];
+        if (i1 < 0 || i2 < 0 || i1 >= nstot || i2 >= nstot) fail(TILD_ERR_PARSE, "bond partner out of range");
+        if (i2 < i1) std::swap(i1, i2);
+        const int t = btype ? btype[b] : 0;
+        if (t < 0 || t >= kMaxBondTypes) fail(TILD_ERR_PARSE, "bond type out of range");
+        if (nBonds[i1] >= MAXBONDS || nBonds[i2] >= MAXBONDS)
+            fail(TILD_ERR_PARSE, "a particle has more than MAXBONDS=" + std::to_string(MAXBONDS) + " bonds");
+        bondedTo[i1 * MAXBONDS + nBonds[i1]] = (int)i2;
+        bondType[i1 * MAXBONDS + nBonds[i1]] = t;
+        nBonds[i1]++;
+        bondedTo[i2 * MAXBONDS + nBonds[i2]] = (int)i1;
+        bondType[i2 * MAXBONDS + nBonds[i2]] = t;
+        nBonds[i2]++;
+    }
+}
+
+void Box::createDefaultGroups()
+{
+    PS_Group all;
+    all.name = "all";
+    all.inputCommand = "group all";
+    all.siteList.resize(nstot);
+    std::iota(all.siteList.begin(), all.siteList.end(), 0);
+    psGroup.push_back(all);
+    for (size_t t = 0; t < species.size(); t++) {
+        PS_Group g;
+        g.name = species[t].label;
+        g.inputCommand = "group type " + std::to_string(t + 1);
+        for (int64_t p = 0; p < nstot; p++)
+            if (intSpecies[p] == (int)t) g.siteList.push_back((int)p);
+        psGroup.push_back(g);
+    }
+    if (doCharges) {
+        PS_Group g;
+        g.name = "charges";
+        g.inputCommand = "group charges";
+        g.isCharges = true;
+        for (int64_t p = 0; p < nstot; p++)
+            if (charges[p] != 0.0f) g.siteList.push_back((int)p);
+        g.forceFlag = true;   // ps_groups.cu:131
+        psGroup.push_back(g);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// endBox
+// ---------------------------------------------------------------------------------------
+void Box::finishInitialization()
+{
+    if (nstot == 0) fail(TILD_ERR_PARSE, "Box created with no particles?!?");
+    if (Dim != 3) fail(TILD_ERR_UNSUPPORTED, "the B200 TILD path runs 3-D boxes (Dim 3)");
+    for (int j = 0; j < 3; j++)
+        if (Nx[j] <= 0) fail(TILD_ERR_PARSE, "grid must be given for every dimension");
+    if (nAnglesTot > 0) fail(TILD_ERR_UNSUPPORTED, "angles are outside the TILD step");
+    if (integrators.empty()) fail(TILD_ERR_PARSE, "no integrator defined");
+    if (species.size() > (size_t)kMaxTypes) fail(TILD_ERR_UNSUPPORTED, "too many species");
+    gvol = 1.0;
+    for (int j = 0; j < Dim; j++) {
+        dx[j] = (double)L[j] / (double)Nx[j];
+        gvol *= dx[j];
+        Lh[j] = 0.5f * L[j];
+    }
+    if (doCharges) {   // PS_Box_initialization.cu:398-412
+        float qtot = 0.f, qneg = 0.f, qpos = 0.f;
+        for (int64_t p = 0; p < nstot; p++) {
+            qtot += charges[p];
+            if (charges[p] < 0.f) qneg += charges[p];
+            else if (charges[p] > 0.f) qpos += charges[p];
+        }
+        if (qtot != 0.f)
+            fail(TILD_ERR_PARSE, "Box net charge is not zero! qtotal: " + std::to_string(qtot) +
+                                     "total negative: " + std::to_string(qneg) + ", positive: " + std::to_string(qpos));
+    }
+    nBondsTot = 0;
+    for (int64_t p = 0; p < nstot; p++)
+        for (int b = 0; b < nBonds[p]; b++)
+            if (bondedTo[p * MAXBONDS + b] > p) nBondsTot++;
+    for (int64_t p = 0; p < nstot; p++)
+        for (int b = 0; b < nBonds[p]; b++)
+            if (bondType[p * MAXBONDS + b] >= nBondTypes)
+                fail(TILD_ERR_PARSE, "bond type " + std::to_string(bondType[p * MAXBONDS + b] + 1) + " has no 'bond' command");
+    if (writeFiles) writeDataConfig(initDataFileName);
+    createDefaultGroups();
+    for (auto &g : psGroup)
+        if (g.siteList.empty()) fail(TILD_ERR_PARSE, "A group with size 0 found, exiting! (group '" + g.name + "')");
+    for (auto &in : integrators) in.group_index = findGroupInteger(in.groupName);
+    for (auto &p : potentials) {   // PS_Potential::initializePotential (ps_potential.cu:24-33)
+        if (p.kind == POT_CHARGES) {
+            p.Iind = p.Jind = findGroupInteger("charges");
+        } else {
+            p.Iind = findGroupInteger(p.grpI);
+            p.Jind = findGroupInteger(p.grpJ);
+            psGroup[p.Iind].forceFlag = true;
+            psGroup[p.Jind].forceFlag = true;
+        }
+    }
+    if (writeFiles) { std::ofstream o(resolve(datFileName)); }   // :359-364, :543-544 truncate
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) fail(TILD_ERR_CUDA, "no CUDA device is visible");
+    ck(cudaSetDevice(device), "cudaSetDevice");
+    if (!stream) {
+        ck(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        ownStream = true;
+    }
+    init_fft_attributes();
+    buildPlan();
+    allocDevice();
+    uploadParticles();
+    ready = true;
+}
+
+void Box::buildPlan()
+{
+    const int ng = (int)psGroup.size();
+    dfields.clear();
+    fgroups.clear();
+    auto dfield = [&](int grp, int charge) {
+        for (size_t k = 0; k < dfields.size(); k++)
+            if (dfields[k].group == grp && dfields[k].charge == charge) return (int)k;
+        dfields.push_back({grp, charge});
+        return (int)dfields.size() - 1;
+    };
+    // k-space terms; force groups in psGroup order (PS_Box.cu:268-270)
+    struct T { int grp; int pot; int df; double mult; };
+    std::vector<T> raw;
+    for (size_t pi = 0; pi < potentials.size(); pi++) {
+        const PS_Potential &p = potentials[pi];
+        if (p.kind == POT_CHARGES) {
+            raw.push_back({p.Iind, (int)pi, dfield(p.Iind, 1), 1.0});
+        } else {
+            raw.push_back({p.Iind, (int)pi, dfield(p.Jind, 0), p.Iind == p.Jind ? 2.0 : 1.0});
+            if (p.Iind != p.Jind) raw.push_back({p.Jind, (int)pi, dfield(p.Iind, 0), 1.0});
+        }
+    }
+    for (int gi = 0; gi < ng; gi++)
+        for (auto &t : raw)
+            if (t.grp == gi && psGroup[gi].forceFlag) { fgroups.push_back(gi); break; }
+    if ((int)dfields.size() > kMaxFields) fail(TILD_ERR_UNSUPPORTED, "more than 8 density fields");
+    if ((int)fgroups.size() > kMaxFGroups) fail(TILD_ERR_UNSUPPORTED, "more than 4 force groups");
+    if ((int)raw.size() > kMaxTerms) fail(TILD_ERR_UNSUPPORTED, "too many k-space terms");
+
+    // geometry
+    Geom &g = geom;
+    g.nx = Nx[0]; g.ny = Nx[1]; g.nz = Nx[2];
+    g.nxh = g.nx / 2 + 1;
+    g.hp = (g.nxh + 3) & ~3;
+    g.M = (long long)g.nx * g.ny * g.nz;
+    g.hstride = (long long)g.nz * g.ny * g.hp;
+    for (int j = 0; j < 3; j++) {
+        g.dxf[j] = (float)dx[j];
+        g.L[j] = L[j];
+        g.Lh[j] = Lh[j];
+    }
+    // FP32 grid volume of the reference weights (ps_grid_utils.cu:97-101) and the FP64 one
+    // of the gathers (ps_groups.cu:186-193): forces scale by gvol_d/(gvol_f^2 M).
+    const double gvf = (double)((1.0f * g.dxf[0]) * g.dxf[1] * g.dxf[2]);
+    const double norm = gvol / (gvf * gvf * (double)g.M);
+
+    KSpace &ks = ksHost;
+    std::memset(&ks, 0, sizeof(ks));
+    ks.npots = (int)potentials.size();
+    for (size_t pi = 0; pi < potentials.size(); pi++) {
+        const PS_Potential &p = potentials[pi];
+        PotDev &d = ks.pots[pi];
+        d.kind = p.kind;
+        d.amp = p.amp_eff;
+        d.sig2 = (double)(p.sigma * p.sigma);   // sig2 = sigma*sigma in float
+        d.Rp = p.Rp;
+        d.lB = p.LB;
+        ETerm &e = ks.eterms[pi];
+        e.pot = (int)pi;
+        if (p.kind == POT_CHARGES) {
+            e.dI = e.dJ = dfield(p.Iind, 1);
+            e.fac = 0.5 * norm;
+        } else {
+            e.dI = dfield(p.Iind, 0);
+            e.dJ = dfield(p.Jind, 0);
+            e.fac = norm;
+        }
+    }
+    ks.neterms = (int)potentials.size();
+    ks.nterms = 0;
+    for (auto &t : raw) {
+        int f = -1;
+        for (size_t k = 0; k < fgroups.size(); k++)
+            if (fgroups[k] == t.grp) f = (int)k;
+        if (f < 0) continue;
+        ks.terms[ks.nterms++] = KTerm{f, t.pot, t.df, t.mult * norm};
+    }
+    ks.nfg = (int)fgroups.size();
+    ks.nd = (int)dfields.size();
+    for (int j = 0; j < 3; j++) ks.twopi_over_L[j] = 2.0 * M_PI / (double)L[j];
+
+    // particle params
+    ParticleParams &pp = ppHost;
+    std::memset(&pp, 0, sizeof(pp));
+    pp.N = (int)nstot;
+    pp.order = pmeorder;
+    pp.quirk4 = exact4 ? 0 : 1;
+    pp.nd = ks.nd;
+    pp.npair = (ks.nd + 1) / 2;
+    for (size_t k = 0; k < dfields.size(); k++)
+        if (dfields[k].charge) pp.dchan_charge |= 1u << k;
+    pp.nfg = ks.nfg;
+    for (size_t k = 0; k < fgroups.size(); k++)
+        if (psGroup[fgroups[k]].isCharges) pp.fg_qweighted |= 1u << k;
+    pp.maxb = MAXBONDS;
+    pp.nbtypes = nBondTypes;
+    for (int t = 0; t < nBondTypes; t++) {
+        pp.bk[t] = bondK[t];
+        pp.breq[t] = bondReq[t];
+        pp.bstyle[t] = bondStyle[t];
+    }
+    if (integrators.size() > 4) fail(TILD_ERR_UNSUPPORTED, "more than 4 integrators");
+    for (size_t s = 0; s < integrators.size(); s++) {   // ps_integratorGJF.cu:43-95
+        const Integrator &in = integrators[s];
+        pp.integ_kind[s] = in.name == "GJF" ? 0 : 1;
+        const float delt = in.delt, delt2 = delt * delt, root2dt = sqrtf(2.0f * delt);
+        pp.em_delt[s] = delt;
+        pp.em_noise[s] = sqrtf((float)(2.0 * (double)delt));   // ps_integratorEM.cu:22-26
+        for (size_t t = 0; t < species.size(); t++) {
+            const float m = species[t].mass, Di = species[t].mobility;
+            const float b = m / (m + delt / (2.0f * Di));
+            const float a = (1.0f - delt / (2.0f * Di * m)) / (1.0f + delt / (2.0f * Di * m));
+            pp.coef[s][t] = TypeCoef{a, b, root2dt / sqrtf(Di), b * delt2 / m, b * delt / (2.0f * m)};
+        }
+    }
+    pp.seed = (unsigned long long)RANDSEED;
+    pp.rng_compat = rngCompat;
+}
+
+void Box::allocDevice()
+{
+    const Geom &g = geom;
+    const int64_t N = nstot;
+    dX[0] = dalloc<float>(3 * N);
+    dX[1] = dalloc<float>(3 * N);
+    dNoise = dalloc<float>(3 * N);
+    dF = dalloc<float>(3 * N);
+    dFlags = dalloc<uint32_t>(N);
+    dOrig = dalloc<int>(N);
+    if (doCharges) dQ = dalloc<float>(N);
+    dNb = dalloc<uint8_t>(N);
+    dPartner = dalloc<int>(N * MAXBONDS);
+    dBtype = dalloc<uint8_t>(N * MAXBONDS);
+    if (rngCompat) dRng = dalloc<unsigned char>(N * rng_state_bytes());
+    const int nd = std::max(1, (int)dfields.size()), nfg = std::max(1, (int)fgroups.size());
+    const int npair = (nd + 1) / 2;
+    if (deterministic) dDepFix = dalloc<unsigned long long>((size_t)2 * npair * g.M);
+    else dDep = dalloc<float2>((size_t)npair * g.M);
+    dH = dalloc<float2>((size_t)nd * g.hstride);
+    dHg = dalloc<float2>((size_t)3 * nfg * g.hstride);
+    dRec = dalloc<float4>((size_t)nfg * g.M);
+    dTw = dalloc<float2>((size_t)g.nx + g.ny + g.nz);
+    build_fft_line(g.nx, lx, dTw);
+    build_fft_line(g.ny, ly, dTw + g.nx);
+    build_fft_line(g.nz, lz, dTw + g.nx + g.ny);
+    for (FftLine *l : {&lx, &ly, &lz})
+        if (l->ns > kMaxStages) fail(TILD_ERR_UNSUPPORTED, "grid size factors into too many stages");
+    dStep = dalloc<long long>(1);
+    dKs = dalloc<KSpace>(1);
+    dPp = dalloc<ParticleParams>(1);
+    const int TXz = 8;
+    nblkZ = ((g.nxh + TXz - 1) / TXz) * g.ny;
+    nblkP = (int)((N + 255) / 256);
+    dEpart = dalloc<double>((size_t)nblkZ * std::max(1, ksHost.neterms));
+    dBpart = dalloc<double>((size_t)nblkP * 7);
+    dRes = dalloc<double>(kMaxPots + 8);
+    ck(cudaMallocHost(&hKsPinned, sizeof(KSpace)), "cudaMallocHost");
+}
+
+void Box::uploadParticles()
+{
+    const int64_t N = nstot;
+    std::vector<float> x3(3 * N);
+    for (int64_t p = 0; p < N; p++)
+        for (int j = 0; j < 3; j++) x3[3 * p + j] = x[p * Dim + j];
+    ck(cudaMemcpy(dX[0], x3.data(), 12 * N, cudaMemcpyHostToDevice), "upload x");
+    ck(cudaMemcpy(dX[1], x3.data(), 12 * N, cudaMemcpyHostToDevice), "upload xOld");   // GJF: xOld = x
+    ck(cudaMemset(dNoise, 0, 12 * N), "zero noise");
+    // membership flags
+    std::vector<uint32_t> fl(N, 0u);
+    std::vector<std::vector<char>> member(psGroup.size(), std::vector<char>(N, 0));
+    for (size_t gi = 0; gi < psGroup.size(); gi++)
+        for (int s : psGroup[gi].siteList) member[gi][s] = 1;
+    for (size_t k = 0; k < dfields.size(); k++)
+        for (int64_t p = 0; p < N; p++)
+            if (member[dfields[k].group][p]) fl[p] |= 1u << k;
+    for (size_t k = 0; k < fgroups.size(); k++)
+        for (int64_t p = 0; p < N; p++)
+            if (member[fgroups[k]][p]) fl[p] |= 1u << (8 + k);
+    std::vector<int> slot(N, kNoIntegrator);
+    for (size_t s = 0; s < integrators.size(); s++)
+        for (int p : psGroup[integrators[s].group_index].siteList) {
+            if (slot[p] != kNoIntegrator) fail(TILD_ERR_UNSUPPORTED, "a particle belongs to two integrator groups");
+            slot[p] = (int)s;
+        }
+    for (int64_t p = 0; p < N; p++) fl[p] |= ((uint32_t)slot[p] << 16) | ((uint32_t)intSpecies[p] << 20);
+    ck(cudaMemcpy(dFlags, fl.data(), 4 * N, cudaMemcpyHostToDevice), "upload flags");
+    std::vector<int> orig(N);
+    std::iota(orig.begin(), orig.end(), 0);
+    ck(cudaMemcpy(dOrig, orig.data(), 4 * N, cudaMemcpyHostToDevice), "upload ids");
+    if (doCharges) ck(cudaMemcpy(dQ, charges.data(), 4 * N, cudaMemcpyHostToDevice), "upload q");
+    std::vector<uint8_t> nb8(N), bt8(N * MAXBONDS);
+    for (int64_t p = 0; p < N; p++) nb8[p] = (uint8_t)nBonds[p];
+    for (int64_t k = 0; k < N * MAXBONDS; k++) bt8[k] = (uint8_t)bondType[k];
+    ck(cudaMemcpy(dNb, nb8.data(), N, cudaMemcpyHostToDevice), "upload nb");
+    ck(cudaMemcpy(dPartner, bondedTo.data(), 4 * N * MAXBONDS, cudaMemcpyHostToDevice), "upload partners");
+    ck(cudaMemcpy(dBtype, bt8.data(), N * MAXBONDS, cudaMemcpyHostToDevice), "upload bond types");
+    long long zero = 0;
+    ck(cudaMemcpy(dStep, &zero, sizeof(zero), cudaMemcpyHostToDevice), "upload step");
+    ck(cudaMemcpy(dKs, &ksHost, sizeof(KSpace), cudaMemcpyHostToDevice), "upload k-space plan");
+    ck(cudaMemcpy(dPp, &ppHost, sizeof(ParticleParams), cudaMemcpyHostToDevice), "upload particle params");
+    if (rngCompat) {   // d_initDeviceRNG (device_utils.cu:465-472), seed = RANDSEED (unsigned int)
+        ck(launch_rng_init(dRng, dOrig, (int)N, (unsigned long long)(unsigned int)RANDSEED, stream), "rng init");
+        ck(cudaStreamSynchronize(stream), "rng init sync");
+    }
+    ck(cudaDeviceSynchronize(), "upload");
+}
+
+// ---------------------------------------------------------------------------------------
+// Step pipeline
+// ---------------------------------------------------------------------------------------
+void Box::mark(int stage)
+{
+    if (!timing) return;
+    cudaEvent_t ev;
+    ck(cudaEventCreate(&ev), "event");
+    ck(cudaEventRecord(ev, stream), "event record");
+    marks.push_back({stage, ev});
+}
+
+void Box::enqueueStep(bool energy, bool integrate, float *fout_dev)
+{
+    const Geom &g = geom;
+    cudaStream_t st = stream;
+    const int nd = (int)dfields.size(), nfg = (int)fgroups.size();
+    const int npair = (nd + 1) / 2;
+    mark(-1);
+    if (nd > 0) {
+        if (deterministic)
+            ck(launch_zero(dDepFix, sizeof(unsigned long long) * 2 * npair * g.M, st), "zero");
+        else
+            ck(launch_zero(dDep, sizeof(float2) * npair * g.M, st), "zero");
+        ck(launch_deposit(g, ppHost, dX[0], dX[1], dStep, dFlags, dQ, dDep, dDepFix, deterministic, st), "deposit");
+        mark(STAGE_DEPOSIT);
+        ck(launch_xfwd(g, lx, npair, nd, dDep, deterministic ? dDepFix : nullptr, dH, st), "fft x forward");
+        mark(STAGE_XFWD);
+        ck(launch_ypass(g, ly, nd, 0, dH, st), "fft y forward");
+        mark(STAGE_YFWD);
+        ck(launch_kspace_z(g, lz, ksHost, dKs, dH, dHg, dEpart, energy ? 1 : 0, nfg > 0 ? 1 : 0, nullptr, st), "kspace");
+        if (energy && ksHost.neterms > 0) ck(launch_reduce_partials(dEpart, nblkZ, ksHost.neterms, dRes, st), "reduce");
+        mark(STAGE_KSPACE);
+        if (nfg > 0) {
+            ck(launch_ypass(g, ly, 3 * nfg, 1, dHg, st), "fft y inverse");
+            mark(STAGE_YINV);
+            ck(launch_xinv(g, lx, nfg, dHg, dRec, st), "fft x inverse");
+            mark(STAGE_XINV);
+        }
+    }
+    ck(launch_particles(g, ppHost, dPp, dX[0], dX[1], dNoise, dFlags, dQ, dNb, dPartner, dBtype, dRec, dOrig, dRng,
+                        dStep, fout_dev, integrate ? 1 : 0, st),
+       "particles");
+    mark(STAGE_PARTICLES);
+    if (integrate) ck(launch_tick(dStep, st), "tick");
+    if (energy) {
+        ck(launch_bond_energy(g, ppHost, dPp, dX[0], dX[1], dStep, dNb, dPartner, dBtype, dBpart, nullptr, st), "bond energy");
+        ck(launch_reduce_partials(dBpart, nblkP, 7, dRes + kMaxPots, st), "reduce bonds");
+    }
+}
+
+void Box::enqueueEnergyOnly()
+{
+    const Geom &g = geom;
+    cudaStream_t st = stream;
+    const int nd = (int)dfields.size();
+    const int npair = (nd + 1) / 2;
+    if (nd > 0 && ksHost.neterms > 0) {
+        if (deterministic)
+            ck(launch_zero(dDepFix, sizeof(unsigned long long) * 2 * npair * g.M, st), "zero");
+        else
+            ck(launch_zero(dDep, sizeof(float2) * npair * g.M, st), "zero");
+        ck(launch_deposit(g, ppHost, dX[0], dX[1], dStep, dFlags, dQ, dDep, dDepFix, deterministic, st), "deposit");
+        ck(launch_xfwd(g, lx, npair, nd, dDep, deterministic ? dDepFix : nullptr, dH, st), "fft x forward");
+        ck(launch_ypass(g, ly, nd, 0, dH, st), "fft y forward");
+        ck(launch_kspace_z(g, lz, ksHost, dKs, dH, dHg, dEpart, 1, 0, nullptr, st), "kspace energy");
+        ck(launch_reduce_partials(dEpart, nblkZ, ksHost.neterms, dRes, st), "reduce");
+    }
+    ck(launch_bond_energy(g, ppHost, dPp, dX[0], dX[1], dStep, dNb, dPartner, dBtype, dBpart, nullptr, st), "bond energy");
+    ck(launch_reduce_partials(dBpart, nblkP, 7, dRes + kMaxPots, st), "reduce bonds");
+}
+
+std::vector<double> Box::readEnergies(bool)
+{
+    std::vector<double> r(kMaxPots + 8, 0.0);
+    ck(cudaStreamSynchronize(stream), "sync");
+    ck(cudaMemcpy(r.data(), dRes, sizeof(double) * r.size(), cudaMemcpyDeviceToHost), "read energies");
+    return r;
+}
+
+void Box::dropGraphs()
+{
+    if (gNorm) cudaGraphExecDestroy(gNorm);
+    if (gEnergy) cudaGraphExecDestroy(gEnergy);
+    gNorm = gEnergy = nullptr;
+}
+
+void Box::captureGraphs()
+{
+    if (gNorm && gEnergy) return;
+    for (int e = 0; e < 2; e++) {
+        cudaGraph_t gr;
+        ck(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        try {
+            enqueueStep(e == 1, true, nullptr);
+        } catch (...) {
+            cudaStreamEndCapture(stream, &gr);
+            throw;
+        }
+        ck(cudaStreamEndCapture(stream, &gr), "end capture");
+        cudaGraphExec_t ex;
+        ck(cudaGraphInstantiate(&ex, gr, 0), "graph instantiate");
+        cudaGraphDestroy(gr);
+        (e ? gEnergy : gNorm) = ex;
+    }
+}
+
+void Box::updateRamps(int64_t step, int64_t maxSteps)
+{
+    bool any = false;
+    for (size_t pi = 0; pi < potentials.size(); pi++) {   // ps_potential.cu:227-248
+        PS_Potential &p = potentials[pi];
+        if (!p.ramp) continue;
+        any = true;
+        const double Ao_current = p.Ao_initial + (p.Ao_final - p.Ao_initial) / double(maxSteps) * double(step + 1);
+        p.amp_eff = Ao_current / p.T0();
+        ksHost.pots[pi].amp = p.amp_eff;
+    }
+    if (!any) return;
+    *hKsPinned = ksHost;
+    ck(cudaMemcpyAsync(dKs, hKsPinned, sizeof(KSpace), cudaMemcpyHostToDevice, stream), "ramp upload");
+    ck(cudaStreamSynchronize(stream), "ramp sync");
+}
+
+void Box::steps(int64_t n)
+{
+    if (!ready) fail(TILD_ERR_STATE, "endBox has not been processed");
+    ck(cudaSetDevice(device), "cudaSetDevice");
+    if (stageTiming) {   // instrumented launches: an event after every kernel
+        timing = true;
+        marks.clear();
+        for (int64_t i = 0; i < n; i++) {
+            enqueueStep(false, true, nullptr);
+            totSteps++;
+        }
+        timing = false;
+        ck(cudaStreamSynchronize(stream), "sync");
+        stageSec.assign(STAGE_COUNT, 0.0);
+        std::vector<int> cnt(STAGE_COUNT, 0);
+        for (size_t k = 1; k < marks.size(); k++) {
+            const int s = marks[k].first;
+            if (s < 0) continue;
+            float ms = 0.f;
+            ck(cudaEventElapsedTime(&ms, marks[k - 1].second, marks[k].second), "elapsed");
+            stageSec[s] += ms * 1e-3;
+            cnt[s]++;
+        }
+        for (int s = 0; s < STAGE_COUNT; s++)
+            if (cnt[s]) stageSec[s] /= cnt[s];
+        for (auto &m : marks) cudaEventDestroy(m.second);
+        marks.clear();
+        return;
+    }
+    captureGraphs();
+    for (int64_t i = 0; i < n; i++) {
+        ck(cudaGraphLaunch(gNorm, stream), "graph launch");
+        totSteps++;
+    }
+    ck(cudaGetLastError(), "step");
+}
+
+void Box::NVT(int64_t nSteps)
+{
+    if (!ready) fail(TILD_ERR_STATE, "run nvt before endBox");
+    ck(cudaSetDevice(device), "cudaSetDevice");
+    {   // writeData(-1) (PS_Box.cu:215)
+        std::vector<double> t = thermo();
+        std::vector<double> pe(t.begin() + 2, t.begin() + 2 + potentials.size());
+        writeData(-1, pe, t[1]);
+    }
+    bool anyRamp = false;
+    for (auto &p : potentials) anyRamp |= p.ramp;
+    if (!anyRamp) captureGraphs();
+    const int npot = (int)potentials.size();
+    std::vector<double> ampUsed(npot);
+    std::vector<double> lastPair(npot, 0.0);
+    double lastBond = 0.0;
+    for (int64_t i = 0; i < nSteps; i++) {
+        const bool energy = (i % logFreq == 0) || (i == nSteps - 1);
+        for (int k = 0; k < npot; k++) ampUsed[k] = potentials[k].amp_eff;
+        if (anyRamp) enqueueStep(energy, true, nullptr);
+        else ck(cudaGraphLaunch(energy ? gEnergy : gNorm, stream), "graph launch");
+        totSteps++;
+        updateRamps(i, nSteps);
+        if (energy) {
+            std::vector<double> r = readEnergies(true);
+            for (int k = 0; k < npot; k++)   // CalcEnergy runs after update_prefactor (PS_Box.cu:159-172)
+                lastPair[k] = r[k] * (ampUsed[k] != 0.0 ? potentials[k].amp_eff / ampUsed[k] : 1.0);
+            lastBond = 0.5 * r[kMaxPots];
+            if (i % logFreq == 0) writeData(i, lastPair, lastBond);
+        }
+    }
+    ck(cudaStreamSynchronize(stream), "run");
+    if (nSteps > 0) writeData(nSteps, lastPair, lastBond);   // PS_Box.cu:227
+    if (writeFiles) writeDataConfig("final.input.data");      // PS_Box.cu:230
+}
+
+void Box::writeData(int64_t step, const std::vector<double> &pairE, double ubond)
+{
+    double upe = ubond;
+    for (size_t k = 0; k < pairE.size() && k < potentials.size(); k++) {
+        potentials[k].energy = pairE[k];
+        upe += pairE[k];
+    }
+    std::vector<double> row;
+    row.push_back((double)step);
+    row.push_back(ubond);
+    for (size_t k = 0; k < potentials.size(); k++) row.push_back(potentials[k].energy);
+    logRows.push_back(row);
+    std::ostringstream ln, echoLn;   // PS_Box.cu:339-370 (default stream formatting)
+    ln << step;
+    echoLn << "step: " << step << " Upe: " << upe;
+    if (nBondsTot > 0) {
+        ln << " " << ubond;
+        echoLn << " Ubond: " << ubond;
+    }
+    for (size_t k = 0; k < potentials.size(); k++) {
+        ln << " " << potentials[k].energy;
+        echoLn << " pot[" << k << "]: " << potentials[k].energy;
+    }
+    if (writeFiles) {
+        std::ofstream o(resolve(datFileName), std::ios_base::app);
+        o << ln.str() << std::endl;
+    }
+    if (echo) std::cout << echoLn.str() << std::endl;
+}
+
+std::vector<double> Box::thermo()
+{
+    if (!ready) fail(TILD_ERR_STATE, "endBox has not been processed");
+    ck(cudaSetDevice(device), "cudaSetDevice");
+    enqueueEnergyOnly();
+    std::vector<double> r = readEnergies(true);
+    std::vector<double> out;
+    double ubond = 0.5 * r[kMaxPots], upe = ubond;
+    for (size_t k = 0; k < potentials.size(); k++) upe += r[k];
+    out.push_back(upe);
+    out.push_back(ubond);
+    for (size_t k = 0; k < potentials.size(); k++) out.push_back(r[k]);
+    for (int c = 0; c < 6; c++) out.push_back(0.5 * r[kMaxPots + 1 + c]);
+    return out;
+}
+
+void Box::forces(float *f_out)
+{
+    if (!ready) fail(TILD_ERR_STATE, "endBox has not been processed");
+    ck(cudaSetDevice(device), "cudaSetDevice");
+    enqueueStep(false, false, dF);
+    ck(cudaStreamSynchronize(stream), "forces");
+    ck(cudaMemcpy(f_out, dF, 12 * nstot, cudaMemcpyDeviceToHost), "read forces");
+}
+
+void Box::getPositions(float *xo) const
+{
+    if (!ready) fail(TILD_ERR_STATE, "endBox has not been processed");
+    long long s = 0;
+    ck(cudaStreamSynchronize(stream), "sync");
+    ck(cudaMemcpy(&s, dStep, sizeof(s), cudaMemcpyDeviceToHost), "read step");
+    ck(cudaMemcpyAsync(xo, dX[s & 1], 12 * nstot, cudaMemcpyDeviceToHost, stream), "read positions");
+    ck(cudaStreamSynchronize(stream), "read positions");
+}
+
+void Box::setPositions(const float *xi)
+{
+    if (!ready) fail(TILD_ERR_STATE, "endBox has not been processed");
+    ck(cudaStreamSynchronize(stream), "sync");
+    ck(cudaMemcpyAsync(dX[0], xi, 12 * nstot, cudaMemcpyHostToDevice, stream), "set positions");
+    ck(cudaMemcpyAsync(dX[1], dX[0], 12 * nstot, cudaMemcpyDeviceToDevice, stream), "set positions");
+    ck(cudaMemsetAsync(dNoise, 0, 12 * nstot, stream), "zero noise");
+    ck(cudaStreamSynchronize(stream), "set positions");
+}
+
+void Box::getDensity(const std::string &group, int charge, float *rho)
+{
+    if (!ready) fail(TILD_ERR_STATE, "endBox has not been processed");
+    const int gi = findGroupInteger(group);
+    if (charge && !psGroup[gi].isCharges) fail(TILD_ERR_ARG, "only the 'charges' group has a charge density");
+    long long s = 0;
+    ck(cudaStreamSynchronize(stream), "sync");
+    ck(cudaMemcpy(&s, dStep, sizeof(s), cudaMemcpyDeviceToHost), "read step");
+    const std::vector<int> &sites = psGroup[gi].siteList;
+    int *dSites = nullptr;
+    float *dRho = nullptr;
+    ck(cudaMalloc(&dSites, 4 * sites.size()), "malloc");
+    ck(cudaMalloc(&dRho, 4 * geom.M), "malloc");
+    cudaMemcpy(dSites, sites.data(), 4 * sites.size(), cudaMemcpyHostToDevice);
+    cudaMemset(dRho, 0, 4 * geom.M);
+    cudaError_t e = launch_density_single(geom, ppHost, dX[s & 1], dSites, (int)sites.size(), dQ, charge, dRho, stream);
+    cudaStreamSynchronize(stream);
+    if (e == cudaSuccess) e = cudaMemcpy(rho, dRho, 4 * geom.M, cudaMemcpyDeviceToHost);
+    cudaFree(dSites);
+    cudaFree(dRho);
+    ck(e, "density");
+}
+
+void Box::gridWeights(int32_t *inds, float *w)
+{
+    if (!ready) fail(TILD_ERR_STATE, "endBox has not been processed");
+    long long s = 0;
+    ck(cudaStreamSynchronize(stream), "sync");
+    ck(cudaMemcpy(&s, dStep, sizeof(s), cudaMemcpyDeviceToHost), "read step");
+    const int G = (pmeorder + 1) * (pmeorder + 1) * (pmeorder + 1);
+    int *dI = nullptr;
+    float *dW = nullptr;
+    ck(cudaMalloc(&dI, 4 * nstot * G), "malloc");
+    ck(cudaMalloc(&dW, 4 * nstot * G), "malloc");
+    cudaError_t e = launch_grid_weights(geom, pmeorder, exact4 ? 0 : 1, dX[s & 1], (int)nstot, dI, dW, stream);
+    cudaStreamSynchronize(stream);
+    if (e == cudaSuccess) e = cudaMemcpy(inds, dI, 4 * nstot * G, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(w, dW, 4 * nstot * G, cudaMemcpyDeviceToHost);
+    cudaFree(dI);
+    cudaFree(dW);
+    ck(e, "grid weights");
+}
+
+void Box::modifyBox(const std::string &rest)
+{
+    std::vector<std::string> w = split(rest);
+    if (w.size() >= 3 && w[0] == "potential" && (w[1] == "remove" || w[1] == "delete")) {
+        const long long id = std::strtoll(w[2].c_str(), nullptr, 10);
+        if (id > 0 && id <= (long long)potentials.size()) {
+            potentials.erase(potentials.begin() + (id - 1));
+            if (ready) {
+                ck(cudaStreamSynchronize(stream), "sync");
+                dropGraphs();
+                const int ndOld = (int)dfields.size(), nfOld = (int)fgroups.size();
+                buildPlan();
+                if ((int)dfields.size() > std::max(1, ndOld) || (int)fgroups.size() > std::max(1, nfOld))
+                    fail(TILD_ERR_STATE, "plan grew after removing a potential");
+                // refresh membership flags and plans; positions and GJF state are kept
+                std::vector<float> xcur(3 * nstot), xold(3 * nstot), nz(3 * nstot);
+                long long s = 0;
+                cudaMemcpy(&s, dStep, sizeof(s), cudaMemcpyDeviceToHost);
+                cudaMemcpy(xcur.data(), dX[s & 1], 12 * nstot, cudaMemcpyDeviceToHost);
+                cudaMemcpy(xold.data(), dX[(s + 1) & 1], 12 * nstot, cudaMemcpyDeviceToHost);
+                cudaMemcpy(nz.data(), dNoise, 12 * nstot, cudaMemcpyDeviceToHost);
+                uploadParticles();
+                cudaMemcpy(dStep, &s, sizeof(s), cudaMemcpyHostToDevice);
+                cudaMemcpy(dX[s & 1], xcur.data(), 12 * nstot, cudaMemcpyHostToDevice);
+                cudaMemcpy(dX[(s + 1) & 1], xold.data(), 12 * nstot, cudaMemcpyHostToDevice);
+                cudaMemcpy(dNoise, nz.data(), 12 * nstot, cudaMemcpyHostToDevice);
+                ck(cudaDeviceSynchronize(), "modify");
+            }
+        }
+    }
+}
+
+void Box::writeDataConfig(const std::string &name)   // PS_Box.cu:629-748
+{
+    std::vector<float> xs(x);
+    if (ready) {
+        std::vector<float> x3(3 * nstot);
+        getPositions(x3.data());
+        for (int64_t p = 0; p < nstot; p++)
+            for (int j = 0; j < Dim; j++) xs[p * Dim + j] = x3[3 * p + j];
+    }
+    std::ofstream out(resolve(name));
+    if (!out) fail(TILD_ERR_IO, "cannot write " + name);
+    out << "Created by MATILDA.FT\n\n";
+    out << nstot << " atoms" << "\n";
+    out << nBondsTot << " bonds" << "\n";
+    out << nAnglesTot << " angles" << "\n";
+    out << "\n";
+    int mx = -342332;
+    for (int64_t p = 0; p < nstot; p++) mx = std::max(mx, intSpecies[p]);
+    out << mx + 1 << " atom types" << "\n";
+    mx = -1;
+    for (int64_t p = 0; p < nstot; p++)
+        for (int b = 0; b < nBonds[p]; b++) mx = std::max(mx, bondType[p * MAXBONDS + b]);
+    out << mx + 1 << " bond types" << "\n";
+    out << 0 << " angle types" << "\n";
+    out << "\n";
+    out << "0.0 " << L[0] << " xlo xhi" << "\n";
+    out << "0.0 " << L[1] << " ylo yhi" << "\n";
+    if (Dim > 2) out << "0.0 " << L[2] << " zlo zhi" << "\n";
+    else out << "0.0 1.0 zlo zhi" << "\n";
+    out << "\n";
+    out << "Masses\n" << "\n";
+    for (size_t t = 0; t < species.size(); t++) out << t + 1 << " " << species[t].mass << "\n";
+    out << "\n";
+    out << "Atoms\n" << std::endl;
+    for (int64_t p = 0; p < nstot; p++) {
+        out << p + 1 << " " << mID[p] + 1 << " " << intSpecies[p] + 1 << "  ";
+        if (doCharges) out << charges[p] << " ";
+        for (int j = 0; j < Dim; j++) out << xs[p * Dim + j] << " ";
+        if (Dim < 3) out << "0.0 ";
+        out << "\n";
+    }
+    out << "\n";
+    out << "Bonds\n" << "\n";
+    int64_t bc = 0;
+    for (int64_t p = 0; p < nstot; p++)
+        for (int b = 0; b < nBonds[p]; b++)
+            if (p < bondedTo[p * MAXBONDS + b]) {
+                out << bc + 1 << " " << bondType[p * MAXBONDS + b] + 1 << " " << p + 1 << " " << bondedTo[p * MAXBONDS + b] + 1 << "\n";
+                bc++;
+            }
+}
+
+std::string Box::describe() const
+{
+    auto q = [](const std::string &v) {
+        std::string o = "\"";
+        for (char c : v) {
+            if (c == '"' || c == '\\') o += '\\';
+            o += c;
+        }
+        return o + "\"";
+    };
+    std::ostringstream j;
+    j.precision(9);
+    j << "{\"ready\": " << (ready ? "true" : "false") << ", \"Dim\": " << Dim << ", \"nstot\": " << nstot
+      << ", \"grid\": [" << Nx[0] << ", " << Nx[1] << ", " << Nx[2] << "], \"L\": [" << L[0] << ", " << L[1] << ", "
+      << L[2] << "], \"pmeorder\": " << pmeorder << ", \"randSeed\": " << RANDSEED << ", \"logFreq\": " << logFreq
+      << ", \"doCharges\": " << (doCharges ? "true" : "false") << ", \"MAXBONDS\": " << MAXBONDS
+      << ", \"nBonds\": " << nBondsTot << ", \"datFileName\": " << q(datFileName) << ", \"species\": [";
+    for (size_t t = 0; t < species.size(); t++)
+        j << (t ? ", " : "") << "{\"label\": " << q(species[t].label) << ", \"mass\": " << species[t].mass
+          << ", \"mobility\": " << species[t].mobility << "}";
+    j << "], \"bonds\": [";
+    for (int t = 0; t < nBondTypes; t++)
+        j << (t ? ", " : "") << "{\"style\": " << bondStyle[t] << ", \"k\": " << bondK[t] << ", \"req\": " << bondReq[t] << "}";
+    j << "], \"groups\": [";
+    for (size_t g = 0; g < psGroup.size(); g++)
+        j << (g ? ", " : "") << "{\"name\": " << q(psGroup[g].name) << ", \"nsites\": " << psGroup[g].siteList.size()
+          << ", \"force\": " << (psGroup[g].forceFlag ? "true" : "false") << "}";
+    j << "], \"potentials\": [";
+    for (size_t k = 0; k < potentials.size(); k++) {
+        const PS_Potential &p = potentials[k];
+        j << (k ? ", " : "") << "{\"kind\": " << q(p.word) << ", \"I\": " << q(p.grpI) << ", \"J\": " << q(p.grpJ)
+          << ", \"A\": " << p.Ao << ", \"sigma\": " << p.sigma << ", \"Rp\": " << p.Rp << ", \"lB\": " << p.LB
+          << ", \"ramp\": " << (p.ramp ? "true" : "false") << ", \"A_final\": " << p.Ao_final << "}";
+    }
+    j << "], \"integrators\": [";
+    for (size_t k = 0; k < integrators.size(); k++)
+        j << (k ? ", " : "") << "{\"group\": " << q(integrators[k].groupName) << ", \"name\": " << q(integrators[k].name)
+          << ", \"delt\": " << integrators[k].delt << "}";
+    j << "]}";
+    return j.str();
+}
+
+}  // namespace tild

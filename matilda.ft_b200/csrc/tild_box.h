@@ -1,0 +1,196 @@
+// tild_box.h -- host-side mirror of MATILDA.FT's PS_Box object model.
+//
+// Class and member names follow the reference (PS_Box.h:19-212, ps_groups.h:27-63,
+// ps_potential.h:13-53, ps_integrator.h:21-39, ps_species.h); the device work is the
+// fused B200 pipeline of tild_device.h instead of per-object kernels.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "tild_device.h"
+
+namespace tild {
+
+struct BoxError {
+    int code;
+    std::string msg;
+};
+
+struct PS_Species {          // ps_species.cu:13-38
+    std::string label;
+    float mass = 1.0f;
+    float mobility = 1.0f;
+};
+
+struct PS_Group {            // ps_groups.h:27-63
+    std::string name;
+    std::string inputCommand;
+    std::vector<int> siteList;
+    bool forceFlag = false;
+    bool isCharges = false;
+};
+
+struct PS_Potential {        // ps_potential.h:13-53 and the Gaussian/Erf2/ErfG/Charge kinds
+    std::string word;        // script word: gaussian, erf2, erfG, charges
+    int kind = POT_GAUSSIAN;
+    std::string grpI, grpJ;
+    int Iind = -1, Jind = -1;
+    float Ao = 0.f, sigma = 0.f, Rp = 0.f, LB = 0.f;
+    bool ramp = false;
+    double Ao_initial = 0.0, Ao_final = 0.0;
+    double amp_eff = 0.0;    // amplitude the k-space tables currently carry
+    double energy = 0.0;     // last CalcEnergy value
+    std::string input_command;
+    double T0() const;       // u(k=0)/amplitude of the kind
+};
+
+struct Integrator {          // ps_integrator.h:21-39, GJF and EM kinds
+    std::string groupName;
+    std::string name;        // GJF / EM
+    float delt = 0.002f;
+    int group_index = -1;
+    std::string command_line;
+};
+
+class Box {
+public:
+    explicit Box(int device);
+    ~Box();
+
+    // ---- input (PS_Box::readInput, PS_Box_initialization.cu:32-345) ----
+    void command(const std::string &line);          // one line, word by word
+    void finishInitialization();                      // endBox (:352-569)
+    void readDataConfig(const std::string &name);     // :787-997
+    void setParticles(int64_t n, const float *x, const int32_t *type, const int32_t *mol, const float *q);
+    void setBonds(int64_t nb, const int64_t *pairs, const int32_t *btype);
+    void setOption(const std::string &key, int64_t value);
+    void setStream(cudaStream_t st);
+    void setBaseDir(const std::string &d) { baseDir = d; }
+    bool initialized() const { return ready; }
+
+    // ---- run ----
+    void NVT(int64_t nSteps);                          // PS_Box.cu:210-234
+    void steps(int64_t n);                             // doTimeStep x n, no I/O
+    void forces(float *f_out);                         // PS_Box::forces at current x
+    std::vector<double> thermo();                      // computeThermoProps (+ virial)
+    void getPositions(float *x) const;
+    void setPositions(const float *x);
+    void getDensity(const std::string &group, int charge, float *rho);
+    void gridWeights(int32_t *inds, float *w);
+    void modifyBox(const std::string &rest);           // PS_Box.cu:848-870
+    void stageTimes(std::vector<double> &out) const { out = stageSec; }
+    std::string describe() const;
+
+    // info
+    int64_t nstot = 0;
+    int Dim = 0;
+    int Nx[3] = {0, 0, 0};
+    float L[3] = {0, 0, 0}, Lh[3] = {0, 0, 0};
+    double dx[3] = {0, 0, 0};
+    double gvol = 0.0;
+    int pmeorder = 1;
+    int64_t nBondsTot = 0;
+    int nBondTypes = 0;
+    int64_t totSteps = 0;
+    std::vector<PS_Group> psGroup;
+    std::vector<PS_Potential> potentials;
+    std::vector<std::vector<double>> logRows;
+    int nDensityFields() const { return (int)dfields.size(); }
+    int nForceGroups() const { return (int)fgroups.size(); }
+    int64_t deviceBytes() const { return devBytes; }
+    bool echo = false;
+
+private:
+    // parse helpers
+    void parseWords(std::vector<std::string> &w, size_t &i);
+    void addPotential(std::vector<std::string> &w, size_t &i);
+    int findGroupInteger(const std::string &name) const;
+    int findSpeciesInteger(const std::string &name) const;
+    void createDefaultGroups();
+    void writeDataConfig(const std::string &name);
+    void writeData(int64_t step, const std::vector<double> &pairE, double ubond);
+    std::string resolve(const std::string &name) const;
+
+    // device plan
+    void buildPlan();
+    void allocDevice();
+    void freeDevice();
+    void uploadParticles();
+    void enqueueStep(bool energy, bool integrate, float *fout_dev);
+    void enqueueEnergyOnly();
+    void updateRamps(int64_t step, int64_t maxSteps);
+    void captureGraphs();
+    void dropGraphs();
+    std::vector<double> readEnergies(bool with_bond);
+    void ck(cudaError_t e, const char *what) const;
+    template <typename T> T *dalloc(size_t count);
+
+    int device = 0;
+    bool ready = false;
+    bool readDimension = false;
+    std::string baseDir = ".";
+    // reference defaults (PS_Box_initialization.cu:36-62)
+    int blockSize = 512, NSEXTRA = 0, MAXBONDS = 2, MAXANGLES = 3, Nr = 100;
+    double rho0 = -1.0;
+    long long RANDSEED = 0;
+    int logFreq = 100;
+    std::string datFileName = "ps_data.dat", initDataFileName = "init.input.data";
+    bool doCharges = false;
+    bool verbose = false;
+    int nAnglesTot = 0;
+
+    // options
+    int rngCompat = 0, deterministic = 0, exact4 = 0, writeFiles = 1, stageTiming = 0;
+
+    std::vector<PS_Species> species;
+    std::vector<Integrator> integrators;
+    std::vector<float> bondK, bondReq;
+    std::vector<int> bondStyle;
+
+    // host particle state
+    std::vector<float> x, charges;
+    std::vector<int> intSpecies, mID;
+    std::vector<int> nBonds, bondedTo, bondType;   // [n], [n*MAXBONDS]
+
+    // derived plan
+    struct DField { int group; int charge; };
+    std::vector<DField> dfields;
+    std::vector<int> fgroups;                      // group indices receiving grid forces
+    Geom geom{};
+    KSpace ksHost{};
+    ParticleParams ppHost{};
+    FftLine lx{}, ly{}, lz{};
+    int nblkZ = 0, nblkP = 0;
+
+    // device state
+    cudaStream_t stream = nullptr;
+    bool ownStream = false;
+    std::vector<void *> allocs;
+    int64_t devBytes = 0;
+    float *dX[2] = {nullptr, nullptr};
+    float *dNoise = nullptr, *dQ = nullptr, *dF = nullptr;
+    uint32_t *dFlags = nullptr;
+    uint8_t *dNb = nullptr, *dBtype = nullptr;
+    int *dPartner = nullptr, *dOrig = nullptr;
+    void *dRng = nullptr;
+    float2 *dDep = nullptr, *dH = nullptr, *dHg = nullptr, *dTw = nullptr;
+    unsigned long long *dDepFix = nullptr;
+    float4 *dRec = nullptr;
+    long long *dStep = nullptr;
+    KSpace *dKs = nullptr;
+    ParticleParams *dPp = nullptr;
+    double *dEpart = nullptr, *dBpart = nullptr, *dRes = nullptr;
+    KSpace *hKsPinned = nullptr;
+    cudaGraphExec_t gNorm = nullptr, gEnergy = nullptr;
+    std::vector<double> stageSec;
+    // per-kernel event timing (option "stage_timing")
+    enum { STAGE_DEPOSIT, STAGE_XFWD, STAGE_YFWD, STAGE_KSPACE, STAGE_YINV, STAGE_XINV, STAGE_PARTICLES, STAGE_COUNT };
+    bool timing = false;
+    std::vector<std::pair<int, cudaEvent_t>> marks;
+    void mark(int stage);
+};
+
+}  // namespace tild

@@ -1,0 +1,148 @@
+// tild_device.h -- device-side data layout and kernel launchers of the TILD step.
+//
+// Layout in HBM (one box):
+//   X[2][N*3]      float   positions, ping-pong: x_t in X[t&1], x_{t-1} in X[(t+1)&1]
+//   noise[N*3]     float   GJF previous noise
+//   pflags[N]      uint32  bits 0-7 density-field membership, 8-15 force-group
+//                          membership, 16-19 integrator slot (15 = none), 20-23 type
+//   q[N]           float   charges (only with doCharges)
+//   nb[N], partner[N*maxb], btype[N*maxb]   bonds, both directions (readDataConfig)
+//   dep[npair][M]  float2  deposit target: field 2i in .x, 2i+1 in .y
+//   H[D][Nz][Ny][hp]  float2  density half spectra (kx in [0, Nx/2])
+//   Hg[3F][Nz][Ny][hp] float2 gradient half spectra
+//   rec[F][M]      float4  grid force of each force group (x, y, z, 0)
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tild {
+
+constexpr int kMaxFields = 8;     // density fields D
+constexpr int kMaxFGroups = 4;    // force groups F (3F gradient fields)
+constexpr int kMaxPots = 16;
+constexpr int kMaxTerms = 32;
+constexpr int kMaxTypes = 16;
+constexpr int kMaxBondTypes = 16;
+constexpr int kMaxStages = 20;
+constexpr int kNoIntegrator = 15;
+constexpr double kFixScale = 4294967296.0;  // deterministic deposit: 2^32 per unit weight
+
+enum PotKind { POT_GAUSSIAN = 0, POT_ERF2 = 1, POT_ERFG = 2, POT_CHARGES = 3 };
+
+struct FftLine {          // Stockham mixed-radix plan of one line length
+    int n;
+    int ns;
+    int R[kMaxStages];
+    int P[kMaxStages];
+    const float2 *tw;     // device twiddles W_n^t, t in [0, n)  (forward sign)
+};
+
+struct Geom {
+    int nx, ny, nz, nxh, hp;   // grid, half-spectrum width nx/2+1, row pitch (complex)
+    long long M;               // nx*ny*nz
+    long long hstride;         // elements per half-spectrum field = nz*ny*hp
+    float dxf[3];              // (float)(L/Nx)
+    float L[3];
+    float Lh[3];
+};
+
+struct PotDev {
+    int kind;
+    double amp;    // effective amplitude (after any ramp update)
+    double sig2;   // sigma^2
+    double Rp;
+    double lB;
+};
+
+struct KTerm {      // phi_f += mult * u_pot(k) * rhohat_d(k)
+    int fgroup;
+    int pot;
+    int dfield;
+    double mult;
+};
+
+struct ETerm {      // U_pot = fac * sum_k u_pot(k) Re(rhohat_J conj rhohat_I)
+    int pot;
+    int dI, dJ;
+    double fac;
+};
+
+struct KSpace {
+    int npots;
+    PotDev pots[kMaxPots];
+    int nterms;
+    KTerm terms[kMaxTerms];
+    int nfg;              // force groups receiving k-space terms
+    int nd;               // density fields
+    int neterms;
+    ETerm eterms[kMaxPots];
+    double twopi_over_L[3];
+};
+
+struct TypeCoef {   // per-type integrator constants (ps_integratorGJF.cu:63-76)
+    float a, b, noiseMag, bdt2m, bdt2m2;
+};
+
+struct ParticleParams {
+    int N;
+    int order;
+    int quirk4;
+    int nd;                         // density fields
+    int npair;
+    unsigned dchan_charge;          // bit i set: field i is a charge-weighted channel
+    int nfg;
+    unsigned fg_qweighted;          // bit f set: force group f gathers q-weighted
+    int maxb;
+    int nbtypes;
+    float bk[kMaxBondTypes], breq[kMaxBondTypes];
+    int bstyle[kMaxBondTypes];
+    int integ_kind[4];              // 0 GJF, 1 EM per integrator slot
+    float em_delt[4], em_noise[4];
+    TypeCoef coef[4][kMaxTypes];
+    unsigned long long seed;
+    int rng_compat;
+};
+
+struct DevState;   // defined in tild_kernels.cu
+
+// -------------------------------------------------------------------------------------
+// Launchers (tild_kernels.cu).  All run on `st`; none synchronises.
+void build_fft_line(int n, FftLine &pl, float2 *dev_tw_dst);
+void init_fft_attributes();   // opt every FFT kernel into large dynamic shared memory
+cudaError_t launch_zero(void *p, size_t bytes, cudaStream_t st);
+cudaError_t launch_deposit(const Geom &g, const ParticleParams &pp, const float *X0,
+                           const float *X1, const long long *d_step, const uint32_t *pflags,
+                           const float *q, float2 *dep, unsigned long long *dep_fixed,
+                           int deterministic, cudaStream_t st);
+cudaError_t launch_xfwd(const Geom &g, const FftLine &lx, int npair, int nd, const float2 *dep,
+                        const unsigned long long *dep_fixed, float2 *H, cudaStream_t st);
+cudaError_t launch_ypass(const Geom &g, const FftLine &ly, int nfields, int inverse, float2 *H,
+                         cudaStream_t st);
+cudaError_t launch_kspace_z(const Geom &g, const FftLine &lz, const KSpace &ks,
+                            const KSpace *ks_dev, const float2 *H, float2 *Hg, double *epart,
+                            int energy, int forces, int *nblocks_out, cudaStream_t st);
+cudaError_t launch_xinv(const Geom &g, const FftLine &lx, int nfg, const float2 *Hg, float4 *rec,
+                        cudaStream_t st);
+cudaError_t launch_particles(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd,
+                             float *X0, float *X1, float *noise, const uint32_t *pflags,
+                             const float *q, const uint8_t *nb, const int *partner,
+                             const uint8_t *btype, const float4 *rec, const int *orig_id,
+                             void *rng_states, const long long *d_step, float *fout,
+                             int integrate, cudaStream_t st);
+cudaError_t launch_tick(long long *d_step, cudaStream_t st);
+cudaError_t launch_rng_init(void *states, const int *orig_id, int n, unsigned long long seed,
+                            cudaStream_t st);
+size_t rng_state_bytes();
+cudaError_t launch_bond_energy(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd,
+                               const float *X0, const float *X1, const long long *d_step,
+                               const uint8_t *nb, const int *partner, const uint8_t *btype,
+                               double *partials, int *nblocks_out, cudaStream_t st);
+cudaError_t launch_reduce_partials(const double *partials, int nblocks, int ncols, double *out,
+                                   cudaStream_t st);
+cudaError_t launch_grid_weights(const Geom &g, int order, int quirk4, const float *X, int N,
+                                int *inds, float *W, cudaStream_t st);
+cudaError_t launch_density_single(const Geom &g, const ParticleParams &pp, const float *X,
+                                  const int *sites, int ns, const float *q, int charge,
+                                  float *rho, cudaStream_t st);
+
+}  // namespace tild

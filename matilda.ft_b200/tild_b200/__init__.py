@@ -1,0 +1,256 @@
+"""Python binding of the B200-native TILD particle-mesh library (libtild_b200.so).
+
+A thin ctypes layer over the C ABI in include/tild_b200.h.  The compute path is the
+CUDA library; there is no Python or CPU fallback: importing this module loads the
+in-tree ``lib/libtild_b200.so`` and raises if it is missing.
+
+``Box`` mirrors MATILDA.FT's PS_Box surface: feed it the same ``box ps ... endBox``
+script lines (PS_Box::readInput), then ``run_nvt`` (PS_Box::NVT), ``forces``
+(PS_Box::forces), ``thermo`` (PS_Box::computeThermoProps).
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libtild_b200.so")
+
+TILD_OK = 0
+STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_PARSE", 3: "ERR_IO", 4: "ERR_CUDA", 5: "ERR_STATE",
+          6: "ERR_UNSUPPORTED", 7: "ERR_DEVICE"}
+
+# Every entry point of include/tild_b200.h with its ctypes signature.
+_SIGS = {
+    "tild_version": ([], ctypes.c_char_p),
+    "tild_last_error": ([], ctypes.c_char_p),
+    "tild_box_create": ([ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    "tild_box_destroy": ([ctypes.c_void_p], ctypes.c_int),
+    "tild_box_set_stream": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "tild_box_set_base_dir": ([ctypes.c_void_p, ctypes.c_char_p], ctypes.c_int),
+    "tild_box_command": ([ctypes.c_void_p, ctypes.c_char_p], ctypes.c_int),
+    "tild_box_read_input": ([ctypes.c_void_p, ctypes.c_char_p], ctypes.c_int),
+    "tild_box_set_particles": ([ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                                ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "tild_box_set_bonds": ([ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "tild_box_set_option": ([ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int64], ctypes.c_int),
+    "tild_box_describe": ([ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)],
+                          ctypes.c_int),
+    "tild_box_get_info": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "tild_box_run_nvt": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
+    "tild_box_step": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
+    "tild_box_forces": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "tild_box_thermo": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)],
+                        ctypes.c_int),
+    "tild_box_get_positions": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "tild_box_set_positions": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "tild_box_get_density": ([ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+    "tild_box_grid_weights": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "tild_box_get_log": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64),
+                          ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
+    "tild_run_script_file": ([ctypes.c_char_p, ctypes.c_int], ctypes.c_int),
+    "tild_box_stage_times": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)],
+                             ctypes.c_int),
+}
+
+
+class TildError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (STATUS.get(code, "?"), code, msg))
+        self.code = code
+
+
+class BoxInfo(ctypes.Structure):
+    _fields_ = [("nstot", ctypes.c_int64), ("dim", ctypes.c_int32), ("nx", ctypes.c_int32 * 3),
+                ("L", ctypes.c_float * 3), ("pmeorder", ctypes.c_int32), ("n_groups", ctypes.c_int32),
+                ("n_potentials", ctypes.c_int32), ("n_density_fields", ctypes.c_int32),
+                ("n_force_groups", ctypes.c_int32), ("n_bond_types", ctypes.c_int32),
+                ("n_bonds", ctypes.c_int64), ("step", ctypes.c_int64), ("device_bytes", ctypes.c_int64)]
+
+
+_lib = None
+
+
+def lib():
+    """Load the in-tree CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libtild_b200.so is not built (run `make -C matilda.ft_b200`): " + LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (args, res) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != TILD_OK:
+        raise TildError(rc, lib().tild_last_error().decode())
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+class Box:
+    """One PS box on one GPU (PS_Box, PS_Box.h:19-212)."""
+
+    def __init__(self, device=0, base_dir=None, options=None):
+        h = ctypes.c_void_p()
+        _check(lib().tild_box_create(int(device), ctypes.byref(h)))
+        self._h = h
+        if base_dir:
+            _check(lib().tild_box_set_base_dir(self._h, base_dir.encode()))
+        for k, v in (options or {}).items():
+            self.set_option(k, v)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().tild_box_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- input -------------------------------------------------------------------
+    def command(self, line: str):
+        _check(lib().tild_box_command(self._h, line.encode()))
+
+    def read_input(self, text: str):
+        _check(lib().tild_box_read_input(self._h, text.encode()))
+
+    def set_option(self, key: str, value: int):
+        _check(lib().tild_box_set_option(self._h, key.encode(), int(value)))
+
+    def set_stream(self, stream_handle: int):
+        _check(lib().tild_box_set_stream(self._h, ctypes.c_void_p(stream_handle)))
+
+    def set_particles(self, x, types, mol=None, q=None):
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(types, np.int32)
+        m = None if mol is None else np.ascontiguousarray(mol, np.int32)
+        qq = None if q is None else np.ascontiguousarray(q, np.float32)
+        _check(lib().tild_box_set_particles(self._h, len(t), _ptr(x), _ptr(t), _ptr(m), _ptr(qq)))
+
+    def set_bonds(self, pairs, btype=None):
+        p = np.ascontiguousarray(pairs, np.int64).reshape(-1, 2)
+        b = None if btype is None else np.ascontiguousarray(btype, np.int32)
+        _check(lib().tild_box_set_bonds(self._h, len(p), _ptr(p), _ptr(b)))
+
+    # -- queries -------------------------------------------------------------------
+    def describe(self) -> dict:
+        need = ctypes.c_int64()
+        _check(lib().tild_box_describe(self._h, None, 0, ctypes.byref(need)))
+        buf = ctypes.create_string_buffer(need.value)
+        _check(lib().tild_box_describe(self._h, buf, need.value, None))
+        return json.loads(buf.value.decode())
+
+    def info(self) -> BoxInfo:
+        out = BoxInfo()
+        _check(lib().tild_box_get_info(self._h, ctypes.byref(out)))
+        return out
+
+    @property
+    def N(self):
+        return int(self.info().nstot)
+
+    # -- run -----------------------------------------------------------------------
+    def run_nvt(self, nsteps: int):
+        _check(lib().tild_box_run_nvt(self._h, int(nsteps)))
+
+    def step(self, nsteps: int = 1):
+        _check(lib().tild_box_step(self._h, int(nsteps)))
+
+    def forces(self):
+        f = np.zeros((self.N, 3), np.float32)
+        _check(lib().tild_box_forces(self._h, _ptr(f)))
+        return f
+
+    def thermo(self):
+        nmax = 64
+        out = np.zeros(nmax, np.float64)
+        n = ctypes.c_int()
+        _check(lib().tild_box_thermo(self._h, _ptr(out), nmax, ctypes.byref(n)))
+        npot = self.info().n_potentials
+        v = out[: n.value]
+        return dict(Upe=float(v[0]), Ubond=float(v[1]), potentials=[float(e) for e in v[2:2 + npot]],
+                    virial=v[2 + npot:2 + npot + 6].copy())
+
+    def positions(self):
+        x = np.zeros((self.N, 3), np.float32)
+        _check(lib().tild_box_get_positions(self._h, _ptr(x)))
+        return x
+
+    def set_positions(self, x):
+        x = np.ascontiguousarray(x, np.float32)
+        _check(lib().tild_box_set_positions(self._h, _ptr(x)))
+
+    def density(self, group: str, charge=False):
+        i = self.info()
+        rho = np.zeros(int(i.nx[0]) * int(i.nx[1]) * int(i.nx[2]), np.float32)
+        _check(lib().tild_box_get_density(self._h, group.encode(), int(bool(charge)), _ptr(rho)))
+        return rho
+
+    def grid_weights(self):
+        i = self.info()
+        G = (i.pmeorder + 1) ** 3
+        inds = np.zeros((self.N, G), np.int32)
+        w = np.zeros((self.N, G), np.float32)
+        _check(lib().tild_box_grid_weights(self._h, _ptr(inds), _ptr(w)))
+        return inds, w
+
+    def log(self):
+        rows, cols = ctypes.c_int64(), ctypes.c_int32()
+        _check(lib().tild_box_get_log(self._h, None, ctypes.byref(rows), ctypes.byref(cols)))
+        out = np.zeros((rows.value, cols.value), np.float64)
+        _check(lib().tild_box_get_log(self._h, _ptr(out), None, None))
+        return out
+
+
+def run_script_file(path: str, device: int = 0):
+    """Execute a MATILDA.FT input script (main.cu:21-156) with the B200 library."""
+    _check(lib().tild_run_script_file(path.encode(), int(device)))
+
+
+def box_from_spec(spec, device=0, options=None, steps_script=False):
+    """Build a Box directly from a synth.SystemSpec (arrays instead of readData)."""
+    b = Box(device, options=options)
+    D = spec.dim
+    b.command("Dim %d" % D)
+    b.command("boxLengths " + " ".join("%.9g" % v for v in spec.L[:D]))
+    b.command("grid " + " ".join(str(int(v)) for v in spec.grid[:D]))
+    b.command("pmeorder %d" % spec.order)
+    b.command("randSeed %d" % spec.seed)
+    if spec.charges is not None:
+        b.command("doCharges")
+    for t, lb in enumerate(spec.species):
+        b.command("species %s mass %.9g mobility %.9g" % (lb, spec.masses[t], spec.mobility[t]))
+    b.set_particles(spec.x, spec.types, spec.mol, spec.charges)
+    if len(spec.bonds):
+        b.command("bond 1 harmonic %.9g %.9g" % (spec.bond_k, spec.bond_req))
+        b.set_bonds(spec.bonds)
+    for p in spec.potentials:
+        if p["kind"] == "gaussian":
+            b.command("potential gaussian %s %s %.9g %.9g" % (p["I"], p["J"], p["A"], p["sigma"]))
+        elif p["kind"] in ("erf2", "erfG"):
+            b.command("potential %s %s %s %.9g %.9g %.9g" % (p["kind"], p["I"], p["J"], p["A"], p["Rp"], p["sigma"]))
+        else:
+            b.command("potential charges %.9g %.9g" % (p["lB"], p["sigma"]))
+    b.command("integrator all %s delt %.9g" % (spec.integrator, spec.delt))
+    b.command("logFreq %d" % spec.log_freq)
+    return b

@@ -1,0 +1,48 @@
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+for p in (ROOT, os.path.join(ROOT, "oracle"), os.path.join(ROOT, "matilda.ft_b200")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
+
+
+def spec_to_system(spec, maxb=2, **kw):
+    """synth.SystemSpec -> oracle.System."""
+    import oracle
+    nb, partner, btype = spec.partner_lists(maxb)
+    D = spec.dim
+    return oracle.System(
+        Dim=D, L=np.asarray(spec.L[:D], np.float32), Nx=np.asarray(spec.grid[:D], np.int32),
+        order=spec.order, x=np.asarray(spec.x[:, :D], np.float32), types=spec.types,
+        mass=np.asarray(spec.masses, np.float32), mobility=np.asarray(spec.mobility, np.float32),
+        species=spec.species, charges=spec.charges, nb=nb, partner=partner, btype=btype,
+        bond_k=np.array([spec.bond_k], np.float32), bond_req=np.array([spec.bond_req], np.float32),
+        bond_style=np.array([0], np.int32), potentials=spec.potentials, delt=spec.delt,
+        integrator=spec.integrator, **kw)
+
+
+def force_error(f, fref):
+    """max_p |f_p - fref_p| / max(|fref_p|, f_rms) (the per-particle metric of the tests)."""
+    fref = np.asarray(fref, np.float64)
+    f = np.asarray(f, np.float64)
+    mag = np.linalg.norm(fref, axis=1)
+    rms = np.sqrt(np.mean(mag ** 2))
+    den = np.maximum(mag, rms)
+    return float(np.max(np.linalg.norm(f - fref, axis=1) / den))
+
+
+@pytest.fixture(scope="session")
+def gpu_available():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False

@@ -1,0 +1,243 @@
+"""GPU parity of the CUDA TILD path against the CPU oracle, through the C ABI.
+
+Tolerances (written here, used below):
+  * stencil indices: bit-exact with the FP32 restatement of d_calcGridWeights;
+    weights: bit-exact as well (same IEEE operations, explicit FMAs);
+  * densities: |drho| <= 1e-6 * max|rho| (FP32 atomics vs FP64 sums);
+  * forces: max_p |df_p| / max(|f_p|, f_rms) <= 1e-5 against the FP64 oracle;
+  * energies: relative 1e-5 (pair terms) and 1e-6 (bond term);
+  * 100-step GJF trajectories with identical Philox noise: max |dx| <= 2e-4.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import tild_b200
+from conftest import force_error, spec_to_system
+from tild_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+F_TOL = 1e-5
+
+
+def make_box(spec, **opts):
+    o = {"write_files": 0}
+    o.update(opts)
+    b = tild_b200.box_from_spec(spec, options=o)
+    b.command("endBox")
+    return b
+
+
+SYSTEMS = {
+    "diblock_o3": lambda: synth.small_system(seed=1, order=3),
+    "charged_o3": lambda: synth.small_system(seed=2, order=3, charges=True),
+    "o0": lambda: synth.small_system(seed=3, order=0),
+    "o1": lambda: synth.small_system(seed=4, order=1),
+    "o2": lambda: synth.small_system(seed=5, order=2),
+    "o4_quirk": lambda: synth.small_system(seed=6, order=4),
+    "erf": lambda: synth.small_system(seed=7, order=3, pots=[
+        dict(kind="erf2", I="A", J="B", A=0.05, Rp=1.0, sigma=0.5),
+        dict(kind="erfG", I="B", J="B", A=0.3, Rp=0.8, sigma=0.5),
+        dict(kind="gaussian", I="all", J="A", A=1.5, sigma=0.8)]),
+    "odd_grid": lambda: synth.small_system(seed=8, order=3, grid=(15, 9, 21), charges=True),
+    "free_particles": lambda: synth.small_system(seed=9, order=3, n_free=50, charges=True),
+}
+
+
+@pytest.mark.parametrize("name", sorted(SYSTEMS))
+def test_forces_match_oracle(name):
+    spec = SYSTEMS[name]()
+    sysm = spec_to_system(spec)
+    with make_box(spec) as b:
+        f = b.forces()
+    fref, _ = oracle.forces(sysm, prec=64)
+    err = force_error(f, fref)
+    assert err <= F_TOL, "%s: force error %.3g" % (name, err)
+
+
+@pytest.mark.parametrize("order", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("exact4", [0, 1])
+def test_grid_weights_bit_exact(order, exact4):
+    if exact4 and order != 4:
+        pytest.skip("exact flag only changes order 4")
+    spec = synth.small_system(seed=20 + order, order=order)
+    rng = np.random.default_rng(order)
+    # edge cases: 0, exactly on grid lines/cell centres, just below L, exactly L
+    L = spec.L
+    h = L / spec.grid
+    extra = np.array([[0, 0, 0], L * 0.999999, L, h * 3, h * 3.5, h * 2.5 + 1e-6], np.float32)
+    spec.x = np.concatenate([spec.x, extra]).astype(np.float32)
+    spec.types = np.r_[spec.types, np.zeros(len(extra), np.int32)]
+    spec.mol = np.r_[spec.mol, np.arange(len(extra)) + 10000].astype(np.int32)
+    sysm = spec_to_system(spec, quirk4=0 if exact4 else 1)
+    with make_box(spec, bspline4_exact=exact4) as b:
+        inds, w = b.grid_weights()
+    ri, rw = oracle.weights(sysm, prec=32)
+    assert np.array_equal(inds, ri)
+    assert np.array_equal(w.view(np.uint32), rw.astype(np.float32).view(np.uint32))
+
+
+def test_densities_match_oracle():
+    spec = synth.small_system(seed=11, order=3, charges=True)
+    sysm = spec_to_system(spec)
+    dens, _, _ = oracle.densities(sysm, prec=64)
+    with make_box(spec) as b:
+        for name, (rho, rhoq) in dens.items():
+            got = b.density(name)
+            assert np.abs(got - rho).max() <= 1e-6 * np.abs(rho).max()
+            if rhoq is not None:
+                gq = b.density(name, charge=True)
+                assert np.abs(gq - rhoq).max() <= 1e-6 * np.abs(rhoq).max()
+
+
+@pytest.mark.parametrize("name", ["diblock_o3", "charged_o3", "erf", "odd_grid"])
+def test_energies_match_oracle(name):
+    spec = SYSTEMS[name]()
+    sysm = spec_to_system(spec)
+    dens, _, _ = oracle.densities(sysm)
+    ref = oracle.pair_energies(sysm, dens)
+    ub, vir = oracle.bond_energy(sysm)
+    with make_box(spec) as b:
+        t = b.thermo()
+    for e, r in zip(t["potentials"], ref):
+        assert abs(e - r) <= 1e-5 * max(abs(r), 1e-12) + 1e-9, (e, r)
+    assert abs(t["Ubond"] - ub) <= 1e-6 * abs(ub)
+    assert abs(t["Upe"] - (sum(ref) + ub)) <= 1e-5 * abs(sum(ref) + ub)
+
+
+def test_deterministic_mode_bit_reproducible_and_accurate():
+    spec = synth.small_system(seed=12, order=3, charges=True)
+    sysm = spec_to_system(spec)
+    fref, _ = oracle.forces(sysm)
+    outs = []
+    for _ in range(2):
+        with make_box(spec, deterministic=1) as b:
+            outs.append(b.forces())
+            b.step(5)
+            outs.append(b.positions())
+    assert np.array_equal(outs[0], outs[2]) and np.array_equal(outs[1], outs[3])
+    assert force_error(outs[0], fref) <= F_TOL
+
+
+@pytest.mark.parametrize("integ", ["GJF", "EM"])
+def test_trajectory_matches_oracle_100_steps(integ):
+    spec = synth.small_system(seed=13, order=3, charges=True)
+    spec.integrator = integ
+    sysm = spec_to_system(spec)
+    traj = oracle.Trajectory(sysm, 64)
+    ids = np.arange(sysm.N)
+    with make_box(spec) as b:
+        b.step(100)
+        x = b.positions()
+    for step in range(100):
+        traj.step(oracle.philox_normals(spec.seed, step, ids))
+    d = np.abs(x - traj.positions())
+    d = np.minimum(d, spec.L - d)
+    assert d.max() <= 2e-4, d.max()
+
+
+def test_forces_unchanged_by_forces_call_and_positions_round_trip():
+    spec = synth.small_system(seed=14, order=3)
+    with make_box(spec) as b:
+        x0 = b.positions()
+        assert np.array_equal(x0, spec.x.astype(np.float32))
+        f1 = b.forces()
+        f2 = b.forces()
+        assert np.array_equal(f1, f2)
+        assert np.array_equal(b.positions(), x0)
+
+
+def test_rng_compat_mode_statistics():
+    """cuRAND XORWOW mode (curand_init(seed, i, 0) + curand_normal): free particles with no
+    forces diffuse with <dx^2> = 2 D dt per step under EM."""
+    n = 4000
+    rng = np.random.default_rng(0)
+    L = 50.0
+    spec = synth.SystemSpec("free", [L, L, L], [16, 16, 16], rng.uniform(10, 40, size=(n, 3)),
+                            np.zeros(n, np.int32), ["A"], np.zeros((0, 2)), np.arange(n),
+                            potentials=[], order=1, integrator="EM", delt=0.01)
+    with make_box(spec, rng=1) as b:
+        x0 = b.positions().astype(np.float64)
+        b.step(10)
+        x1 = b.positions().astype(np.float64)
+    msd = ((x1 - x0) ** 2).mean()
+    assert abs(msd - 10 * 2 * 0.01) < 0.05 * 10 * 2 * 0.01
+
+
+def test_run_script_file_writes_ps_data(tmp_path):
+    spec = synth.small_system(seed=15, order=3, charges=True)
+    spec.log_freq = 10
+    scr, _ = spec.write(str(tmp_path), steps=30)
+    tild_b200.run_script_file(scr)
+    rows = [l.split() for l in open(os.path.join(tmp_path, "ps_data.dat")) if l.strip()]
+    # writeData(-1), steps 0, 10, 20, final writeData(30)
+    assert [r[0] for r in rows] == ["-1", "0", "10", "20", "30"]
+    assert all(len(r) == 2 + len(spec.potentials) for r in rows)   # step Ubond pot...
+    assert os.path.exists(os.path.join(tmp_path, "final.input.data"))
+    assert os.path.exists(os.path.join(tmp_path, "init.input.data"))
+
+
+def test_nvt_log_matches_thermo():
+    spec = synth.small_system(seed=16, order=3, charges=True)
+    sysm = spec_to_system(spec)
+    dens, _, _ = oracle.densities(sysm)
+    ref = oracle.pair_energies(sysm, dens)
+    ub, _ = oracle.bond_energy(sysm)
+    with make_box(spec) as b:
+        b.run_nvt(3)
+        log = b.log()
+    assert log.shape[0] == 3   # -1, 0, final
+    assert log[0, 0] == -1 and abs(log[0, 1] - ub) <= 1e-6 * abs(ub)
+    for k, r in enumerate(ref):
+        assert abs(log[0, 2 + k] - r) <= 1e-5 * abs(r)
+    # step-0 row: pair energies from the step's start densities (x0), bonds after the update
+    for k, r in enumerate(ref):
+        assert abs(log[1, 2 + k] - r) <= 1e-5 * abs(r)
+
+
+def test_ramp_updates_amplitude():
+    spec = synth.small_system(seed=17, order=3)
+    spec.potentials = [dict(kind="gaussian", I="A", J="B", A=2.0, sigma=0.7)]
+    sysm = spec_to_system(spec)
+    b = tild_b200.box_from_spec(spec, options={"write_files": 0})
+    b.close()
+    # ramp from 2 to 4 over 4 steps: after run_nvt(4) the amplitude is 4
+    bb = tild_b200.Box(0, options={"write_files": 0})
+    bb.command("Dim 3")
+    bb.command("boxLengths %g %g %g" % tuple(spec.L))
+    bb.command("grid %d %d %d" % tuple(spec.grid))
+    bb.command("species A")
+    bb.command("species B")
+    bb.set_particles(spec.x, spec.types, spec.mol)
+    bb.command("bond 1 harmonic 1.5 0.0")
+    bb.set_bonds(spec.bonds)
+    bb.command("potential gaussian A B 2.0 0.7 ramp 4.0")
+    bb.command("integrator all GJF delt 0.005")
+    bb.command("endBox")
+    bb.run_nvt(4)
+    log = bb.log()
+    x = bb.positions()
+    dens, _, _ = oracle.densities(sysm, x=x)
+    e4 = oracle.pair_energies(sysm, dens)[0] * 2.0   # amplitude 4 = 2 x 2
+    t = bb.thermo()
+    assert abs(t["potentials"][0] - e4) <= 1e-5 * abs(e4)
+    assert log.shape[0] == 3
+    bb.close()
+
+
+def test_full_size_c2_properties():
+    """Coacervate at full size (2,097,152 particles, 192^3): momentum conservation of the
+    grid forces and bonds (sum_p f_p ~ 0), finite forces, and a step that keeps every
+    particle in the box."""
+    spec = synth.config_c2()
+    with make_box(spec) as b:
+        f = b.forces().astype(np.float64)
+        assert np.isfinite(f).all()
+        frms = np.sqrt((f ** 2).sum(1).mean())
+        assert np.abs(f.sum(0)).max() < 1e-4 * frms * np.sqrt(len(f))
+        b.step(2)
+        x = b.positions()
+        assert (x >= 0).all() and (x <= spec.L).all()
