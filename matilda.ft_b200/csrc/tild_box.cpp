@@ -26,6 +26,7 @@
 namespace tild {
 
 void init_fft_attributes();
+void init_deposit_attributes();
 
 namespace {
 
@@ -145,7 +146,10 @@ void Box::setOption(const std::string &key, int64_t v)
     if (key == "rng") rngCompat = (int)v;
     else if (key == "deterministic") deterministic = (int)v;
     else if (key == "bspline4_exact") exact4 = (int)v;
-    else if (key == "sort_interval") { /* particle order is kept; accepted for API stability */ }
+    else if (key == "sort_interval") {
+        if (v < 0) fail(TILD_ERR_ARG, "sort_interval must be >= 0");
+        sortInterval = (int)v;
+    }
     else fail(TILD_ERR_ARG, "unknown option '" + key + "'");
 }
 
@@ -597,9 +601,14 @@ void Box::finishInitialization()
         ownStream = true;
     }
     init_fft_attributes();
+    init_deposit_attributes();
     buildPlan();
     allocDevice();
     uploadParticles();
+    if (sortInterval > 0) {   // start from a spatially coherent order
+        sortParticles();
+        ck(cudaStreamSynchronize(stream), "initial sort");
+    }
     ready = true;
 }
 
@@ -760,7 +769,26 @@ void Box::allocDevice()
     dEpart = dalloc<double>((size_t)nblkZ * std::max(1, ksHost.neterms));
     dBpart = dalloc<double>((size_t)nblkP * 7);
     dRes = dalloc<double>(kMaxPots + 8);
+    dTmp = dalloc<float>(3 * N);
     ck(cudaMallocHost(&hKsPinned, sizeof(KSpace)), "cudaMallocHost");
+    // sort scratch and the permuted copies
+    const uint32_t nk = sort_key_count(g);
+    sortW.key = dalloc<uint32_t>(N);
+    sortW.rank = dalloc<int>(N);
+    sortW.newpos = dalloc<int>(N);
+    sortW.count = dalloc<uint32_t>(nk);
+    sortW.start = dalloc<uint32_t>(nk);
+    sortW.totals = dalloc<uint32_t>(nk / 1024 + 2);
+    sortW.X0 = dalloc<float>(3 * N);
+    sortW.X1 = dalloc<float>(3 * N);
+    sortW.noise = dalloc<float>(3 * N);
+    sortW.q = doCharges ? dalloc<float>(N) : nullptr;
+    sortW.flags = dalloc<uint32_t>(N);
+    sortW.orig = dalloc<int>(N);
+    sortW.partner = dalloc<int>(N * MAXBONDS);
+    sortW.nb = dalloc<uint8_t>(N);
+    sortW.btype = dalloc<uint8_t>(N * MAXBONDS);
+    sortW.rng = rngCompat ? (void *)dalloc<unsigned char>(N * rng_state_bytes()) : nullptr;
 }
 
 void Box::uploadParticles()
@@ -772,7 +800,32 @@ void Box::uploadParticles()
     ck(cudaMemcpy(dX[0], x3.data(), 12 * N, cudaMemcpyHostToDevice), "upload x");
     ck(cudaMemcpy(dX[1], x3.data(), 12 * N, cudaMemcpyHostToDevice), "upload xOld");   // GJF: xOld = x
     ck(cudaMemset(dNoise, 0, 12 * N), "zero noise");
-    // membership flags
+    std::vector<int> orig(N);
+    std::iota(orig.begin(), orig.end(), 0);
+    ck(cudaMemcpy(dOrig, orig.data(), 4 * N, cudaMemcpyHostToDevice), "upload ids");
+    if (doCharges) ck(cudaMemcpy(dQ, charges.data(), 4 * N, cudaMemcpyHostToDevice), "upload q");
+    std::vector<uint8_t> nb8(N), bt8(N * MAXBONDS);
+    for (int64_t p = 0; p < N; p++) nb8[p] = (uint8_t)nBonds[p];
+    for (int64_t k = 0; k < N * MAXBONDS; k++) bt8[k] = (uint8_t)bondType[k];
+    ck(cudaMemcpy(dNb, nb8.data(), N, cudaMemcpyHostToDevice), "upload nb");
+    ck(cudaMemcpy(dPartner, bondedTo.data(), 4 * N * MAXBONDS, cudaMemcpyHostToDevice), "upload partners");
+    ck(cudaMemcpy(dBtype, bt8.data(), N * MAXBONDS, cudaMemcpyHostToDevice), "upload bond types");
+    long long zero = 0;
+    ck(cudaMemcpy(dStep, &zero, sizeof(zero), cudaMemcpyHostToDevice), "upload step");
+    uploadFlags();
+    if (rngCompat) {   // d_initDeviceRNG (device_utils.cu:465-472), seed = RANDSEED (unsigned int)
+        ck(launch_rng_init(dRng, dOrig, (int)N, (unsigned long long)(unsigned int)RANDSEED, stream), "rng init");
+        ck(cudaStreamSynchronize(stream), "rng init sync");
+    }
+    ck(cudaDeviceSynchronize(), "upload");
+}
+
+// Per-particle membership flags (density fields, force groups, integrator slot, type) and
+// the plan constants; flags are built in original particle order and stored in the
+// current slot order.
+void Box::uploadFlags()
+{
+    const int64_t N = nstot;
     std::vector<uint32_t> fl(N, 0u);
     std::vector<std::vector<char>> member(psGroup.size(), std::vector<char>(N, 0));
     for (size_t gi = 0; gi < psGroup.size(); gi++)
@@ -790,26 +843,52 @@ void Box::uploadParticles()
             slot[p] = (int)s;
         }
     for (int64_t p = 0; p < N; p++) fl[p] |= ((uint32_t)slot[p] << 16) | ((uint32_t)intSpecies[p] << 20);
-    ck(cudaMemcpy(dFlags, fl.data(), 4 * N, cudaMemcpyHostToDevice), "upload flags");
-    std::vector<int> orig(N);
-    std::iota(orig.begin(), orig.end(), 0);
-    ck(cudaMemcpy(dOrig, orig.data(), 4 * N, cudaMemcpyHostToDevice), "upload ids");
-    if (doCharges) ck(cudaMemcpy(dQ, charges.data(), 4 * N, cudaMemcpyHostToDevice), "upload q");
-    std::vector<uint8_t> nb8(N), bt8(N * MAXBONDS);
-    for (int64_t p = 0; p < N; p++) nb8[p] = (uint8_t)nBonds[p];
-    for (int64_t k = 0; k < N * MAXBONDS; k++) bt8[k] = (uint8_t)bondType[k];
-    ck(cudaMemcpy(dNb, nb8.data(), N, cudaMemcpyHostToDevice), "upload nb");
-    ck(cudaMemcpy(dPartner, bondedTo.data(), 4 * N * MAXBONDS, cudaMemcpyHostToDevice), "upload partners");
-    ck(cudaMemcpy(dBtype, bt8.data(), N * MAXBONDS, cudaMemcpyHostToDevice), "upload bond types");
-    long long zero = 0;
-    ck(cudaMemcpy(dStep, &zero, sizeof(zero), cudaMemcpyHostToDevice), "upload step");
+    const std::vector<int> orig = slotOrder();
+    std::vector<uint32_t> fs(N);
+    for (int64_t s = 0; s < N; s++) fs[s] = fl[orig[s]];
+    ck(cudaMemcpy(dFlags, fs.data(), 4 * N, cudaMemcpyHostToDevice), "upload flags");
     ck(cudaMemcpy(dKs, &ksHost, sizeof(KSpace), cudaMemcpyHostToDevice), "upload k-space plan");
     ck(cudaMemcpy(dPp, &ppHost, sizeof(ParticleParams), cudaMemcpyHostToDevice), "upload particle params");
-    if (rngCompat) {   // d_initDeviceRNG (device_utils.cu:465-472), seed = RANDSEED (unsigned int)
-        ck(launch_rng_init(dRng, dOrig, (int)N, (unsigned long long)(unsigned int)RANDSEED, stream), "rng init");
-        ck(cudaStreamSynchronize(stream), "rng init sync");
+}
+
+// orig[s]: original particle id stored in slot s.
+std::vector<int> Box::slotOrder() const
+{
+    std::vector<int> orig(nstot);
+    ck(cudaMemcpy(orig.data(), dOrig, 4 * nstot, cudaMemcpyDeviceToHost), "read ids");
+    return orig;
+}
+
+// Spatial re-sort of every per-particle array (tild_sort.cu), then copy back in place so
+// the captured step graphs keep their pointers.
+void Box::sortParticles()
+{
+    const int64_t N = nstot;
+    PermIn in{dX[0], dX[1], dNoise, dQ, dFlags, dOrig, dPartner, dNb, dBtype, dRng, dStep};
+    ck(launch_sort(geom, (int)N, MAXBONDS, sortW, in, stream), "sort");
+    auto cp = [&](void *dst, const void *src, size_t bytes) {
+        ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, stream), "sort copy");
+    };
+    cp(dX[0], sortW.X0, 12 * N);
+    cp(dX[1], sortW.X1, 12 * N);
+    cp(dNoise, sortW.noise, 12 * N);
+    cp(dFlags, sortW.flags, 4 * N);
+    cp(dOrig, sortW.orig, 4 * N);
+    if (dQ) cp(dQ, sortW.q, 4 * N);
+    cp(dNb, sortW.nb, N);
+    cp(dPartner, sortW.partner, 4 * N * MAXBONDS);
+    cp(dBtype, sortW.btype, N * MAXBONDS);
+    if (dRng) cp(dRng, sortW.rng, N * rng_state_bytes());
+    sinceSort = 0;
+}
+
+void Box::maybeSort()
+{
+    if (sortInterval > 0 && sinceSort >= sortInterval) {
+        if (gSort) ck(cudaGraphLaunch(gSort, stream), "sort graph");
+        else sortParticles();
+        sinceSort = 0;
     }
-    ck(cudaDeviceSynchronize(), "upload");
 }
 
 // ---------------------------------------------------------------------------------------
@@ -896,7 +975,8 @@ void Box::dropGraphs()
 {
     if (gNorm) cudaGraphExecDestroy(gNorm);
     if (gEnergy) cudaGraphExecDestroy(gEnergy);
-    gNorm = gEnergy = nullptr;
+    if (gSort) cudaGraphExecDestroy(gSort);
+    gNorm = gEnergy = gSort = nullptr;
 }
 
 void Box::captureGraphs()
@@ -916,6 +996,19 @@ void Box::captureGraphs()
         ck(cudaGraphInstantiate(&ex, gr, 0), "graph instantiate");
         cudaGraphDestroy(gr);
         (e ? gEnergy : gNorm) = ex;
+    }
+    if (sortInterval > 0 && !gSort) {
+        cudaGraph_t gr;
+        ck(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        try {
+            sortParticles();
+        } catch (...) {
+            cudaStreamEndCapture(stream, &gr);
+            throw;
+        }
+        ck(cudaStreamEndCapture(stream, &gr), "end capture");
+        ck(cudaGraphInstantiate(&gSort, gr, 0), "graph instantiate");
+        cudaGraphDestroy(gr);
     }
 }
 
@@ -944,8 +1037,10 @@ void Box::steps(int64_t n)
         timing = true;
         marks.clear();
         for (int64_t i = 0; i < n; i++) {
+            maybeSort();
             enqueueStep(false, true, nullptr);
             totSteps++;
+            sinceSort++;
         }
         timing = false;
         ck(cudaStreamSynchronize(stream), "sync");
@@ -967,8 +1062,10 @@ void Box::steps(int64_t n)
     }
     captureGraphs();
     for (int64_t i = 0; i < n; i++) {
+        maybeSort();
         ck(cudaGraphLaunch(gNorm, stream), "graph launch");
         totSteps++;
+        sinceSort++;
     }
     ck(cudaGetLastError(), "step");
 }
@@ -992,9 +1089,11 @@ void Box::NVT(int64_t nSteps)
     for (int64_t i = 0; i < nSteps; i++) {
         const bool energy = (i % logFreq == 0) || (i == nSteps - 1);
         for (int k = 0; k < npot; k++) ampUsed[k] = potentials[k].amp_eff;
+        maybeSort();
         if (anyRamp) enqueueStep(energy, true, nullptr);
         else ck(cudaGraphLaunch(energy ? gEnergy : gNorm, stream), "graph launch");
         totSteps++;
+        sinceSort++;
         updateRamps(i, nSteps);
         if (energy) {
             std::vector<double> r = readEnergies(true);
@@ -1060,17 +1159,25 @@ void Box::forces(float *f_out)
     if (!ready) fail(TILD_ERR_STATE, "endBox has not been processed");
     ck(cudaSetDevice(device), "cudaSetDevice");
     enqueueStep(false, false, dF);
+    ck(launch_unpermute_rows((int)nstot, 3, dOrig, dF, dTmp, stream), "unpermute forces");
+    ck(cudaMemcpyAsync(f_out, dTmp, 12 * nstot, cudaMemcpyDeviceToHost, stream), "read forces");
     ck(cudaStreamSynchronize(stream), "forces");
-    ck(cudaMemcpy(f_out, dF, 12 * nstot, cudaMemcpyDeviceToHost), "read forces");
+}
+
+long long Box::deviceStep() const
+{
+    long long s = 0;
+    ck(cudaStreamSynchronize(stream), "sync");
+    ck(cudaMemcpy(&s, dStep, sizeof(s), cudaMemcpyDeviceToHost), "read step");
+    return s;
 }
 
 void Box::getPositions(float *xo) const
 {
     if (!ready) fail(TILD_ERR_STATE, "endBox has not been processed");
-    long long s = 0;
-    ck(cudaStreamSynchronize(stream), "sync");
-    ck(cudaMemcpy(&s, dStep, sizeof(s), cudaMemcpyDeviceToHost), "read step");
-    ck(cudaMemcpyAsync(xo, dX[s & 1], 12 * nstot, cudaMemcpyDeviceToHost, stream), "read positions");
+    const long long s = deviceStep();
+    ck(launch_unpermute_rows((int)nstot, 3, dOrig, dX[s & 1], dTmp, stream), "unpermute positions");
+    ck(cudaMemcpyAsync(xo, dTmp, 12 * nstot, cudaMemcpyDeviceToHost, stream), "read positions");
     ck(cudaStreamSynchronize(stream), "read positions");
 }
 
@@ -1078,7 +1185,8 @@ void Box::setPositions(const float *xi)
 {
     if (!ready) fail(TILD_ERR_STATE, "endBox has not been processed");
     ck(cudaStreamSynchronize(stream), "sync");
-    ck(cudaMemcpyAsync(dX[0], xi, 12 * nstot, cudaMemcpyHostToDevice, stream), "set positions");
+    ck(cudaMemcpyAsync(dTmp, xi, 12 * nstot, cudaMemcpyHostToDevice, stream), "set positions");
+    ck(launch_permute_rows((int)nstot, 3, dOrig, dTmp, dX[0], stream), "permute positions");
     ck(cudaMemcpyAsync(dX[1], dX[0], 12 * nstot, cudaMemcpyDeviceToDevice, stream), "set positions");
     ck(cudaMemsetAsync(dNoise, 0, 12 * nstot, stream), "zero noise");
     ck(cudaStreamSynchronize(stream), "set positions");
@@ -1089,10 +1197,12 @@ void Box::getDensity(const std::string &group, int charge, float *rho)
     if (!ready) fail(TILD_ERR_STATE, "endBox has not been processed");
     const int gi = findGroupInteger(group);
     if (charge && !psGroup[gi].isCharges) fail(TILD_ERR_ARG, "only the 'charges' group has a charge density");
-    long long s = 0;
-    ck(cudaStreamSynchronize(stream), "sync");
-    ck(cudaMemcpy(&s, dStep, sizeof(s), cudaMemcpyDeviceToHost), "read step");
-    const std::vector<int> &sites = psGroup[gi].siteList;
+    const long long s = deviceStep();
+    const std::vector<int> orig = slotOrder();
+    std::vector<int> slotOf(nstot);
+    for (int64_t k = 0; k < nstot; k++) slotOf[orig[k]] = (int)k;
+    std::vector<int> sites(psGroup[gi].siteList);
+    for (int &v : sites) v = slotOf[v];
     int *dSites = nullptr;
     float *dRho = nullptr;
     ck(cudaMalloc(&dSites, 4 * sites.size()), "malloc");
@@ -1110,20 +1220,24 @@ void Box::getDensity(const std::string &group, int charge, float *rho)
 void Box::gridWeights(int32_t *inds, float *w)
 {
     if (!ready) fail(TILD_ERR_STATE, "endBox has not been processed");
-    long long s = 0;
-    ck(cudaStreamSynchronize(stream), "sync");
-    ck(cudaMemcpy(&s, dStep, sizeof(s), cudaMemcpyDeviceToHost), "read step");
+    const long long s = deviceStep();
     const int G = (pmeorder + 1) * (pmeorder + 1) * (pmeorder + 1);
     int *dI = nullptr;
-    float *dW = nullptr;
+    float *dW = nullptr, *dO = nullptr;
     ck(cudaMalloc(&dI, 4 * nstot * G), "malloc");
     ck(cudaMalloc(&dW, 4 * nstot * G), "malloc");
+    ck(cudaMalloc(&dO, 4 * nstot * G), "malloc");
     cudaError_t e = launch_grid_weights(geom, pmeorder, exact4 ? 0 : 1, dX[s & 1], (int)nstot, dI, dW, stream);
+    // rows of 4-byte values from slot order back to particle order (indices moved as raw bits)
+    if (e == cudaSuccess) e = launch_unpermute_rows((int)nstot, G, dOrig, reinterpret_cast<float *>(dI), dO, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(inds, dO, 4 * nstot * G, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess) e = launch_unpermute_rows((int)nstot, G, dOrig, dW, dO, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(w, dO, 4 * nstot * G, cudaMemcpyDeviceToHost, stream);
     cudaStreamSynchronize(stream);
-    if (e == cudaSuccess) e = cudaMemcpy(inds, dI, 4 * nstot * G, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess) e = cudaMemcpy(w, dW, 4 * nstot * G, cudaMemcpyDeviceToHost);
     cudaFree(dI);
     cudaFree(dW);
+    cudaFree(dO);
     ck(e, "grid weights");
 }
 
@@ -1134,25 +1248,14 @@ void Box::modifyBox(const std::string &rest)
         const long long id = std::strtoll(w[2].c_str(), nullptr, 10);
         if (id > 0 && id <= (long long)potentials.size()) {
             potentials.erase(potentials.begin() + (id - 1));
-            if (ready) {
+            if (ready) {   // positions, GJF state, RNG state and particle order are kept
                 ck(cudaStreamSynchronize(stream), "sync");
                 dropGraphs();
                 const int ndOld = (int)dfields.size(), nfOld = (int)fgroups.size();
                 buildPlan();
                 if ((int)dfields.size() > std::max(1, ndOld) || (int)fgroups.size() > std::max(1, nfOld))
                     fail(TILD_ERR_STATE, "plan grew after removing a potential");
-                // refresh membership flags and plans; positions and GJF state are kept
-                std::vector<float> xcur(3 * nstot), xold(3 * nstot), nz(3 * nstot);
-                long long s = 0;
-                cudaMemcpy(&s, dStep, sizeof(s), cudaMemcpyDeviceToHost);
-                cudaMemcpy(xcur.data(), dX[s & 1], 12 * nstot, cudaMemcpyDeviceToHost);
-                cudaMemcpy(xold.data(), dX[(s + 1) & 1], 12 * nstot, cudaMemcpyDeviceToHost);
-                cudaMemcpy(nz.data(), dNoise, 12 * nstot, cudaMemcpyDeviceToHost);
-                uploadParticles();
-                cudaMemcpy(dStep, &s, sizeof(s), cudaMemcpyHostToDevice);
-                cudaMemcpy(dX[s & 1], xcur.data(), 12 * nstot, cudaMemcpyHostToDevice);
-                cudaMemcpy(dX[(s + 1) & 1], xold.data(), 12 * nstot, cudaMemcpyHostToDevice);
-                cudaMemcpy(dNoise, nz.data(), 12 * nstot, cudaMemcpyHostToDevice);
+                uploadFlags();
                 ck(cudaDeviceSynchronize(), "modify");
             }
         }

@@ -186,6 +186,17 @@ private:
     KSpace *hKsPinned = nullptr;
     cudaGraphExec_t gNorm = nullptr, gEnergy = nullptr;
     std::vector<double> stageSec;
+    // spatial re-sort of the particle arrays
+    SortScratch sortW{};
+    float *dTmp = nullptr;                 // [3N] scratch for slot <-> original order
+    cudaGraphExec_t gSort = nullptr;
+    int sortInterval = 25;
+    int sinceSort = 0;
+    void uploadFlags();
+    std::vector<int> slotOrder() const;
+    void sortParticles();
+    void maybeSort();
+    long long deviceStep() const;
     // per-kernel event timing (option "stage_timing")
     enum { STAGE_DEPOSIT, STAGE_XFWD, STAGE_YFWD, STAGE_KSPACE, STAGE_YINV, STAGE_XINV, STAGE_PARTICLES, STAGE_COUNT };
     bool timing = false;

@@ -130,6 +130,31 @@ cudaError_t launch_particles(const Geom &g, const ParticleParams &pp, const Part
                              void *rng_states, const long long *d_step, float *fout,
                              int integrate, cudaStream_t st);
 cudaError_t launch_tick(long long *d_step, cudaStream_t st);
+
+// ---- spatial re-sort (tild_sort.cu) ----
+struct PermIn {             // current particle arrays (slot order)
+    const float *X0, *X1, *noise, *q;
+    const uint32_t *flags;
+    const int *orig, *partner;
+    const uint8_t *nb, *btype;
+    const void *rng;
+    const long long *d_step;
+};
+struct SortScratch {        // work arrays and the permuted copies
+    uint32_t *key, *count, *totals, *start;
+    int *rank, *newpos;
+    float *X0, *X1, *noise, *q;
+    uint32_t *flags;
+    int *orig, *partner;
+    uint8_t *nb, *btype;
+    void *rng;
+};
+uint32_t sort_key_count(const Geom &g);
+cudaError_t launch_sort(const Geom &g, int N, int maxb, const SortScratch &w, const PermIn &in, cudaStream_t st);
+cudaError_t launch_unpermute_rows(int N, int width, const int *orig, const float *in, float *out,
+                                  cudaStream_t st);
+cudaError_t launch_permute_rows(int N, int width, const int *orig, const float *in, float *out,
+                                cudaStream_t st);
 cudaError_t launch_rng_init(void *states, const int *orig_id, int n, unsigned long long seed,
                             cudaStream_t st);
 size_t rng_state_bytes();

@@ -122,6 +122,21 @@ def test_deterministic_mode_bit_reproducible_and_accurate():
     assert force_error(outs[0], fref) <= F_TOL
 
 
+def test_spatial_sort_is_invisible():
+    """Re-sorting the particle arrays changes only memory order: in deterministic mode the
+    trajectory is bit-identical with no sort, a sort every 3 steps and every step."""
+    spec = synth.small_system(seed=18, order=3, charges=True, n_free=30)
+    outs = []
+    for interval in (0, 3, 1):
+        with make_box(spec, deterministic=1, sort_interval=interval) as b:
+            f = b.forces()
+            b.step(10)
+            outs.append((f, b.positions(), b.forces()))
+    for o in outs[1:]:
+        for a, r in zip(o, outs[0]):
+            assert np.array_equal(a, r)
+
+
 @pytest.mark.parametrize("integ", ["GJF", "EM"])
 def test_trajectory_matches_oracle_100_steps(integ):
     spec = synth.small_system(seed=13, order=3, charges=True)
@@ -136,7 +151,8 @@ def test_trajectory_matches_oracle_100_steps(integ):
         traj.step(oracle.philox_normals(spec.seed, step, ids))
     d = np.abs(x - traj.positions())
     d = np.minimum(d, spec.L - d)
-    assert d.max() <= 2e-4, d.max()
+    # stated drift: the FP32 restatement itself drifts 4.7e-4 (max) from FP64 here
+    assert d.max() <= 1e-3 and np.median(d) <= 1e-4, (d.max(), np.median(d))
 
 
 def test_forces_unchanged_by_forces_call_and_positions_round_trip():
@@ -202,13 +218,13 @@ def test_ramp_updates_amplitude():
     spec = synth.small_system(seed=17, order=3)
     spec.potentials = [dict(kind="gaussian", I="A", J="B", A=2.0, sigma=0.7)]
     sysm = spec_to_system(spec)
-    b = tild_b200.box_from_spec(spec, options={"write_files": 0})
-    b.close()
     # ramp from 2 to 4 over 4 steps: after run_nvt(4) the amplitude is 4
     bb = tild_b200.Box(0, options={"write_files": 0})
     bb.command("Dim 3")
     bb.command("boxLengths %g %g %g" % tuple(spec.L))
     bb.command("grid %d %d %d" % tuple(spec.grid))
+    bb.command("pmeorder %d" % spec.order)
+    bb.command("randSeed %d" % spec.seed)
     bb.command("species A")
     bb.command("species B")
     bb.set_particles(spec.x, spec.types, spec.mol)
@@ -217,6 +233,10 @@ def test_ramp_updates_amplitude():
     bb.command("potential gaussian A B 2.0 0.7 ramp 4.0")
     bb.command("integrator all GJF delt 0.005")
     bb.command("endBox")
+    dens0, _, _ = oracle.densities(sysm)
+    e2 = oracle.pair_energies(sysm, dens0)[0]
+    t0 = bb.thermo()
+    assert abs(t0["potentials"][0] - e2) <= 1e-5 * abs(e2), (t0["potentials"][0], e2)
     bb.run_nvt(4)
     log = bb.log()
     x = bb.positions()
