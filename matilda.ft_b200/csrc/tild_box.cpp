@@ -27,6 +27,7 @@ namespace tild {
 
 void init_fft_attributes();
 void init_deposit_attributes();
+void init_particle_attributes();
 
 namespace {
 
@@ -602,6 +603,7 @@ void Box::finishInitialization()
     }
     init_fft_attributes();
     init_deposit_attributes();
+    init_particle_attributes();
     buildPlan();
     allocDevice();
     uploadParticles();
@@ -648,6 +650,7 @@ void Box::buildPlan()
     g.nxh = g.nx / 2 + 1;
     g.hp = (g.nxh + 3) & ~3;
     g.M = (long long)g.nx * g.ny * g.nz;
+    if (g.M >= (1ll << 31)) fail(TILD_ERR_UNSUPPORTED, "grids of 2^31 points or more");
     g.hstride = (long long)g.nz * g.ny * g.hp;
     for (int j = 0; j < 3; j++) {
         g.dxf[j] = (float)dx[j];
@@ -773,6 +776,25 @@ void Box::allocDevice()
     ck(cudaMallocHost(&hKsPinned, sizeof(KSpace)), "cudaMallocHost");
     // sort scratch and the permuted copies
     const uint32_t nk = sort_key_count(g);
+    sortKeys = nk;
+    {   // tile geometry: about one particle per thread, box sized for the tile plus drift
+        const double perCode = 64.0 * (double)N / (double)g.M;   // particles per 4^3-cell brick
+        int codes = 8;
+        while (codes < 64 && perCode * codes * 2.0 <= 192.0) codes *= 2;
+        const double e = perCode * codes;
+        int thr = (int)std::ceil((e + 2.0 * std::sqrt(e) + 8.0) / 32.0) * 32;
+        thr = std::max(64, std::min(512, thr));
+        int bits = 0;
+        while ((1 << bits) < codes) bits++;
+        const int cx = 4 << ((bits + 2) / 3), cy = 4 << ((bits + 1) / 3), cz = 4 << (bits / 3);
+        const int slack = pmeorder + 1 + 3;   // stencil width + drift between sorts
+        long long box = (long long)(((cx + slack) | 1) * (cy + slack) | 1) * (cz + slack);
+        box = std::min<long long>(box, 3072);
+        tiles.nkeys = (int)nk;
+        tiles.codes = codes;
+        tiles.threads = thr;
+        tiles.box = (int)box;
+    }
     sortW.key = dalloc<uint32_t>(N);
     sortW.rank = dalloc<int>(N);
     sortW.newpos = dalloc<int>(N);
@@ -880,6 +902,7 @@ void Box::sortParticles()
     cp(dBtype, sortW.btype, N * MAXBONDS);
     if (dRng) cp(dRng, sortW.rng, N * rng_state_bytes());
     sinceSort = 0;
+    sortedTiles = true;
 }
 
 void Box::maybeSort()
@@ -915,7 +938,7 @@ void Box::enqueueStep(bool energy, bool integrate, float *fout_dev)
             ck(launch_zero(dDepFix, sizeof(unsigned long long) * 2 * npair * g.M, st), "zero");
         else
             ck(launch_zero(dDep, sizeof(float2) * npair * g.M, st), "zero");
-        ck(launch_deposit(g, ppHost, dX[0], dX[1], dStep, dFlags, dQ, dDep, dDepFix, deterministic, st), "deposit");
+        ck(launch_deposit(g, ppHost, dX[0], dX[1], dStep, dFlags, dQ, dDep, dDepFix, deterministic, tileCfg(), st), "deposit");
         mark(STAGE_DEPOSIT);
         ck(launch_xfwd(g, lx, npair, nd, dDep, deterministic ? dDepFix : nullptr, dH, st), "fft x forward");
         mark(STAGE_XFWD);
@@ -932,7 +955,7 @@ void Box::enqueueStep(bool energy, bool integrate, float *fout_dev)
         }
     }
     ck(launch_particles(g, ppHost, dPp, dX[0], dX[1], dNoise, dFlags, dQ, dNb, dPartner, dBtype, dRec, dOrig, dRng,
-                        dStep, fout_dev, integrate ? 1 : 0, st),
+                        dStep, fout_dev, integrate ? 1 : 0, tileCfg(), st),
        "particles");
     mark(STAGE_PARTICLES);
     if (integrate) ck(launch_tick(dStep, st), "tick");
@@ -953,7 +976,7 @@ void Box::enqueueEnergyOnly()
             ck(launch_zero(dDepFix, sizeof(unsigned long long) * 2 * npair * g.M, st), "zero");
         else
             ck(launch_zero(dDep, sizeof(float2) * npair * g.M, st), "zero");
-        ck(launch_deposit(g, ppHost, dX[0], dX[1], dStep, dFlags, dQ, dDep, dDepFix, deterministic, st), "deposit");
+        ck(launch_deposit(g, ppHost, dX[0], dX[1], dStep, dFlags, dQ, dDep, dDepFix, deterministic, tileCfg(), st), "deposit");
         ck(launch_xfwd(g, lx, npair, nd, dDep, deterministic ? dDepFix : nullptr, dH, st), "fft x forward");
         ck(launch_ypass(g, ly, nd, 0, dH, st), "fft y forward");
         ck(launch_kspace_z(g, lz, ksHost, dKs, dH, dHg, dEpart, 1, 0, nullptr, st), "kspace energy");
@@ -1162,6 +1185,13 @@ void Box::forces(float *f_out)
     ck(launch_unpermute_rows((int)nstot, 3, dOrig, dF, dTmp, stream), "unpermute forces");
     ck(cudaMemcpyAsync(f_out, dTmp, 12 * nstot, cudaMemcpyDeviceToHost, stream), "read forces");
     ck(cudaStreamSynchronize(stream), "forces");
+}
+
+TileCfg Box::tileCfg() const
+{
+    TileCfg t = tiles;
+    t.start = sortedTiles ? sortW.start : nullptr;
+    return t;
 }
 
 long long Box::deviceStep() const

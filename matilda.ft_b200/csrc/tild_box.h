@@ -190,8 +190,12 @@ private:
     SortScratch sortW{};
     float *dTmp = nullptr;                 // [3N] scratch for slot <-> original order
     cudaGraphExec_t gSort = nullptr;
-    int sortInterval = 25;
+    int sortInterval = 10;
     int sinceSort = 0;
+    bool sortedTiles = false;       // sortW.start holds the tile ranges of the current order
+    uint32_t sortKeys = 0;
+    TileCfg tiles{};                // codes / threads / box chosen from the density
+    TileCfg tileCfg() const;
     void uploadFlags();
     std::vector<int> slotOrder() const;
     void sortParticles();

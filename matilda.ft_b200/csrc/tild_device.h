@@ -29,11 +29,25 @@ constexpr double kFixScale = 4294967296.0;  // deterministic deposit: 2^32 per u
 
 enum PotKind { POT_GAUSSIAN = 0, POT_ERF2 = 1, POT_ERFG = 2, POT_CHARGES = 3 };
 
+// Division by a runtime constant d through a multiply: exact for i * d < 2^32.
+struct FastDiv {
+    unsigned d, m;        // m = ceil(2^32 / d); d == 1 handled separately
+};
+inline FastDiv make_fastdiv(unsigned d)
+{
+    FastDiv f;
+    f.d = d;
+    f.m = d <= 1 ? 0u : (unsigned)((0x100000000ull + d - 1) / d);
+    return f;
+}
+
 struct FftLine {          // Stockham mixed-radix plan of one line length
     int n;
     int ns;
     int R[kMaxStages];
     int P[kMaxStages];
+    FastDiv dP[kMaxStages];   // division by P[s]
+    FastDiv dNB[kMaxStages];  // division by n / R[s]
     const float2 *tw;     // device twiddles W_n^t, t in [0, n)  (forward sign)
 };
 
@@ -103,17 +117,28 @@ struct ParticleParams {
     int rng_compat;
 };
 
-struct DevState;   // defined in tild_kernels.cu
+// Work split of the particle kernels over a sorted particle order: a CTA of `threads`
+// threads takes the slots of `codes` consecutive brick codes; boxes of up to `box`
+// grid points are staged in shared memory.  start == nullptr: fixed windows of slots.
+struct TileCfg {
+    const uint32_t *start;
+    int nkeys;
+    int codes;
+    int threads;
+    int box;
+};
 
 // -------------------------------------------------------------------------------------
-// Launchers (tild_kernels.cu).  All run on `st`; none synchronises.
+// Launchers (tild_grid.cu, tild_fft.cu, tild_particles.cu, tild_sort.cu).  All run on `st`;
+// none synchronises.
 void build_fft_line(int n, FftLine &pl, float2 *dev_tw_dst);
-void init_fft_attributes();   // opt every FFT kernel into large dynamic shared memory
+void init_fft_attributes();      // opt the FFT kernels into large dynamic shared memory
+void init_deposit_attributes();  // same for the staged deposit
 cudaError_t launch_zero(void *p, size_t bytes, cudaStream_t st);
 cudaError_t launch_deposit(const Geom &g, const ParticleParams &pp, const float *X0,
                            const float *X1, const long long *d_step, const uint32_t *pflags,
                            const float *q, float2 *dep, unsigned long long *dep_fixed,
-                           int deterministic, cudaStream_t st);
+                           int deterministic, const TileCfg &tc, cudaStream_t st);
 cudaError_t launch_xfwd(const Geom &g, const FftLine &lx, int npair, int nd, const float2 *dep,
                         const unsigned long long *dep_fixed, float2 *H, cudaStream_t st);
 cudaError_t launch_ypass(const Geom &g, const FftLine &ly, int nfields, int inverse, float2 *H,
@@ -128,7 +153,8 @@ cudaError_t launch_particles(const Geom &g, const ParticleParams &pp, const Part
                              const float *q, const uint8_t *nb, const int *partner,
                              const uint8_t *btype, const float4 *rec, const int *orig_id,
                              void *rng_states, const long long *d_step, float *fout,
-                             int integrate, cudaStream_t st);
+                             int integrate, const TileCfg &tc, cudaStream_t st);
+void init_particle_attributes();
 cudaError_t launch_tick(long long *d_step, cudaStream_t st);
 
 // ---- spatial re-sort (tild_sort.cu) ----

@@ -29,24 +29,38 @@ __device__ __forceinline__ float2 twid(const float2 *tw, int t)
     return w;
 }
 
+__device__ __forceinline__ FastDiv make_fastdiv_dev(unsigned d)
+{
+    FastDiv f;
+    f.d = d;
+    f.m = d <= 1 ? 0u : (unsigned)((0x100000000ull + d - 1) / d);
+    return f;
+}
+
+__device__ __forceinline__ unsigned fdiv(unsigned i, const FastDiv &f)
+{
+    return f.d == 1 ? i : __umulhi(i, f.m);
+}
+
 template <bool INV>
 __device__ float2 *fft_lines(float2 *a, float2 *b, int L, int lp, int ls, const FftLine &pl,
-                             const float2 *tw, bool line_fast)
+                             const float2 *tw, bool line_fast, const FastDiv &dL)
 {
     const int n = pl.n;
     for (int s = 0; s < pl.ns; ++s) {
         const int R = pl.R[s], p = pl.P[s], nb = n / R, stride = n / (p * R);
         const int total = L * nb;
+        const FastDiv dp = pl.dP[s], dnb = pl.dNB[s];
         for (int w = threadIdx.x; w < total; w += blockDim.x) {
             int l, i;
             if (line_fast) {
-                l = w % L;
-                i = w / L;
+                i = (int)fdiv((unsigned)w, dL);
+                l = w - i * L;
             } else {
-                i = w % nb;
-                l = w / nb;
+                l = (int)fdiv((unsigned)w, dnb);
+                i = w - l * nb;
             }
-            const int k = i % p;
+            const int k = i - p * (int)fdiv((unsigned)i, dp);
             const float2 *src = a + l * lp;
             float2 *dst = b + l * lp;
             const int j = (i - k) * R + k;
@@ -147,6 +161,36 @@ static int lines_per_block(int n)
 }
 
 // -------------------------------------------------------------------------------------
+// Asynchronous tile loads: 16-byte cp.async copies (two complex values each), all in
+// flight at once; bytes past the valid part of a row are zero-filled without a read.
+// -------------------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc, int src_bytes)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gsrc), "r"(src_bytes) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// rows x cols complex tile: smem dst[r*dpitch + c] <- src[r*spitch + c] for c < valid;
+// cols and dpitch even; src and spitch 16-byte aligned (even element offsets).
+__device__ __forceinline__ void tile_load_async(float2 *dst, int dpitch, const float2 *src, long long spitch, int rows,
+                                                int cols, int valid)
+{
+    const int cpr = cols >> 1;   // 16-byte chunks per row
+    for (int e = threadIdx.x; e < rows * cpr; e += blockDim.x) {
+        const int r = e / cpr, c2 = (e - r * cpr) << 1;
+        const int nv = valid - c2;
+        const int bytes = nv >= 2 ? 16 : (nv == 1 ? 8 : 0);
+        const float2 *s = bytes ? src + r * spitch + c2 : src;
+        cp_async16(dst + r * dpitch + c2, s, bytes);
+    }
+}
+
+// -------------------------------------------------------------------------------------
 // x-axis forward pass.  Fields 2t and 2t+1 are packed as z = a + i b; after the complex
 // FFT A(k) = (Z(k) + conj Z(n-k))/2 and B(k) = (Z(k) - conj Z(n-k))/(2i), k in [0, n/2].
 // -------------------------------------------------------------------------------------
@@ -155,31 +199,38 @@ __global__ void __launch_bounds__(256) k_xfwd(Geom g, FftLine lx, int nd, const 
                                               const unsigned long long *__restrict__ depfix,
                                               double fscale, float2 *__restrict__ H, int L)
 {
-    extern __shared__ float2 sm[];
+    extern __shared__ __align__(16) float2 sm[];
     const int n = g.nx;
     float2 *A = sm, *B = sm + L * n, *tw = sm + 2 * L * n;
     const int pair = blockIdx.y;
     const long long nlines = (long long)g.ny * g.nz;
     const long long line0 = (long long)blockIdx.x * L;
     for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = lx.tw[t];
-    for (int e = threadIdx.x; e < L * n; e += blockDim.x) {
-        const int l = e / n;
-        const long long gl = line0 + l;
-        float2 v = make_float2(0.f, 0.f);
-        if (gl < nlines) {
-            const long long idx = gl * n + (e - l * n);
-            if (FIXED) {
-                v.x = (float)((double)(long long)depfix[(2 * pair) * g.M + idx] * fscale);
-                if (2 * pair + 1 < nd)
-                    v.y = (float)((double)(long long)depfix[(2 * pair + 1) * g.M + idx] * fscale);
-            } else {
-                v = dep[pair * g.M + idx];
+    const int lv = (int)min((long long)L, nlines - line0);   // lines present in this block
+    if (!FIXED && (n % 2) == 0) {
+        tile_load_async(A, n, dep + pair * g.M + line0 * n, n, lv, n, n);
+        for (int e = lv * n + threadIdx.x; e < L * n; e += blockDim.x) A[e] = make_float2(0.f, 0.f);
+        cp_async_wait_all();
+    } else {
+        for (int e = threadIdx.x; e < L * n; e += blockDim.x) {
+            const int l = e / n;
+            const long long gl = line0 + l;
+            float2 v = make_float2(0.f, 0.f);
+            if (gl < nlines) {
+                const long long idx = gl * n + (e - l * n);
+                if (FIXED) {
+                    v.x = (float)((double)(long long)depfix[(2 * pair) * g.M + idx] * fscale);
+                    if (2 * pair + 1 < nd)
+                        v.y = (float)((double)(long long)depfix[(2 * pair + 1) * g.M + idx] * fscale);
+                } else {
+                    v = dep[pair * g.M + idx];
+                }
             }
+            A[e] = v;
         }
-        A[e] = v;
     }
     __syncthreads();
-    const float2 *R = fft_lines<false>(A, B, L, n, 1, lx, tw, false);
+    const float2 *R = fft_lines<false>(A, B, L, n, 1, lx, tw, false, make_fastdiv_dev(L));
     const int nxh = g.nxh;
     for (int e = threadIdx.x; e < L * nxh; e += blockDim.x) {
         const int l = e / nxh, k = e - l * nxh;
@@ -197,18 +248,16 @@ __global__ void __launch_bounds__(256) k_xfwd(Geom g, FftLine lx, int nd, const 
 template <bool INV>
 __global__ void __launch_bounds__(256) k_ypass(Geom g, FftLine ly, float2 *__restrict__ H, int TX)
 {
-    extern __shared__ float2 sm[];
+    extern __shared__ __align__(16) float2 sm[];
     const int ny = g.ny;
     float2 *A = sm, *B = sm + ny * TX, *tw = sm + 2 * ny * TX;
     const int kx0 = blockIdx.x * TX;
     const long long base = (long long)blockIdx.z * g.hstride + (long long)blockIdx.y * ny * g.hp + kx0;
     for (int t = threadIdx.x; t < ny; t += blockDim.x) tw[t] = ly.tw[t];
-    for (int e = threadIdx.x; e < ny * TX; e += blockDim.x) {
-        const int y = e / TX, c = e - y * TX;
-        A[e] = (kx0 + c < g.nxh) ? H[base + (long long)y * g.hp + c] : make_float2(0.f, 0.f);
-    }
+    tile_load_async(A, TX, H + base, g.hp, ny, TX, g.nxh - kx0);
+    cp_async_wait_all();
     __syncthreads();
-    const float2 *R = fft_lines<INV>(A, B, TX, 1, TX, ly, tw, true);
+    const float2 *R = fft_lines<INV>(A, B, TX, 1, TX, ly, tw, true, make_fastdiv_dev(TX));
     for (int e = threadIdx.x; e < ny * TX; e += blockDim.x) {
         const int y = e / TX, c = e - y * TX;
         if (kx0 + c < g.nxh) H[base + (long long)y * g.hp + c] = R[e];
@@ -244,7 +293,7 @@ __global__ void __launch_bounds__(256) k_kspace_z(Geom g, FftLine lz, const KSpa
                                                   float2 *__restrict__ Hg, double *__restrict__ epart,
                                                   int energy, int forces, int TX)
 {
-    extern __shared__ float2 sm[];
+    extern __shared__ __align__(16) float2 sm[];
     const KSpace &ks = *ksp;
     const int nz = g.nz, nd = ks.nd;
     const int ndb = nd < 2 ? 2 : nd;
@@ -252,13 +301,12 @@ __global__ void __launch_bounds__(256) k_kspace_z(Geom g, FftLine lz, const KSpa
     double *red = reinterpret_cast<double *>(tw + nz);
     const int kx0 = blockIdx.x * TX, y = blockIdx.y;
     for (int t = threadIdx.x; t < nz; t += blockDim.x) tw[t] = lz.tw[t];
-    for (int e = threadIdx.x; e < nz * nd * TX; e += blockDim.x) {
-        const int z = e / (nd * TX), r = e - z * nd * TX, d = r / TX, c = r - d * TX;
-        Rho[e] = (kx0 + c < g.nxh) ? H[d * g.hstride + ((long long)z * g.ny + y) * g.hp + kx0 + c]
-                                   : make_float2(0.f, 0.f);
-    }
+    for (int d = 0; d < nd; d++)
+        tile_load_async(Rho + d * TX, nd * TX, H + d * g.hstride + (long long)y * g.hp + kx0, (long long)g.ny * g.hp,
+                        nz, TX, g.nxh - kx0);
+    cp_async_wait_all();
     __syncthreads();
-    float2 *R = fft_lines<false>(Rho, S, nd * TX, 1, nd * TX, lz, tw, true);
+    float2 *R = fft_lines<false>(Rho, S, nd * TX, 1, nd * TX, lz, tw, true, make_fastdiv_dev(nd * TX));
     float2 *Wk = (R == Rho) ? S : Rho;  // free buffer: two halves of nz*TX for the outputs
     const int ky = signed_index(y, g.ny);
     const double kyv = ks.twopi_over_L[1] * ky;
@@ -318,29 +366,37 @@ __global__ void __launch_bounds__(256) k_kspace_z(Geom g, FftLine lz, const KSpa
             Phi[e] = make_float2((float)px, (float)py);
         }
         __syncthreads();
-        for (int d = 0; d < 3; d++) {
-            float2 *W1 = Wk, *W2 = Wk + nz * TX;
+        // x and y are fixed along a z line, so IFFT_z(-i k_x phi) = -i k_x IFFT_z(phi) and the
+        // same for y: one transform serves both; -i k_z phi needs its own.
+        float2 *W1 = Wk, *W2 = Wk + nz * TX;
+        for (int pass = 0; pass < 2; pass++) {
             for (int e = threadIdx.x; e < nz * TX; e += blockDim.x) {
-                const int z = e / TX, c = e - z * TX, kx = kx0 + c;
-                float kd = 0.f;
-                if (d == 0) {
-                    if (!(g.nx % 2 == 0 && kx == g.nx / 2))
-                        kd = (float)(ks.twopi_over_L[0] * signed_index(kx, g.nx));
-                } else if (d == 1) {
-                    if (!nyq_y) kd = (float)kyv;
-                } else {
-                    if (!(g.nz % 2 == 0 && z == g.nz / 2))
-                        kd = (float)(ks.twopi_over_L[2] * signed_index(z, g.nz));
-                }
                 const float2 ph = Phi[e];
-                W1[e] = make_float2(kd * ph.y, -kd * ph.x);  // -i k_d phi
+                if (pass == 0) {
+                    W1[e] = ph;
+                } else {
+                    const int z = e / TX;
+                    const float kz = (g.nz % 2 == 0 && z == g.nz / 2)
+                                         ? 0.f : (float)(ks.twopi_over_L[2] * signed_index(z, g.nz));
+                    W1[e] = make_float2(kz * ph.y, -kz * ph.x);   // -i k_z phi
+                }
             }
             __syncthreads();
-            const float2 *O = fft_lines<true>(W1, W2, TX, 1, TX, lz, tw, true);
-            const long long fo = (long long)(3 * f + d) * g.hstride;
+            const float2 *O = fft_lines<true>(W1, W2, TX, 1, TX, lz, tw, true, make_fastdiv_dev(TX));
             for (int e = threadIdx.x; e < nz * TX; e += blockDim.x) {
-                const int z = e / TX, c = e - z * TX;
-                if (kx0 + c < g.nxh) Hg[fo + ((long long)z * g.ny + y) * g.hp + kx0 + c] = O[e];
+                const int z = e / TX, c = e - z * TX, kx = kx0 + c;
+                if (kx >= g.nxh) continue;
+                const long long o = ((long long)z * g.ny + y) * g.hp + kx;
+                const float2 v = O[e];
+                if (pass == 0) {
+                    const float kxv = (g.nx % 2 == 0 && kx == g.nx / 2)
+                                          ? 0.f : (float)(ks.twopi_over_L[0] * signed_index(kx, g.nx));
+                    const float kyf = nyq_y ? 0.f : (float)kyv;
+                    Hg[(long long)(3 * f) * g.hstride + o] = make_float2(kxv * v.y, -kxv * v.x);
+                    Hg[(long long)(3 * f + 1) * g.hstride + o] = make_float2(kyf * v.y, -kyf * v.x);
+                } else {
+                    Hg[(long long)(3 * f + 2) * g.hstride + o] = v;
+                }
             }
             __syncthreads();
         }
@@ -353,25 +409,30 @@ __global__ void __launch_bounds__(256) k_kspace_z(Geom g, FftLine lz, const KSpa
 __global__ void __launch_bounds__(256) k_xinv(Geom g, FftLine lx, int nfg, const float2 *__restrict__ Hg,
                                               float4 *__restrict__ rec, int L)
 {
-    extern __shared__ float2 sm[];
-    const int n = g.nx, nf = 3 * nfg, nxh = g.nxh;
-    float2 *A = sm, *B = sm + L * n, *tw = sm + 2 * L * n;
-    float *Out = reinterpret_cast<float *>(tw + n);
+    extern __shared__ __align__(16) float2 sm[];
+    const int n = g.nx, nf = 3 * nfg, nxh = g.nxh, hp = g.hp;
+    float2 *A = sm, *B = sm + L * n, *tw = sm + 2 * L * n, *St = tw + n + (n & 1);
+    float *Out = reinterpret_cast<float *>(St + 2 * L * hp);
     const long long nlines = (long long)g.ny * g.nz;
     const long long line0 = (long long)blockIdx.x * L;
+    const int lv = (int)min((long long)L, nlines - line0);
+    const FastDiv dL = make_fastdiv_dev(L), dn = make_fastdiv_dev(n);
     for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = lx.tw[t];
     for (int pr = 0; pr < (nf + 1) / 2; pr++) {
         const int f1 = 2 * pr, f2 = 2 * pr + 1;
+        // consecutive lines are consecutive rows of pitch hp: stage both fields' rows
+        tile_load_async(St, hp, Hg + f1 * g.hstride + line0 * hp, hp, lv, hp, nxh);
+        if (f2 < nf) tile_load_async(St + L * hp, hp, Hg + f2 * g.hstride + line0 * hp, hp, lv, hp, nxh);
+        cp_async_wait_all();
+        __syncthreads();
         for (int e = threadIdx.x; e < L * n; e += blockDim.x) {
-            const int l = e / n, x = e - l * n;
-            const long long gl = line0 + l;
+            const int l = (int)fdiv((unsigned)e, dn), x = e - l * n;
             float2 v = make_float2(0.f, 0.f);
-            if (gl < nlines) {
+            if (l < lv) {
                 const bool direct = x < nxh;
                 const int kk = direct ? x : n - x;
-                const long long o = gl * g.hp + kk;
-                float2 g1 = Hg[f1 * g.hstride + o];
-                float2 g2 = (f2 < nf) ? Hg[f2 * g.hstride + o] : make_float2(0.f, 0.f);
+                float2 g1 = St[l * hp + kk];
+                float2 g2 = (f2 < nf) ? St[L * hp + l * hp + kk] : make_float2(0.f, 0.f);
                 if (kk == 0 || (n % 2 == 0 && kk == n / 2)) {
                     g1.y = 0.f;
                     g2.y = 0.f;
@@ -385,7 +446,7 @@ __global__ void __launch_bounds__(256) k_xinv(Geom g, FftLine lx, int nfg, const
             A[e] = v;
         }
         __syncthreads();
-        const float2 *R = fft_lines<true>(A, B, L, n, 1, lx, tw, false);
+        const float2 *R = fft_lines<true>(A, B, L, n, 1, lx, tw, false, dL);
         for (int e = threadIdx.x; e < L * n; e += blockDim.x) {
             Out[f1 * L * n + e] = R[e].x;
             if (f2 < nf) Out[f2 * L * n + e] = R[e].y;
@@ -393,13 +454,9 @@ __global__ void __launch_bounds__(256) k_xinv(Geom g, FftLine lx, int nfg, const
         __syncthreads();
     }
     for (int f = 0; f < nfg; f++) {
-        for (int e = threadIdx.x; e < L * n; e += blockDim.x) {
-            const int l = e / n;
-            const long long gl = line0 + l;
-            if (gl >= nlines) continue;
-            rec[f * g.M + gl * n + (e - l * n)] =
-                make_float4(Out[(3 * f) * L * n + e], Out[(3 * f + 1) * L * n + e], Out[(3 * f + 2) * L * n + e], 0.f);
-        }
+        float4 *rf = rec + f * g.M + line0 * n;
+        for (int e = threadIdx.x; e < lv * n; e += blockDim.x)
+            rf[e] = make_float4(Out[(3 * f) * L * n + e], Out[(3 * f + 1) * L * n + e], Out[(3 * f + 2) * L * n + e], 0.f);
     }
 }
 
@@ -423,6 +480,8 @@ void build_fft_line(int n, FftLine &pl, float2 *dev_tw_dst)
     auto push = [&](int r) {
         pl.R[pl.ns] = r;
         pl.P[pl.ns] = p;
+        pl.dP[pl.ns] = make_fastdiv((unsigned)p);
+        pl.dNB[pl.ns] = make_fastdiv((unsigned)(n / r));
         pl.ns++;
         p *= r;
         m /= r;
@@ -481,9 +540,11 @@ cudaError_t launch_kspace_z(const Geom &g, const FftLine &lz, const KSpace &ks, 
 
 cudaError_t launch_xinv(const Geom &g, const FftLine &lx, int nfg, const float2 *Hg, float4 *rec, cudaStream_t st)
 {
-    const int L = lines_per_block(g.nx);
+    int L = 768 / g.nx;
+    L = L < 1 ? 1 : (L > 8 ? 8 : L);
     const long long nlines = (long long)g.ny * g.nz;
-    const size_t smx = (size_t)(2 * L * g.nx + g.nx) * sizeof(float2) + (size_t)3 * nfg * L * g.nx * sizeof(float);
+    const size_t smx = (size_t)(2 * L * g.nx + g.nx + (g.nx & 1) + 2 * L * g.hp) * sizeof(float2) +
+                       (size_t)3 * nfg * L * g.nx * sizeof(float);
     k_xinv<<<(unsigned)((nlines + L - 1) / L), 256, smx, st>>>(g, lx, nfg, Hg, rec, L);
     return cudaGetLastError();
 }

@@ -1,6 +1,7 @@
 // tild_grid.cu -- density deposit and reference-exact stencil tables (sm_100a).
 #include "tild_stencil.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -80,50 +81,63 @@ constexpr int kDepPB = 512;
 constexpr int kDepSmemFast = 64 * 1024;
 constexpr int kDepSmemFixed = 128 * 1024;
 
-__device__ __forceinline__ int unwrap_delta(int d, int n)
+// Coefficient of field f for a particle: membership bit, charge channel -> q.
+__device__ __forceinline__ float field_coef(uint32_t dm, unsigned dq, int f, float qp)
 {
-    int t = d % n;
-    if (t < 0) t += n;
-    if (t >= (n + 1) / 2) t -= n;
-    return t;
+    return ((dm >> f) & 1u) ? (((dq >> f) & 1u) ? qp : 1.f) : 0.f;
 }
 
-template <int P>
-__device__ __forceinline__ int stencil_origin(float x, float d)
+template <bool FIXED>
+__device__ __forceinline__ void smem_add(float *tf, unsigned long long *tu, int i, float v)
 {
-    int g;
-    if (P % 2 == 0) g = (int)__fdiv_rn(__fmaf_rn(0.5f, d, x), d);
-    else g = (int)__fdiv_rn(x, d);
-    return g - P / 2;
+    if (FIXED) atomicAdd(tu + i, (unsigned long long)__double2ll_rn((double)v * kFixScale));
+    else atomicAdd(tf + i, v);
 }
 
-template <int P, bool FIXED>
-__global__ void __launch_bounds__(256) k_deposit_tiled(Geom g, int N, int quirk4, int nd, unsigned dq,
+template <bool FIXED>
+__device__ __forceinline__ void global_add(float2 *dep, unsigned long long *depfix, long long M, int f, long long m,
+                                           float v)
+{
+    if (FIXED) atomicAdd(depfix + f * M + m, (unsigned long long)__double2ll_rn((double)v * kFixScale));
+    else atomicAdd(FIELD_PTR(dep, f, M) + 2 * m, v);
+}
+
+// Deposit of one tile of sorted particles (or a window of slots).  The box of grid points
+// is accumulated in shared memory by warp-cooperative atomics: a warp takes one particle
+// at a time and its lanes cover the particle's (P+1)^3 stencil points, so the addresses
+// of one atomic instruction form a compact block.  Each touched point is flushed once.
+// NF: number of density fields when 1 or 2 (unrolled), 0 = any.
+template <int P, int NF, bool FIXED>
+__global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4, int nd, unsigned dq,
                                                        const float *__restrict__ X0, const float *__restrict__ X1,
                                                        const long long *__restrict__ d_step,
                                                        const uint32_t *__restrict__ pflags,
                                                        const float *__restrict__ q, float2 *__restrict__ dep,
-                                                       unsigned long long *__restrict__ depfix, int cap_bytes)
+                                                       unsigned long long *__restrict__ depfix, int cap_bytes,
+                                                       TileCfg tc)
 {
+    constexpr int P1 = P + 1, G = P1 * P1 * P1, NPASS = (G + 31) / 32;
+    constexpr int WREC = 3 * P1 + 4;   // per-particle record of the warp table: weights, offset, dm, q
     extern __shared__ __align__(16) unsigned char smraw[];
-    __shared__ int s_ref[3], s_min[3], s_max[3];
+    __shared__ TileShared ts;
     const float *__restrict__ X = (*d_step & 1) ? X1 : X0;
-    const int b0 = blockIdx.x * kDepPB;
-    const int nloc = min(kDepPB, N - b0);
+    const float inv[3] = {1.f / g.dxf[0], 1.f / g.dxf[1], 1.f / g.dxf[2]};
+    int b0, b1;
+    tile_range(tc, N, kDepPB, b0, b1);
+    if (b1 <= b0) return;
     const int nn[3] = {g.nx, g.ny, g.nz};
     if (threadIdx.x < 3) {
-        s_ref[threadIdx.x] = stencil_origin<P>(X[3 * b0 + threadIdx.x], g.dxf[threadIdx.x]);
-        s_min[threadIdx.x] = 0x7fffffff;
-        s_max[threadIdx.x] = -0x7fffffff;
+        ts.ref[threadIdx.x] = stencil_origin<P>(X[3 * b0 + threadIdx.x], inv[threadIdx.x]);
+        ts.lo[threadIdx.x] = 0x7fffffff;
+        ts.hi[threadIdx.x] = -0x7fffffff;
     }
     __syncthreads();
     int lo[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, hi[3] = {-0x7fffffff, -0x7fffffff, -0x7fffffff};
-    for (int k = threadIdx.x; k < nloc; k += blockDim.x) {
-        const int p = b0 + k;
+    for (int p = b0 + threadIdx.x; p < b1; p += blockDim.x) {
         if (!(pflags[p] & 0xffu)) continue;
 #pragma unroll
         for (int j = 0; j < 3; j++) {
-            const int dd = unwrap_delta(stencil_origin<P>(X[3 * p + j], g.dxf[j]) - s_ref[j], nn[j]);
+            const int dd = unwrap_delta(stencil_origin<P>(X[3 * p + j], inv[j]) - ts.ref[j], nn[j]);
             lo[j] = min(lo[j], dd);
             hi[j] = max(hi[j], dd);
         }
@@ -135,92 +149,121 @@ __global__ void __launch_bounds__(256) k_deposit_tiled(Geom g, int N, int quirk4
             hi[j] = max(hi[j], __shfl_xor_sync(0xffffffffu, hi[j], o));
         }
         if ((threadIdx.x & 31) == 0) {
-            atomicMin(&s_min[j], lo[j]);
-            atomicMax(&s_max[j], hi[j]);
+            atomicMin(&ts.lo[j], lo[j]);
+            atomicMax(&ts.hi[j], hi[j]);
         }
     }
     __syncthreads();
-    if (s_max[0] < s_min[0]) return;   // no depositing particle in this CTA
-    const int E0 = s_max[0] - s_min[0] + P + 1, E1 = s_max[1] - s_min[1] + P + 1, E2 = s_max[2] - s_min[2] + P + 1;
-    const long long V = (long long)E0 * E1 * E2;
+    if (ts.hi[0] < ts.lo[0]) return;   // no depositing particle in this CTA
+    const int E[3] = {ts.hi[0] - ts.lo[0] + P1, ts.hi[1] - ts.lo[1] + P1, ts.hi[2] - ts.lo[2] + P1};
+    const int nfields = NF ? NF : nd;
     const size_t esz = FIXED ? sizeof(unsigned long long) : sizeof(float);
-    const bool staged = V * nd * (long long)esz <= cap_bytes;
+    const long long Vl = (long long)E[0] * E[1] * E[2];
+    const bool staged = E[0] <= kMaxBoxEdge && E[1] <= kMaxBoxEdge && E[2] <= kMaxBoxEdge &&
+                        Vl * nfields * (long long)esz <= cap_bytes;
+    const int V = staged ? (int)Vl : 0, E0 = E[0], E01 = E[0] * E[1];
     float *tf = reinterpret_cast<float *>(smraw);
     unsigned long long *tu = reinterpret_cast<unsigned long long *>(smraw);
     if (staged) {
-        for (long long v = threadIdx.x; v < V * nd; v += blockDim.x) {
+        tile_tables(ts, g.nx, g.ny, g.nz, E);
+        for (int v = threadIdx.x; v < V * nfields; v += blockDim.x) {
             if (FIXED) tu[v] = 0ull;
             else tf[v] = 0.f;
         }
     }
     __syncthreads();
-    const long long plane = (long long)g.nx * g.ny;
-    for (int k = threadIdx.x; k < nloc; k += blockDim.x) {
-        const int p = b0 + k;
-        const uint32_t dm = pflags[p] & 0xffu;
-        if (!dm) continue;
-        float Wx[P + 1], Wy[P + 1], Wz[P + 1];
-        const int gx = stencil_axis<P>(X[3 * p + 0], g.dxf[0], quirk4, Wx);
-        const int gy = stencil_axis<P>(X[3 * p + 1], g.dxf[1], quirk4, Wy);
-        const int gz = stencil_axis<P>(X[3 * p + 2], g.dxf[2], quirk4, Wz);
-        const float qp = q ? q[p] : 0.f;
-        float c[kMaxFields];
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    if (staged) {
+        // this lane's stencil points: s = lane + 32*pass -> (a, b, e), x fastest
+        int sa[NPASS], sb[NPASS], se[NPASS];
 #pragma unroll
-        for (int i = 0; i < kMaxFields; i++)
-            c[i] = (i < nd && ((dm >> i) & 1u)) ? (((dq >> i) & 1u) ? qp : 1.f) : 0.f;
-        if (staged) {
-            const int lx = unwrap_delta(gx - s_ref[0], g.nx) - s_min[0];
-            const int ly = unwrap_delta(gy - s_ref[1], g.ny) - s_min[1];
-            const int lz = unwrap_delta(gz - s_ref[2], g.nz) - s_min[2];
-#pragma unroll 1
-            for (int e = 0; e <= P; e++) {
-                const float wz = sel<P>(Wz, e);
+        for (int k = 0; k < NPASS; k++) {
+            const int s = lane + 32 * k;
+            sa[k] = s % P1;
+            sb[k] = (s / P1) % P1;
+            se[k] = s / (P1 * P1);
+        }
+        // per-warp table of the batch's particles (weights, box offset, membership, charge)
+        float *wt = reinterpret_cast<float *>(smraw + (size_t)cap_bytes) + (threadIdx.x >> 5) * 32 * WREC;
+        for (int base = b0 + (threadIdx.x & ~31); base < b1; base += blockDim.x) {
+            const int p = base + lane;
+            uint32_t dm = 0u;
+            if (p < b1) dm = pflags[p] & 0xffu;
+            float *mine = wt + lane * WREC;
+            if (dm) {
+                float Wx[P1], Wy[P1], Wz[P1];
+                const int gx = stencil_fast<P>(X[3 * p + 0], inv[0], quirk4, Wx);
+                const int gy = stencil_fast<P>(X[3 * p + 1], inv[1], quirk4, Wy);
+                const int gz = stencil_fast<P>(X[3 * p + 2], inv[2], quirk4, Wz);
 #pragma unroll
-                for (int b = 0; b <= P; b++) {
-                    const float wyz = Wy[b] * wz;
-                    const long long row = (long long)(lz + e) * E1 * E0 + (long long)(ly + b) * E0 + lx;
+                for (int i = 0; i < P1; i++) {
+                    mine[i] = Wx[i];
+                    mine[P1 + i] = Wy[i];
+                    mine[2 * P1 + i] = Wz[i];
+                }
+                mine[3 * P1] = __int_as_float((unwrap_delta(gz - ts.ref[2], g.nz) - ts.lo[2]) * E01 +
+                                              (unwrap_delta(gy - ts.ref[1], g.ny) - ts.lo[1]) * E0 +
+                                              (unwrap_delta(gx - ts.ref[0], g.nx) - ts.lo[0]));
+                mine[3 * P1 + 1] = __uint_as_float(dm);
+                mine[3 * P1 + 2] = q ? q[p] : 0.f;
+            }
+            unsigned rem = __ballot_sync(full, dm != 0u);
+            __syncwarp();
+            while (rem) {
+                const int j = __ffs(rem) - 1;
+                rem &= rem - 1;
+                const float *pj = wt + j * WREC;
+                const int offj = __float_as_int(pj[3 * P1]);
+                const uint32_t dmj = __float_as_uint(pj[3 * P1 + 1]);
+                const float qj = pj[3 * P1 + 2];
+                float cf[NF ? NF : kMaxFields];
 #pragma unroll
-                    for (int a = 0; a <= P; a++) {
-                        const float w = Wx[a] * wyz;
-                        for (int f = 0; f < nd; f++) {
-                            const float v = c[f] * w;
-                            if (v == 0.f) continue;
-                            if (FIXED)
-                                atomicAdd(tu + f * V + row + a,
-                                          (unsigned long long)__double2ll_rn((double)v * kFixScale));
-                            else
-                                atomicAdd(tf + f * V + row + a, v);
-                        }
-                    }
+                for (int f = 0; f < (NF ? NF : kMaxFields); f++) cf[f] = f < nfields ? field_coef(dmj, dq, f, qj) : 0.f;
+#pragma unroll
+                for (int k = 0; k < NPASS; k++) {
+                    if (lane + 32 * k >= G) break;
+                    // Wx * (Wy * Wz): the association of the unstaged path, so that the
+                    // deterministic mode's fixed-point values do not depend on staging
+                    const float w = pj[sa[k]] * (pj[P1 + sb[k]] * pj[2 * P1 + se[k]]);
+                    const int idx = offj + se[k] * E01 + sb[k] * E0 + sa[k];
+#pragma unroll
+                    for (int f = 0; f < (NF ? NF : kMaxFields); f++)
+                        if (cf[f] != 0.f) smem_add<FIXED>(tf, tu, f * V + idx, cf[f] * w);
                 }
             }
-        } else {
-            int ix[P + 1], iy[P + 1], iz[P + 1];
+            __syncwarp();
+        }
+    } else {
+        for (int p = b0 + threadIdx.x; p < b1; p += blockDim.x) {
+            const uint32_t dm = pflags[p] & 0xffu;
+            if (!dm) continue;
+            float Wx[P1], Wy[P1], Wz[P1];
+            const int gx = stencil_fast<P>(X[3 * p + 0], inv[0], quirk4, Wx);
+            const int gy = stencil_fast<P>(X[3 * p + 1], inv[1], quirk4, Wy);
+            const int gz = stencil_fast<P>(X[3 * p + 2], inv[2], quirk4, Wz);
+            const float qp = q ? q[p] : 0.f;
+            int ix[P1], iy[P1], iz[P1];
 #pragma unroll
-            for (int i = 0; i <= P; i++) {
+            for (int i = 0; i < P1; i++) {
                 ix[i] = wrapi(gx + i, g.nx);
                 iy[i] = wrapi(gy + i, g.ny);
                 iz[i] = wrapi(gz + i, g.nz);
             }
 #pragma unroll 1
-            for (int e = 0; e <= P; e++) {
+            for (int e = 0; e < P1; e++) {
                 const float wz = sel<P>(Wz, e);
-                const long long mz = plane * sel<P>(iz, e);
+                const long long mz = (long long)g.nx * g.ny * sel<P>(iz, e);
 #pragma unroll
-                for (int b = 0; b <= P; b++) {
+                for (int b = 0; b < P1; b++) {
                     const float wyz = Wy[b] * wz;
                     const long long my = mz + (long long)g.nx * iy[b];
 #pragma unroll
-                    for (int a = 0; a <= P; a++) {
+                    for (int a = 0; a < P1; a++) {
                         const float w = Wx[a] * wyz;
                         for (int f = 0; f < nd; f++) {
-                            const float v = c[f] * w;
-                            if (v == 0.f) continue;
-                            if (FIXED)
-                                atomicAdd(depfix + f * g.M + my + ix[a],
-                                          (unsigned long long)__double2ll_rn((double)v * kFixScale));
-                            else
-                                atomicAdd(FIELD_PTR(dep, f, g.M) + 2 * (my + ix[a]), v);
+                            const float v = field_coef(dm, dq, f, qp) * w;
+                            if (v != 0.f) global_add<FIXED>(dep, depfix, g.M, f, my + ix[a], v);
                         }
                     }
                 }
@@ -229,71 +272,90 @@ __global__ void __launch_bounds__(256) k_deposit_tiled(Geom g, int N, int quirk4
     }
     if (!staged) return;
     __syncthreads();
-    const int npair = (nd + 1) >> 1;
-    for (long long v = threadIdx.x; v < V; v += blockDim.x) {
-        const int lz = (int)(v / ((long long)E1 * E0));
-        const int rem = (int)(v - (long long)lz * E1 * E0);
-        const int ly = rem / E0, lx = rem - ly * E0;
-        const long long m = wrapi(s_ref[0] + s_min[0] + lx, g.nx) +
-                            (long long)g.nx * (wrapi(s_ref[1] + s_min[1] + ly, g.ny) +
-                                               (long long)g.ny * wrapi(s_ref[2] + s_min[2] + lz, g.nz));
+    const int npair = (nfields + 1) >> 1;
+    tile_for_each(ts, E, E[0], E[0] * E[1], [&](int v, int m) {
         if (FIXED) {
-            for (int f = 0; f < nd; f++) {
+            for (int f = 0; f < nfields; f++) {
                 const unsigned long long u = tu[f * V + v];
                 if (u) atomicAdd(depfix + f * g.M + m, u);
             }
         } else {
             for (int t = 0; t < npair; t++) {
                 const float a0 = tf[(2 * t) * V + v];
-                const float a1 = (2 * t + 1 < nd) ? tf[(2 * t + 1) * V + v] : 0.f;
+                const float a1 = (2 * t + 1 < nfields) ? tf[(2 * t + 1) * V + v] : 0.f;
                 if (a0 != 0.f && a1 != 0.f) atomicAdd(dep + t * g.M + m, make_float2(a0, a1));
                 else if (a0 != 0.f) atomicAdd(&dep[t * g.M + m].x, a0);
                 else if (a1 != 0.f) atomicAdd(&dep[t * g.M + m].y, a1);
             }
         }
-    }
+    });
+}
+
+template <int P, int NF>
+static void dep_launch_nf(int nb, int threads, const Geom &g, const ParticleParams &pp, const float *X0,
+                          const float *X1, const long long *d_step, const uint32_t *pflags, const float *q,
+                          float2 *dep, unsigned long long *depfix, const TileCfg &tc, cudaStream_t st)
+{
+    // box capacity: the host's estimate for sorted tiles, else the fixed maximum
+    const int nf = NF ? NF : pp.nd;
+    const size_t esz = depfix ? 8 : 4;
+    int cap = tc.start ? (int)((size_t)tc.box * nf * esz) : (depfix ? kDepSmemFixed : kDepSmemFast);
+    cap = std::min(cap, depfix ? kDepSmemFixed : kDepSmemFast);
+    cap = (cap + 15) & ~15;
+    const size_t table = (size_t)(threads / 32) * 32 * (3 * (P + 1) + 4) * sizeof(float);
+    if (depfix)
+        k_deposit_tiled<P, NF, true><<<nb, threads, cap + table, st>>>(g, pp.N, pp.quirk4, pp.nd, pp.dchan_charge, X0,
+                                                                       X1, d_step, pflags, q, dep, depfix, cap, tc);
+    else
+        k_deposit_tiled<P, NF, false><<<nb, threads, cap + table, st>>>(g, pp.N, pp.quirk4, pp.nd, pp.dchan_charge, X0,
+                                                                        X1, d_step, pflags, q, dep, depfix, cap, tc);
 }
 
 template <int P>
 static void dep_launch(const Geom &g, const ParticleParams &pp, const float *X0, const float *X1,
                        const long long *d_step, const uint32_t *pflags, const float *q, float2 *dep,
-                       unsigned long long *depfix, cudaStream_t st)
+                       unsigned long long *depfix, const TileCfg &tc, cudaStream_t st)
 {
-    const int nb = (pp.N + kDepPB - 1) / kDepPB;
-    if (depfix)
-        k_deposit_tiled<P, true><<<nb, 256, kDepSmemFixed, st>>>(g, pp.N, pp.quirk4, pp.nd, pp.dchan_charge, X0, X1,
-                                                                 d_step, pflags, q, dep, depfix, kDepSmemFixed);
+    const int nb = tc.start ? (tc.nkeys + tc.codes - 1) / tc.codes : (pp.N + kDepPB - 1) / kDepPB;
+    const int threads = tc.start ? tc.threads : 256;
+    if (pp.nd == 1)
+        dep_launch_nf<P, 1>(nb, threads, g, pp, X0, X1, d_step, pflags, q, dep, depfix, tc, st);
+    else if (pp.nd == 2)
+        dep_launch_nf<P, 2>(nb, threads, g, pp, X0, X1, d_step, pflags, q, dep, depfix, tc, st);
     else
-        k_deposit_tiled<P, false><<<nb, 256, kDepSmemFast, st>>>(g, pp.N, pp.quirk4, pp.nd, pp.dchan_charge, X0, X1,
-                                                                 d_step, pflags, q, dep, depfix, kDepSmemFast);
+        dep_launch_nf<P, 0>(nb, threads, g, pp, X0, X1, d_step, pflags, q, dep, depfix, tc, st);
 }
 
 void init_deposit_attributes()
 {
-#define TILD_DA(P)                                                                                       \
-    cudaFuncSetAttribute(k_deposit_tiled<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDepSmemFixed); \
-    cudaFuncSetAttribute(k_deposit_tiled<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDepSmemFast)
+#define TILD_DA1(P, NF)                                                                                        \
+    cudaFuncSetAttribute(k_deposit_tiled<P, NF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDepSmemFixed + 40960); \
+    cudaFuncSetAttribute(k_deposit_tiled<P, NF, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDepSmemFast + 40960)
+#define TILD_DA(P) TILD_DA1(P, 0); TILD_DA1(P, 1); TILD_DA1(P, 2)
     TILD_DA(0);
     TILD_DA(1);
     TILD_DA(2);
     TILD_DA(3);
     TILD_DA(4);
 #undef TILD_DA
+#undef TILD_DA1
 }
 
 cudaError_t launch_deposit(const Geom &g, const ParticleParams &pp, const float *X0, const float *X1,
                            const long long *d_step, const uint32_t *pflags, const float *q, float2 *dep,
-                           unsigned long long *dep_fixed, int deterministic, cudaStream_t st)
+                           unsigned long long *dep_fixed, int deterministic, const TileCfg &tc, cudaStream_t st)
 {
     if (pp.N == 0) return cudaSuccess;
     unsigned long long *df = deterministic ? dep_fixed : nullptr;
+#define TILD_DL(P) dep_launch<P>(g, pp, X0, X1, d_step, pflags, q, dep, df, tc, st)
     switch (pp.order) {
-        case 0: dep_launch<0>(g, pp, X0, X1, d_step, pflags, q, dep, df, st); break;
-        case 1: dep_launch<1>(g, pp, X0, X1, d_step, pflags, q, dep, df, st); break;
-        case 2: dep_launch<2>(g, pp, X0, X1, d_step, pflags, q, dep, df, st); break;
-        case 3: dep_launch<3>(g, pp, X0, X1, d_step, pflags, q, dep, df, st); break;
-        default: dep_launch<4>(g, pp, X0, X1, d_step, pflags, q, dep, df, st); break;
+        case 0: TILD_DL(0); break;
+        case 1: TILD_DL(1); break;
+        case 2: TILD_DL(2); break;
+        case 3: TILD_DL(3); break;
+        default: TILD_DL(4); break;
     }
+#undef TILD_DL
     return cudaGetLastError();
 }
 

@@ -4,6 +4,7 @@
 
 #include <curand_kernel.h>
 
+#include <algorithm>
 #include <cmath>
 
 namespace tild {
@@ -48,36 +49,18 @@ __device__ __forceinline__ void philox_normals3(unsigned long long seed, uint32_
     out[2] = r1 * cospif(2.f * u3);
 }
 
-template <int P>
-__global__ void __launch_bounds__(256) k_particles(Geom g, const ParticleParams *__restrict__ ppd, int N,
-                                                   float *__restrict__ X0, float *__restrict__ X1,
-                                                   float *__restrict__ noise,
-                                                   const uint32_t *__restrict__ pflags,
-                                                   const float *__restrict__ q, const uint8_t *__restrict__ nb,
-                                                   const int *__restrict__ partner,
-                                                   const uint8_t *__restrict__ btype,
-                                                   const float4 *__restrict__ rec,
-                                                   const int *__restrict__ orig_id,
-                                                   curandState *__restrict__ rng,
-                                                   const long long *__restrict__ d_step,
-                                                   float *__restrict__ fout, int integrate)
+// Bond force on particle p (ps_deviceBonds.cu:7-79): minimum image with Lh, skipped for
+// r^2 <= 1e-4, harmonic mf = 2k(r - req)/r or FENE; f -= mf * dr over every stored partner.
+__device__ __forceinline__ void bond_force(const Geom &g, const ParticleParams &pp, int p, const float *x,
+                                           const float *__restrict__ Xc, const uint8_t *__restrict__ nb,
+                                           const int *__restrict__ partner, const uint8_t *__restrict__ btype,
+                                           float *f)
 {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= N) return;
-    const ParticleParams &pp = *ppd;
-    const long long step = *d_step;
-    const float *__restrict__ Xc = (step & 1) ? X1 : X0;   // x_t
-    float *__restrict__ Xn = (step & 1) ? X0 : X1;         // x_{t-1} in, x_{t+1} out
-    const uint32_t fl = pflags[p];
-    const float x0 = Xc[3 * p], x1 = Xc[3 * p + 1], x2 = Xc[3 * p + 2];
-    float f0 = 0.f, f1 = 0.f, f2 = 0.f;
-
-    // 1. bonds
     const int nbp = nb ? nb[p] : 0;
     for (int b = 0; b < nbp; b++) {
         const int o = partner[p * pp.maxb + b];
         const int t = btype[p * pp.maxb + b];
-        float dr[3] = {x0 - Xc[3 * o], x1 - Xc[3 * o + 1], x2 - Xc[3 * o + 2]};
+        float dr[3] = {x[0] - Xc[3 * o], x[1] - Xc[3 * o + 1], x[2] - Xc[3 * o + 2]};
         float mdr2 = 0.f;
 #pragma unroll
         for (int j = 0; j < 3; j++) {
@@ -95,73 +78,23 @@ __global__ void __launch_bounds__(256) k_particles(Geom g, const ParticleParams 
                 mf = 2.0f * pp.bk[t] * mdr / (1.f - u * u) / mdr;
             }
         }
-        f0 = __fmaf_rn(-mf, dr[0], f0);
-        f1 = __fmaf_rn(-mf, dr[1], f1);
-        f2 = __fmaf_rn(-mf, dr[2], f2);
+#pragma unroll
+        for (int j = 0; j < 3; j++) f[j] = __fmaf_rn(-mf, dr[j], f[j]);
     }
+}
 
-    // 2. grid forces, force groups in the reference's group order
-    const uint32_t fm = (fl >> 8) & 0xffu;
-    if (fm) {
-        float Wx[P + 1], Wy[P + 1], Wz[P + 1];
-        int ix[P + 1], iy[P + 1], iz[P + 1];
-        const int gx = stencil_axis<P>(x0, g.dxf[0], pp.quirk4, Wx);
-        const int gy = stencil_axis<P>(x1, g.dxf[1], pp.quirk4, Wy);
-        const int gz = stencil_axis<P>(x2, g.dxf[2], pp.quirk4, Wz);
-#pragma unroll
-        for (int i = 0; i <= P; i++) {
-            ix[i] = wrapi(gx + i, g.nx);
-            iy[i] = wrapi(gy + i, g.ny);
-            iz[i] = wrapi(gz + i, g.nz);
-        }
-        const long long plane = (long long)g.nx * g.ny;
-        for (int fg = 0; fg < pp.nfg; fg++) {
-            if (!((fm >> fg) & 1u)) continue;
-            const float4 *rf = rec + (long long)fg * g.M;
-            float a0 = 0.f, a1 = 0.f, a2 = 0.f;
-#pragma unroll 1
-            for (int e = 0; e <= P; e++) {
-                const float wz = sel<P>(Wz, e);
-                const float4 *rz = rf + plane * sel<P>(iz, e);
-#pragma unroll
-                for (int b = 0; b <= P; b++) {
-                    const float4 *ry = rz + (long long)g.nx * iy[b];
-                    const float wyz = Wy[b] * wz;
-#pragma unroll
-                    for (int a = 0; a <= P; a++) {
-                        const float w = Wx[a] * wyz;
-                        const float4 r = __ldg(ry + ix[a]);
-                        a0 = __fmaf_rn(r.x, w, a0);
-                        a1 = __fmaf_rn(r.y, w, a1);
-                        a2 = __fmaf_rn(r.z, w, a2);
-                    }
-                }
-            }
-            if ((pp.fg_qweighted >> fg) & 1u) {
-                const float qp = q[p];
-                f0 = __fmaf_rn(a0, qp, f0);
-                f1 = __fmaf_rn(a1, qp, f1);
-                f2 = __fmaf_rn(a2, qp, f2);
-            } else {
-                f0 += a0;
-                f1 += a1;
-                f2 += a2;
-            }
-        }
-    }
-    if (fout) {
-        fout[3 * p] = f0;
-        fout[3 * p + 1] = f1;
-        fout[3 * p + 2] = f2;
-    }
-    if (!integrate) return;
-
-    // 3. integrator
+// GJF (ps_integratorGJF.cu:102-163) or EM (ps_integratorEM.cu:39-82) update of particle p;
+// x_{t-1} is read from Xn and replaced by x_{t+1}.
+__device__ __forceinline__ void integrate(const Geom &g, const ParticleParams &pp, int p, uint32_t fl,
+                                          const float *xs, const float *fs, float *__restrict__ Xn,
+                                          float *__restrict__ noise, const int *__restrict__ orig_id,
+                                          curandState *__restrict__ rng, long long step)
+{
     const int slot = (fl >> 16) & 0xfu;
     if (slot == kNoIntegrator) {
-        Xn[3 * p] = x0;
-        Xn[3 * p + 1] = x1;
-        Xn[3 * p + 2] = x2;
+        Xn[3 * p] = xs[0];
+        Xn[3 * p + 1] = xs[1];
+        Xn[3 * p + 2] = xs[2];
         return;
     }
     float nz3[3];
@@ -174,7 +107,6 @@ __global__ void __launch_bounds__(256) k_particles(Geom g, const ParticleParams 
     } else {
         philox_normals3(pp.seed, (uint32_t)step, (uint32_t)orig_id[p], nz3);
     }
-    const float xs[3] = {x0, x1, x2}, fs[3] = {f0, f1, f2};
     if (pp.integ_kind[slot] == 0) {
         const int t = (fl >> 20) & 0xfu;
         const TypeCoef cf = pp.coef[slot][t];
@@ -201,6 +133,198 @@ __global__ void __launch_bounds__(256) k_particles(Geom g, const ParticleParams 
             else if (xv < 0.0f) xv += g.L[j];
             Xn[3 * p + j] = xv;
         }
+    }
+}
+
+__device__ __forceinline__ void cp_async16p(void *smem_dst, const void *gsrc)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+
+constexpr int kPartBox = 4096;     // float4 records staged per force group (64 KB)
+constexpr int kPartWindow = 256;   // slots per CTA when the particles are not sorted
+
+// Particle pass over one Morton tile of particles (or a window of slots), one particle
+// per thread and pass: bonds, then per force group the tile's box of force records is
+// staged in shared memory with cp.async and gathered from there
+// (device_utils.cu:358-461), then GJF/EM.  Position, flags, stencil weights and the
+// force stay in registers across the force groups.
+template <int P>
+__global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticleParams *__restrict__ ppd, int N,
+                                                   float *__restrict__ X0, float *__restrict__ X1,
+                                                   float *__restrict__ noise, const uint32_t *__restrict__ pflags,
+                                                   const float *__restrict__ q, const uint8_t *__restrict__ nb,
+                                                   const int *__restrict__ partner,
+                                                   const uint8_t *__restrict__ btype,
+                                                   const float4 *__restrict__ rec, const int *__restrict__ orig_id,
+                                                   curandState *__restrict__ rng,
+                                                   const long long *__restrict__ d_step, float *__restrict__ fout,
+                                                   int integrate_flag, TileCfg tc, int box_cap)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    float4 *box = reinterpret_cast<float4 *>(smraw);
+    __shared__ TileShared ts;
+    const ParticleParams &pp = *ppd;
+    const long long step = *d_step;
+    const float *__restrict__ Xc = (step & 1) ? X1 : X0;   // x_t
+    float *__restrict__ Xn = (step & 1) ? X0 : X1;         // x_{t-1} in, x_{t+1} out
+    const float inv[3] = {1.f / g.dxf[0], 1.f / g.dxf[1], 1.f / g.dxf[2]};
+    const int nn[3] = {g.nx, g.ny, g.nz};
+    int r0, r1;
+    tile_range(tc, N, kPartWindow, r0, r1);
+    for (int c0 = r0; c0 < r1; c0 += blockDim.x) {
+        const int p = c0 + threadIdx.x;
+        const bool act = p < r1;
+        float x[3] = {0.f, 0.f, 0.f};
+        uint32_t fl = 0u;
+        if (act) {
+            x[0] = Xc[3 * p];
+            x[1] = Xc[3 * p + 1];
+            x[2] = Xc[3 * p + 2];
+            fl = pflags[p];
+        }
+        const unsigned fm = (fl >> 8) & 0xffu;
+        float Wx[P + 1], Wy[P + 1], Wz[P + 1];
+        int gs[3] = {0, 0, 0};
+        if (fm) {
+            gs[0] = stencil_fast<P>(x[0], inv[0], pp.quirk4, Wx);
+            gs[1] = stencil_fast<P>(x[1], inv[1], pp.quirk4, Wy);
+            gs[2] = stencil_fast<P>(x[2], inv[2], pp.quirk4, Wz);
+        }
+        if (threadIdx.x < 3) {
+            ts.ref[threadIdx.x] = stencil_origin<P>(Xc[3 * c0 + threadIdx.x], inv[threadIdx.x]);
+            ts.lo[threadIdx.x] = 0x7fffffff;
+            ts.hi[threadIdx.x] = -0x7fffffff;
+        }
+        if (threadIdx.x == 0) ts.fm = 0u;
+        __syncthreads();
+        // 1. box of the stencil origins of the pass's particles that gather
+        int d[3], lo[3], hi[3];
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            d[j] = fm ? unwrap_delta(gs[j] - ts.ref[j], nn[j]) : 0;
+            lo[j] = fm ? d[j] : 0x7fffffff;
+            hi[j] = fm ? d[j] : -0x7fffffff;
+            for (int o = 16; o > 0; o >>= 1) {
+                lo[j] = min(lo[j], __shfl_xor_sync(0xffffffffu, lo[j], o));
+                hi[j] = max(hi[j], __shfl_xor_sync(0xffffffffu, hi[j], o));
+            }
+        }
+        unsigned fmor = fm;
+        for (int o = 16; o > 0; o >>= 1) fmor |= __shfl_xor_sync(0xffffffffu, fmor, o);
+        if ((threadIdx.x & 31) == 0 && fmor) {
+            for (int j = 0; j < 3; j++) {
+                atomicMin(&ts.lo[j], lo[j]);
+                atomicMax(&ts.hi[j], hi[j]);
+            }
+            atomicOr(&ts.fm, fmor);
+        }
+        __syncthreads();
+        const unsigned fmall = ts.fm;
+        const int E[3] = {ts.hi[0] - ts.lo[0] + P + 1, ts.hi[1] - ts.lo[1] + P + 1, ts.hi[2] - ts.lo[2] + P + 1};
+        // odd row/plane pitches (in 16-byte records) spread neighbouring rows over the
+        // shared-memory bank groups
+        const int E0 = E[0] | 1, E01 = (E0 * E[1]) | 1;
+        const long long Vl = fmall ? (long long)E01 * E[2] : 0;
+        const bool staged = Vl > 0 && Vl <= box_cap && E[0] <= kMaxBoxEdge && E[1] <= kMaxBoxEdge &&
+                            E[2] <= kMaxBoxEdge;
+        if (staged) tile_tables(ts, g.nx, g.ny, g.nz, E);
+        __syncthreads();
+        int fg = 0;
+        while (fg < pp.nfg && !((fmall >> fg) & 1u)) fg++;
+        // 2. start staging the first force group's box, compute bonds meanwhile
+        if (staged && fg < pp.nfg) {
+            const float4 *rf = rec + (long long)fg * g.M;
+            tile_for_each(ts, E, E0, E01, [&](int v, int m) { cp_async16p(box + v, rf + m); });
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
+        }
+        float f[3] = {0.f, 0.f, 0.f};
+        if (act) bond_force(g, pp, p, x, Xc, nb, partner, btype, f);
+        const int base = (d[2] - ts.lo[2]) * E01 + (d[1] - ts.lo[1]) * E0 + (d[0] - ts.lo[0]);
+        const float qp = (act && q) ? q[p] : 0.f;
+        // 3. gather each force group in group order
+        bool first = true;
+        for (; fg < pp.nfg; fg++) {
+            if (!((fmall >> fg) & 1u)) continue;
+            const float4 *rf = rec + (long long)fg * g.M;
+            if (staged) {
+                if (!first) {
+                    __syncthreads();   // every gather from the previous group's box is done
+                    tile_for_each(ts, E, E0, E01, [&](int v, int m) { cp_async16p(box + v, rf + m); });
+                    asm volatile("cp.async.commit_group;\n" ::: "memory");
+                }
+                asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+                __syncthreads();
+            }
+            first = false;
+            if (!((fl >> (8 + fg)) & 1u)) continue;
+            float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+            if (staged) {
+#pragma unroll
+                for (int e = 0; e <= P; e++) {
+#pragma unroll
+                    for (int b = 0; b <= P; b++) {
+                        const float wyz = Wy[b] * Wz[e];
+                        const int row = base + e * E01 + b * E0;
+#pragma unroll
+                        for (int a = 0; a <= P; a++) {
+                            const float w = Wx[a] * wyz;
+                            const float4 r = box[row + a];
+                            a0 = __fmaf_rn(r.x, w, a0);
+                            a1 = __fmaf_rn(r.y, w, a1);
+                            a2 = __fmaf_rn(r.z, w, a2);
+                        }
+                    }
+                }
+            } else {
+                const long long plane = (long long)g.nx * g.ny;
+                int ix[P + 1], iy[P + 1], iz[P + 1];
+#pragma unroll
+                for (int i = 0; i <= P; i++) {
+                    ix[i] = wrapi(gs[0] + i, g.nx);
+                    iy[i] = wrapi(gs[1] + i, g.ny);
+                    iz[i] = wrapi(gs[2] + i, g.nz);
+                }
+#pragma unroll 1
+                for (int e = 0; e <= P; e++) {
+                    const float wz = sel<P>(Wz, e);
+                    const float4 *rz = rf + plane * sel<P>(iz, e);
+#pragma unroll
+                    for (int b = 0; b <= P; b++) {
+                        const float4 *ry = rz + (long long)g.nx * iy[b];
+                        const float wyz = Wy[b] * wz;
+#pragma unroll
+                        for (int a = 0; a <= P; a++) {
+                            const float w = Wx[a] * wyz;
+                            const float4 r = __ldg(ry + ix[a]);
+                            a0 = __fmaf_rn(r.x, w, a0);
+                            a1 = __fmaf_rn(r.y, w, a1);
+                            a2 = __fmaf_rn(r.z, w, a2);
+                        }
+                    }
+                }
+            }
+            if ((pp.fg_qweighted >> fg) & 1u) {
+                f[0] = __fmaf_rn(a0, qp, f[0]);
+                f[1] = __fmaf_rn(a1, qp, f[1]);
+                f[2] = __fmaf_rn(a2, qp, f[2]);
+            } else {
+                f[0] += a0;
+                f[1] += a1;
+                f[2] += a2;
+            }
+        }
+        // 4. integrate
+        if (act) {
+            if (fout) {
+                fout[3 * p] = f[0];
+                fout[3 * p + 1] = f[1];
+                fout[3 * p + 2] = f[2];
+            }
+            if (integrate_flag) integrate(g, pp, p, fl, x, f, Xn, noise, orig_id, rng, step);
+        }
+        __syncthreads();   // the box and ts are reused by the next pass
     }
 }
 
@@ -296,27 +420,40 @@ __global__ void k_reduce_partials(const double *partials, int nblocks, int ncols
 }
 
 
-// ---- launchers ----
+constexpr size_t kPartSmemMax = kPartBox * sizeof(float4);
+
 template <int P>
 static void part_launch(const Geom &g, const ParticleParams *ppd, int N, float *X0, float *X1, float *noise,
                         const uint32_t *pflags, const float *q, const uint8_t *nb, const int *partner,
                         const uint8_t *btype, const float4 *rec, const int *orig_id, void *rng,
-                        const long long *d_step, float *fout, int integrate, cudaStream_t st)
+                        const long long *d_step, float *fout, int integrate, const TileCfg &tc, cudaStream_t st)
 {
-    const int bs = 256, nbk = (N + bs - 1) / bs;
-    k_particles<P><<<nbk, bs, 0, st>>>(g, ppd, N, X0, X1, noise, pflags, q, nb, partner, btype, rec, orig_id,
-                                       reinterpret_cast<curandState *>(rng), d_step, fout, integrate);
+    const int nbk = tc.start ? (tc.nkeys + tc.codes - 1) / tc.codes : (N + kPartWindow - 1) / kPartWindow;
+    const int threads = tc.start ? tc.threads : 256;
+    const int cap = tc.start ? std::min(tc.box, kPartBox) : kPartBox;
+    const size_t smem = (size_t)cap * sizeof(float4);
+    k_particles<P><<<nbk, threads, smem, st>>>(g, ppd, N, X0, X1, noise, pflags, q, nb, partner, btype, rec, orig_id,
+                                               reinterpret_cast<curandState *>(rng), d_step, fout, integrate, tc, cap);
+}
+
+void init_particle_attributes()
+{
+    cudaFuncSetAttribute(k_particles<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
+    cudaFuncSetAttribute(k_particles<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
+    cudaFuncSetAttribute(k_particles<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
+    cudaFuncSetAttribute(k_particles<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
+    cudaFuncSetAttribute(k_particles<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
 }
 
 cudaError_t launch_particles(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd, float *X0,
                              float *X1, float *noise, const uint32_t *pflags, const float *q, const uint8_t *nb,
                              const int *partner, const uint8_t *btype, const float4 *rec, const int *orig_id,
                              void *rng_states, const long long *d_step, float *fout, int integrate,
-                             cudaStream_t st)
+                             const TileCfg &tc, cudaStream_t st)
 {
     if (pp.N == 0) return cudaSuccess;
 #define TILD_PL(P) part_launch<P>(g, ppd, pp.N, X0, X1, noise, pflags, q, nb, partner, btype, rec, orig_id, \
-                                  rng_states, d_step, fout, integrate, st)
+                                  rng_states, d_step, fout, integrate, tc, st)
     switch (pp.order) {
         case 0: TILD_PL(0); break;
         case 1: TILD_PL(1); break;

@@ -60,6 +60,131 @@ __device__ __forceinline__ int stencil_axis(float x, float d, int quirk4, float 
     return g - P / 2;
 }
 
+// Fast stencil for the deposit and the gather: same cell choice and the same spline
+// polynomials, evaluated with a reciprocal multiply and Horner FMAs instead of IEEE
+// divisions.  Weights differ from the reference's by rounding only (the splines are
+// continuous across cell edges, so a different cell pick at an edge moves nothing).
+// Returns the first stencil index; W[0..P] are the 1-D weights (unscaled, sum 1).
+template <int P>
+__device__ __forceinline__ int stencil_fast(float x, float inv_d, int quirk4, float *W)
+{
+    const float t = x * inv_d;
+    int g;
+    float s;
+    if (P % 2 == 0) {
+        g = (int)(t + 0.5f);
+        s = t - (float)g;
+    } else {
+        g = (int)t;
+        s = t - (float)g - 0.5f;
+    }
+    if (P == 0) {
+        W[0] = 1.f;
+    } else if (P == 1) {
+        W[0] = 0.5f - s;
+        W[1] = 0.5f + s;
+    } else if (P == 2) {
+        const float s2 = s * s;
+        W[0] = fmaf(0.5f, s2, fmaf(-0.5f, s, 0.125f));
+        W[1] = 0.75f - s2;
+        W[2] = fmaf(0.5f, s2, fmaf(0.5f, s, 0.125f));
+    } else if (P == 3) {
+        W[0] = fmaf(fmaf(fmaf(-1.f / 6.f, s, 0.25f), s, -0.125f), s, 1.f / 48.f);
+        W[1] = fmaf(fmaf(fmaf(0.5f, s, -0.25f), s, -0.625f), s, 23.f / 48.f);
+        W[2] = fmaf(fmaf(fmaf(-0.5f, s, -0.25f), s, 0.625f), s, 23.f / 48.f);
+        W[3] = fmaf(fmaf(fmaf(1.f / 6.f, s, 0.25f), s, 0.125f), s, 1.f / 48.f);
+    } else {
+        const float s2 = s * s, s4 = s2 * s2, s3 = quirk4 ? s4 : s2 * s;
+        W[0] = (1.f - 8.f * s + 24.f * s2 - 32.f * s3 + 16.f * s4) * (1.f / 384.f);
+        W[1] = (19.f - 44.f * s + 24.f * s2 + 16.f * s3 - 16.f * s4) * (1.f / 96.f);
+        W[2] = (115.f - 120.f * s2 + 48.f * s4) * (1.f / 192.f);
+        W[3] = (19.f + 44.f * s + 24.f * s2 - 16.f * s3 - 16.f * s4) * (1.f / 96.f);
+        W[4] = (1.f + 8.f * s + 24.f * s2 + 32.f * s3 + 16.f * s4) * (1.f / 384.f);
+    }
+    return g - P / 2;
+}
+
+// -------------------------------------------------------------------------------------
+// Tiles of spatially sorted particles.  A CTA takes the particles of `codes` (a power of
+// two >= 8) consecutive brick Morton codes -- contiguous slots after the sort, an aligned
+// block of bricks of 4^3 cells -- and works on the box of grid points their stencils
+// cover, staged in shared memory.  The host sizes codes and the CTA from the density so
+// that a CTA holds about one particle per thread.  The box is described relative to the stencil origin of the CTA's first
+// particle (periodic unwrap); per-axis index tables turn a box coordinate into a grid
+// offset without divisions.
+// -------------------------------------------------------------------------------------
+constexpr int kMaxBoxEdge = 64;
+
+struct TileShared {
+    int ref[3], lo[3], hi[3];
+    unsigned fm;
+    int xi[kMaxBoxEdge];   // wrapped x index of box column lx
+    int yb[kMaxBoxEdge];   // nx * wrapped y of box row ly
+    int zb[kMaxBoxEdge];   // nx * ny * wrapped z of box plane lz
+};
+
+__device__ __forceinline__ int unwrap_delta(int d, int n)
+{
+    int t = d % n;
+    if (t < 0) t += n;
+    if (t >= (n + 1) / 2) t -= n;
+    return t;
+}
+
+// first stencil index of the fast stencil (same arithmetic as stencil_fast)
+template <int P>
+__device__ __forceinline__ int stencil_origin(float x, float inv_d)
+{
+    const float t = x * inv_d;
+    const int g = (P % 2 == 0) ? (int)(t + 0.5f) : (int)t;
+    return g - P / 2;
+}
+
+// [b0, b1) of the CTA: a tile of sorted particles, or a fixed window of slots
+__device__ __forceinline__ void tile_range(const TileCfg &tc, int N, int window, int &b0, int &b1)
+{
+    if (tc.start) {
+        const int k0 = blockIdx.x * tc.codes;
+        b0 = (int)tc.start[k0];
+        b1 = (k0 + tc.codes < tc.nkeys) ? (int)tc.start[k0 + tc.codes] : N;
+    } else {
+        b0 = blockIdx.x * window;
+        b1 = min(N, b0 + window);
+    }
+}
+
+// Fill the per-axis index tables of a box with edges E (all threads; E[d] <= kMaxBoxEdge).
+__device__ __forceinline__ void tile_tables(TileShared &ts, int nx, int ny, int nz, const int *E)
+{
+    const int n3[3] = {nx, ny, nz};
+    for (int t = threadIdx.x; t < E[0] + E[1] + E[2]; t += blockDim.x) {
+        const int d = t < E[0] ? 0 : (t < E[0] + E[1] ? 1 : 2);
+        const int l = t - (d == 0 ? 0 : (d == 1 ? E[0] : E[0] + E[1]));
+        int v = (ts.ref[d] + ts.lo[d] + l) % n3[d];
+        if (v < 0) v += n3[d];
+        if (d == 0) ts.xi[l] = v;
+        else if (d == 1) ts.yb[l] = v * nx;
+        else ts.zb[l] = v * nx * ny;
+    }
+}
+
+// Visit every box element (x fastest) with lanes along x: f(v, grid_offset), where v is
+// the element's offset in a box stored with row pitch p1 and plane pitch p2.
+template <typename F>
+__device__ __forceinline__ void tile_for_each(const TileShared &ts, const int *E, int p1, int p2, F f)
+{
+    const int E0 = E[0], rows = E[1] * E[2];
+    const int xw = E0 <= 16 ? 16 : 32;   // x runs of 16 or 32 lanes
+    const int rpp = blockDim.x / xw;
+    const int lx0 = threadIdx.x % xw;
+    for (int row = threadIdx.x / xw; row < rows; row += rpp) {
+        const int lz = row / E[1], ly = row - lz * E[1];
+        const int rb = ts.zb[lz] + ts.yb[ly];
+        const int vb = lz * p2 + ly * p1;
+        for (int lx = lx0; lx < E0; lx += xw) f(vb + lx, rb + ts.xi[lx]);
+    }
+}
+
 // (g + i - shift + N) % N in the reference; a true modulo here so that positions the
 // reference would send out of bounds still land on the grid.
 __device__ __forceinline__ int wrapi(int v, int n)
