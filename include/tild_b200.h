@@ -150,6 +150,18 @@ int tild_box_set_positions(tild_box *box, const float *x_in);
  * when charge_channel != 0), rho_out[M] in the reference's x-fastest order. */
 int tild_box_get_density(tild_box *box, const char *group, int charge_channel, float *rho_out);
 
+/* No reference counterpart.  tild_box_get_density with no allocation of any kind: its
+ * device scratch (4 bytes per grid point, per particle and per site of the group) comes
+ * from one static device array of TILD_NOALLOC_SCRATCH_BYTES (16 MiB) per device, and a
+ * box needing more is refused with TILD_ERR_ARG ("... the static scratch holds ...").
+ * The first call on a device looks the array's address up (cudaGetSymbolAddress), which
+ * can load the library's device code: make that call outside any stream capture.  All
+ * boxes and threads share the array of a device, so calls on one device must not
+ * overlap; the call clears the part that must start at zero (the density accumulator)
+ * itself and returns after the copy to rho_out[M] has finished. */
+#define TILD_NOALLOC_SCRATCH_BYTES (16u << 20)
+int tild_box_get_density_noalloc(tild_box *box, const char *group, int charge_channel, float *rho_out);
+
 /* Stencil indices and weights of every particle at the current positions
  * (d_calcGridWeights, ps_grid_utils.cu:74-204): inds_out/w_out[n*(pmeorder+1)^Dim],
  * same order and float arithmetic as the reference (weights divided by gvol). */

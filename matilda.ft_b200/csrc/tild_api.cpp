@@ -227,6 +227,13 @@ int tild_box_get_density(tild_box *box, const char *group, int charge_channel, f
     return guarded([&] { box->impl->getDensity(group, charge_channel, rho_out); });
 }
 
+int tild_box_get_density_noalloc(tild_box *box, const char *group, int charge_channel, float *rho_out)
+{
+    NEED_BOX;
+    if (!group || !rho_out) return fail(TILD_ERR_ARG, "NULL argument");
+    return guarded([&] { box->impl->getDensityNoAlloc(group, charge_channel, rho_out); });
+}
+
 int tild_box_grid_weights(tild_box *box, int32_t *inds_out, float *w_out)
 {
     NEED_BOX;

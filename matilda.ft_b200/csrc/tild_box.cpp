@@ -1247,6 +1247,38 @@ void Box::getDensity(const std::string &group, int charge, float *rho)
     ck(e, "density");
 }
 
+// getDensity without any allocation: the accumulator rho[M], the slot-of-particle table
+// slot_of[N] and the group's sites[ns] live in the static device scratch, in that order.
+// rho must start at zero and is cleared here on every call; slot_of and sites are fully
+// overwritten.  Calls on one device share the scratch and must not overlap.
+void Box::getDensityNoAlloc(const std::string &group, int charge, float *rho)
+{
+    if (!ready) fail(TILD_ERR_STATE, "endBox has not been processed");
+    const int gi = findGroupInteger(group);
+    if (charge && !psGroup[gi].isCharges) fail(TILD_ERR_ARG, "only the 'charges' group has a charge density");
+    const std::vector<int> &sites = psGroup[gi].siteList;
+    const size_t need = 4 * ((size_t)geom.M + (size_t)nstot + sites.size());
+    if (need > kStaticScratchBytes)
+        fail(TILD_ERR_ARG, "get_density_noalloc needs " + std::to_string(need) +
+                               " bytes of device scratch (4 bytes per grid point, particle and group site); "
+                               "the static scratch holds " + std::to_string(kStaticScratchBytes));
+    ck(cudaSetDevice(device), "cudaSetDevice");
+    void *scr = nullptr;
+    ck(static_scratch(device, &scr), "static scratch address");
+    float *dRho = static_cast<float *>(scr);
+    int *dSlotOf = reinterpret_cast<int *>(dRho + geom.M);
+    int *dSites = dSlotOf + nstot;
+    const long long s = deviceStep();
+    ck(cudaMemsetAsync(dRho, 0, 4 * geom.M, stream), "clear density scratch");
+    if (!sites.empty())
+        ck(cudaMemcpyAsync(dSites, sites.data(), 4 * sites.size(), cudaMemcpyHostToDevice, stream), "copy sites");
+    ck(launch_slot_map(dOrig, (int)nstot, dSlotOf, dSites, (int)sites.size(), stream), "slot map");
+    ck(launch_density_single(geom, ppHost, dX[s & 1], dSites, (int)sites.size(), dQ, charge, dRho, stream),
+       "density");
+    ck(cudaMemcpyAsync(rho, dRho, 4 * geom.M, cudaMemcpyDeviceToHost, stream), "read density");
+    ck(cudaStreamSynchronize(stream), "density");
+}
+
 void Box::gridWeights(int32_t *inds, float *w)
 {
     if (!ready) fail(TILD_ERR_STATE, "endBox has not been processed");

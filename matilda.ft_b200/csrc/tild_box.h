@@ -79,6 +79,7 @@ public:
     void getPositions(float *x) const;
     void setPositions(const float *x);
     void getDensity(const std::string &group, int charge, float *rho);
+    void getDensityNoAlloc(const std::string &group, int charge, float *rho);
     void gridWeights(int32_t *inds, float *w);
     void modifyBox(const std::string &rest);           // PS_Box.cu:848-870
     void stageTimes(std::vector<double> &out) const { out = stageSec; }

@@ -196,4 +196,11 @@ cudaError_t launch_density_single(const Geom &g, const ParticleParams &pp, const
                                   const int *sites, int ns, const float *q, int charge,
                                   float *rho, cudaStream_t st);
 
+// Static device scratch of the allocation-free density read-back (tild_noalloc.cu):
+// kStaticScratchBytes in one file-scope __device__ array, address looked up once per device.
+constexpr size_t kStaticScratchBytes = size_t(16) << 20;
+cudaError_t static_scratch(int device, void **ptr);
+// slot_of[orig[s]] = s for s < n, then sites[k] = slot_of[sites[k]] for k < ns
+cudaError_t launch_slot_map(const int *orig, int n, int *slot_of, int *sites, int ns, cudaStream_t st);
+
 }  // namespace tild

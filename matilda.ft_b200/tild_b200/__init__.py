@@ -20,6 +20,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libtild_b200.so")
 
 TILD_OK = 0
+NOALLOC_SCRATCH_BYTES = 16 << 20   # TILD_NOALLOC_SCRATCH_BYTES of the C header
 STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_PARSE", 3: "ERR_IO", 4: "ERR_CUDA", 5: "ERR_STATE",
           6: "ERR_UNSUPPORTED", 7: "ERR_DEVICE"}
 
@@ -48,6 +49,8 @@ _SIGS = {
     "tild_box_get_positions": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "tild_box_set_positions": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "tild_box_get_density": ([ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+    "tild_box_get_density_noalloc": ([ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p],
+                                     ctypes.c_int),
     "tild_box_grid_weights": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "tild_box_get_log": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64),
                           ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
@@ -204,6 +207,13 @@ class Box:
         i = self.info()
         rho = np.zeros(int(i.nx[0]) * int(i.nx[1]) * int(i.nx[2]), np.float32)
         _check(lib().tild_box_get_density(self._h, group.encode(), int(bool(charge)), _ptr(rho)))
+        return rho
+
+    def density_noalloc(self, group: str, charge=False):
+        """density() through the allocation-free entry point (static device scratch)."""
+        i = self.info()
+        rho = np.zeros(int(i.nx[0]) * int(i.nx[1]) * int(i.nx[2]), np.float32)
+        _check(lib().tild_box_get_density_noalloc(self._h, group.encode(), int(bool(charge)), _ptr(rho)))
         return rho
 
     def grid_weights(self):
