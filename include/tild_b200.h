@@ -150,15 +150,21 @@ int tild_box_set_positions(tild_box *box, const float *x_in);
  * when charge_channel != 0), rho_out[M] in the reference's x-fastest order. */
 int tild_box_get_density(tild_box *box, const char *group, int charge_channel, float *rho_out);
 
-/* No reference counterpart.  tild_box_get_density with no allocation of any kind: its
- * device scratch (4 bytes per grid point, per particle and per site of the group) comes
- * from one static device array of TILD_NOALLOC_SCRATCH_BYTES (16 MiB) per device, and a
- * box needing more is refused with TILD_ERR_ARG ("... the static scratch holds ...").
- * The first call on a device looks the array's address up (cudaGetSymbolAddress), which
- * can load the library's device code: make that call outside any stream capture.  All
- * boxes and threads share the array of a device, so calls on one device must not
- * overlap; the call clears the part that must start at zero (the density accumulator)
- * itself and returns after the copy to rho_out[M] has finished. */
+/* No counterpart in the reference.  tild_box_get_density for callers that cannot
+ * allocate device memory: a host program whose pool allocator has reserved the device's
+ * memory up front (so cudaMalloc fails or fragments the pool), or one that reads
+ * densities between steps of other work on other streams, where cudaFree would
+ * synchronise the whole device.  The device scratch (4 bytes per grid point, per
+ * particle and per site of the group) comes instead from one static device array of
+ * TILD_NOALLOC_SCRATCH_BYTES (16 MiB), which every GPU that loads the library holds until
+ * the process exits.  A box needing more is refused with TILD_ERR_ARG ("... the static
+ * scratch holds ...").  The first call on a device looks the array's address up
+ * (cudaGetSymbolAddress, with that device current), which can load the library's device
+ * code: make that first call before any stream capture.  Every call on a device shares
+ * the array, which keeps the last call's contents; the call clears the part that must
+ * start at zero (the density accumulator) itself.  Calls that overlap on one device
+ * (two boxes, or two host threads) race on the array.  The call returns after the copy
+ * to rho_out[M] has finished. */
 #define TILD_NOALLOC_SCRATCH_BYTES (16u << 20)
 int tild_box_get_density_noalloc(tild_box *box, const char *group, int charge_channel, float *rho_out);
 

@@ -1,10 +1,12 @@
 // tild_noalloc.cu -- device scratch for the allocation-free density read-back.
 //
-// tild_box_get_density_noalloc needs the same device scratch as tild_box_get_density (a
-// density accumulator, a slot-of-particle table and the group's site list) but takes it
-// from one file-scope __device__ array instead of cudaMalloc, so the call allocates
-// nothing.  Every call on a device shares that one array: calls on the same device must
-// not overlap (two boxes or two host threads using it at once race on it).
+// tild_box_get_density_noalloc serves callers that cannot allocate device memory (a
+// pool allocator already holds the device's memory, or a cudaFree would synchronise
+// streams the caller keeps busy).  It needs the same device scratch as
+// tild_box_get_density (a density accumulator, a slot-of-particle table and the group's
+// site list) but takes it from one file-scope __device__ array instead of cudaMalloc.
+// Every call on a device shares that one array and finds the previous call's contents in
+// it; calls that overlap on the same device (two boxes or two host threads) race on it.
 #include "tild_device.h"
 
 #include <mutex>

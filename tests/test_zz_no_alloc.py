@@ -1,13 +1,16 @@
 """The allocation-free density read-back against the allocating one, on the GPU.
 
-tild_box_get_density_noalloc takes its device scratch from one static device array
-instead of cudaMalloc.  It must return the density tild_box_get_density returns, call
-after call (the accumulator in the static array is re-zeroed by every call), and it must
-refuse a box whose scratch does not fit.  Tolerance: |drho| <= 1e-6 * max|rho| (the two
-calls deposit with FP32 atomics in different orders).
+tild_box_get_density_noalloc is for callers that cannot allocate device memory (their
+pool allocator holds the device's memory, or a cudaFree would synchronise streams they
+keep busy); it takes its device scratch from one static device array instead of
+cudaMalloc.  It must return the density tild_box_get_density returns on two calls in a
+row (the accumulator in the static array keeps the previous call's contents, so every
+call has to clear it), and it must refuse a box whose scratch does not fit.  Tolerance:
+|drho| <= 1e-6 * max|rho| (the two entry points deposit with FP32 atomics in different
+orders).
 
-The file name sorts last so the static scratch is exercised after every other GPU test
-of the session has used the library.
+The file name sorts last so that a run stopping at the first failure has run every other
+test before this one.
 """
 import numpy as np
 import pytest
