@@ -266,7 +266,7 @@ def run_ours(args):
     achieved = ab[dom] / stage_s[dom] / 1e9
     traffic = None
     tf = os.path.join(ROOT, "profiles", "dram_traffic_c2.json")
-    if os.path.exists(tf):
+    if args.scale == 1.0 and os.path.exists(tf):   # captured on the full-size workload only
         traffic = json.load(open(tf)).get(KERNEL_NAMES[dom])
     step_bytes = sum(ab.values())
 
