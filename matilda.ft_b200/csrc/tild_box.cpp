@@ -550,6 +550,10 @@ void Box::finishInitialization()
     if (Dim != 3) fail(TILD_ERR_UNSUPPORTED, "the B200 TILD path runs 3-D boxes (Dim 3)");
     for (int j = 0; j < 3; j++)
         if (Nx[j] <= 0) fail(TILD_ERR_PARSE, "grid must be given for every dimension");
+    for (int j = 0; j < 3; j++)   // the kernels wrap stencil indices with one add or subtract
+        if (Nx[j] < pmeorder + 2)
+            fail(TILD_ERR_UNSUPPORTED, "grid of " + std::to_string(Nx[j]) + " points is too small for pmeorder " +
+                                           std::to_string(pmeorder) + " (needs at least pmeorder + 2)");
     if (nAnglesTot > 0) fail(TILD_ERR_UNSUPPORTED, "angles are outside the TILD step");
     if (integrators.empty()) fail(TILD_ERR_PARSE, "no integrator defined");
     if (species.size() > (size_t)kMaxTypes) fail(TILD_ERR_UNSUPPORTED, "too many species");
@@ -790,10 +794,17 @@ void Box::allocDevice()
         const int slack = pmeorder + 1 + 3;   // stencil width + drift between sorts
         long long box = (long long)(((cx + slack) | 1) * (cy + slack) | 1) * (cz + slack);
         box = std::min<long long>(box, 3072);
+        // particle pass: the tile's bricks widened by the stencil and one cell of drift per
+        // side (particles that drift further are gathered from global memory)
+        const int margin = 1, ev = (pmeorder % 2 == 0) ? 1 : 0;
+        auto edge = [&](int cells, int n) { return std::min(cells, n) - 1 + ev + 2 * margin + pmeorder + 1; };
+        const int ex = edge(cx, g.nx), ey = edge(cy, g.ny), ez = edge(cz, g.nz);
         tiles.nkeys = (int)nk;
         tiles.codes = codes;
         tiles.threads = thr;
         tiles.box = (int)box;
+        tiles.pbox = (((ex | 1) * ey) | 1) * ez;
+        tiles.margin = margin;
     }
     sortW.key = dalloc<uint32_t>(N);
     sortW.rank = dalloc<int>(N);

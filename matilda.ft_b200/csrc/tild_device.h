@@ -125,7 +125,9 @@ struct TileCfg {
     int nkeys;
     int codes;
     int threads;
-    int box;
+    int box;      // deposit: shared-memory records of a tile's bounding box (estimate)
+    int pbox;     // particle pass: records of the fixed tile box (odd pitches)
+    int margin;   // particle pass: drift margin of the fixed box, cells per side
 };
 
 // -------------------------------------------------------------------------------------

@@ -145,26 +145,81 @@ __device__ __forceinline__ void cp_async16p(void *smem_dst, const void *gsrc)
 constexpr int kPartBox = 4096;     // float4 records staged per force group (64 KB)
 constexpr int kPartWindow = 256;   // slots per CTA when the particles are not sorted
 
+// Gather of one force group's records at a particle's stencil straight from global memory
+// (device_utils.cu:358-461), summed in the same order as the shared-memory gather so the
+// two paths give the same bits.
+template <int P>
+__device__ __forceinline__ void gather_global(const Geom &g, const float4 *__restrict__ rf, const int *gs,
+                                              const float *Wx, const float *Wy, const float *Wz, float *acc)
+{
+    // stencil origins lie in [-P, n]: one conditional add or subtract wraps an index
+    auto wrap = [](int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); };
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll 1
+    for (int e = 0; e <= P; e++) {
+        const float wz = sel<P>(Wz, e);
+        const float4 *rz = rf + (long long)g.nx * g.ny * wrap(gs[2] + e, g.nz);
+#pragma unroll
+        for (int b = 0; b <= P; b++) {
+            const float4 *ry = rz + (long long)g.nx * wrap(gs[1] + b, g.ny);
+            const float wyz = Wy[b] * wz;
+#pragma unroll
+            for (int a = 0; a <= P; a++) {
+                const float w = Wx[a] * wyz;
+                const float4 r = __ldg(ry + wrap(gs[0] + a, g.nx));
+                a0 = __fmaf_rn(r.x, w, a0);
+                a1 = __fmaf_rn(r.y, w, a1);
+                a2 = __fmaf_rn(r.z, w, a2);
+            }
+        }
+    }
+    acc[0] = a0;
+    acc[1] = a1;
+    acc[2] = a2;
+}
+
+// every third bit -> 10-bit value (inverse of the sort's spread3)
+__device__ __forceinline__ int compact3(uint32_t v)
+{
+    v &= 0x09249249u;
+    v = (v | (v >> 2)) & 0x030C30C3u;
+    v = (v | (v >> 4)) & 0x0300F00Fu;
+    v = (v | (v >> 8)) & 0x030000FFu;
+    v = (v | (v >> 16)) & 0x000003FFu;
+    return (int)v;
+}
+
+constexpr int kPartOut = 32;   // particles per pass gathered from global memory by helpers
+
 // Particle pass over one Morton tile of particles (or a window of slots), one particle
-// per thread and pass: bonds, then per force group the tile's box of force records is
-// staged in shared memory with cp.async and gathered from there
-// (device_utils.cu:358-461), then GJF/EM.  Position, flags, stencil weights and the
-// force stay in registers across the force groups.
+// per thread and pass: bonds, then per force group the gather (device_utils.cu:358-461),
+// then GJF/EM.  Position, flags, stencil weights and the force stay in registers across
+// the force groups.
+//
+// Sorted tiles stage a fixed box per force group in shared memory with cp.async: the grid
+// points of the tile's block of bricks (where its particles were at the last sort), widened
+// by the stencil and by `tc.margin` cells for the drift since.  A particle whose stencil
+// has drifted out of the box is gathered from global memory, before the staging wait, by a
+// helper thread (thread o for the pass's o-th such particle); its owner adds the result in
+// group order like any other, so the sums do not depend on which path served them.
 template <int P>
 __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticleParams *__restrict__ ppd, int N,
-                                                   float *__restrict__ X0, float *__restrict__ X1,
-                                                   float *__restrict__ noise, const uint32_t *__restrict__ pflags,
-                                                   const float *__restrict__ q, const uint8_t *__restrict__ nb,
-                                                   const int *__restrict__ partner,
-                                                   const uint8_t *__restrict__ btype,
-                                                   const float4 *__restrict__ rec, const int *__restrict__ orig_id,
-                                                   curandState *__restrict__ rng,
-                                                   const long long *__restrict__ d_step, float *__restrict__ fout,
-                                                   int integrate_flag, TileCfg tc, int box_cap)
+                                                      float *__restrict__ X0, float *__restrict__ X1,
+                                                      float *__restrict__ noise, const uint32_t *__restrict__ pflags,
+                                                      const float *__restrict__ q, const uint8_t *__restrict__ nb,
+                                                      const int *__restrict__ partner,
+                                                      const uint8_t *__restrict__ btype,
+                                                      const float4 *__restrict__ rec, const int *__restrict__ orig_id,
+                                                      curandState *__restrict__ rng,
+                                                      const long long *__restrict__ d_step, float *__restrict__ fout,
+                                                      int integrate_flag, TileCfg tc, int box_cap)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     float4 *box = reinterpret_cast<float4 *>(smraw);
     __shared__ TileShared ts;
+    __shared__ float Ao[kPartOut][kMaxFGroups][3];
+    __shared__ int outP[kPartOut];
+    __shared__ int nout;
     const ParticleParams &pp = *ppd;
     const long long step = *d_step;
     const float *__restrict__ Xc = (step & 1) ? X1 : X0;   // x_t
@@ -173,6 +228,34 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
     const int nn[3] = {g.nx, g.ny, g.nz};
     int r0, r1;
     tile_range(tc, N, kPartWindow, r0, r1);
+    // the tile's fixed box: stencil origins lo[j] .. lo[j] + span[j]
+    int lo[3] = {0, 0, 0}, span[3] = {-1, -1, -1}, E[3] = {0, 0, 0};
+    bool staged = false;
+    if (tc.start) {
+        int bits = 0;
+        while ((1 << bits) < tc.codes) bits++;
+        const uint32_t k0 = (uint32_t)blockIdx.x * (uint32_t)tc.codes;
+        const int nbr[3] = {1 << ((bits + 2) / 3), 1 << ((bits + 1) / 3), 1 << (bits / 3)};
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const int c0 = 4 * compact3(k0 >> j);
+            const int c1 = min(c0 + 4 * nbr[j], nn[j]) - 1;
+            lo[j] = c0 - P / 2 - tc.margin;
+            span[j] = c1 - c0 + (P % 2 == 0 ? 1 : 0) + 2 * tc.margin;
+            E[j] = span[j] + P + 1;
+        }
+        staged = E[0] <= kMaxBoxEdge && E[1] <= kMaxBoxEdge && E[2] <= kMaxBoxEdge &&
+                 (long long)((((E[0] | 1) * E[1]) | 1)) * E[2] <= box_cap;
+    }
+    const int E0 = E[0] | 1, E01 = (E0 * E[1]) | 1;   // odd pitches (16-byte records)
+    if (staged) {
+        if (threadIdx.x < 3) {
+            ts.ref[threadIdx.x] = lo[threadIdx.x];
+            ts.lo[threadIdx.x] = 0;
+        }
+        __syncthreads();
+        tile_tables(ts, g.nx, g.ny, g.nz, E);
+    }
     for (int c0 = r0; c0 < r1; c0 += blockDim.x) {
         const int p = c0 + threadIdx.x;
         const bool act = p < r1;
@@ -185,65 +268,67 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
             fl = pflags[p];
         }
         const unsigned fm = (fl >> 8) & 0xffu;
-        float Wx[P + 1], Wy[P + 1], Wz[P + 1];
         int gs[3] = {0, 0, 0};
         if (fm) {
-            gs[0] = stencil_fast<P>(x[0], inv[0], pp.quirk4, Wx);
-            gs[1] = stencil_fast<P>(x[1], inv[1], pp.quirk4, Wy);
-            gs[2] = stencil_fast<P>(x[2], inv[2], pp.quirk4, Wz);
+            gs[0] = stencil_origin<P>(x[0], inv[0]);
+            gs[1] = stencil_origin<P>(x[1], inv[1]);
+            gs[2] = stencil_origin<P>(x[2], inv[2]);
         }
-        if (threadIdx.x < 3) {
-            ts.ref[threadIdx.x] = stencil_origin<P>(Xc[3 * c0 + threadIdx.x], inv[threadIdx.x]);
-            ts.lo[threadIdx.x] = 0x7fffffff;
-            ts.hi[threadIdx.x] = -0x7fffffff;
+        if (threadIdx.x == 0) {
+            nout = 0;
+            ts.fm = 0u;
         }
-        if (threadIdx.x == 0) ts.fm = 0u;
         __syncthreads();
-        // 1. box of the stencil origins of the pass's particles that gather
-        int d[3], lo[3], hi[3];
+        // 1. box offset, or a slot in the helpers' list
+        int d[3], slot = -1;
+        bool inbox = false;
 #pragma unroll
-        for (int j = 0; j < 3; j++) {
-            d[j] = fm ? unwrap_delta(gs[j] - ts.ref[j], nn[j]) : 0;
-            lo[j] = fm ? d[j] : 0x7fffffff;
-            hi[j] = fm ? d[j] : -0x7fffffff;
-            for (int o = 16; o > 0; o >>= 1) {
-                lo[j] = min(lo[j], __shfl_xor_sync(0xffffffffu, lo[j], o));
-                hi[j] = max(hi[j], __shfl_xor_sync(0xffffffffu, hi[j], o));
+        for (int j = 0; j < 3; j++) d[j] = staged ? wrapi(gs[j] - lo[j], nn[j]) : 0;
+        if (fm) {
+            inbox = staged && d[0] <= span[0] && d[1] <= span[1] && d[2] <= span[2];
+            if (staged && !inbox) {
+                slot = atomicAdd(&nout, 1);
+                if (slot < kPartOut) outP[slot] = p;
             }
         }
         unsigned fmor = fm;
         for (int o = 16; o > 0; o >>= 1) fmor |= __shfl_xor_sync(0xffffffffu, fmor, o);
-        if ((threadIdx.x & 31) == 0 && fmor) {
-            for (int j = 0; j < 3; j++) {
-                atomicMin(&ts.lo[j], lo[j]);
-                atomicMax(&ts.hi[j], hi[j]);
-            }
-            atomicOr(&ts.fm, fmor);
-        }
+        if ((threadIdx.x & 31) == 0 && fmor) atomicOr(&ts.fm, fmor);
         __syncthreads();
         const unsigned fmall = ts.fm;
-        const int E[3] = {ts.hi[0] - ts.lo[0] + P + 1, ts.hi[1] - ts.lo[1] + P + 1, ts.hi[2] - ts.lo[2] + P + 1};
-        // odd row/plane pitches (in 16-byte records) spread neighbouring rows over the
-        // shared-memory bank groups
-        const int E0 = E[0] | 1, E01 = (E0 * E[1]) | 1;
-        const long long Vl = fmall ? (long long)E01 * E[2] : 0;
-        const bool staged = Vl > 0 && Vl <= box_cap && E[0] <= kMaxBoxEdge && E[1] <= kMaxBoxEdge &&
-                            E[2] <= kMaxBoxEdge;
-        if (staged) tile_tables(ts, g.nx, g.ny, g.nz, E);
-        __syncthreads();
+        const int nhelp = min(nout, kPartOut);
         int fg = 0;
         while (fg < pp.nfg && !((fmall >> fg) & 1u)) fg++;
-        // 2. start staging the first force group's box, compute bonds meanwhile
+        // 2. start staging the first force group's box
         if (staged && fg < pp.nfg) {
             const float4 *rf = rec + (long long)fg * g.M;
             tile_for_each(ts, E, E0, E01, [&](int v, int m) { cp_async16p(box + v, rf + m); });
             asm volatile("cp.async.commit_group;\n" ::: "memory");
         }
+        // 3. helpers gather the out-of-box particles of every group from global memory
+        if (threadIdx.x < nhelp) {
+            const int ph = outP[threadIdx.x];
+            const uint32_t flh = pflags[ph];
+            float Hx[P + 1], Hy[P + 1], Hz[P + 1];
+            int hs[3];
+            hs[0] = stencil_fast<P>(Xc[3 * ph], inv[0], pp.quirk4, Hx);
+            hs[1] = stencil_fast<P>(Xc[3 * ph + 1], inv[1], pp.quirk4, Hy);
+            hs[2] = stencil_fast<P>(Xc[3 * ph + 2], inv[2], pp.quirk4, Hz);
+            for (int h = 0; h < pp.nfg; h++)
+                if ((flh >> (8 + h)) & 1u) gather_global<P>(g, rec + (long long)h * g.M, hs, Hx, Hy, Hz, Ao[threadIdx.x][h]);
+        }
+        // 4. bonds
         float f[3] = {0.f, 0.f, 0.f};
         if (act) bond_force(g, pp, p, x, Xc, nb, partner, btype, f);
-        const int base = (d[2] - ts.lo[2]) * E01 + (d[1] - ts.lo[1]) * E0 + (d[0] - ts.lo[0]);
+        const int base = d[2] * E01 + d[1] * E0 + d[0];
         const float qp = (act && q) ? q[p] : 0.f;
-        // 3. gather each force group in group order
+        float Wx[P + 1], Wy[P + 1], Wz[P + 1];
+        if (fm) {
+            stencil_fast<P>(x[0], inv[0], pp.quirk4, Wx);
+            stencil_fast<P>(x[1], inv[1], pp.quirk4, Wy);
+            stencil_fast<P>(x[2], inv[2], pp.quirk4, Wz);
+        }
+        // 5. gather each force group in group order
         bool first = true;
         for (; fg < pp.nfg; fg++) {
             if (!((fmall >> fg) & 1u)) continue;
@@ -255,12 +340,15 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
                     asm volatile("cp.async.commit_group;\n" ::: "memory");
                 }
                 asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-                __syncthreads();
+                __syncthreads();   // every thread's copies have landed (and the helpers' results)
+            } else if (first) {
+                __syncthreads();   // the helpers' results are visible
             }
             first = false;
             if (!((fl >> (8 + fg)) & 1u)) continue;
-            float a0 = 0.f, a1 = 0.f, a2 = 0.f;
-            if (staged) {
+            float a[3];
+            if (inbox) {
+                float a0 = 0.f, a1 = 0.f, a2 = 0.f;
 #pragma unroll
                 for (int e = 0; e <= P; e++) {
 #pragma unroll
@@ -268,63 +356,48 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
                         const float wyz = Wy[b] * Wz[e];
                         const int row = base + e * E01 + b * E0;
 #pragma unroll
-                        for (int a = 0; a <= P; a++) {
-                            const float w = Wx[a] * wyz;
-                            const float4 r = box[row + a];
+                        for (int aa = 0; aa <= P; aa++) {
+                            const float w = Wx[aa] * wyz;
+                            const float4 r = box[row + aa];
                             a0 = __fmaf_rn(r.x, w, a0);
                             a1 = __fmaf_rn(r.y, w, a1);
                             a2 = __fmaf_rn(r.z, w, a2);
                         }
                     }
                 }
+                a[0] = a0;
+                a[1] = a1;
+                a[2] = a2;
+            } else if (slot >= 0 && slot < kPartOut) {
+                a[0] = Ao[slot][fg][0];
+                a[1] = Ao[slot][fg][1];
+                a[2] = Ao[slot][fg][2];
             } else {
-                const long long plane = (long long)g.nx * g.ny;
-                int ix[P + 1], iy[P + 1], iz[P + 1];
-#pragma unroll
-                for (int i = 0; i <= P; i++) {
-                    ix[i] = wrapi(gs[0] + i, g.nx);
-                    iy[i] = wrapi(gs[1] + i, g.ny);
-                    iz[i] = wrapi(gs[2] + i, g.nz);
-                }
-#pragma unroll 1
-                for (int e = 0; e <= P; e++) {
-                    const float wz = sel<P>(Wz, e);
-                    const float4 *rz = rf + plane * sel<P>(iz, e);
-#pragma unroll
-                    for (int b = 0; b <= P; b++) {
-                        const float4 *ry = rz + (long long)g.nx * iy[b];
-                        const float wyz = Wy[b] * wz;
-#pragma unroll
-                        for (int a = 0; a <= P; a++) {
-                            const float w = Wx[a] * wyz;
-                            const float4 r = __ldg(ry + ix[a]);
-                            a0 = __fmaf_rn(r.x, w, a0);
-                            a1 = __fmaf_rn(r.y, w, a1);
-                            a2 = __fmaf_rn(r.z, w, a2);
-                        }
-                    }
-                }
+                gather_global<P>(g, rf, gs, Wx, Wy, Wz, a);
             }
             if ((pp.fg_qweighted >> fg) & 1u) {
-                f[0] = __fmaf_rn(a0, qp, f[0]);
-                f[1] = __fmaf_rn(a1, qp, f[1]);
-                f[2] = __fmaf_rn(a2, qp, f[2]);
+                f[0] = __fmaf_rn(a[0], qp, f[0]);
+                f[1] = __fmaf_rn(a[1], qp, f[1]);
+                f[2] = __fmaf_rn(a[2], qp, f[2]);
             } else {
-                f[0] += a0;
-                f[1] += a1;
-                f[2] += a2;
+                f[0] += a[0];
+                f[1] += a[1];
+                f[2] += a[2];
             }
         }
-        // 4. integrate
+        // 6. integrate
         if (act) {
             if (fout) {
                 fout[3 * p] = f[0];
                 fout[3 * p + 1] = f[1];
                 fout[3 * p + 2] = f[2];
             }
-            if (integrate_flag) integrate(g, pp, p, fl, x, f, Xn, noise, orig_id, rng, step);
+            if (integrate_flag) {
+                const float xr[3] = {Xc[3 * p], Xc[3 * p + 1], Xc[3 * p + 2]};
+                integrate(g, pp, p, fl, xr, f, Xn, noise, orig_id, rng, step);
+            }
         }
-        __syncthreads();   // the box and ts are reused by the next pass
+        __syncthreads();   // the box, nout and the helpers' results are reused by the next pass
     }
 }
 
@@ -430,7 +503,7 @@ static void part_launch(const Geom &g, const ParticleParams *ppd, int N, float *
 {
     const int nbk = tc.start ? (tc.nkeys + tc.codes - 1) / tc.codes : (N + kPartWindow - 1) / kPartWindow;
     const int threads = tc.start ? tc.threads : 256;
-    const int cap = tc.start ? std::min(tc.box, kPartBox) : kPartBox;
+    const int cap = tc.start ? std::min(tc.pbox, kPartBox) : 0;
     const size_t smem = (size_t)cap * sizeof(float4);
     k_particles<P><<<nbk, threads, smem, st>>>(g, ppd, N, X0, X1, noise, pflags, q, nb, partner, btype, rec, orig_id,
                                                reinterpret_cast<curandState *>(rng), d_step, fout, integrate, tc, cap);
