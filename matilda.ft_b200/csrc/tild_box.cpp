@@ -769,6 +769,7 @@ void Box::allocDevice()
         if (l->ns > kMaxStages) fail(TILD_ERR_UNSUPPORTED, "grid size factors into too many stages");
     dStep = dalloc<long long>(1);
     dKs = dalloc<KSpace>(1);
+    dUk = dalloc<float>((size_t)std::max<size_t>(1, potentials.size()) * g.hstride);
     dPp = dalloc<ParticleParams>(1);
     const int TXz = 8;
     nblkZ = ((g.nxh + TXz - 1) / TXz) * g.ny;
@@ -881,6 +882,10 @@ void Box::uploadFlags()
     for (int64_t s = 0; s < N; s++) fs[s] = fl[orig[s]];
     ck(cudaMemcpy(dFlags, fs.data(), 4 * N, cudaMemcpyHostToDevice), "upload flags");
     ck(cudaMemcpy(dKs, &ksHost, sizeof(KSpace), cudaMemcpyHostToDevice), "upload k-space plan");
+    if (ksHost.npots > 0) {
+        ck(launch_uk_table(geom, dKs, dUk, stream), "u(k) table");
+        ck(cudaStreamSynchronize(stream), "u(k) table");
+    }
     ck(cudaMemcpy(dPp, &ppHost, sizeof(ParticleParams), cudaMemcpyHostToDevice), "upload particle params");
 }
 
@@ -955,7 +960,7 @@ void Box::enqueueStep(bool energy, bool integrate, float *fout_dev)
         mark(STAGE_XFWD);
         ck(launch_ypass(g, ly, nd, 0, dH, st), "fft y forward");
         mark(STAGE_YFWD);
-        ck(launch_kspace_z(g, lz, ksHost, dKs, dH, dHg, dEpart, energy ? 1 : 0, nfg > 0 ? 1 : 0, nullptr, st), "kspace");
+        ck(launch_kspace_z(g, lz, ksHost, dKs, dH, dUk, dHg, dEpart, energy ? 1 : 0, nfg > 0 ? 1 : 0, nullptr, st), "kspace");
         if (energy && ksHost.neterms > 0) ck(launch_reduce_partials(dEpart, nblkZ, ksHost.neterms, dRes, st), "reduce");
         mark(STAGE_KSPACE);
         if (nfg > 0) {
@@ -990,7 +995,7 @@ void Box::enqueueEnergyOnly()
         ck(launch_deposit(g, ppHost, dX[0], dX[1], dStep, dFlags, dQ, dDep, dDepFix, deterministic, tileCfg(), st), "deposit");
         ck(launch_xfwd(g, lx, npair, nd, dDep, deterministic ? dDepFix : nullptr, dH, st), "fft x forward");
         ck(launch_ypass(g, ly, nd, 0, dH, st), "fft y forward");
-        ck(launch_kspace_z(g, lz, ksHost, dKs, dH, dHg, dEpart, 1, 0, nullptr, st), "kspace energy");
+        ck(launch_kspace_z(g, lz, ksHost, dKs, dH, dUk, dHg, dEpart, 1, 0, nullptr, st), "kspace energy");
         ck(launch_reduce_partials(dEpart, nblkZ, ksHost.neterms, dRes, st), "reduce");
     }
     ck(launch_bond_energy(g, ppHost, dPp, dX[0], dX[1], dStep, dNb, dPartner, dBtype, dBpart, nullptr, st), "bond energy");

@@ -182,6 +182,7 @@ private:
     float4 *dRec = nullptr;
     long long *dStep = nullptr;
     KSpace *dKs = nullptr;
+    float *dUk = nullptr;   // FP32 û(k) shape table, one half-spectrum field per potential
     ParticleParams *dPp = nullptr;
     double *dEpart = nullptr, *dBpart = nullptr, *dRes = nullptr;
     KSpace *hKsPinned = nullptr;

@@ -145,9 +145,11 @@ cudaError_t launch_xfwd(const Geom &g, const FftLine &lx, int npair, int nd, con
                         const unsigned long long *dep_fixed, float2 *H, cudaStream_t st);
 cudaError_t launch_ypass(const Geom &g, const FftLine &ly, int nfields, int inverse, float2 *H,
                          cudaStream_t st);
-cudaError_t launch_kspace_z(const Geom &g, const FftLine &lz, const KSpace &ks,
-                            const KSpace *ks_dev, const float2 *H, float2 *Hg, double *epart,
-                            int energy, int forces, int *nblocks_out, cudaStream_t st);
+cudaError_t launch_kspace_z(const Geom &g, const FftLine &lz, const KSpace &ks, const KSpace *ks_dev,
+                            const float2 *H, const float *uk, float2 *Hg, double *epart, int energy, int forces,
+                            int *nblocks_out, cudaStream_t st);
+// FP32 table of every potential's û(k) shape (amplitude 1) over the half spectrum
+cudaError_t launch_uk_table(const Geom &g, const KSpace *ks_dev, float *tab, cudaStream_t st);
 cudaError_t launch_xinv(const Geom &g, const FftLine &lx, int nfg, const float2 *Hg, float4 *rec,
                         cudaStream_t st);
 cudaError_t launch_particles(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd,

@@ -42,101 +42,166 @@ __device__ __forceinline__ unsigned fdiv(unsigned i, const FastDiv &f)
     return f.d == 1 ? i : __umulhi(i, f.m);
 }
 
+__device__ __forceinline__ float2 mul_mi(float2 v) { return make_float2(v.y, -v.x); }   // -i v
+__device__ __forceinline__ float2 mul_pi(float2 v) { return make_float2(-v.y, v.x); }   // +i v
+
+// In-register DFT of R points, v[q] <- sum_s v[s] W_R^{+-qs} (forward sign -), R = 2, 3, 4, 5, 8.
+template <bool INV>
+__device__ __forceinline__ void dft4(float2 &a0, float2 &a1, float2 &a2, float2 &a3)
+{
+    const float2 t0 = cadd(a0, a2), t1 = csub(a0, a2), t2 = cadd(a1, a3), t3 = csub(a1, a3);
+    const float2 m = INV ? mul_pi(t3) : mul_mi(t3);
+    a0 = cadd(t0, t2);
+    a1 = cadd(t1, m);
+    a2 = csub(t0, t2);
+    a3 = csub(t1, m);
+}
+
+template <bool INV, int R>
+__device__ __forceinline__ void dft_reg(float2 *v)
+{
+    if (R == 2) {
+        const float2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if (R == 4) {
+        dft4<INV>(v[0], v[1], v[2], v[3]);
+    } else if (R == 8) {
+        // radix-2 split into even and odd outputs, W_8 twiddles, two 4-point DFTs
+        const float c = 0.70710678118654752f;
+        float2 a0 = cadd(v[0], v[4]), b0 = csub(v[0], v[4]);
+        float2 a1 = cadd(v[1], v[5]), b1 = csub(v[1], v[5]);
+        float2 a2 = cadd(v[2], v[6]), b2 = csub(v[2], v[6]);
+        float2 a3 = cadd(v[3], v[7]), b3 = csub(v[3], v[7]);
+        if (INV) {
+            b1 = make_float2(c * (b1.x - b1.y), c * (b1.x + b1.y));     // * W_8^-1
+            b2 = mul_pi(b2);                                            // * W_8^-2
+            b3 = make_float2(-c * (b3.x + b3.y), c * (b3.x - b3.y));    // * W_8^-3
+        } else {
+            b1 = make_float2(c * (b1.x + b1.y), c * (b1.y - b1.x));     // * W_8^1
+            b2 = mul_mi(b2);                                            // * W_8^2
+            b3 = make_float2(c * (b3.y - b3.x), -c * (b3.x + b3.y));    // * W_8^3
+        }
+        dft4<INV>(a0, a1, a2, a3);
+        dft4<INV>(b0, b1, b2, b3);
+        v[0] = a0; v[2] = a1; v[4] = a2; v[6] = a3;
+        v[1] = b0; v[3] = b1; v[5] = b2; v[7] = b3;
+    } else if (R == 3) {
+        const float s3 = INV ? 0.86602540378443865f : -0.86602540378443865f;
+        const float2 a0 = v[0], t = cadd(v[1], v[2]), u = csub(v[1], v[2]);
+        const float2 m = make_float2(a0.x - 0.5f * t.x, a0.y - 0.5f * t.y);
+        const float2 iu = make_float2(-s3 * u.y, s3 * u.x);   // i * s3 * u
+        v[0] = cadd(a0, t);
+        v[1] = cadd(m, iu);
+        v[2] = csub(m, iu);
+    } else if (R == 5) {
+        const float c1 = 0.30901699437494742f, c2 = -0.80901699437494742f;
+        const float s1 = INV ? -0.95105651629515357f : 0.95105651629515357f;
+        const float s2 = INV ? -0.58778525229247313f : 0.58778525229247313f;
+        const float2 a0 = v[0];
+        const float2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]), t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+        const float2 m1 = make_float2(a0.x + c1 * t1.x + c2 * t2.x, a0.y + c1 * t1.y + c2 * t2.y);
+        const float2 m2 = make_float2(a0.x + c2 * t1.x + c1 * t2.x, a0.y + c2 * t1.y + c1 * t2.y);
+        // n1 = s1 t3 + s2 t4, n2 = s2 t3 - s1 t4; b1 = m1 - i n1, b4 = m1 + i n1,
+        // b2 = m2 - i n2, b3 = m2 + i n2
+        const float2 n1 = make_float2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y);
+        const float2 n2 = make_float2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y);
+        v[0] = make_float2(a0.x + t1.x + t2.x, a0.y + t1.y + t2.y);
+        v[1] = make_float2(m1.x + n1.y, m1.y - n1.x);
+        v[4] = make_float2(m1.x - n1.y, m1.y + n1.x);
+        v[2] = make_float2(m2.x + n2.y, m2.y - n2.x);
+        v[3] = make_float2(m2.x - n2.y, m2.y + n2.x);
+    }
+}
+
+// One radix-R Stockham stage over L lines: butterfly i of line l reads i + q*nb, is
+// twiddled by W_{pR}^{q*(i mod p)} and writes (i - i mod p)*R + i mod p + q*p.
+template <bool INV, int R>
+__device__ __forceinline__ void fft_stage(const float2 *__restrict__ src, float2 *__restrict__ dst, int L, int lp,
+                                          int ls, int n, int p, const FastDiv &dp, const FastDiv &dsplit,
+                                          bool line_fast, const float2 *tw)
+{
+    const int nb = n / R, stride = n / (p * R);
+    const int total = L * nb, snb = nb * ls, sp = p * ls;
+    for (int w = threadIdx.x; w < total; w += blockDim.x) {
+        int l, i;
+        if (line_fast) {
+            i = (int)fdiv((unsigned)w, dsplit);
+            l = w - i * L;
+        } else {
+            l = (int)fdiv((unsigned)w, dsplit);
+            i = w - l * nb;
+        }
+        const int blk = (int)fdiv((unsigned)i, dp);
+        const int k = i - blk * p;
+        const int sb = l * lp + i * ls, db = l * lp + (blk * p * R + k) * ls;
+        float2 v[R];
+#pragma unroll
+        for (int q = 0; q < R; q++) v[q] = src[sb + q * snb];
+        if (k) {
+            const int ks = k * stride;
+#pragma unroll
+            for (int q = 1; q < R; q++) v[q] = cmul(v[q], twid<INV>(tw, q * ks));
+        }
+        dft_reg<INV, R>(v);
+#pragma unroll
+        for (int q = 0; q < R; q++) dst[db + q * sp] = v[q];
+    }
+}
+
+// Generic radix stage: b_q = sum_s a_s W_{pR}^{s k} W_R^{q s}.
+template <bool INV>
+__device__ void fft_stage_generic(const float2 *__restrict__ src, float2 *__restrict__ dst, int L, int lp, int ls,
+                                  int n, int R, int p, const FastDiv &dp, const FastDiv &dsplit, bool line_fast,
+                                  const float2 *tw)
+{
+    const int nb = n / R, stride = n / (p * R), nR = n / R;
+    for (int w = threadIdx.x; w < L * nb; w += blockDim.x) {
+        int l, i;
+        if (line_fast) {
+            i = (int)fdiv((unsigned)w, dsplit);
+            l = w - i * L;
+        } else {
+            l = (int)fdiv((unsigned)w, dsplit);
+            i = w - l * nb;
+        }
+        const int k = i - p * (int)fdiv((unsigned)i, dp);
+        const float2 *s = src + l * lp;
+        float2 *d = dst + l * lp;
+        const int j = (i - k) * R + k;
+        for (int qq = 0; qq < R; qq++) {
+            float2 acc = make_float2(0.f, 0.f);
+            for (int ss = 0; ss < R; ss++) {
+                float2 v = s[(i + ss * nb) * ls];
+                if (k && ss) v = cmul(v, twid<INV>(tw, ss * k * stride));
+                const int e = (qq * ss) % R;
+                if (e) v = cmul(v, twid<INV>(tw, e * nR));
+                acc = cadd(acc, v);
+            }
+            d[(j + qq * p) * ls] = acc;
+        }
+    }
+}
+
+// Shared-memory Stockham FFT of L lines of length n (mixed radix, natural order in and
+// out).  Element t of line l lives at l*lp + t*ls.  line_fast: consecutive threads take
+// consecutive lines (lines interleaved, ls = L), else consecutive butterflies of a line.
+// dL divides by L.  Returns the buffer holding the result.
 template <bool INV>
 __device__ float2 *fft_lines(float2 *a, float2 *b, int L, int lp, int ls, const FftLine &pl,
                              const float2 *tw, bool line_fast, const FastDiv &dL)
 {
     const int n = pl.n;
     for (int s = 0; s < pl.ns; ++s) {
-        const int R = pl.R[s], p = pl.P[s], nb = n / R, stride = n / (p * R);
-        const int total = L * nb;
-        const FastDiv dp = pl.dP[s], dnb = pl.dNB[s];
-        for (int w = threadIdx.x; w < total; w += blockDim.x) {
-            int l, i;
-            if (line_fast) {
-                i = (int)fdiv((unsigned)w, dL);
-                l = w - i * L;
-            } else {
-                l = (int)fdiv((unsigned)w, dnb);
-                i = w - l * nb;
-            }
-            const int k = i - p * (int)fdiv((unsigned)i, dp);
-            const float2 *src = a + l * lp;
-            float2 *dst = b + l * lp;
-            const int j = (i - k) * R + k;
-            if (R == 2) {
-                float2 a0 = src[i * ls], a1 = src[(i + nb) * ls];
-                if (k) a1 = cmul(a1, twid<INV>(tw, k * stride));
-                dst[j * ls] = cadd(a0, a1);
-                dst[(j + p) * ls] = csub(a0, a1);
-            } else if (R == 4) {
-                float2 a0 = src[i * ls], a1 = src[(i + nb) * ls], a2 = src[(i + 2 * nb) * ls],
-                       a3 = src[(i + 3 * nb) * ls];
-                if (k) {
-                    a1 = cmul(a1, twid<INV>(tw, k * stride));
-                    a2 = cmul(a2, twid<INV>(tw, 2 * k * stride));
-                    a3 = cmul(a3, twid<INV>(tw, 3 * k * stride));
-                }
-                const float2 t0 = cadd(a0, a2), t1 = csub(a0, a2), t2 = cadd(a1, a3), t3 = csub(a1, a3);
-                // forward: b1 = t1 - i t3, b3 = t1 + i t3; inverse swaps them
-                const float2 mi = INV ? make_float2(-t3.y, t3.x) : make_float2(t3.y, -t3.x);
-                dst[j * ls] = cadd(t0, t2);
-                dst[(j + p) * ls] = cadd(t1, mi);
-                dst[(j + 2 * p) * ls] = csub(t0, t2);
-                dst[(j + 3 * p) * ls] = csub(t1, mi);
-            } else if (R == 3) {
-                float2 a0 = src[i * ls], a1 = src[(i + nb) * ls], a2 = src[(i + 2 * nb) * ls];
-                if (k) {
-                    a1 = cmul(a1, twid<INV>(tw, k * stride));
-                    a2 = cmul(a2, twid<INV>(tw, 2 * k * stride));
-                }
-                const float s3 = INV ? 0.86602540378443865f : -0.86602540378443865f;
-                const float2 t = cadd(a1, a2), u = csub(a1, a2);
-                const float2 m = make_float2(a0.x - 0.5f * t.x, a0.y - 0.5f * t.y);
-                // b1 = m + i*s3*u, b2 = m - i*s3*u
-                const float2 iu = make_float2(-s3 * u.y, s3 * u.x);
-                dst[j * ls] = cadd(a0, t);
-                dst[(j + p) * ls] = cadd(m, iu);
-                dst[(j + 2 * p) * ls] = csub(m, iu);
-            } else if (R == 5) {
-                float2 a0 = src[i * ls], a1 = src[(i + nb) * ls], a2 = src[(i + 2 * nb) * ls],
-                       a3 = src[(i + 3 * nb) * ls], a4 = src[(i + 4 * nb) * ls];
-                if (k) {
-                    a1 = cmul(a1, twid<INV>(tw, k * stride));
-                    a2 = cmul(a2, twid<INV>(tw, 2 * k * stride));
-                    a3 = cmul(a3, twid<INV>(tw, 3 * k * stride));
-                    a4 = cmul(a4, twid<INV>(tw, 4 * k * stride));
-                }
-                const float c1 = 0.30901699437494742f, c2 = -0.80901699437494742f;
-                const float s1 = INV ? -0.95105651629515357f : 0.95105651629515357f;
-                const float s2 = INV ? -0.58778525229247313f : 0.58778525229247313f;
-                const float2 t1 = cadd(a1, a4), t2 = cadd(a2, a3), t3 = csub(a1, a4), t4 = csub(a2, a3);
-                const float2 m1 = make_float2(a0.x + c1 * t1.x + c2 * t2.x, a0.y + c1 * t1.y + c2 * t2.y);
-                const float2 m2 = make_float2(a0.x + c2 * t1.x + c1 * t2.x, a0.y + c2 * t1.y + c1 * t2.y);
-                // n1 = s1 t3 + s2 t4, n2 = s2 t3 - s1 t4; b1 = m1 - i n1, b4 = m1 + i n1,
-                // b2 = m2 - i n2, b3 = m2 + i n2
-                const float2 n1 = make_float2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y);
-                const float2 n2 = make_float2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y);
-                dst[j * ls] = make_float2(a0.x + t1.x + t2.x, a0.y + t1.y + t2.y);
-                dst[(j + p) * ls] = make_float2(m1.x + n1.y, m1.y - n1.x);
-                dst[(j + 4 * p) * ls] = make_float2(m1.x - n1.y, m1.y + n1.x);
-                dst[(j + 2 * p) * ls] = make_float2(m2.x + n2.y, m2.y - n2.x);
-                dst[(j + 3 * p) * ls] = make_float2(m2.x - n2.y, m2.y + n2.x);
-            } else {
-                // generic radix: b_q = sum_s a_s W_{pR}^{s k} W_R^{q s}
-                const int nR = n / R;
-                for (int qq = 0; qq < R; qq++) {
-                    float2 acc = make_float2(0.f, 0.f);
-                    for (int ss = 0; ss < R; ss++) {
-                        float2 v = src[(i + ss * nb) * ls];
-                        if (k && ss) v = cmul(v, twid<INV>(tw, ss * k * stride));
-                        const int e = (qq * ss) % R;
-                        if (e) v = cmul(v, twid<INV>(tw, e * nR));
-                        acc = cadd(acc, v);
-                    }
-                    dst[(j + qq * p) * ls] = acc;
-                }
-            }
+        const int R = pl.R[s], p = pl.P[s];
+        const FastDiv &dsplit = line_fast ? dL : pl.dNB[s];
+        switch (R) {
+            case 8: fft_stage<INV, 8>(a, b, L, lp, ls, n, p, pl.dP[s], dsplit, line_fast, tw); break;
+            case 4: fft_stage<INV, 4>(a, b, L, lp, ls, n, p, pl.dP[s], dsplit, line_fast, tw); break;
+            case 2: fft_stage<INV, 2>(a, b, L, lp, ls, n, p, pl.dP[s], dsplit, line_fast, tw); break;
+            case 3: fft_stage<INV, 3>(a, b, L, lp, ls, n, p, pl.dP[s], dsplit, line_fast, tw); break;
+            case 5: fft_stage<INV, 5>(a, b, L, lp, ls, n, p, pl.dP[s], dsplit, line_fast, tw); break;
+            default: fft_stage_generic<INV>(a, b, L, lp, ls, n, R, p, pl.dP[s], dsplit, line_fast, tw); break;
         }
         __syncthreads();
         float2 *t = a;
@@ -181,8 +246,9 @@ __device__ __forceinline__ void tile_load_async(float2 *dst, int dpitch, const f
                                                 int cols, int valid)
 {
     const int cpr = cols >> 1;   // 16-byte chunks per row
+    const FastDiv dc = make_fastdiv_dev((unsigned)cpr);
     for (int e = threadIdx.x; e < rows * cpr; e += blockDim.x) {
-        const int r = e / cpr, c2 = (e - r * cpr) << 1;
+        const int r = (int)fdiv((unsigned)e, dc), c2 = (e - r * cpr) << 1;
         const int nv = valid - c2;
         const int bytes = nv >= 2 ? 16 : (nv == 1 ? 8 : 0);
         const float2 *s = bytes ? src + r * spitch + c2 : src;
@@ -232,8 +298,9 @@ __global__ void __launch_bounds__(256) k_xfwd(Geom g, FftLine lx, int nd, const 
     __syncthreads();
     const float2 *R = fft_lines<false>(A, B, L, n, 1, lx, tw, false, make_fastdiv_dev(L));
     const int nxh = g.nxh;
+    const FastDiv dh = make_fastdiv_dev((unsigned)nxh);
     for (int e = threadIdx.x; e < L * nxh; e += blockDim.x) {
-        const int l = e / nxh, k = e - l * nxh;
+        const int l = (int)fdiv((unsigned)e, dh), k = e - l * nxh;
         const long long gl = line0 + l;
         if (gl >= nlines) continue;
         const float2 zk = R[l * n + k], zm = R[l * n + (k == 0 ? 0 : n - k)];
@@ -245,8 +312,8 @@ __global__ void __launch_bounds__(256) k_xfwd(Geom g, FftLine lx, int nd, const 
 }
 
 // y-axis pass over TX half-spectrum columns of one z plane of field blockIdx.z.
-template <bool INV>
-__global__ void __launch_bounds__(256) k_ypass(Geom g, FftLine ly, float2 *__restrict__ H, int TX)
+template <bool INV, int TX>
+__global__ void __launch_bounds__(256) k_ypass(Geom g, FftLine ly, float2 *__restrict__ H)
 {
     extern __shared__ __align__(16) float2 sm[];
     const int ny = g.ny;
@@ -265,33 +332,60 @@ __global__ void __launch_bounds__(256) k_ypass(Geom g, FftLine ly, float2 *__res
 }
 
 // û(k) of each potential kind, FP64 (ps_potentialGaussian.cu:38-46,
-// ps_potentialErf2.cu:111-124, ps_potentialErfG.cu:177-190, ps_potentialCharges.cu:241-258).
-__device__ double uk_eval(const PotDev &p, double k2)
+// ps_potentialErf2.cu:111-124, ps_potentialErfG.cu:177-190, ps_potentialCharges.cu:241-258),
+// as amplitude x shape: the shape is fixed for a box, the amplitude follows the ramp.
+__device__ double uk_shape(const PotDev &p, double k2)
 {
     const double PI4 = 12.566370614359172953850573533118;
-    if (p.kind == POT_GAUSSIAN) return p.amp * exp(-0.5 * k2 * p.sig2);
+    if (p.kind == POT_GAUSSIAN) return exp(-0.5 * k2 * p.sig2);
     if (p.kind == POT_CHARGES) return k2 > 0.0 ? PI4 * p.lB * exp(-k2 * p.sig2) / k2 : 0.0;
     const double R = p.Rp;
     double t;
     if (k2 == 0.0) {
         t = PI4 * R * R * R / 3.0;
-        return p.kind == POT_ERF2 ? p.amp * t * t : p.amp * t;
+        return p.kind == POT_ERF2 ? t * t : t;
     }
     const double k = sqrt(k2);
     double sn, cs;
     sincos(R * k, &sn, &cs);
     t = PI4 * (sn - R * k * cs) / (k2 * k);
     const double gs = exp(-0.5 * k2 * p.sig2);
-    return p.kind == POT_ERF2 ? p.amp * gs * t * t : p.amp * gs * t;
+    return p.kind == POT_ERF2 ? gs * t * t : gs * t;
 }
+
+__device__ __forceinline__ double uk_amp(const PotDev &p) { return p.kind == POT_CHARGES ? 1.0 : p.amp; }
+
+__device__ __forceinline__ double uk_eval(const PotDev &p, double k2) { return uk_amp(p) * uk_shape(p, k2); }
 
 __device__ __forceinline__ int signed_index(int i, int n) { return (i < n - i) ? i : i - n; }
 
+// FP32 shape table of every potential over the half spectrum, layout of one density field
+// (the reference keeps û(k) as a precomputed FP32 array, ps_potential.cu:41-78).
+__global__ void k_uk_table(Geom g, const KSpace *__restrict__ ksp, float *__restrict__ tab)
+{
+    const KSpace &ks = *ksp;
+    const long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= g.hstride) return;
+    const int kx = (int)(o % g.hp);
+    const long long zy = o / g.hp;
+    const int y = (int)(zy % g.ny), z = (int)(zy / g.ny);
+    double k2 = 0.0;
+    if (kx < g.nxh) {
+        const double kxv = ks.twopi_over_L[0] * signed_index(kx, g.nx);
+        const double kyv = ks.twopi_over_L[1] * signed_index(y, g.ny);
+        const double kzv = ks.twopi_over_L[2] * signed_index(z, g.nz);
+        k2 = kxv * kxv + kyv * kyv + kzv * kzv;
+    }
+    for (int p = 0; p < ks.npots; p++)
+        tab[(long long)p * g.hstride + o] = kx < g.nxh ? (float)uk_shape(ks.pots[p], k2) : 0.f;
+}
+
 // Fused z pass: forward z FFT of every density field, k-space combine, gradient and
 // inverse z FFT of each gradient field; FP64 energies on request.
+template <int TX>
 __global__ void __launch_bounds__(256) k_kspace_z(Geom g, FftLine lz, const KSpace *__restrict__ ksp, const float2 *__restrict__ H,
-                                                  float2 *__restrict__ Hg, double *__restrict__ epart,
-                                                  int energy, int forces, int TX)
+                                                  const float *__restrict__ uk, float2 *__restrict__ Hg,
+                                                  double *__restrict__ epart, int energy, int forces)
 {
     extern __shared__ __align__(16) float2 sm[];
     const KSpace &ks = *ksp;
@@ -346,24 +440,32 @@ __global__ void __launch_bounds__(256) k_kspace_z(Geom g, FftLine lz, const KSpa
     }
     if (!forces) return;
 
+    __shared__ float tcoef[kMaxTerms];
+    __shared__ int tfg[kMaxTerms], tpot[kMaxTerms], tdf[kMaxTerms];
+    const int nterms = ks.nterms;
+    for (int t = threadIdx.x; t < nterms; t += blockDim.x) {
+        const KTerm &kt = ks.terms[t];
+        tcoef[t] = (float)(kt.mult * uk_amp(ks.pots[kt.pot]));
+        tfg[t] = kt.fgroup;
+        tpot[t] = kt.pot;
+        tdf[t] = kt.dfield;
+    }
+    __syncthreads();
     for (int f = 0; f < ks.nfg; f++) {
         for (int e = threadIdx.x; e < nz * TX; e += blockDim.x) {
             const int z = e / TX, c = e - z * TX, kx = kx0 + c;
-            double px = 0.0, py = 0.0;
+            float px = 0.f, py = 0.f;
             if (kx < g.nxh) {
-                const double kxv = ks.twopi_over_L[0] * signed_index(kx, g.nx);
-                const double kzv = ks.twopi_over_L[2] * signed_index(z, g.nz);
-                const double k2 = kxv * kxv + kyv * kyv + kzv * kzv;
-                for (int t = 0; t < ks.nterms; t++) {
-                    const KTerm &kt = ks.terms[t];
-                    if (kt.fgroup != f) continue;
-                    const double u = kt.mult * uk_eval(ks.pots[kt.pot], k2);
-                    const float2 r = R[z * nd * TX + kt.dfield * TX + c];
-                    px += u * r.x;
-                    py += u * r.y;
+                const long long o = ((long long)z * g.ny + y) * g.hp + kx;
+                for (int t = 0; t < nterms; t++) {
+                    if (tfg[t] != f) continue;
+                    const float u = tcoef[t] * __ldg(uk + tpot[t] * g.hstride + o);
+                    const float2 r = R[z * nd * TX + tdf[t] * TX + c];
+                    px = fmaf(u, r.x, px);
+                    py = fmaf(u, r.y, py);
                 }
             }
-            Phi[e] = make_float2((float)px, (float)py);
+            Phi[e] = make_float2(px, py);
         }
         __syncthreads();
         // x and y are fixed along a z line, so IFFT_z(-i k_x phi) = -i k_x IFFT_z(phi) and the
@@ -462,13 +564,15 @@ __global__ void __launch_bounds__(256) k_xinv(Geom g, FftLine lx, int nfg, const
 
 
 // ---- plans and launchers ----
+constexpr int kTXy = 16;   // half-spectrum columns per y-pass block
+constexpr int kTXz = 8;    // half-spectrum columns per z-pass block
 void init_fft_attributes()
 {
     set_max_smem(k_xfwd<true>, 200 * 1024);
     set_max_smem(k_xfwd<false>, 200 * 1024);
-    set_max_smem(k_ypass<false>, 200 * 1024);
-    set_max_smem(k_ypass<true>, 200 * 1024);
-    set_max_smem(k_kspace_z, 220 * 1024);
+    set_max_smem(k_ypass<false, kTXy>, 200 * 1024);
+    set_max_smem(k_ypass<true, kTXy>, 200 * 1024);
+    set_max_smem(k_kspace_z<kTXz>, 220 * 1024);
     set_max_smem(k_xinv, 200 * 1024);
 }
 
@@ -486,6 +590,7 @@ void build_fft_line(int n, FftLine &pl, float2 *dev_tw_dst)
         p *= r;
         m /= r;
     };
+    while (m % 8 == 0) push(8);
     while (m % 4 == 0) push(4);
     while (m % 2 == 0) push(2);
     while (m % 3 == 0) push(3);
@@ -517,23 +622,23 @@ cudaError_t launch_xfwd(const Geom &g, const FftLine &lx, int npair, int nd, con
 
 cudaError_t launch_ypass(const Geom &g, const FftLine &ly, int nfields, int inverse, float2 *H, cudaStream_t st)
 {
-    const int TX = 16;
+    constexpr int TX = kTXy;
     dim3 gy((g.nxh + TX - 1) / TX, g.nz, nfields);
     const size_t smy = (size_t)(2 * g.ny * TX + g.ny) * sizeof(float2);
-    if (inverse) k_ypass<true><<<gy, 256, smy, st>>>(g, ly, H, TX);
-    else k_ypass<false><<<gy, 256, smy, st>>>(g, ly, H, TX);
+    if (inverse) k_ypass<true, TX><<<gy, 256, smy, st>>>(g, ly, H);
+    else k_ypass<false, TX><<<gy, 256, smy, st>>>(g, ly, H);
     return cudaGetLastError();
 }
 
 cudaError_t launch_kspace_z(const Geom &g, const FftLine &lz, const KSpace &ks, const KSpace *ks_dev,
-                            const float2 *H, float2 *Hg, double *epart, int energy, int forces,
+                            const float2 *H, const float *uk, float2 *Hg, double *epart, int energy, int forces,
                             int *nblocks_out, cudaStream_t st)
 {
-    const int TX = 8;
+    constexpr int TX = kTXz;
     const int ndb = ks.nd < 2 ? 2 : ks.nd;
     dim3 grid((g.nxh + TX - 1) / TX, g.ny);
     const size_t sm = (size_t)(2 * ndb * g.nz * TX + g.nz * TX + g.nz) * sizeof(float2) + 8 * sizeof(double);
-    k_kspace_z<<<grid, 256, sm, st>>>(g, lz, ks_dev, H, Hg, epart, energy, forces, TX);
+    k_kspace_z<TX><<<grid, 256, sm, st>>>(g, lz, ks_dev, H, uk, Hg, epart, energy, forces);
     if (nblocks_out) *nblocks_out = (int)(grid.x * grid.y);
     return cudaGetLastError();
 }
@@ -546,6 +651,12 @@ cudaError_t launch_xinv(const Geom &g, const FftLine &lx, int nfg, const float2 
     const size_t smx = (size_t)(2 * L * g.nx + g.nx + (g.nx & 1) + 2 * L * g.hp) * sizeof(float2) +
                        (size_t)3 * nfg * L * g.nx * sizeof(float);
     k_xinv<<<(unsigned)((nlines + L - 1) / L), 256, smx, st>>>(g, lx, nfg, Hg, rec, L);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_uk_table(const Geom &g, const KSpace *ks_dev, float *tab, cudaStream_t st)
+{
+    k_uk_table<<<(unsigned)((g.hstride + 255) / 256), 256, 0, st>>>(g, ks_dev, tab);
     return cudaGetLastError();
 }
 
