@@ -2,6 +2,7 @@
 // k-space potential/gradient multiply (sm_100a).
 #include "tild_stencil.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -507,58 +508,63 @@ __global__ void __launch_bounds__(256) k_kspace_z(Geom g, FftLine lz, const KSpa
 
 // x-axis inverse pass: gradient fields 2t, 2t+1 packed as Z = G1 + i G2 (Hermitian
 // completion of both half spectra), one complex inverse FFT, real -> field 2t,
-// imaginary -> field 2t+1; then float4 records (x, y, z, 0) per force group.
+// imaginary -> field 2t+1; then float4 records (x, y, z, 0) per force group.  A block
+// takes L lines of every field: all rows are staged at once, every pair is transformed
+// in one pass over npair*L lines, and the records are written from the transform.
 __global__ void __launch_bounds__(256) k_xinv(Geom g, FftLine lx, int nfg, const float2 *__restrict__ Hg,
                                               float4 *__restrict__ rec, int L)
 {
     extern __shared__ __align__(16) float2 sm[];
-    const int n = g.nx, nf = 3 * nfg, nxh = g.nxh, hp = g.hp;
-    float2 *A = sm, *B = sm + L * n, *tw = sm + 2 * L * n, *St = tw + n + (n & 1);
-    float *Out = reinterpret_cast<float *>(St + 2 * L * hp);
+    const int n = g.nx, nf = 3 * nfg, npair = (nf + 1) / 2, nxh = g.nxh, hp = g.hp;
+    const int lines = npair * L;
+    const int stsz = nf * L * hp, bsz = lines * n;
+    float2 *A = sm, *St = sm + bsz, *tw = St + (stsz > bsz ? stsz : bsz);
     const long long nlines = (long long)g.ny * g.nz;
     const long long line0 = (long long)blockIdx.x * L;
     const int lv = (int)min((long long)L, nlines - line0);
-    const FastDiv dL = make_fastdiv_dev(L), dn = make_fastdiv_dev(n);
+    const FastDiv dn = make_fastdiv_dev(n), dL = make_fastdiv_dev(L);
     for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = lx.tw[t];
-    for (int pr = 0; pr < (nf + 1) / 2; pr++) {
+    // consecutive lines are consecutive rows of pitch hp: stage every field's rows
+    for (int f = 0; f < nf; f++)
+        tile_load_async(St + f * L * hp, hp, Hg + f * g.hstride + line0 * hp, hp, lv, hp, nxh);
+    cp_async_wait_all();
+    __syncthreads();
+    // line (pr, l) of A holds pair pr of line l
+    for (int e = threadIdx.x; e < bsz; e += blockDim.x) {
+        const int ln = (int)fdiv((unsigned)e, dn), x = e - ln * n;
+        const int pr = (int)fdiv((unsigned)ln, dL), l = ln - pr * L;
         const int f1 = 2 * pr, f2 = 2 * pr + 1;
-        // consecutive lines are consecutive rows of pitch hp: stage both fields' rows
-        tile_load_async(St, hp, Hg + f1 * g.hstride + line0 * hp, hp, lv, hp, nxh);
-        if (f2 < nf) tile_load_async(St + L * hp, hp, Hg + f2 * g.hstride + line0 * hp, hp, lv, hp, nxh);
-        cp_async_wait_all();
-        __syncthreads();
-        for (int e = threadIdx.x; e < L * n; e += blockDim.x) {
-            const int l = (int)fdiv((unsigned)e, dn), x = e - l * n;
-            float2 v = make_float2(0.f, 0.f);
-            if (l < lv) {
-                const bool direct = x < nxh;
-                const int kk = direct ? x : n - x;
-                float2 g1 = St[l * hp + kk];
-                float2 g2 = (f2 < nf) ? St[L * hp + l * hp + kk] : make_float2(0.f, 0.f);
-                if (kk == 0 || (n % 2 == 0 && kk == n / 2)) {
-                    g1.y = 0.f;
-                    g2.y = 0.f;
-                }
-                if (!direct) {
-                    g1.y = -g1.y;
-                    g2.y = -g2.y;
-                }
-                v = make_float2(g1.x - g2.y, g1.y + g2.x);
+        float2 v = make_float2(0.f, 0.f);
+        if (l < lv) {
+            const bool direct = x < nxh;
+            const int kk = direct ? x : n - x;
+            float2 g1 = St[(f1 * L + l) * hp + kk];
+            float2 g2 = (f2 < nf) ? St[(f2 * L + l) * hp + kk] : make_float2(0.f, 0.f);
+            if (kk == 0 || (n % 2 == 0 && kk == n / 2)) {
+                g1.y = 0.f;
+                g2.y = 0.f;
             }
-            A[e] = v;
+            if (!direct) {
+                g1.y = -g1.y;
+                g2.y = -g2.y;
+            }
+            v = make_float2(g1.x - g2.y, g1.y + g2.x);
         }
-        __syncthreads();
-        const float2 *R = fft_lines<true>(A, B, L, n, 1, lx, tw, false, dL);
-        for (int e = threadIdx.x; e < L * n; e += blockDim.x) {
-            Out[f1 * L * n + e] = R[e].x;
-            if (f2 < nf) Out[f2 * L * n + e] = R[e].y;
-        }
-        __syncthreads();
+        A[e] = v;
     }
+    __syncthreads();
+    const float2 *R = fft_lines<true>(A, St, lines, n, 1, lx, tw, false, dL);
+    // field k is component k % 2 of pair k / 2
+    auto comp = [&](int k, int l, int x) {
+        const float2 v = R[((k >> 1) * L + l) * n + x];
+        return (k & 1) ? v.y : v.x;
+    };
     for (int f = 0; f < nfg; f++) {
         float4 *rf = rec + f * g.M + line0 * n;
-        for (int e = threadIdx.x; e < lv * n; e += blockDim.x)
-            rf[e] = make_float4(Out[(3 * f) * L * n + e], Out[(3 * f + 1) * L * n + e], Out[(3 * f + 2) * L * n + e], 0.f);
+        for (int e = threadIdx.x; e < lv * n; e += blockDim.x) {
+            const int l = (int)fdiv((unsigned)e, dn), x = e - l * n;
+            rf[e] = make_float4(comp(3 * f, l, x), comp(3 * f + 1, l, x), comp(3 * f + 2, l, x), 0.f);
+        }
     }
 }
 
@@ -645,11 +651,12 @@ cudaError_t launch_kspace_z(const Geom &g, const FftLine &lz, const KSpace &ks, 
 
 cudaError_t launch_xinv(const Geom &g, const FftLine &lx, int nfg, const float2 *Hg, float4 *rec, cudaStream_t st)
 {
-    int L = 768 / g.nx;
-    L = L < 1 ? 1 : (L > 8 ? 8 : L);
+    const int nf = 3 * nfg, npair = (nf + 1) / 2;
+    int L = (2560 + npair * g.nx - 1) / (npair * g.nx);   // about 2.5k complex points per block
+    L = L < 1 ? 1 : (L > 16 ? 16 : L);
     const long long nlines = (long long)g.ny * g.nz;
-    const size_t smx = (size_t)(2 * L * g.nx + g.nx + (g.nx & 1) + 2 * L * g.hp) * sizeof(float2) +
-                       (size_t)3 * nfg * L * g.nx * sizeof(float);
+    const size_t bsz = (size_t)npair * L * g.nx, stsz = (size_t)nf * L * g.hp;
+    const size_t smx = (bsz + std::max(bsz, stsz) + g.nx) * sizeof(float2);
     k_xinv<<<(unsigned)((nlines + L - 1) / L), 256, smx, st>>>(g, lx, nfg, Hg, rec, L);
     return cudaGetLastError();
 }
