@@ -125,7 +125,7 @@ struct TileShared {
 
 __device__ __forceinline__ int unwrap_delta(int d, int n)
 {
-    int t = d % n;
+    int t = (d >= 0 && d < n) ? d : d % n;
     if (t < 0) t += n;
     if (t >= (n + 1) / 2) t -= n;
     return t;
@@ -169,19 +169,30 @@ __device__ __forceinline__ void tile_tables(TileShared &ts, int nx, int ny, int 
 }
 
 // Visit every box element (x fastest) with lanes along x: f(v, grid_offset), where v is
-// the element's offset in a box stored with row pitch p1 and plane pitch p2.
+// the element's offset in a box stored with row pitch p1 and plane pitch p2.  A row of
+// E[0] <= 32 elements takes E[0] consecutive threads; rows advance by counters, with no
+// division inside the loop.
 template <typename F>
 __device__ __forceinline__ void tile_for_each(const TileShared &ts, const int *E, int p1, int p2, F f)
 {
-    const int E0 = E[0], rows = E[1] * E[2];
-    const int xw = E0 <= 16 ? 16 : 32;   // x runs of 16 or 32 lanes
+    const int E0 = E[0], E1 = E[1], rows = E1 * E[2];
+    const int xw = E0 <= 32 ? E0 : 32;
     const int rpp = blockDim.x / xw;
-    const int lx0 = threadIdx.x % xw;
-    for (int row = threadIdx.x / xw; row < rows; row += rpp) {
-        const int lz = row / E[1], ly = row - lz * E[1];
+    if ((int)threadIdx.x >= rpp * xw) return;
+    int row = threadIdx.x / xw;
+    const int lx0 = threadIdx.x - row * xw;
+    int lz = row / E1, ly = row - lz * E1;
+    const int dz = rpp / E1, dy = rpp - dz * E1;
+    for (; row < rows; row += rpp) {
         const int rb = ts.zb[lz] + ts.yb[ly];
         const int vb = lz * p2 + ly * p1;
         for (int lx = lx0; lx < E0; lx += xw) f(vb + lx, rb + ts.xi[lx]);
+        lz += dz;
+        ly += dy;
+        if (ly >= E1) {
+            ly -= E1;
+            lz++;
+        }
     }
 }
 
@@ -189,6 +200,7 @@ __device__ __forceinline__ void tile_for_each(const TileShared &ts, const int *E
 // reference would send out of bounds still land on the grid.
 __device__ __forceinline__ int wrapi(int v, int n)
 {
+    if ((unsigned)v < (unsigned)n) return v;   // the common case: already on the grid
     v %= n;
     return v < 0 ? v + n : v;
 }
