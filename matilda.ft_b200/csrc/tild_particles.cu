@@ -266,6 +266,17 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
             x[1] = Xc[3 * p + 1];
             x[2] = Xc[3 * p + 2];
             fl = pflags[p];
+            // operands of the bonds and of the integrator, needed only after the gathers:
+            // start bringing them into L2 now
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(Xn + 3 * p));
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(noise + 3 * p));
+            if (nb) {
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(partner + p * pp.maxb));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(nb + p));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(btype + p * pp.maxb));
+            }
+            if (q) asm volatile("prefetch.global.L2 [%0];" ::"l"(q + p));
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(orig_id + p));
         }
         const unsigned fm = (fl >> 8) & 0xffu;
         int gs[3] = {0, 0, 0};
