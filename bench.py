@@ -195,6 +195,30 @@ def run_reference(args):
     return 0
 
 
+def cufft_times(torch, spec, nd, nfg, reps=20):
+    """cuFFT (through torch.fft) on the step's transforms: R2C of the nd density fields and
+    C2R of the 3*nfg gradient fields, same grid, device-timed."""
+    nx, ny, nz = (int(v) for v in spec.grid)
+    a = torch.randn((nd, nz, ny, nx), device="cuda", dtype=torch.float32)
+    b = torch.randn((3 * nfg, nz, ny, nx // 2 + 1), device="cuda", dtype=torch.complex64)
+    out = {}
+    for name, fn in (("forward", lambda: torch.fft.rfftn(a, dim=(1, 2, 3))),
+                     ("inverse", lambda: torch.fft.irfftn(b, s=(nz, ny, nx), dim=(1, 2, 3)))):
+        for _ in range(3):
+            fn()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        out[name] = e0.elapsed_time(e1) / reps
+    del a, b
+    return out
+
+
 def run_ours(args):
     import torch
     import tild_b200
@@ -269,6 +293,15 @@ def run_ours(args):
     if args.scale == 1.0 and os.path.exists(tf):   # captured on the full-size workload only
         traffic = json.load(open(tf)).get(KERNEL_NAMES[dom])
     step_bytes = sum(ab.values())
+    cf = cufft_times(torch, spec, info.n_density_fields, info.n_force_groups)
+    ours_fft = sum(stage_s[k] for k in ("fft_x_fwd", "fft_y_fwd", "kspace_z", "fft_y_inv", "fft_x_inv")) * 1e3
+    fft_cmp = {"ours_ms": ours_fft, "cufft_ms": cf["forward"] + cf["inverse"],
+               "cufft_forward_ms": cf["forward"], "cufft_inverse_ms": cf["inverse"],
+               "note": "ours = x/y/z passes incl. the k-space multiply and gradient and the float4 force "
+                       "records; cuFFT = R2C of the density fields + C2R of the gradient fields only"}
+    # sorts inside the timed region: every sort_interval steps, 6 kernels each
+    si = 10
+    nsort = (args.warmup + args.steps) // si - args.warmup // si
 
     if rank == 0:
         cpu = None
@@ -294,7 +327,8 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": METRIC, "steps_per_job": S,
                     "h2d_bytes_per_step": spec.N * 12 / S, "d2h_bytes_per_step": spec.N * 12 / S},
-            "gpu_launches": KERNELS_PER_STEP * args.steps,
+            "fft_vs_cufft": fft_cmp,
+            "gpu_launches": KERNELS_PER_STEP * args.steps + 6 * nsort,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
