@@ -191,6 +191,41 @@ int tild_run_script_file(const char *path, int device);
  * second-resolution timers only, timing.h:8-12).  *n receives the count written. */
 int tild_box_stage_times(tild_box *box, double *out, int nmax, int *n);
 
+/* ---- Job pool: many boxes on one GPU (batched replicas, served jobs) ----------------
+ * No counterpart in the reference, which runs one box per process (main.cu:21-156).  A
+ * job is a box whose script and particles are given but whose endBox has NOT been
+ * processed, plus a number of steps (doTimeStep without I/O, like tild_box_step).  A
+ * scheduler thread admits queued jobs in arrival order while their estimated device
+ * memory fits mem_budget_bytes and fewer than max_active (<= 0: no limit) are running,
+ * allocates them then (stream-ordered, no device-wide synchronisation), and keeps chunks
+ * of steps in flight on each job's own stream so that the jobs overlap on the GPU.  When a
+ * job finishes, its positions and thermo are copied to the host and its device memory is
+ * freed, so queued jobs enter while others are still running (continuous batching). */
+typedef struct tild_pool tild_pool;
+enum { TILD_JOB_QUEUED = 0, TILD_JOB_RUNNING = 1, TILD_JOB_DONE = 2, TILD_JOB_FAILED = 3 };
+
+int tild_pool_create(int device, int64_t mem_budget_bytes, int32_t max_active, tild_pool **out);
+/* Cancels queued jobs, waits for running ones, frees everything. */
+int tild_pool_destroy(tild_pool *pool);
+/* Hands `box` to the pool (its handle is emptied; still call tild_box_destroy on it).  The
+ * script is checked and the device memory estimated here: TILD_ERR_ARG if the job alone
+ * exceeds the budget, TILD_ERR_STATE if endBox was already processed; on an error the
+ * caller keeps the box. */
+int tild_pool_submit(tild_pool *pool, tild_box *box, int64_t nsteps, int64_t *job_id);
+/* state: TILD_JOB_*; times3 (may be NULL): submit, admission and completion times in
+ * seconds since the pool was created (0 until reached). */
+int tild_pool_status(tild_pool *pool, int64_t job_id, int32_t *state, int64_t *steps_done, double *times3);
+/* Blocks until the job is done; TILD_ERR_STATE with the job's error if it failed. */
+int tild_pool_wait(tild_pool *pool, int64_t job_id);
+/* Final positions x_out[n*3] (particle order, may be NULL) and up to nthermo values of
+ * tild_box_thermo's layout at the last step. */
+int tild_pool_result(tild_pool *pool, int64_t job_id, float *x_out, double *thermo_out, int32_t nthermo,
+                     int32_t *nwritten);
+/* Forgets a finished or failed job. */
+int tild_pool_release(tild_pool *pool, int64_t job_id);
+/* out[0..5]: queued, running, done, failed, device bytes reserved by running jobs, budget. */
+int tild_pool_stats(tild_pool *pool, int64_t *out, int32_t nout);
+
 #ifdef __cplusplus
 }
 #endif

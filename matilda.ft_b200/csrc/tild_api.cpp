@@ -7,9 +7,14 @@
 
 #include "tild_b200.h"
 #include "tild_box.h"
+#include "tild_pool.h"
 
 struct tild_box {
     tild::Box *impl;
+};
+
+struct tild_pool {
+    tild::Pool *impl;
 };
 
 namespace {
@@ -316,6 +321,83 @@ int tild_run_script_file(const char *path, int device)
     });
     delete box;
     return rc;
+}
+
+
+#define NEED_POOL                                                   \
+    if (!pool || !pool->impl) return fail(TILD_ERR_ARG, "pool is NULL")
+
+int tild_pool_create(int device, int64_t mem_budget_bytes, int32_t max_active, tild_pool **out)
+{
+    if (!out) return fail(TILD_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (mem_budget_bytes <= 0) return fail(TILD_ERR_ARG, "mem_budget_bytes must be > 0");
+    return guarded([&] { *out = new tild_pool{new tild::Pool(device, mem_budget_bytes, max_active)}; });
+}
+
+int tild_pool_destroy(tild_pool *pool)
+{
+    if (!pool) return TILD_OK;
+    delete pool->impl;
+    delete pool;
+    return TILD_OK;
+}
+
+int tild_pool_submit(tild_pool *pool, tild_box *box, int64_t nsteps, int64_t *job_id)
+{
+    NEED_POOL;
+    if (!box || !box->impl) return fail(TILD_ERR_ARG, "box is NULL or already submitted");
+    if (!job_id) return fail(TILD_ERR_ARG, "job_id is NULL");
+    return guarded([&] {
+        *job_id = pool->impl->submit(box->impl, nsteps);   // on an error the caller keeps the box
+        box->impl = nullptr;
+    });
+}
+
+int tild_pool_status(tild_pool *pool, int64_t job_id, int32_t *state, int64_t *steps_done, double *times3)
+{
+    NEED_POOL;
+    return guarded([&] {
+        int st = 0;
+        int64_t d = 0;
+        pool->impl->status(job_id, st, d, times3);
+        if (state) *state = st;
+        if (steps_done) *steps_done = d;
+    });
+}
+
+int tild_pool_wait(tild_pool *pool, int64_t job_id)
+{
+    NEED_POOL;
+    return guarded([&] { pool->impl->wait(job_id); });
+}
+
+int tild_pool_result(tild_pool *pool, int64_t job_id, float *x_out, double *thermo_out, int32_t nthermo,
+                     int32_t *nwritten)
+{
+    NEED_POOL;
+    return guarded([&] {
+        int n = 0;
+        pool->impl->result(job_id, x_out, thermo_out, nthermo, &n);
+        if (nwritten) *nwritten = n;
+    });
+}
+
+int tild_pool_release(tild_pool *pool, int64_t job_id)
+{
+    NEED_POOL;
+    return guarded([&] { pool->impl->release(job_id); });
+}
+
+int tild_pool_stats(tild_pool *pool, int64_t *out, int32_t nout)
+{
+    NEED_POOL;
+    if (!out) return fail(TILD_ERR_ARG, "out is NULL");
+    return guarded([&] {
+        std::vector<int64_t> v;
+        pool->impl->stats(v);
+        for (int32_t i = 0; i < nout && i < (int32_t)v.size(); i++) out[i] = v[i];
+    });
 }
 
 }  // extern "C"

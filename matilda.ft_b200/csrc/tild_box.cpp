@@ -29,6 +29,8 @@ void init_fft_attributes();
 void init_deposit_attributes();
 void init_particle_attributes();
 
+[[noreturn]] void fail(int code, const std::string &msg) { throw BoxError{code, msg}; }
+
 namespace {
 
 std::vector<std::string> split(const std::string &line)
@@ -39,8 +41,6 @@ std::vector<std::string> split(const std::string &line)
     while (iss >> s) w.push_back(s);
     return w;
 }
-
-[[noreturn]] void fail(int code, const std::string &msg) { throw BoxError{code, msg}; }
 
 const std::string &need(const std::vector<std::string> &w, size_t &i, const char *what)
 {
@@ -96,7 +96,10 @@ Box::~Box()
 {
     dropGraphs();
     freeDevice();
-    if (hKsPinned) cudaFreeHost(hKsPinned);
+    if (hKsPinned) {
+        if (sharedDevice) delete hKsPinned;
+        else cudaFreeHost(hKsPinned);
+    }
     if (ownStream && stream) cudaStreamDestroy(stream);
 }
 
@@ -110,7 +113,12 @@ T *Box::dalloc(size_t count)
 {
     void *p = nullptr;
     const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
-    ck(cudaMalloc(&p, bytes), "cudaMalloc");
+    if (sharedDevice) {   // usable by the synchronous uploads once the stream has reached it
+        ck(cudaMallocAsync(&p, bytes, stream), "cudaMallocAsync");
+        ck(cudaStreamSynchronize(stream), "cudaMallocAsync");
+    } else {
+        ck(cudaMalloc(&p, bytes), "cudaMalloc");
+    }
     allocs.push_back(p);
     devBytes += (int64_t)bytes;
     return reinterpret_cast<T *>(p);
@@ -119,7 +127,10 @@ T *Box::dalloc(size_t count)
 void Box::freeDevice()
 {
     cudaSetDevice(device);
-    for (void *p : allocs) cudaFree(p);
+    for (void *p : allocs) {
+        if (sharedDevice) cudaFreeAsync(p, stream);
+        else cudaFree(p);
+    }
     allocs.clear();
     devBytes = 0;
 }
@@ -546,6 +557,13 @@ void Box::createDefaultGroups()
 // ---------------------------------------------------------------------------------------
 void Box::finishInitialization()
 {
+    if (!hostPrepared) prepareHost();
+    initDevice();
+}
+
+void Box::prepareHost()
+{
+    if (hostPrepared) return;
     if (nstot == 0) fail(TILD_ERR_PARSE, "Box created with no particles?!?");
     if (Dim != 3) fail(TILD_ERR_UNSUPPORTED, "the B200 TILD path runs 3-D boxes (Dim 3)");
     for (int j = 0; j < 3; j++)
@@ -598,6 +616,14 @@ void Box::finishInitialization()
         }
     }
     if (writeFiles) { std::ofstream o(resolve(datFileName)); }   // :359-364, :543-544 truncate
+    buildPlan();
+    hostPrepared = true;
+}
+
+void Box::initDevice()
+{
+    if (!hostPrepared) fail(TILD_ERR_STATE, "the box has not been prepared");
+    if (ready) fail(TILD_ERR_STATE, "endBox was already processed");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) fail(TILD_ERR_CUDA, "no CUDA device is visible");
     ck(cudaSetDevice(device), "cudaSetDevice");
@@ -608,7 +634,6 @@ void Box::finishInitialization()
     init_fft_attributes();
     init_deposit_attributes();
     init_particle_attributes();
-    buildPlan();
     allocDevice();
     uploadParticles();
     if (sortInterval > 0) {   // start from a spatially coherent order
@@ -616,6 +641,21 @@ void Box::finishInitialization()
         ck(cudaStreamSynchronize(stream), "initial sort");
     }
     ready = true;
+}
+
+int64_t Box::deviceBytesEstimate() const
+{
+    if (!hostPrepared) fail(TILD_ERR_STATE, "the box has not been prepared");
+    const int64_t N = nstot, M = geom.M, hs = geom.hstride;
+    const int64_t nd = std::max<int64_t>(1, (int64_t)dfields.size()), nfg = std::max<int64_t>(1, (int64_t)fgroups.size());
+    const int64_t npair = (nd + 1) / 2, mb = MAXBONDS;
+    const int64_t rng = rngCompat ? (int64_t)rng_state_bytes() : 0, q = doCharges ? 4 : 0;
+    const int64_t perParticle = 12 * 4 + 4 + 4 + q + 1 + 5 * mb + rng + 12   // state, scratch
+                                + 12 + 36 + q + 8 + 1 + 5 * mb + rng;         // sort keys and copies
+    const int64_t nk = (int64_t)sort_key_count(geom);
+    const int64_t grid = (deterministic ? 16 : 8) * npair * M + 8 * nd * hs + 24 * nfg * hs + 16 * nfg * M +
+                         4 * std::max<int64_t>(1, (int64_t)potentials.size()) * hs + 8 * nk;
+    return N * perParticle + grid + (int64_t(4) << 20);   // + small arrays, alignment, graphs
 }
 
 void Box::buildPlan()
@@ -778,7 +818,8 @@ void Box::allocDevice()
     dBpart = dalloc<double>((size_t)nblkP * 7);
     dRes = dalloc<double>(kMaxPots + 8);
     dTmp = dalloc<float>(3 * N);
-    ck(cudaMallocHost(&hKsPinned, sizeof(KSpace)), "cudaMallocHost");
+    if (sharedDevice) hKsPinned = new KSpace;   // pinned host memory would synchronise the device when freed
+    else ck(cudaMallocHost(&hKsPinned, sizeof(KSpace)), "cudaMallocHost");
     // sort scratch and the permuted copies
     const uint32_t nk = sort_key_count(g);
     sortKeys = nk;
@@ -851,7 +892,7 @@ void Box::uploadParticles()
         ck(launch_rng_init(dRng, dOrig, (int)N, (unsigned long long)(unsigned int)RANDSEED, stream), "rng init");
         ck(cudaStreamSynchronize(stream), "rng init sync");
     }
-    ck(cudaDeviceSynchronize(), "upload");
+    ck(sharedDevice ? cudaStreamSynchronize(stream) : cudaDeviceSynchronize(), "upload");
 }
 
 // Per-particle membership flags (density fields, force groups, integrator slot, type) and

@@ -19,6 +19,8 @@ struct BoxError {
     std::string msg;
 };
 
+[[noreturn]] void fail(int code, const std::string &msg);   // throws BoxError
+
 struct PS_Species {          // ps_species.cu:13-38
     std::string label;
     float mass = 1.0f;
@@ -62,7 +64,13 @@ public:
 
     // ---- input (PS_Box::readInput, PS_Box_initialization.cu:32-345) ----
     void command(const std::string &line);          // one line, word by word
-    void finishInitialization();                      // endBox (:352-569)
+    void finishInitialization();                      // endBox (:352-569) = prepareHost + initDevice
+    void prepareHost();                               // host checks, default groups, k-space plan
+    void initDevice();                                // device arrays, uploads, first sort
+    int64_t deviceBytesEstimate() const;              // device bytes initDevice will allocate (after prepareHost)
+    // stream-ordered allocation (cudaMallocAsync/cudaFreeAsync on the box's stream) and no
+    // device-wide synchronisation: for boxes that share a GPU with other running work
+    void setSharedDevice(bool on) { sharedDevice = on; }
     void readDataConfig(const std::string &name);     // :787-997
     void setParticles(int64_t n, const float *x, const int32_t *type, const int32_t *mol, const float *q);
     void setBonds(int64_t nb, const int64_t *pairs, const int32_t *btype);
@@ -70,6 +78,7 @@ public:
     void setStream(cudaStream_t st);
     void setBaseDir(const std::string &d) { baseDir = d; }
     bool initialized() const { return ready; }
+    cudaStream_t cudaStreamHandle() const { return stream; }
 
     // ---- run ----
     void NVT(int64_t nSteps);                          // PS_Box.cu:210-234
@@ -169,6 +178,8 @@ private:
     // device state
     cudaStream_t stream = nullptr;
     bool ownStream = false;
+    bool sharedDevice = false;
+    bool hostPrepared = false;
     std::vector<void *> allocs;
     int64_t devBytes = 0;
     float *dX[2] = {nullptr, nullptr};

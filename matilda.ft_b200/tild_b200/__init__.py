@@ -57,6 +57,18 @@ _SIGS = {
     "tild_run_script_file": ([ctypes.c_char_p, ctypes.c_int], ctypes.c_int),
     "tild_box_stage_times": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)],
                              ctypes.c_int),
+    "tild_pool_create": ([ctypes.c_int, ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)],
+                         ctypes.c_int),
+    "tild_pool_destroy": ([ctypes.c_void_p], ctypes.c_int),
+    "tild_pool_submit": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)],
+                         ctypes.c_int),
+    "tild_pool_status": ([ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int32),
+                          ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p], ctypes.c_int),
+    "tild_pool_wait": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
+    "tild_pool_result": ([ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                          ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
+    "tild_pool_release": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
+    "tild_pool_stats": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32], ctypes.c_int),
 }
 
 
@@ -184,6 +196,13 @@ class Box:
         _check(lib().tild_box_forces(self._h, _ptr(f)))
         return f
 
+    def thermo_raw(self):
+        """tild_box_thermo's values as one array: Upe, Ubond, per potential, virial[6]."""
+        out = np.zeros(64, np.float64)
+        n = ctypes.c_int()
+        _check(lib().tild_box_thermo(self._h, _ptr(out), 64, ctypes.byref(n)))
+        return out[: n.value].copy()
+
     def thermo(self):
         nmax = 64
         out = np.zeros(nmax, np.float64)
@@ -235,6 +254,68 @@ class Box:
 def run_script_file(path: str, device: int = 0):
     """Execute a MATILDA.FT input script (main.cu:21-156) with the B200 library."""
     _check(lib().tild_run_script_file(path.encode(), int(device)))
+
+
+JOB_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed"}
+
+
+class Pool:
+    """Jobs sharing one GPU (tild_pool_*): admission against a device-memory budget and
+    continuous batching of their steps on per-job streams."""
+
+    def __init__(self, device=0, mem_budget_bytes=16 << 30, max_active=0):
+        h = ctypes.c_void_p()
+        _check(lib().tild_pool_create(int(device), int(mem_budget_bytes), int(max_active), ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().tild_pool_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def submit(self, box: Box, nsteps: int) -> int:
+        """Hand a box (endBox not yet processed) to the pool; returns the job id.  On
+        success the box handle is emptied (the pool owns the box)."""
+        jid = ctypes.c_int64()
+        _check(lib().tild_pool_submit(self._h, box._h, int(nsteps), ctypes.byref(jid)))
+        return jid.value
+
+    def status(self, job: int):
+        st, done = ctypes.c_int32(), ctypes.c_int64()
+        t = np.zeros(3, np.float64)
+        _check(lib().tild_pool_status(self._h, int(job), ctypes.byref(st), ctypes.byref(done), _ptr(t)))
+        return {"state": JOB_STATES[st.value], "steps_done": done.value,
+                "submit_s": t[0], "admit_s": t[1], "done_s": t[2]}
+
+    def wait(self, job: int):
+        _check(lib().tild_pool_wait(self._h, int(job)))
+
+    def result(self, job: int, n: int):
+        x = np.zeros((n, 3), np.float32)
+        th = np.zeros(64, np.float64)
+        nw = ctypes.c_int32()
+        _check(lib().tild_pool_result(self._h, int(job), _ptr(x), _ptr(th), 64, ctypes.byref(nw)))
+        return x, th[: nw.value]
+
+    def release(self, job: int):
+        _check(lib().tild_pool_release(self._h, int(job)))
+
+    def stats(self) -> dict:
+        v = np.zeros(6, np.int64)
+        _check(lib().tild_pool_stats(self._h, _ptr(v), 6))
+        return dict(zip(("queued", "running", "done", "failed", "bytes_in_use", "budget"), (int(a) for a in v)))
 
 
 def box_from_spec(spec, device=0, options=None, steps_script=False):
