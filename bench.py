@@ -219,6 +219,96 @@ def cufft_times(torch, spec, nd, nfg, reps=20):
     return out
 
 
+def job_box(tild_b200, spec):
+    return tild_b200.box_from_spec(spec, options={"write_files": 0})
+
+
+def pct(v, q):
+    return float(np.percentile(np.asarray(v, np.float64), q)) if len(v) else None
+
+
+def run_batched(tild_b200, synth, args):
+    """C3: uneven diblock replicas, all in one pool (continuous batching on per-job
+    streams) against the same jobs run one after another (plain per-job form).  Wall
+    clock from the first endBox/submit to the last result on the host; boxes are built on
+    the host before the clock starts in both forms."""
+    specs = synth.config_c3(replicas=args.c3_replicas)
+    steps = args.c3_steps
+    work = float(sum(s.N for s in specs)) * steps
+    boxes = [job_box(tild_b200, s) for s in specs]
+    t0 = time.perf_counter()
+    for b in boxes:
+        b.command("endBox")
+        b.step(steps)
+        b.positions()
+        b.close()
+    plain_s = time.perf_counter() - t0
+    boxes = [job_box(tild_b200, s) for s in specs]
+    with tild_b200.Pool(mem_budget_bytes=args.pool_budget_gb << 30) as pool:
+        t0 = time.perf_counter()
+        ids = [pool.submit(b, steps) for b in boxes]
+        for jid, s in zip(ids, specs):
+            pool.wait(jid)
+            pool.result(jid, s.N)
+        batched_s = time.perf_counter() - t0
+    for b in boxes:
+        b.close()
+    return {"workload": "c3: %d diblock replicas, %d steps each, N %d..%d (total %d), grids %d^3..%d^3"
+                        % (len(specs), steps, min(s.N for s in specs), max(s.N for s in specs),
+                           sum(s.N for s in specs), min(int(s.grid[0]) for s in specs),
+                           max(int(s.grid[0]) for s in specs)),
+            "value": work / batched_s, "unit": METRIC, "plain_value": work / plain_s,
+            "speedup_vs_plain": plain_s / batched_s, "batched_s": batched_s, "plain_s": plain_s,
+            "timing": "wall clock, host, includes allocation, upload, graph capture and result copies"}
+
+
+def run_served(tild_b200, synth, args, capacity):
+    """C5: jobs arriving as a Poisson process at an offered load of `c5_load` times the
+    batched capacity, admitted by the pool as memory frees up; latency = completion -
+    arrival.  The same jobs run alone give the plain per-job service times."""
+    jobs = synth.config_c5_jobs(njobs=args.c5_jobs)
+    work = np.array([s.N * n for s, n in jobs], np.float64)
+    boxes = [job_box(tild_b200, s) for s, _ in jobs]
+    service = []
+    for b, (s, n) in zip(boxes, jobs):
+        t0 = time.perf_counter()
+        b.command("endBox")
+        b.step(n)
+        b.positions()
+        b.thermo_raw()
+        service.append(time.perf_counter() - t0)
+        b.close()
+    rate = args.c5_load * capacity / float(work.mean())   # jobs per second
+    arrivals = np.cumsum(np.random.default_rng(5).exponential(1.0 / rate, len(jobs)))
+    boxes = [job_box(tild_b200, s) for s, _ in jobs]
+    lat, spans = [], []
+    with tild_b200.Pool(mem_budget_bytes=args.pool_budget_gb << 30) as pool:
+        t0 = time.perf_counter()
+        ids = []
+        for b, a in zip(boxes, arrivals):
+            dt = t0 + a - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            ids.append(pool.submit(b, jobs[len(ids)][1]))
+        for jid, (s, _) in zip(ids, jobs):
+            pool.wait(jid)
+            pool.result(jid, s.N)
+            st = pool.status(jid)
+            lat.append(st["done_s"] - st["submit_s"])
+            spans.append((st["submit_s"], st["done_s"]))
+    for b in boxes:
+        b.close()
+    makespan = max(d for _, d in spans) - min(a for a, _ in spans)
+    return {"workload": "c5: %d jobs (diblock or coacervate), N %d..%d, %d..%d steps, Poisson arrivals at %.0f%% of "
+                        "the batched capacity (%.1f jobs/s)" % (len(jobs), min(s.N for s, _ in jobs),
+                                                                max(s.N for s, _ in jobs), min(n for _, n in jobs),
+                                                                max(n for _, n in jobs), 100 * args.c5_load, rate),
+            "value": float(work.sum()) / makespan, "unit": METRIC, "latency_p50_s": pct(lat, 50),
+            "latency_p99_s": pct(lat, 99), "plain_value": float(work.sum()) / sum(service),
+            "plain_service_p50_s": pct(service, 50), "plain_service_p99_s": pct(service, 99),
+            "timing": "wall clock; latency from submit to result available; plain = each job alone, back to back"}
+
+
 def run_ours(args):
     import torch
     import tild_b200
@@ -331,8 +421,13 @@ def run_ours(args):
             "gpu_launches": KERNELS_PER_STEP * args.steps + 6 * nsort,
             "clocks": clk.summary(),
         }
-        print(json.dumps(line), flush=True)
     box.close()
+    if rank == 0:
+        if world == 1 and not args.no_batch:
+            from tild_b200 import synth
+            line["batched"] = run_batched(tild_b200, synth, args)
+            line["served"] = run_served(tild_b200, synth, args, line["batched"]["value"])
+        print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -350,6 +445,12 @@ def main():
     ap.add_argument("--profile-steps", type=int, default=10)
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched (C3) and served (C5) runs")
+    ap.add_argument("--c3-replicas", type=int, default=64)
+    ap.add_argument("--c3-steps", type=int, default=500)
+    ap.add_argument("--c5-jobs", type=int, default=40)
+    ap.add_argument("--c5-load", type=float, default=0.8)
+    ap.add_argument("--pool-budget-gb", type=int, default=120)
     ap.add_argument("--ref-budget", type=float, default=150.0, help="seconds for the reference arm")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

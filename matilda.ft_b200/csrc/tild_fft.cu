@@ -518,7 +518,8 @@ __global__ void __launch_bounds__(256) k_xinv(Geom g, FftLine lx, int nfg, const
     const int n = g.nx, nf = 3 * nfg, npair = (nf + 1) / 2, nxh = g.nxh, hp = g.hp;
     const int lines = npair * L;
     const int stsz = nf * L * hp, bsz = lines * n;
-    float2 *A = sm, *St = sm + bsz, *tw = St + (stsz > bsz ? stsz : bsz);
+    // St receives 16-byte cp.async copies: start it on an even complex offset
+    float2 *A = sm, *St = sm + ((bsz + 1) & ~1), *tw = St + (stsz > bsz ? stsz : bsz);
     const long long nlines = (long long)g.ny * g.nz;
     const long long line0 = (long long)blockIdx.x * L;
     const int lv = (int)min((long long)L, nlines - line0);
@@ -656,7 +657,7 @@ cudaError_t launch_xinv(const Geom &g, const FftLine &lx, int nfg, const float2 
     L = L < 1 ? 1 : (L > 16 ? 16 : L);
     const long long nlines = (long long)g.ny * g.nz;
     const size_t bsz = (size_t)npair * L * g.nx, stsz = (size_t)nf * L * g.hp;
-    const size_t smx = (bsz + std::max(bsz, stsz) + g.nx) * sizeof(float2);
+    const size_t smx = (((bsz + 1) & ~(size_t)1) + std::max(bsz, stsz) + g.nx) * sizeof(float2);
     k_xinv<<<(unsigned)((nlines + L - 1) / L), 256, smx, st>>>(g, lx, nfg, Hg, rec, L);
     return cudaGetLastError();
 }

@@ -226,6 +226,69 @@ def config_c4(seed=4, scale=1.0):
                         extra_pots=erf)
 
 
+def smooth_grid(n):
+    """Nearest integer >= 8 to n whose prime factors are 2, 3, 5, 7."""
+    def smooth(m):
+        for f in (2, 3, 5, 7):
+            while m % f == 0:
+                m //= f
+        return m == 1
+    best = None
+    for d in range(0, 64):
+        for m in (int(round(n)) - d, int(round(n)) + d):
+            if m >= 8 and smooth(m):
+                best = m if best is None or abs(m - n) < abs(best - n) else best
+        if best is not None:
+            return best
+    return max(8, int(round(n)))
+
+
+def config_c3(seed=3, replicas=64, nmin=1.0e4, nmax=4.0e5):
+    """Uneven AB diblock replicas: chain length in {16, 24, 32, 48}, particle count
+    log-uniform in [nmin, nmax] rounded to whole chains, rho0 = 5, grid spacing ~0.4 on a
+    2,3,5,7-smooth grid (the last replica takes a prime grid size), chi ~ U[0.2, 2.0],
+    A fraction ~ U[0.2, 0.8].  Replica r draws from seed + r."""
+    out = []
+    for r in range(replicas):
+        rng = np.random.default_rng(seed + r)
+        nper = int(rng.choice([16, 24, 32, 48]))
+        ntot = float(np.exp(rng.uniform(np.log(nmin), np.log(nmax))))
+        nch = max(1, int(round(ntot / nper)))
+        L = (nch * nper / 5.0) ** (1.0 / 3.0)
+        grid = smooth_grid(L / 0.4)
+        if r == replicas - 1:   # a prime size exercises the generic radix
+            grid = next(p for p in range(int(L / 0.4) | 1, 10000, 2) if all(p % k for k in range(3, int(p ** 0.5) + 1, 2)))
+        chi = float(rng.uniform(0.2, 2.0))
+        fA = float(rng.uniform(0.2, 0.8))
+        out.append(diblock_melt(nch, nper, L, grid, chi=chi, rho0=5.0, fA=fA, seed=seed + r,
+                                name="c3_replica%d" % r))
+    return out
+
+
+def config_c5_jobs(seed=5, njobs=40, nmin=2.0e4, nmax=2.0e5, smin=100, smax=400):
+    """Served jobs: diblock melts or coacervates (equal odds), particle count log-uniform
+    in [nmin, nmax], steps uniform in [smin, smax].  Returns (spec, steps) pairs; job j
+    draws from seed + j."""
+    jobs = []
+    for j in range(njobs):
+        rng = np.random.default_rng(seed + j)
+        ntot = float(np.exp(rng.uniform(np.log(nmin), np.log(nmax))))
+        steps = int(rng.integers(smin, smax + 1))
+        if rng.uniform() < 0.5:
+            nper = 32
+            nch = max(1, int(round(ntot / nper)))
+            L = (nch * nper / 5.0) ** (1.0 / 3.0)
+            spec = diblock_melt(nch, nper, L, smooth_grid(L / 0.4), chi=float(rng.uniform(0.2, 2.0)), rho0=5.0,
+                                seed=seed + j, name="c5_diblock%d" % j)
+        else:
+            spec = config_c2(seed=seed + j, scale=ntot / 2097152.0)
+            spec.name = "c5_coacervate%d" % j
+            g = smooth_grid(float(spec.L[0]) / 0.4)
+            spec.grid = [g, g, g]
+        jobs.append((spec, steps))
+    return jobs
+
+
 def small_system(seed=0, n_chains=20, nper=8, L=6.0, grid=(12, 12, 12), order=3, charges=False,
                  dim=3, pots=None, n_free=0):
     """A tiny randomised system for oracle comparisons."""

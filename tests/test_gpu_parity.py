@@ -43,6 +43,8 @@ SYSTEMS = {
         dict(kind="erfG", I="B", J="B", A=0.3, Rp=0.8, sigma=0.5),
         dict(kind="gaussian", I="all", J="A", A=1.5, sigma=0.8)]),
     "odd_grid": lambda: synth.small_system(seed=8, order=3, grid=(15, 9, 21), charges=True),
+    # odd x with an odd number of lines per x-inverse block (45: 3 pairs x 19 lines)
+    "odd_grid_wide": lambda: synth.small_system(seed=10, order=3, grid=(45, 10, 12), L=9.0, charges=True),
     "free_particles": lambda: synth.small_system(seed=9, order=3, n_free=50, charges=True),
 }
 
