@@ -108,18 +108,38 @@ void Box::ck(cudaError_t e, const char *what) const
     if (e != cudaSuccess) fail(TILD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-template <typename T>
-T *Box::dalloc(size_t count)
+void *Box::rawAlloc(size_t bytes)
 {
     void *p = nullptr;
-    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
-    if (sharedDevice) {   // usable by the synchronous uploads once the stream has reached it
-        ck(cudaMallocAsync(&p, bytes, stream), "cudaMallocAsync");
+    if (sharedDevice) {   // stream-ordered; usable by the synchronous uploads once the stream has reached it
+        if (memPool) ck(cudaMallocFromPoolAsync(&p, bytes, memPool, stream), "cudaMallocFromPoolAsync");
+        else ck(cudaMallocAsync(&p, bytes, stream), "cudaMallocAsync");
         ck(cudaStreamSynchronize(stream), "cudaMallocAsync");
     } else {
         ck(cudaMalloc(&p, bytes), "cudaMalloc");
     }
-    allocs.push_back(p);
+    return p;
+}
+
+void Box::rawFree(void *p)
+{
+    if (sharedDevice) cudaFreeAsync(p, stream);
+    else cudaFree(p);
+}
+
+template <typename T>
+T *Box::dalloc(size_t count)
+{
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    const size_t padded = (bytes + 255) & ~(size_t)255;
+    void *p;
+    if (arena && arenaUsed + padded <= arenaSize) {
+        p = arena + arenaUsed;
+        arenaUsed += padded;
+    } else {
+        p = rawAlloc(bytes);
+        allocs.push_back(p);
+    }
     devBytes += (int64_t)bytes;
     return reinterpret_cast<T *>(p);
 }
@@ -127,11 +147,11 @@ T *Box::dalloc(size_t count)
 void Box::freeDevice()
 {
     cudaSetDevice(device);
-    for (void *p : allocs) {
-        if (sharedDevice) cudaFreeAsync(p, stream);
-        else cudaFree(p);
-    }
+    for (void *p : allocs) rawFree(p);
     allocs.clear();
+    if (arena) rawFree(arena);
+    arena = nullptr;
+    arenaSize = arenaUsed = 0;
     devBytes = 0;
 }
 
@@ -650,7 +670,7 @@ int64_t Box::deviceBytesEstimate() const
     const int64_t nd = std::max<int64_t>(1, (int64_t)dfields.size()), nfg = std::max<int64_t>(1, (int64_t)fgroups.size());
     const int64_t npair = (nd + 1) / 2, mb = MAXBONDS;
     const int64_t rng = rngCompat ? (int64_t)rng_state_bytes() : 0, q = doCharges ? 4 : 0;
-    const int64_t perParticle = 12 * 4 + 4 + 4 + q + 1 + 5 * mb + rng + 12   // state, scratch
+    const int64_t perParticle = 12 * 4 + 4 + 4 + q + 1 + 5 * mb + rng + 12 + 1   // state, scratch, partials
                                 + 12 + 36 + q + 8 + 1 + 5 * mb + rng;         // sort keys and copies
     const int64_t nk = (int64_t)sort_key_count(geom);
     const int64_t grid = (deterministic ? 16 : 8) * npair * M + 8 * nd * hs + 24 * nfg * hs + 16 * nfg * M +
@@ -783,6 +803,9 @@ void Box::allocDevice()
 {
     const Geom &g = geom;
     const int64_t N = nstot;
+    arenaSize = (size_t)deviceBytesEstimate();
+    arena = static_cast<char *>(rawAlloc(arenaSize));
+    arenaUsed = 0;
     dX[0] = dalloc<float>(3 * N);
     dX[1] = dalloc<float>(3 * N);
     dNoise = dalloc<float>(3 * N);

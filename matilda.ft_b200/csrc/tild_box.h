@@ -70,7 +70,11 @@ public:
     int64_t deviceBytesEstimate() const;              // device bytes initDevice will allocate (after prepareHost)
     // stream-ordered allocation (cudaMallocAsync/cudaFreeAsync on the box's stream) and no
     // device-wide synchronisation: for boxes that share a GPU with other running work
-    void setSharedDevice(bool on) { sharedDevice = on; }
+    void setSharedDevice(bool on, cudaMemPool_t pool = nullptr)
+    {
+        sharedDevice = on;
+        memPool = pool;
+    }
     void readDataConfig(const std::string &name);     // :787-997
     void setParticles(int64_t n, const float *x, const int32_t *type, const int32_t *mol, const float *q);
     void setBonds(int64_t nb, const int64_t *pairs, const int32_t *btype);
@@ -179,6 +183,13 @@ private:
     cudaStream_t stream = nullptr;
     bool ownStream = false;
     bool sharedDevice = false;
+    cudaMemPool_t memPool = nullptr;   // shared-device arenas come from this pool when set
+    // one arena per box: dalloc carves 256-byte aligned pieces, individual allocations
+    // only if the arena is exhausted
+    char *arena = nullptr;
+    size_t arenaSize = 0, arenaUsed = 0;
+    void *rawAlloc(size_t bytes);
+    void rawFree(void *p);
     bool hostPrepared = false;
     std::vector<void *> allocs;
     int64_t devBytes = 0;

@@ -46,7 +46,7 @@ __device__ __forceinline__ unsigned fdiv(unsigned i, const FastDiv &f)
 __device__ __forceinline__ float2 mul_mi(float2 v) { return make_float2(v.y, -v.x); }   // -i v
 __device__ __forceinline__ float2 mul_pi(float2 v) { return make_float2(-v.y, v.x); }   // +i v
 
-// In-register DFT of R points, v[q] <- sum_s v[s] W_R^{+-qs} (forward sign -), R = 2, 3, 4, 5, 8.
+// In-register DFT of R points, v[q] <- sum_s v[s] W_R^{+-qs} (forward sign -), R = 2, 3, 4, 5, 7, 8.
 template <bool INV>
 __device__ __forceinline__ void dft4(float2 &a0, float2 &a1, float2 &a2, float2 &a3)
 {
@@ -112,6 +112,28 @@ __device__ __forceinline__ void dft_reg(float2 *v)
         v[4] = make_float2(m1.x - n1.y, m1.y + n1.x);
         v[2] = make_float2(m2.x + n2.y, m2.y - n2.x);
         v[3] = make_float2(m2.x - n2.y, m2.y + n2.x);
+    } else if (R == 7) {
+        // t_k = a_k + a_{7-k}, u_k = a_k - a_{7-k}; b_q = m_q -+ i n_q with
+        // m_q = a0 + sum_k cos(2 pi qk/7) t_k, n_q = sum_k sin(2 pi qk/7) u_k
+        const float c1 = 0.62348980185873359f, c2 = -0.22252093395631434f, c3 = -0.90096886790241903f;
+        const float sg = INV ? -1.f : 1.f;
+        const float s1 = sg * 0.78183148246802980f, s2 = sg * 0.97492791218182362f, s3 = sg * 0.43388373911755823f;
+        const float2 a0 = v[0];
+        const float2 t1 = cadd(v[1], v[6]), t2 = cadd(v[2], v[5]), t3 = cadd(v[3], v[4]);
+        const float2 u1 = csub(v[1], v[6]), u2 = csub(v[2], v[5]), u3 = csub(v[3], v[4]);
+        const float2 m1 = make_float2(a0.x + c1 * t1.x + c2 * t2.x + c3 * t3.x, a0.y + c1 * t1.y + c2 * t2.y + c3 * t3.y);
+        const float2 m2 = make_float2(a0.x + c2 * t1.x + c3 * t2.x + c1 * t3.x, a0.y + c2 * t1.y + c3 * t2.y + c1 * t3.y);
+        const float2 m3 = make_float2(a0.x + c3 * t1.x + c1 * t2.x + c2 * t3.x, a0.y + c3 * t1.y + c1 * t2.y + c2 * t3.y);
+        const float2 n1 = make_float2(s1 * u1.x + s2 * u2.x + s3 * u3.x, s1 * u1.y + s2 * u2.y + s3 * u3.y);
+        const float2 n2 = make_float2(s2 * u1.x - s3 * u2.x - s1 * u3.x, s2 * u1.y - s3 * u2.y - s1 * u3.y);
+        const float2 n3 = make_float2(s3 * u1.x - s1 * u2.x + s2 * u3.x, s3 * u1.y - s1 * u2.y + s2 * u3.y);
+        v[0] = make_float2(a0.x + t1.x + t2.x + t3.x, a0.y + t1.y + t2.y + t3.y);
+        v[1] = cadd(m1, mul_mi(n1));
+        v[6] = csub(m1, mul_mi(n1));
+        v[2] = cadd(m2, mul_mi(n2));
+        v[5] = csub(m2, mul_mi(n2));
+        v[3] = cadd(m3, mul_mi(n3));
+        v[4] = csub(m3, mul_mi(n3));
     }
 }
 
@@ -202,6 +224,7 @@ __device__ float2 *fft_lines(float2 *a, float2 *b, int L, int lp, int ls, const 
             case 2: fft_stage<INV, 2>(a, b, L, lp, ls, n, p, pl.dP[s], dsplit, line_fast, tw); break;
             case 3: fft_stage<INV, 3>(a, b, L, lp, ls, n, p, pl.dP[s], dsplit, line_fast, tw); break;
             case 5: fft_stage<INV, 5>(a, b, L, lp, ls, n, p, pl.dP[s], dsplit, line_fast, tw); break;
+            case 7: fft_stage<INV, 7>(a, b, L, lp, ls, n, p, pl.dP[s], dsplit, line_fast, tw); break;
             default: fft_stage_generic<INV>(a, b, L, lp, ls, n, R, p, pl.dP[s], dsplit, line_fast, tw); break;
         }
         __syncthreads();
@@ -602,7 +625,8 @@ void build_fft_line(int n, FftLine &pl, float2 *dev_tw_dst)
     while (m % 2 == 0) push(2);
     while (m % 3 == 0) push(3);
     while (m % 5 == 0) push(5);
-    for (int r = 7; m > 1; r += 2)
+    while (m % 7 == 0) push(7);
+    for (int r = 11; m > 1; r += 2)
         while (m % r == 0) push(r);
     std::vector<float2> tw(n);
     for (int t = 0; t < n; t++) {

@@ -29,6 +29,10 @@ Pool::~Pool()
     }
     cvWork.notify_all();
     if (worker.joinable()) worker.join();
+    if (memPool) {
+        cudaSetDevice(device);
+        cudaMemPoolDestroy(memPool);
+    }
     cvDone.notify_all();
 }
 
@@ -151,6 +155,7 @@ void Pool::dropEvents(Job *j)
 bool Pool::admit(Job *j)
 {
     try {
+        j->box->setSharedDevice(true, memPool);
         j->box->initDevice();
         for (int k = 0; k < 2; k++) {
             cudaEvent_t e;
@@ -217,13 +222,30 @@ void Pool::pump(Job *j, bool &progressed)
 
 void Pool::run()
 {
-    cudaSetDevice(device);   // a failure surfaces when a job is admitted
+    // the jobs' arenas come from one memory pool that keeps freed memory (up to the
+    // budget) for the next jobs instead of returning it to the driver; without a GPU the
+    // failure surfaces when a job is admitted
+    if (cudaSetDevice(device) == cudaSuccess) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        if (cudaMemPoolCreate(&memPool, &props) == cudaSuccess) {
+            uint64_t keep = (uint64_t)budget;
+            cudaMemPoolSetAttribute(memPool, cudaMemPoolAttrReleaseThreshold, &keep);
+        } else {
+            memPool = nullptr;
+            cudaGetLastError();
+        }
+    }
     for (;;) {
         std::vector<Job *> toAdmit;
         {
             std::unique_lock<std::mutex> lk(mu);
             if (stop && queue.empty() && active.empty()) break;
-            while (!queue.empty() && (int)(active.size() + toAdmit.size()) < maxActive &&
+            // at most two admissions per pass, so the running jobs keep getting work while
+            // new ones are set up
+            while (!queue.empty() && toAdmit.size() < 2 && (int)(active.size() + toAdmit.size()) < maxActive &&
                    inUse + queue.front()->bytes <= budget) {
                 Job *j = queue.front();
                 queue.pop_front();

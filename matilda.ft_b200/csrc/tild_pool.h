@@ -73,6 +73,7 @@ private:
     int64_t inUse = 0, nextId = 1;
     int nDone = 0, nFailed = 0;
     bool stop = false;
+    cudaMemPool_t memPool = nullptr;   // arenas of the jobs; keeps freed memory up to the budget
     std::chrono::steady_clock::time_point t0;
     std::thread worker;
 };

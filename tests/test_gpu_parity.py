@@ -45,6 +45,9 @@ SYSTEMS = {
     "odd_grid": lambda: synth.small_system(seed=8, order=3, grid=(15, 9, 21), charges=True),
     # odd x with an odd number of lines per x-inverse block (45: 3 pairs x 19 lines)
     "odd_grid_wide": lambda: synth.small_system(seed=10, order=3, grid=(45, 10, 12), L=9.0, charges=True),
+    # radix-7 stages on every axis, and generic prime radices 11 and 13
+    "radix7_grid": lambda: synth.small_system(seed=12, order=2, grid=(21, 14, 28), L=7.0, charges=True),
+    "prime_grid": lambda: synth.small_system(seed=13, order=1, grid=(22, 13, 11), charges=True),
     "free_particles": lambda: synth.small_system(seed=9, order=3, n_free=50, charges=True),
 }
 
