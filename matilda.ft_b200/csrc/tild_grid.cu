@@ -80,6 +80,8 @@ constexpr int kDepPB = 512;
 #define FIELD_PTR(dep, f, M) (reinterpret_cast<float *>((dep) + ((f) >> 1) * (M)) + ((f) & 1))
 constexpr int kDepSmemFast = 64 * 1024;
 constexpr int kDepSmemFixed = 128 * 1024;
+// largest warp table: 16 warps x 32 particles x (5 + 25 + 1 + kMaxFields) floats (order 4)
+constexpr int kDepTableMax = 16 * 32 * (5 + 25 + 1 + kMaxFields) * 4;
 
 // Coefficient of field f for a particle: membership bit, charge channel -> q.
 __device__ __forceinline__ float field_coef(uint32_t dm, unsigned dq, int f, float qp)
@@ -117,7 +119,9 @@ __global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4
                                                        TileCfg tc)
 {
     constexpr int P1 = P + 1, G = P1 * P1 * P1, NPASS = (G + 31) / 32;
-    constexpr int WREC = 3 * P1 + 4;   // per-particle record of the warp table: weights, offset, dm, q
+    constexpr int NC = NF ? NF : kMaxFields;
+    // per-particle record of the warp table: Wx, Wy*Wz, box offset, field coefficients
+    constexpr int WREC = P1 + P1 * P1 + 1 + NC;
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ TileShared ts;
     const float *__restrict__ X = (*d_step & 1) ? X1 : X0;
@@ -126,45 +130,24 @@ __global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4
     tile_range(tc, N, kDepPB, b0, b1);
     if (b1 <= b0) return;
     const int nn[3] = {g.nx, g.ny, g.nz};
-    if (threadIdx.x < 3) {
-        ts.ref[threadIdx.x] = stencil_origin<P>(X[3 * b0 + threadIdx.x], inv[threadIdx.x]);
-        ts.lo[threadIdx.x] = 0x7fffffff;
-        ts.hi[threadIdx.x] = -0x7fffffff;
-    }
-    __syncthreads();
-    int lo[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, hi[3] = {-0x7fffffff, -0x7fffffff, -0x7fffffff};
-    for (int p = b0 + threadIdx.x; p < b1; p += blockDim.x) {
-        if (!(pflags[p] & 0xffu)) continue;
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            const int dd = unwrap_delta(stencil_origin<P>(X[3 * p + j], inv[j]) - ts.ref[j], nn[j]);
-            lo[j] = min(lo[j], dd);
-            hi[j] = max(hi[j], dd);
-        }
-    }
-#pragma unroll
-    for (int j = 0; j < 3; j++) {
-        for (int o = 16; o > 0; o >>= 1) {
-            lo[j] = min(lo[j], __shfl_xor_sync(0xffffffffu, lo[j], o));
-            hi[j] = max(hi[j], __shfl_xor_sync(0xffffffffu, hi[j], o));
-        }
-        if ((threadIdx.x & 31) == 0) {
-            atomicMin(&ts.lo[j], lo[j]);
-            atomicMax(&ts.hi[j], hi[j]);
-        }
-    }
-    __syncthreads();
-    if (ts.hi[0] < ts.lo[0]) return;   // no depositing particle in this CTA
-    const int E[3] = {ts.hi[0] - ts.lo[0] + P1, ts.hi[1] - ts.lo[1] + P1, ts.hi[2] - ts.lo[2] + P1};
+    // sorted tiles: the fixed box of the tile's bricks plus the drift margin; particles
+    // whose stencil left it deposit with global atomics (windows of unsorted slots: all)
+    int lo[3] = {0, 0, 0}, span[3] = {-1, -1, -1}, E[3] = {0, 0, 0};
+    if (tc.start) tile_box<P>(tc, nn, lo, span, E);
     const int nfields = NF ? NF : nd;
     const size_t esz = FIXED ? sizeof(unsigned long long) : sizeof(float);
     const long long Vl = (long long)E[0] * E[1] * E[2];
-    const bool staged = E[0] <= kMaxBoxEdge && E[1] <= kMaxBoxEdge && E[2] <= kMaxBoxEdge &&
+    const bool staged = tc.start && E[0] <= kMaxBoxEdge && E[1] <= kMaxBoxEdge && E[2] <= kMaxBoxEdge &&
                         Vl * nfields * (long long)esz <= cap_bytes;
     const int V = staged ? (int)Vl : 0, E0 = E[0], E01 = E[0] * E[1];
     float *tf = reinterpret_cast<float *>(smraw);
     unsigned long long *tu = reinterpret_cast<unsigned long long *>(smraw);
     if (staged) {
+        if (threadIdx.x < 3) {
+            ts.ref[threadIdx.x] = lo[threadIdx.x];
+            ts.lo[threadIdx.x] = 0;
+        }
+        __syncthreads();
         tile_tables(ts, g.nx, g.ny, g.nz, E);
         for (int v = threadIdx.x; v < V * nfields; v += blockDim.x) {
             if (FIXED) tu[v] = 0ull;
@@ -175,16 +158,17 @@ __global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     if (staged) {
-        // this lane's stencil points: s = lane + 32*pass -> (a, b, e), x fastest
-        int sa[NPASS], sb[NPASS], se[NPASS];
+        // this lane's stencil points: s = lane + 32*pass -> (a, b, e), x fastest; its box
+        // offset and its Wy*Wz index are fixed for the whole tile
+        int sa[NPASS], syz[NPASS], loff[NPASS];
 #pragma unroll
         for (int k = 0; k < NPASS; k++) {
             const int s = lane + 32 * k;
-            sa[k] = s % P1;
-            sb[k] = (s / P1) % P1;
-            se[k] = s / (P1 * P1);
+            const int a = s % P1, bb = (s / P1) % P1, e = s / (P1 * P1);
+            sa[k] = a;
+            syz[k] = e * P1 + bb;
+            loff[k] = e * E01 + bb * E0 + a;
         }
-        // per-warp table of the batch's particles (weights, box offset, membership, charge)
         float *wt = reinterpret_cast<float *>(smraw + (size_t)cap_bytes) + (threadIdx.x >> 5) * 32 * WREC;
         for (int base = b0 + (threadIdx.x & ~31); base < b1; base += blockDim.x) {
             const int p = base + lane;
@@ -193,20 +177,49 @@ __global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4
             float *mine = wt + lane * WREC;
             if (dm) {
                 float Wx[P1], Wy[P1], Wz[P1];
-                const int gx = stencil_fast<P>(X[3 * p + 0], inv[0], quirk4, Wx);
-                const int gy = stencil_fast<P>(X[3 * p + 1], inv[1], quirk4, Wy);
-                const int gz = stencil_fast<P>(X[3 * p + 2], inv[2], quirk4, Wz);
+                const int gs[3] = {stencil_fast<P>(X[3 * p + 0], inv[0], quirk4, Wx),
+                                   stencil_fast<P>(X[3 * p + 1], inv[1], quirk4, Wy),
+                                   stencil_fast<P>(X[3 * p + 2], inv[2], quirk4, Wz)};
+                int d[3];
+                bool in = true;
 #pragma unroll
-                for (int i = 0; i < P1; i++) {
-                    mine[i] = Wx[i];
-                    mine[P1 + i] = Wy[i];
-                    mine[2 * P1 + i] = Wz[i];
+                for (int j = 0; j < 3; j++) {
+                    d[j] = wrapi(gs[j] - lo[j], nn[j]);
+                    in = in && d[j] <= span[j];
                 }
-                mine[3 * P1] = __int_as_float((unwrap_delta(gz - ts.ref[2], g.nz) - ts.lo[2]) * E01 +
-                                              (unwrap_delta(gy - ts.ref[1], g.ny) - ts.lo[1]) * E0 +
-                                              (unwrap_delta(gx - ts.ref[0], g.nx) - ts.lo[0]));
-                mine[3 * P1 + 1] = __uint_as_float(dm);
-                mine[3 * P1 + 2] = q ? q[p] : 0.f;
+                const float qp = q ? q[p] : 0.f;
+                if (!in) {   // drifted out of the tile box: straight to global memory
+#pragma unroll 1
+                    for (int e = 0; e < P1; e++) {
+                        const float wz = sel<P>(Wz, e);
+                        const long long mz = (long long)g.nx * g.ny * wrapi(gs[2] + e, g.nz);
+#pragma unroll 1
+                        for (int bb = 0; bb < P1; bb++) {
+                            const float wyz = sel<P>(Wy, bb) * wz;
+                            const long long my = mz + (long long)g.nx * wrapi(gs[1] + bb, g.ny);
+#pragma unroll
+                            for (int a = 0; a < P1; a++) {
+                                const float w = Wx[a] * wyz;
+                                for (int f = 0; f < nfields; f++) {
+                                    const float v = field_coef(dm, dq, f, qp) * w;
+                                    if (v != 0.f) global_add<FIXED>(dep, depfix, g.M, f, my + wrapi(gs[0] + a, g.nx), v);
+                                }
+                            }
+                        }
+                    }
+                    dm = 0u;
+                } else {
+#pragma unroll
+                    for (int i = 0; i < P1; i++) mine[i] = Wx[i];
+#pragma unroll
+                    for (int e = 0; e < P1; e++)
+#pragma unroll
+                        for (int bb = 0; bb < P1; bb++) mine[P1 + e * P1 + bb] = Wy[bb] * Wz[e];
+                    mine[P1 + P1 * P1] = __int_as_float(d[2] * E01 + d[1] * E0 + d[0]);
+#pragma unroll
+                    for (int f = 0; f < NC; f++)
+                        mine[P1 + P1 * P1 + 1 + f] = f < nfields ? field_coef(dm, dq, f, qp) : 0.f;
+                }
             }
             unsigned rem = __ballot_sync(full, dm != 0u);
             __syncwarp();
@@ -214,21 +227,19 @@ __global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4
                 const int j = __ffs(rem) - 1;
                 rem &= rem - 1;
                 const float *pj = wt + j * WREC;
-                const int offj = __float_as_int(pj[3 * P1]);
-                const uint32_t dmj = __float_as_uint(pj[3 * P1 + 1]);
-                const float qj = pj[3 * P1 + 2];
-                float cf[NF ? NF : kMaxFields];
+                const int offj = __float_as_int(pj[P1 + P1 * P1]);
+                float cf[NC];
 #pragma unroll
-                for (int f = 0; f < (NF ? NF : kMaxFields); f++) cf[f] = f < nfields ? field_coef(dmj, dq, f, qj) : 0.f;
+                for (int f = 0; f < NC; f++) cf[f] = pj[P1 + P1 * P1 + 1 + f];
 #pragma unroll
                 for (int k = 0; k < NPASS; k++) {
                     if (lane + 32 * k >= G) break;
                     // Wx * (Wy * Wz): the association of the unstaged path, so that the
                     // deterministic mode's fixed-point values do not depend on staging
-                    const float w = pj[sa[k]] * (pj[P1 + sb[k]] * pj[2 * P1 + se[k]]);
-                    const int idx = offj + se[k] * E01 + sb[k] * E0 + sa[k];
+                    const float w = pj[sa[k]] * pj[P1 + syz[k]];
+                    const int idx = offj + loff[k];
 #pragma unroll
-                    for (int f = 0; f < (NF ? NF : kMaxFields); f++)
+                    for (int f = 0; f < NC; f++)
                         if (cf[f] != 0.f) smem_add<FIXED>(tf, tu, f * V + idx, cf[f] * w);
                 }
             }
@@ -299,10 +310,11 @@ static void dep_launch_nf(int nb, int threads, const Geom &g, const ParticlePara
     // box capacity: the host's estimate for sorted tiles, else the fixed maximum
     const int nf = NF ? NF : pp.nd;
     const size_t esz = depfix ? 8 : 4;
-    int cap = tc.start ? (int)((size_t)tc.box * nf * esz) : (depfix ? kDepSmemFixed : kDepSmemFast);
+    int cap = tc.start ? (int)((size_t)tc.pbox * nf * esz) : 0;   // the fixed tile box (no staging unsorted)
     cap = std::min(cap, depfix ? kDepSmemFixed : kDepSmemFast);
     cap = (cap + 15) & ~15;
-    const size_t table = (size_t)(threads / 32) * 32 * (3 * (P + 1) + 4) * sizeof(float);
+    constexpr int WREC = (P + 1) + (P + 1) * (P + 1) + 1 + (NF ? NF : kMaxFields);   // as in the kernel
+    const size_t table = (size_t)(threads / 32) * 32 * WREC * sizeof(float);
     if (depfix)
         k_deposit_tiled<P, NF, true><<<nb, threads, cap + table, st>>>(g, pp.N, pp.quirk4, pp.nd, pp.dchan_charge, X0,
                                                                        X1, d_step, pflags, q, dep, depfix, cap, tc);
@@ -329,8 +341,8 @@ static void dep_launch(const Geom &g, const ParticleParams &pp, const float *X0,
 void init_deposit_attributes()
 {
 #define TILD_DA1(P, NF)                                                                                        \
-    cudaFuncSetAttribute(k_deposit_tiled<P, NF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDepSmemFixed + 40960); \
-    cudaFuncSetAttribute(k_deposit_tiled<P, NF, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDepSmemFast + 40960)
+    cudaFuncSetAttribute(k_deposit_tiled<P, NF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDepSmemFixed + kDepTableMax); \
+    cudaFuncSetAttribute(k_deposit_tiled<P, NF, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDepSmemFast + kDepTableMax)
 #define TILD_DA(P) TILD_DA1(P, 0); TILD_DA1(P, 1); TILD_DA1(P, 2)
     TILD_DA(0);
     TILD_DA(1);

@@ -178,17 +178,6 @@ __device__ __forceinline__ void gather_global(const Geom &g, const float4 *__res
     acc[2] = a2;
 }
 
-// every third bit -> 10-bit value (inverse of the sort's spread3)
-__device__ __forceinline__ int compact3(uint32_t v)
-{
-    v &= 0x09249249u;
-    v = (v | (v >> 2)) & 0x030C30C3u;
-    v = (v | (v >> 4)) & 0x0300F00Fu;
-    v = (v | (v >> 8)) & 0x030000FFu;
-    v = (v | (v >> 16)) & 0x000003FFu;
-    return (int)v;
-}
-
 constexpr int kPartOut = 32;   // particles per pass gathered from global memory by helpers
 
 // Particle pass over one Morton tile of particles (or a window of slots), one particle
@@ -232,18 +221,7 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
     int lo[3] = {0, 0, 0}, span[3] = {-1, -1, -1}, E[3] = {0, 0, 0};
     bool staged = false;
     if (tc.start) {
-        int bits = 0;
-        while ((1 << bits) < tc.codes) bits++;
-        const uint32_t k0 = (uint32_t)blockIdx.x * (uint32_t)tc.codes;
-        const int nbr[3] = {1 << ((bits + 2) / 3), 1 << ((bits + 1) / 3), 1 << (bits / 3)};
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            const int c0 = 4 * compact3(k0 >> j);
-            const int c1 = min(c0 + 4 * nbr[j], nn[j]) - 1;
-            lo[j] = c0 - P / 2 - tc.margin;
-            span[j] = c1 - c0 + (P % 2 == 0 ? 1 : 0) + 2 * tc.margin;
-            E[j] = span[j] + P + 1;
-        }
+        tile_box<P>(tc, nn, lo, span, E);
         staged = E[0] <= kMaxBoxEdge && E[1] <= kMaxBoxEdge && E[2] <= kMaxBoxEdge &&
                  (long long)((((E[0] | 1) * E[1]) | 1)) * E[2] <= box_cap;
     }

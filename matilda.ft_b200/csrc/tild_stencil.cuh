@@ -153,6 +153,37 @@ __device__ __forceinline__ void tile_range(const TileCfg &tc, int N, int window,
     }
 }
 
+// every third bit -> 10-bit value (inverse of the sort's brick-key interleave)
+__device__ __forceinline__ int compact3(uint32_t v)
+{
+    v &= 0x09249249u;
+    v = (v | (v >> 2)) & 0x030C30C3u;
+    v = (v | (v >> 4)) & 0x0300F00Fu;
+    v = (v | (v >> 8)) & 0x030000FFu;
+    v = (v | (v >> 16)) & 0x000003FFu;
+    return (int)v;
+}
+
+// Fixed box of a sorted tile: the grid cells of its block of bricks (where its particles
+// were at the last sort) widened by tc.margin cells per side, as stencil origins
+// lo[j] .. lo[j] + span[j]; E[j] = span[j] + P + 1 grid points per axis.
+template <int P>
+__device__ __forceinline__ void tile_box(const TileCfg &tc, const int *nn, int *lo, int *span, int *E)
+{
+    int bits = 0;
+    while ((1 << bits) < tc.codes) bits++;
+    const uint32_t k0 = (uint32_t)blockIdx.x * (uint32_t)tc.codes;
+    const int nbr[3] = {1 << ((bits + 2) / 3), 1 << ((bits + 1) / 3), 1 << (bits / 3)};
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        const int c0 = 4 * compact3(k0 >> j);
+        const int c1 = min(c0 + 4 * nbr[j], nn[j]) - 1;
+        lo[j] = c0 - P / 2 - tc.margin;
+        span[j] = c1 - c0 + (P % 2 == 0 ? 1 : 0) + 2 * tc.margin;
+        E[j] = span[j] + P + 1;
+    }
+}
+
 // Fill the per-axis index tables of a box with edges E (all threads; E[d] <= kMaxBoxEdge).
 __device__ __forceinline__ void tile_tables(TileShared &ts, int nx, int ny, int nz, const int *E)
 {
