@@ -136,8 +136,11 @@ int tild_box_forces(tild_box *box, float *f_out);
 
 /* Thermodynamic terms at the current positions (PS_Box::computeThermoProps,
  * PS_Box.cu:282-317) in FP64: out[0] = Upe, out[1] = Ubond, out[2+i] = energy of
- * potential i; then, if nout >= 2 + npot + 6, the bond virial sum (6 comps, 3-D).
- * Returns the number of values written through *nwritten (may be NULL). */
+ * potential i (i < npot); then three 6-component tensors in the order xx, yy, zz, xy,
+ * xz, yz: the bond virial sum_bonds dr_a f_b, the pair virial -dU_pair/d(strain_ab)
+ * (= U_pair delta_ab + sum_k (du/dk / k) k_a k_b Re(rho_I* rho_J), the reference has no
+ * counterpart), and the pressure tensor (N kT delta_ab + W_pair + W_bond) / V with kT = 1.
+ * Writes min(nout, 2 + npot + 18) values; *nwritten (may be NULL) receives the count. */
 int tild_box_thermo(tild_box *box, double *out, int nout, int *nwritten);
 
 /* Copy positions device -> host (x_out[n*Dim]) / host -> device.  Setting positions
@@ -167,6 +170,15 @@ int tild_box_get_density(tild_box *box, const char *group, int charge_channel, f
  * to rho_out[M] has finished. */
 #define TILD_NOALLOC_SCRATCH_BYTES (16u << 20)
 int tild_box_get_density_noalloc(tild_box *box, const char *group, int charge_channel, float *rho_out);
+
+/* Structure factor of group `group`'s density (or its charge density when charge_channel
+ * != 0) at the current positions: rho^(k) rho^(-k) with rho^ = FFT(rho)/M, as the
+ * reference's S(k) compute defines it (ps_compute_sk.cu:18-50, which the reference never
+ * initialises), over every k-vector of the grid, averaged in nbins shells of |k| of width
+ * kmax/nbins, in FP64: sk_out[b], the mean |k| in the shell k_out[b] and the number of
+ * k-vectors count_out[b] (any of the three may be NULL). */
+int tild_box_structure_factor(tild_box *box, const char *group, int charge_channel, int32_t nbins, double kmax,
+                              double *k_out, double *sk_out, double *count_out);
 
 /* Stencil indices and weights of every particle at the current positions
  * (d_calcGridWeights, ps_grid_utils.cu:74-204): inds_out/w_out[n*(pmeorder+1)^Dim],

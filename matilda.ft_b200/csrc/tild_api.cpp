@@ -239,6 +239,14 @@ int tild_box_get_density_noalloc(tild_box *box, const char *group, int charge_ch
     return guarded([&] { box->impl->getDensityNoAlloc(group, charge_channel, rho_out); });
 }
 
+int tild_box_structure_factor(tild_box *box, const char *group, int charge_channel, int32_t nbins, double kmax,
+                              double *k_out, double *sk_out, double *count_out)
+{
+    NEED_BOX;
+    if (!group) return fail(TILD_ERR_ARG, "NULL argument");
+    return guarded([&] { box->impl->structureFactor(group, charge_channel, nbins, kmax, k_out, sk_out, count_out); });
+}
+
 int tild_box_grid_weights(tild_box *box, int32_t *inds_out, float *w_out)
 {
     NEED_BOX;

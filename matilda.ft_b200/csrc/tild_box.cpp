@@ -837,9 +837,9 @@ void Box::allocDevice()
     const int TXz = 8;
     nblkZ = ((g.nxh + TXz - 1) / TXz) * g.ny;
     nblkP = (int)((N + 255) / 256);
-    dEpart = dalloc<double>((size_t)nblkZ * std::max(1, ksHost.neterms));
+    dEpart = dalloc<double>((size_t)nblkZ * (ksHost.neterms + 6));
     dBpart = dalloc<double>((size_t)nblkP * 7);
-    dRes = dalloc<double>(kMaxPots + 8);
+    dRes = dalloc<double>(kResSize);
     dTmp = dalloc<float>(3 * N);
     if (sharedDevice) hKsPinned = new KSpace;   // pinned host memory would synchronise the device when freed
     else ck(cudaMallocHost(&hKsPinned, sizeof(KSpace)), "cudaMallocHost");
@@ -910,6 +910,7 @@ void Box::uploadParticles()
     ck(cudaMemcpy(dBtype, bt8.data(), N * MAXBONDS, cudaMemcpyHostToDevice), "upload bond types");
     long long zero = 0;
     ck(cudaMemcpy(dStep, &zero, sizeof(zero), cudaMemcpyHostToDevice), "upload step");
+    ck(cudaMemset(dRes, 0, sizeof(double) * kResSize), "zero results");
     uploadFlags();
     if (rngCompat) {   // d_initDeviceRNG (device_utils.cu:465-472), seed = RANDSEED (unsigned int)
         ck(launch_rng_init(dRng, dOrig, (int)N, (unsigned long long)(unsigned int)RANDSEED, stream), "rng init");
@@ -1025,7 +1026,7 @@ void Box::enqueueStep(bool energy, bool integrate, float *fout_dev)
         ck(launch_ypass(g, ly, nd, 0, dH, st), "fft y forward");
         mark(STAGE_YFWD);
         ck(launch_kspace_z(g, lz, ksHost, dKs, dH, dUk, dHg, dEpart, energy ? 1 : 0, nfg > 0 ? 1 : 0, nullptr, st), "kspace");
-        if (energy && ksHost.neterms > 0) ck(launch_reduce_partials(dEpart, nblkZ, ksHost.neterms, dRes, st), "reduce");
+        if (energy && ksHost.neterms > 0) ck(launch_reduce_partials(dEpart, nblkZ, ksHost.neterms + 6, dRes, st), "reduce");
         mark(STAGE_KSPACE);
         if (nfg > 0) {
             ck(launch_ypass(g, ly, 3 * nfg, 1, dHg, st), "fft y inverse");
@@ -1041,7 +1042,7 @@ void Box::enqueueStep(bool energy, bool integrate, float *fout_dev)
     if (integrate) ck(launch_tick(dStep, st), "tick");
     if (energy) {
         ck(launch_bond_energy(g, ppHost, dPp, dX[0], dX[1], dStep, dNb, dPartner, dBtype, dBpart, nullptr, st), "bond energy");
-        ck(launch_reduce_partials(dBpart, nblkP, 7, dRes + kMaxPots, st), "reduce bonds");
+        ck(launch_reduce_partials(dBpart, nblkP, 7, dRes + kResBond, st), "reduce bonds");
     }
 }
 
@@ -1060,15 +1061,15 @@ void Box::enqueueEnergyOnly()
         ck(launch_xfwd(g, lx, npair, nd, dDep, deterministic ? dDepFix : nullptr, dH, st), "fft x forward");
         ck(launch_ypass(g, ly, nd, 0, dH, st), "fft y forward");
         ck(launch_kspace_z(g, lz, ksHost, dKs, dH, dUk, dHg, dEpart, 1, 0, nullptr, st), "kspace energy");
-        ck(launch_reduce_partials(dEpart, nblkZ, ksHost.neterms, dRes, st), "reduce");
+        ck(launch_reduce_partials(dEpart, nblkZ, ksHost.neterms + 6, dRes, st), "reduce");
     }
     ck(launch_bond_energy(g, ppHost, dPp, dX[0], dX[1], dStep, dNb, dPartner, dBtype, dBpart, nullptr, st), "bond energy");
-    ck(launch_reduce_partials(dBpart, nblkP, 7, dRes + kMaxPots, st), "reduce bonds");
+    ck(launch_reduce_partials(dBpart, nblkP, 7, dRes + kResBond, st), "reduce bonds");
 }
 
 std::vector<double> Box::readEnergies(bool)
 {
-    std::vector<double> r(kMaxPots + 8, 0.0);
+    std::vector<double> r(kResSize, 0.0);
     ck(cudaStreamSynchronize(stream), "sync");
     ck(cudaMemcpy(r.data(), dRes, sizeof(double) * r.size(), cudaMemcpyDeviceToHost), "read energies");
     return r;
@@ -1202,7 +1203,7 @@ void Box::NVT(int64_t nSteps)
             std::vector<double> r = readEnergies(true);
             for (int k = 0; k < npot; k++)   // CalcEnergy runs after update_prefactor (PS_Box.cu:159-172)
                 lastPair[k] = r[k] * (ampUsed[k] != 0.0 ? potentials[k].amp_eff / ampUsed[k] : 1.0);
-            lastBond = 0.5 * r[kMaxPots];
+            lastBond = 0.5 * r[kResBond];
             if (i % logFreq == 0) writeData(i, lastPair, lastBond);
         }
     }
@@ -1248,12 +1249,23 @@ std::vector<double> Box::thermo()
     enqueueEnergyOnly();
     std::vector<double> r = readEnergies(true);
     std::vector<double> out;
-    double ubond = 0.5 * r[kMaxPots], upe = ubond;
-    for (size_t k = 0; k < potentials.size(); k++) upe += r[k];
+    const size_t np = potentials.size();
+    double ubond = 0.5 * r[kResBond], upe = ubond, upair = 0.0;
+    for (size_t k = 0; k < np; k++) upair += r[k];
+    upe += upair;
     out.push_back(upe);
     out.push_back(ubond);
-    for (size_t k = 0; k < potentials.size(); k++) out.push_back(r[k]);
-    for (int c = 0; c < 6; c++) out.push_back(0.5 * r[kMaxPots + 1 + c]);
+    for (size_t k = 0; k < np; k++) out.push_back(r[k]);
+    double wb[6], wp[6];
+    for (int c = 0; c < 6; c++) {
+        wb[c] = 0.5 * r[kResBond + 1 + c];                    // bonds: sum over bonds of dr_a f_b
+        wp[c] = r[np + c] + (c < 3 ? upair : 0.0);            // pairs: -dU/d(strain_ab)
+        out.push_back(wb[c]);
+    }
+    // pair virial, then the pressure tensor (N kT delta_ab + W_pair + W_bond) / V, kT = 1
+    for (int c = 0; c < 6; c++) out.push_back(wp[c]);
+    const double V = (double)L[0] * L[1] * L[2];
+    for (int c = 0; c < 6; c++) out.push_back(((c < 3 ? (double)nstot : 0.0) + wp[c] + wb[c]) / V);
     return out;
 }
 
@@ -1357,6 +1369,59 @@ void Box::getDensityNoAlloc(const std::string &group, int charge, float *rho)
        "density");
     ck(cudaMemcpyAsync(rho, dRho, 4 * geom.M, cudaMemcpyDeviceToHost, stream), "read density");
     ck(cudaStreamSynchronize(stream), "density");
+}
+
+// S(k) of a group's density (ps_compute_sk.cu:18-50: rho^(k) rho^(-k) with the forward
+// transform divided by M) for the current positions, binned by |k| in FP64.
+void Box::structureFactor(const std::string &group, int charge, int nbins, double kmax, double *k_out,
+                          double *sk_out, double *count_out)
+{
+    if (!ready) fail(TILD_ERR_STATE, "endBox has not been processed");
+    if (nbins < 1 || nbins > (1 << 16)) fail(TILD_ERR_ARG, "nbins must be in [1, 65536]");
+    if (!(kmax > 0.0)) fail(TILD_ERR_ARG, "kmax must be > 0");
+    const int gi = findGroupInteger(group);
+    if (charge && !psGroup[gi].isCharges) fail(TILD_ERR_ARG, "only the 'charges' group has a charge density");
+    ck(cudaSetDevice(device), "cudaSetDevice");
+    const long long s = deviceStep();
+    const std::vector<int> orig = slotOrder();
+    std::vector<int> slotOf(nstot);
+    for (int64_t k = 0; k < nstot; k++) slotOf[orig[k]] = (int)k;
+    std::vector<int> sites(psGroup[gi].siteList);
+    for (int &v : sites) v = slotOf[v];
+    const Geom &g = geom;
+    int *dSites = nullptr;
+    float *dRho = nullptr;
+    float2 *dPair = nullptr, *dHs = nullptr;
+    double *dBins = nullptr;
+    cudaError_t e = cudaMalloc(&dSites, 4 * std::max<size_t>(1, sites.size()));
+    if (e == cudaSuccess) e = cudaMalloc(&dRho, 4 * g.M);
+    if (e == cudaSuccess) e = cudaMalloc(&dPair, 8 * g.M);
+    if (e == cudaSuccess) e = cudaMalloc(&dHs, 8 * g.hstride);
+    if (e == cudaSuccess) e = cudaMalloc(&dBins, 3 * sizeof(double) * nbins);
+    if (e == cudaSuccess && !sites.empty())
+        e = cudaMemcpy(dSites, sites.data(), 4 * sites.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dRho, 0, 4 * g.M, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dBins, 0, 3 * sizeof(double) * nbins, stream);
+    if (e == cudaSuccess)
+        e = launch_density_single(g, ppHost, dX[s & 1], dSites, (int)sites.size(), dQ, charge, dRho, stream);
+    if (e == cudaSuccess) e = launch_to_pairs(dRho, dPair, g.M, stream);
+    if (e == cudaSuccess)
+        e = launch_structure_factor(g, lx, ly, lz, ksHost.twopi_over_L, dPair, dHs, nbins, kmax / nbins, dBins, stream);
+    std::vector<double> b(3 * (size_t)nbins, 0.0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess) e = cudaMemcpy(b.data(), dBins, 3 * sizeof(double) * nbins, cudaMemcpyDeviceToHost);
+    cudaFree(dSites);
+    cudaFree(dRho);
+    cudaFree(dPair);
+    cudaFree(dHs);
+    cudaFree(dBins);
+    ck(e, "structure factor");
+    for (int i = 0; i < nbins; i++) {
+        const double n = b[3 * i + 2];
+        if (sk_out) sk_out[i] = n > 0.0 ? b[3 * i] / n : 0.0;
+        if (k_out) k_out[i] = n > 0.0 ? b[3 * i + 1] / n : (i + 0.5) * kmax / nbins;
+        if (count_out) count_out[i] = n;
+    }
 }
 
 void Box::gridWeights(int32_t *inds, float *w)

@@ -93,6 +93,8 @@ public:
     void setPositions(const float *x);
     void getDensity(const std::string &group, int charge, float *rho);
     void getDensityNoAlloc(const std::string &group, int charge, float *rho);
+    void structureFactor(const std::string &group, int charge, int nbins, double kmax, double *k_out,
+                         double *sk_out, double *count_out);
     void gridWeights(int32_t *inds, float *w);
     void modifyBox(const std::string &rest);           // PS_Box.cu:848-870
     void stageTimes(std::vector<double> &out) const { out = stageSec; }

@@ -21,6 +21,11 @@ constexpr int kMaxFields = 8;     // density fields D
 constexpr int kMaxFGroups = 4;    // force groups F (3F gradient fields)
 constexpr int kMaxPots = 16;
 constexpr int kMaxTerms = 32;
+// FP64 results of the energy reductions: pair energy of each potential at [0, npots),
+// the summed pair virial W_ab (xx, yy, zz, xy, xz, yz) right after them, the bond energy
+// and bond virial at kResBond
+constexpr int kResBond = kMaxPots + 6;
+constexpr int kResSize = kResBond + 8;
 constexpr int kMaxTypes = 16;
 constexpr int kMaxBondTypes = 16;
 constexpr int kMaxStages = 20;
@@ -150,6 +155,13 @@ cudaError_t launch_kspace_z(const Geom &g, const FftLine &lz, const KSpace &ks, 
                             int *nblocks_out, cudaStream_t st);
 // FP32 table of every potential's û(k) shape (amplitude 1) over the half spectrum
 cudaError_t launch_uk_table(const Geom &g, const KSpace *ks_dev, float *tab, cudaStream_t st);
+// S(|k|) of one real field given as float2 pairs (field in .x): x/y forward passes into
+// Hs, then the z pass bins |FFT(rho)/M|^2 into bins[3*nbins] (S, |k|, count; FP64)
+// out[m] = (rho[m], 0)
+cudaError_t launch_to_pairs(const float *rho, float2 *out, long long M, cudaStream_t st);
+cudaError_t launch_structure_factor(const Geom &g, const FftLine &lx, const FftLine &ly, const FftLine &lz,
+                                   const double *twopi_over_L, const float2 *rho_pair, float2 *Hs, int nbins,
+                                   double dk, double *bins, cudaStream_t st);
 cudaError_t launch_xinv(const Geom &g, const FftLine &lx, int nfg, const float2 *Hg, float4 *rec,
                         cudaStream_t st);
 cudaError_t launch_particles(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd,

@@ -381,6 +381,26 @@ __device__ __forceinline__ double uk_amp(const PotDev &p) { return p.kind == POT
 
 __device__ __forceinline__ double uk_eval(const PotDev &p, double k2) { return uk_amp(p) * uk_shape(p, k2); }
 
+// (d û / d k) / k for k > 0, FP64, amplitude included: the strain derivative of the pair
+// energy.  gaussian: -sigma^2 û; charges: û (-2 sigma^2 - 2/k^2); erf2/erfG with
+// t = 4 pi (sin Rk - Rk cos Rk)/k^3: A g t^(p-1) (-sigma^2 t + p t'/k),
+// t'/k = 4 pi (R^2 sin(Rk)/k^3 - 3 (sin Rk - Rk cos Rk)/k^5).
+__device__ double uk_dk_over_k(const PotDev &p, double k2)
+{
+    if (k2 <= 0.0) return 0.0;
+    if (p.kind == POT_GAUSSIAN) return -p.sig2 * uk_eval(p, k2);
+    if (p.kind == POT_CHARGES) return uk_eval(p, k2) * (-2.0 * p.sig2 - 2.0 / k2);
+    const double PI4 = 12.566370614359172953850573533118;
+    const double R = p.Rp, k = sqrt(k2);
+    double sn, cs;
+    sincos(R * k, &sn, &cs);
+    const double f = sn - R * k * cs;
+    const double t = PI4 * f / (k2 * k);
+    const double dt_k = PI4 * (R * R * sn / (k2 * k) - 3.0 * f / (k2 * k2 * k));
+    const double gs = exp(-0.5 * k2 * p.sig2);
+    return p.kind == POT_ERF2 ? p.amp * gs * t * (-p.sig2 * t + 2.0 * dt_k) : p.amp * gs * (-p.sig2 * t + dt_k);
+}
+
 __device__ __forceinline__ int signed_index(int i, int n) { return (i < n - i) ? i : i - n; }
 
 // FP32 shape table of every potential over the half spectrum, layout of one density field
@@ -431,7 +451,11 @@ __global__ void __launch_bounds__(256) k_kspace_z(Geom g, FftLine lz, const KSpa
     const bool nyq_y = (g.ny % 2 == 0) && (y == g.ny / 2);
 
     if (energy) {
+        // per potential U_t = fac sum_k u(k) Re(rho_I* rho_J) (Parseval); the summed
+        // virial W_ab = sum_t [U_t delta_ab + fac sum_k (u'(k)/k) k_a k_b Re(...)] keeps only
+        // the second part here (the host adds the first)
         double acc[kMaxPots];
+        double vir[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         for (int t = 0; t < ks.neterms; t++) acc[t] = 0.0;
         for (int e = threadIdx.x; e < nz * TX; e += blockDim.x) {
             const int z = e / TX, c = e - z * TX, kx = kx0 + c;
@@ -440,24 +464,33 @@ __global__ void __launch_bounds__(256) k_kspace_z(Geom g, FftLine lz, const KSpa
             const double kzv = ks.twopi_over_L[2] * signed_index(z, g.nz);
             const double k2 = kxv * kxv + kyv * kyv + kzv * kzv;
             const double wgt = (kx == 0 || (g.nx % 2 == 0 && kx == g.nx / 2)) ? 1.0 : 2.0;
+            double sv = 0.0;
             for (int t = 0; t < ks.neterms; t++) {
                 const ETerm &et = ks.eterms[t];
                 const float2 rI = R[z * nd * TX + et.dI * TX + c], rJ = R[z * nd * TX + et.dJ * TX + c];
                 const double re = (double)rJ.x * rI.x + (double)rJ.y * rI.y;
                 acc[t] += wgt * et.fac * uk_eval(ks.pots[et.pot], k2) * re;
+                sv += wgt * et.fac * uk_dk_over_k(ks.pots[et.pot], k2) * re;
             }
+            vir[0] += sv * kxv * kxv;
+            vir[1] += sv * kyv * kyv;
+            vir[2] += sv * kzv * kzv;
+            vir[3] += sv * kxv * kyv;
+            vir[4] += sv * kxv * kzv;
+            vir[5] += sv * kyv * kzv;
         }
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
         const long long blin = (long long)blockIdx.y * gridDim.x + blockIdx.x;
-        for (int t = 0; t < ks.neterms; t++) {
-            double v = acc[t];
+        const int ncol = ks.neterms + 6;
+        for (int t = 0; t < ncol; t++) {
+            double v = t < ks.neterms ? acc[t] : sel<5>(vir, t - ks.neterms);
             for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
             if (lane == 0) red[warp] = v;
             __syncthreads();
             if (threadIdx.x == 0) {
                 double s = 0.0;
                 for (int w = 0; w < nw; w++) s += red[w];
-                epart[blin * ks.neterms + t] = s;
+                epart[blin * ncol + t] = s;
             }
             __syncthreads();
         }
@@ -526,6 +559,40 @@ __global__ void __launch_bounds__(256) k_kspace_z(Geom g, FftLine lz, const KSpa
             }
             __syncthreads();
         }
+    }
+}
+
+// Structure factor pass (after the x and y forward passes of one field): z FFT of a
+// column block, then |rho^(k)|^2 * scale binned by |k| in FP64 over the full grid (the
+// half spectrum's interior kx columns stand for their Hermitian partners too).
+// bins[3b] += S, bins[3b+1] += |k|, bins[3b+2] += count.
+template <int TX>
+__global__ void __launch_bounds__(256) k_sk_z(Geom g, FftLine lz, const float2 *__restrict__ H, double tx,
+                                              double ty, double tz, double scale, int nbins, double inv_dk,
+                                              double *__restrict__ bins)
+{
+    extern __shared__ __align__(16) float2 sm[];
+    const int nz = g.nz;
+    float2 *A = sm, *B = sm + nz * TX, *tw = sm + 2 * nz * TX;
+    const int kx0 = blockIdx.x * TX, y = blockIdx.y;
+    for (int t = threadIdx.x; t < nz; t += blockDim.x) tw[t] = lz.tw[t];
+    tile_load_async(A, TX, H + (long long)y * g.hp + kx0, (long long)g.ny * g.hp, nz, TX, g.nxh - kx0);
+    cp_async_wait_all();
+    __syncthreads();
+    const float2 *R = fft_lines<false>(A, B, TX, 1, TX, lz, tw, true, make_fastdiv_dev(TX));
+    const double kyv = ty * signed_index(y, g.ny);
+    for (int e = threadIdx.x; e < nz * TX; e += blockDim.x) {
+        const int z = e / TX, c = e - z * TX, kx = kx0 + c;
+        if (kx >= g.nxh) continue;
+        const double kxv = tx * signed_index(kx, g.nx), kzv = tz * signed_index(z, g.nz);
+        const double k = sqrt(kxv * kxv + kyv * kyv + kzv * kzv);
+        const int b = (int)(k * inv_dk);
+        if (b >= nbins) continue;
+        const double w = (kx == 0 || (g.nx % 2 == 0 && kx == g.nx / 2)) ? 1.0 : 2.0;
+        const float2 v = R[e];
+        atomicAdd(bins + 3 * b, w * scale * ((double)v.x * v.x + (double)v.y * v.y));
+        atomicAdd(bins + 3 * b + 1, w * k);
+        atomicAdd(bins + 3 * b + 2, w);
     }
 }
 
@@ -603,6 +670,7 @@ void init_fft_attributes()
     set_max_smem(k_ypass<false, kTXy>, 200 * 1024);
     set_max_smem(k_ypass<true, kTXy>, 200 * 1024);
     set_max_smem(k_kspace_z<kTXz>, 220 * 1024);
+    set_max_smem(k_sk_z<kTXz>, 200 * 1024);
     set_max_smem(k_xinv, 200 * 1024);
 }
 
@@ -689,6 +757,22 @@ cudaError_t launch_xinv(const Geom &g, const FftLine &lx, int nfg, const float2 
 cudaError_t launch_uk_table(const Geom &g, const KSpace *ks_dev, float *tab, cudaStream_t st)
 {
     k_uk_table<<<(unsigned)((g.hstride + 255) / 256), 256, 0, st>>>(g, ks_dev, tab);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_structure_factor(const Geom &g, const FftLine &lx, const FftLine &ly, const FftLine &lz,
+                                   const double *twopi_over_L, const float2 *rho_pair, float2 *Hs, int nbins,
+                                   double dk, double *bins, cudaStream_t st)
+{
+    cudaError_t e = launch_xfwd(g, lx, 1, 1, rho_pair, nullptr, Hs, st);
+    if (e == cudaSuccess) e = launch_ypass(g, ly, 1, 0, Hs, st);
+    if (e != cudaSuccess) return e;
+    constexpr int TX = kTXz;
+    dim3 grid((g.nxh + TX - 1) / TX, g.ny);
+    const size_t sm = (size_t)(2 * g.nz * TX + g.nz) * sizeof(float2);
+    const double M = (double)g.M;
+    k_sk_z<TX><<<grid, 256, sm, st>>>(g, lz, Hs, twopi_over_L[0], twopi_over_L[1], twopi_over_L[2],
+                                      1.0 / (M * M), nbins, 1.0 / dk, bins);
     return cudaGetLastError();
 }
 

@@ -401,4 +401,16 @@ cudaError_t launch_density_single(const Geom &g, const ParticleParams &pp, const
     return cudaGetLastError();
 }
 
+__global__ void k_to_pairs(const float *__restrict__ rho, float2 *__restrict__ out, long long M)
+{
+    const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < M) out[m] = make_float2(rho[m], 0.f);
+}
+
+cudaError_t launch_to_pairs(const float *rho, float2 *out, long long M, cudaStream_t st)
+{
+    k_to_pairs<<<(unsigned)((M + 255) / 256), 256, 0, st>>>(rho, out, M);
+    return cudaGetLastError();
+}
+
 }  // namespace tild

@@ -52,6 +52,8 @@ _SIGS = {
     "tild_box_get_density_noalloc": ([ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p],
                                      ctypes.c_int),
     "tild_box_grid_weights": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "tild_box_structure_factor": ([ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int32, ctypes.c_double,
+                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "tild_box_get_log": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64),
                           ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
     "tild_run_script_file": ([ctypes.c_char_p, ctypes.c_int], ctypes.c_int),
@@ -211,7 +213,8 @@ class Box:
         npot = self.info().n_potentials
         v = out[: n.value]
         return dict(Upe=float(v[0]), Ubond=float(v[1]), potentials=[float(e) for e in v[2:2 + npot]],
-                    virial=v[2 + npot:2 + npot + 6].copy())
+                    virial=v[2 + npot:2 + npot + 6].copy(), pair_virial=v[8 + npot:14 + npot].copy(),
+                    pressure=v[14 + npot:20 + npot].copy())
 
     def positions(self):
         x = np.zeros((self.N, 3), np.float32)
@@ -234,6 +237,13 @@ class Box:
         rho = np.zeros(int(i.nx[0]) * int(i.nx[1]) * int(i.nx[2]), np.float32)
         _check(lib().tild_box_get_density_noalloc(self._h, group.encode(), int(bool(charge)), _ptr(rho)))
         return rho
+
+    def structure_factor(self, group: str, nbins: int, kmax: float, charge=False):
+        """(k, S(k), count) in nbins shells of |k| up to kmax (FP64)."""
+        k, sk, n = (np.zeros(int(nbins), np.float64) for _ in range(3))
+        _check(lib().tild_box_structure_factor(self._h, group.encode(), int(bool(charge)), int(nbins), float(kmax),
+                                               _ptr(k), _ptr(sk), _ptr(n)))
+        return k, sk, n
 
     def grid_weights(self):
         i = self.info()

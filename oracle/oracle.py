@@ -188,6 +188,91 @@ def uk(pot, k2):
     raise ValueError(kind)
 
 
+def duk_over_k(pot, k2):
+    """(d û/dk)/k of each kind (FP64), 0 at k = 0: the strain derivative of û."""
+    kind = pot["kind"]
+    pos = k2 > 0.0
+    with np.errstate(divide="ignore", invalid="ignore"):
+        if kind == "gaussian":
+            return -pot["sigma"] ** 2 * uk(pot, k2)
+        if kind == "charges":
+            return np.where(pos, uk(pot, k2) * (-2.0 * pot["sigma"] ** 2 - 2.0 / k2), 0.0)
+        if kind in ("erf2", "erfG"):
+            R, s2 = pot["Rp"], pot["sigma"] ** 2
+            k = np.sqrt(k2)
+            f = np.sin(R * k) - R * k * np.cos(R * k)
+            t = PI4 * f / (k2 * k)
+            dt_k = PI4 * (R * R * np.sin(R * k) / (k2 * k) - 3.0 * f / (k2 * k2 * k))
+            g = np.exp(-0.5 * k2 * s2)
+            if kind == "erf2":
+                v = pot["A"] * g * t * (-s2 * t + 2.0 * dt_k)
+            else:
+                v = pot["A"] * g * (-s2 * t + dt_k)
+            return np.where(pos, v, 0.0)
+    raise ValueError(kind)
+
+
+def pair_virial(sysm: System, dens):
+    """Pair virial W_ab = -dU_pair/d(strain_ab) for an affine strain of the box and the
+    positions (the grid follows the box, so the deposited weights do not change):
+    U = C/V sum_k û(|k|) Re(rho_I* rho_J) gives W_ab = U delta_ab + C/V sum_k (û'(k)/k)
+    k_a k_b Re(rho_I* rho_J).  Components xx, yy, zz, xy, xz, yz (FP64)."""
+    glist = groups(sysm)
+    shape = _grid_shape(sysm)
+    M = int(np.prod(sysm.Nx))
+    ks = kvectors(sysm, 64)
+    k2 = sum(k * k for k in ks)
+    _, _, gvol = grid_geometry(sysm)
+    W = np.zeros(6)
+    utot = 0.0
+    pairs = ((0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2))
+    for pot in sysm.potentials:
+        if pot["kind"] == "charges":
+            rI = rJ = dens["charges"][1]
+            fac = 0.5
+        else:
+            rI = dens[glist[find_group(glist, pot["I"])][0]][0]
+            rJ = dens[glist[find_group(glist, pot["J"])][0]][0]
+            fac = 1.0
+        fI = np.fft.fftn(rI.astype(np.float64).reshape(shape)) / M
+        fJ = np.fft.fftn(rJ.astype(np.float64).reshape(shape)) / M
+        re = (np.conj(fI) * fJ).real
+        c = fac * gvol * M
+        utot += c * float(np.sum(uk(pot, k2) * re))
+        d = duk_over_k(pot, k2) * re
+        for i, (a, b) in enumerate(pairs):
+            W[i] += c * float(np.sum(d * ks[a] * ks[b]))
+    W[:3] += utot
+    return W
+
+
+def structure_factor(sysm: System, rho, nbins: int, kmax: float):
+    """S(k) = |FFT(rho)/M|^2 over every k-vector of the grid (ps_compute_sk.cu:18-50),
+    averaged in nbins shells of |k| (width kmax/nbins), k_d = (2 pi/L_d) n_d with the
+    signed index of Box.cu:157-178.  Returns (mean |k|, mean S, count) per shell, FP64."""
+    shape = _grid_shape(sysm)
+    M = int(np.prod(sysm.Nx))
+    f = np.fft.fftn(np.asarray(rho, np.float64).reshape(shape)) / M
+    S = (f.real ** 2 + f.imag ** 2).reshape(-1)
+    ks = []
+    for d in range(3):
+        N = int(sysm.Nx[d])
+        n = np.arange(N)
+        k = (2.0 * np.pi / float(np.float32(sysm.L[d]))) * np.where(n < N - n, n, n - N)
+        s = [1, 1, 1]
+        s[2 - d] = N
+        ks.append(k.reshape(s))
+    kk = np.sqrt(np.broadcast_to(ks[0] ** 2 + ks[1] ** 2 + ks[2] ** 2, shape)).reshape(-1)
+    b = np.floor(kk * (nbins / kmax)).astype(np.int64)
+    ok = b < nbins
+    cnt = np.bincount(b[ok], minlength=nbins).astype(np.float64)
+    ssum = np.bincount(b[ok], weights=S[ok], minlength=nbins)
+    ksum = np.bincount(b[ok], weights=kk[ok], minlength=nbins)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        return (np.where(cnt > 0, ksum / cnt, (np.arange(nbins) + 0.5) * kmax / nbins),
+                np.where(cnt > 0, ssum / cnt, 0.0), cnt)
+
+
 def _grid_shape(sysm):
     return tuple(int(v) for v in sysm.Nx[::-1])
 

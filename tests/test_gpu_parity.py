@@ -268,3 +268,37 @@ def test_full_size_c2_properties():
         b.step(2)
         x = b.positions()
         assert (x >= 0).all() and (x <= spec.L).all()
+
+
+@pytest.mark.parametrize("name", ["diblock_o3", "charged_o3", "erf", "odd_grid"])
+def test_pair_virial_and_pressure_match_oracle(name):
+    """FP64 pair virial W_ab against the oracle (relative 1e-5 of max |W|), and the pressure
+    tensor equal to (N kT delta + W_pair + W_bond)/V with kT = 1."""
+    spec = SYSTEMS[name]()
+    sysm = spec_to_system(spec)
+    dens, _, _ = oracle.densities(sysm)
+    Wref = oracle.pair_virial(sysm, dens)
+    with make_box(spec) as b:
+        t = b.thermo()
+    W = t["pair_virial"]
+    assert np.abs(W - Wref).max() <= 1e-5 * np.abs(Wref).max(), (W, Wref)
+    V = float(np.prod(np.asarray(spec.L, np.float64)))
+    P = (np.r_[np.full(3, spec.N), np.zeros(3)] + W + t["virial"]) / V
+    assert np.allclose(t["pressure"], P, rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("charge", [False, True])
+def test_structure_factor_matches_oracle(charge):
+    spec = synth.small_system(seed=81, order=3, charges=True, grid=(15, 12, 18))
+    sysm = spec_to_system(spec)
+    dens, _, _ = oracle.densities(sysm)
+    group = "charges" if charge else "A"
+    rho = dens[group][1] if charge else dens[group][0]
+    kmax, nb = 8.0, 40
+    kr, sr, nr = oracle.structure_factor(sysm, rho, nb, kmax)
+    with make_box(spec) as b:
+        k, sk, n = b.structure_factor(group, nb, kmax, charge=charge)
+    assert np.array_equal(n, nr)
+    assert np.allclose(k, kr, rtol=1e-12, atol=0)
+    assert np.all(np.abs(sk - sr) <= 1e-5 * sr + 1e-7 * sr.max())
+

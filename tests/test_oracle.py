@@ -178,3 +178,58 @@ def test_gjf_trajectory_fp32_vs_fp64():
     d = np.abs(t64.positions() - t32.positions())
     d = np.minimum(d, sysm.L - d)
     assert d.max() < 1e-4
+
+
+def _energy_scaled(sysm, dens, scale):
+    """Total pair energy, FP64, after an affine stretch of the box by `scale` per axis.
+    The grid follows the box, so each field's weight sums rho * gvol stay fixed."""
+    glist = oracle.groups(sysm)
+    Nx = sysm.Nx.astype(np.int64)
+    shape = tuple(int(v) for v in Nx[::-1])
+    M = int(np.prod(Nx))
+    L0 = sysm.L.astype(np.float32).astype(np.float64)
+    L = L0 * np.asarray(scale, np.float64)
+    gvol0, gvol = float(np.prod(L0 / Nx)), float(np.prod(L / Nx))
+    ks = []
+    for d in range(3):
+        n = np.arange(Nx[d])
+        k = 2.0 * np.pi * np.where(n < Nx[d] / 2.0, n, n - Nx[d]) / L[d]
+        s = [1, 1, 1]
+        s[2 - d] = int(Nx[d])
+        ks.append(k.reshape(s))
+    k2 = ks[0] ** 2 + ks[1] ** 2 + ks[2] ** 2
+    U = 0.0
+    for pot in sysm.potentials:
+        if pot["kind"] == "charges":
+            rI = rJ = dens["charges"][1]
+            fac = 0.5
+        else:
+            rI = dens[glist[oracle.find_group(glist, pot["I"])][0]][0]
+            rJ = dens[glist[oracle.find_group(glist, pot["J"])][0]][0]
+            fac = 1.0
+        fI = np.fft.fftn(rI.astype(np.float64).reshape(shape) * gvol0 / gvol) / M
+        fJ = np.fft.fftn(rJ.astype(np.float64).reshape(shape) * gvol0 / gvol) / M
+        U += fac * gvol * M * float(np.sum(np.broadcast_to(oracle.uk(pot, k2), shape) * (np.conj(fI) * fJ).real))
+    return U
+
+
+@pytest.mark.parametrize("kind", ["gaussian", "charges", "erf"])
+def test_pair_virial_is_the_strain_derivative_of_the_energy(kind):
+    """W_aa = -dU/d(strain_aa): the FP64 pair virial against central differences of the
+    pair energy under stretching the box along each axis (relative 1e-7)."""
+    if kind == "erf":
+        spec = synth.small_system(seed=71, order=3, pots=[
+            dict(kind="erf2", I="A", J="B", A=0.05, Rp=1.0, sigma=0.5),
+            dict(kind="erfG", I="B", J="B", A=0.3, Rp=0.8, sigma=0.5)])
+    else:
+        spec = synth.small_system(seed=72, order=3, charges=(kind == "charges"))
+    sysm = spec_to_system(spec)
+    dens, _, _ = oracle.densities(sysm)
+    W = oracle.pair_virial(sysm, dens)
+    assert abs(_energy_scaled(sysm, dens, [1, 1, 1]) - sum(oracle.pair_energies(sysm, dens))) <= 1e-9 * abs(W[:3]).max()
+    h = 1e-5
+    for a in range(3):
+        sp, sm = np.ones(3), np.ones(3)
+        sp[a], sm[a] = 1 + h, 1 - h
+        fd = -(_energy_scaled(sysm, dens, sp) - _energy_scaled(sysm, dens, sm)) / (2 * h)
+        assert abs(W[a] - fd) <= 1e-7 * abs(W[:3]).max(), (kind, a, W[a], fd)
