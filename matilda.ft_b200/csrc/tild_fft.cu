@@ -435,7 +435,10 @@ __global__ void __launch_bounds__(256) k_kspace_z(Geom g, FftLine lz, const KSpa
     const KSpace &ks = *ksp;
     const int nz = g.nz, nd = ks.nd;
     const int ndb = nd < 2 ? 2 : nd;
-    float2 *Rho = sm, *S = sm + ndb * nz * TX, *Phi = sm + 2 * ndb * nz * TX, *tw = Phi + nz * TX;
+    // two buffers of nsets line sets (nsets = max(density fields, 2 x force groups)),
+    // each set TX lines of nz points, sets interleaved per z row
+    const int nsets = ndb > 2 * ks.nfg ? ndb : 2 * ks.nfg;
+    float2 *Rho = sm, *S = sm + nsets * nz * TX, *tw = sm + 2 * nsets * nz * TX;
     double *red = reinterpret_cast<double *>(tw + nz);
     const int kx0 = blockIdx.x * TX, y = blockIdx.y;
     for (int t = threadIdx.x; t < nz; t += blockDim.x) tw[t] = lz.tw[t];
@@ -445,7 +448,7 @@ __global__ void __launch_bounds__(256) k_kspace_z(Geom g, FftLine lz, const KSpa
     cp_async_wait_all();
     __syncthreads();
     float2 *R = fft_lines<false>(Rho, S, nd * TX, 1, nd * TX, lz, tw, true, make_fastdiv_dev(nd * TX));
-    float2 *Wk = (R == Rho) ? S : Rho;  // free buffer: two halves of nz*TX for the outputs
+    float2 *Wk = (R == Rho) ? S : Rho;  // the other buffer, free for the inverse transforms
     const int ky = signed_index(y, g.ny);
     const double kyv = ks.twopi_over_L[1] * ky;
     const bool nyq_y = (g.ny % 2 == 0) && (y == g.ny / 2);
@@ -508,12 +511,17 @@ __global__ void __launch_bounds__(256) k_kspace_z(Geom g, FftLine lz, const KSpa
         tdf[t] = kt.dfield;
     }
     __syncthreads();
-    for (int f = 0; f < ks.nfg; f++) {
-        for (int e = threadIdx.x; e < nz * TX; e += blockDim.x) {
-            const int z = e / TX, c = e - z * TX, kx = kx0 + c;
+    // line set 2f: phi_f = sum c u rho; set 2f+1: -i k_z phi_f.  x and y are fixed along a z
+    // line, so IFFT_z(-i k_x phi) = -i k_x IFFT_z(phi) and the same for y: one transform of
+    // phi serves both, -i k_z phi needs its own.  All 2F sets go through one transform.
+    const int nf2 = 2 * ks.nfg, pitch = nf2 * TX;
+    for (int e = threadIdx.x; e < nz * TX; e += blockDim.x) {
+        const int z = e / TX, c = e - z * TX, kx = kx0 + c;
+        const float kz = (g.nz % 2 == 0 && z == g.nz / 2) ? 0.f : (float)(ks.twopi_over_L[2] * signed_index(z, g.nz));
+        const long long o = ((long long)z * g.ny + y) * g.hp + kx;
+        for (int f = 0; f < ks.nfg; f++) {
             float px = 0.f, py = 0.f;
             if (kx < g.nxh) {
-                const long long o = ((long long)z * g.ny + y) * g.hp + kx;
                 for (int t = 0; t < nterms; t++) {
                     if (tfg[t] != f) continue;
                     const float u = tcoef[t] * __ldg(uk + tpot[t] * g.hstride + o);
@@ -522,42 +530,24 @@ __global__ void __launch_bounds__(256) k_kspace_z(Geom g, FftLine lz, const KSpa
                     py = fmaf(u, r.y, py);
                 }
             }
-            Phi[e] = make_float2(px, py);
+            Wk[z * pitch + (2 * f) * TX + c] = make_float2(px, py);
+            Wk[z * pitch + (2 * f + 1) * TX + c] = make_float2(kz * py, -kz * px);
         }
-        __syncthreads();
-        // x and y are fixed along a z line, so IFFT_z(-i k_x phi) = -i k_x IFFT_z(phi) and the
-        // same for y: one transform serves both; -i k_z phi needs its own.
-        float2 *W1 = Wk, *W2 = Wk + nz * TX;
-        for (int pass = 0; pass < 2; pass++) {
-            for (int e = threadIdx.x; e < nz * TX; e += blockDim.x) {
-                const float2 ph = Phi[e];
-                if (pass == 0) {
-                    W1[e] = ph;
-                } else {
-                    const int z = e / TX;
-                    const float kz = (g.nz % 2 == 0 && z == g.nz / 2)
-                                         ? 0.f : (float)(ks.twopi_over_L[2] * signed_index(z, g.nz));
-                    W1[e] = make_float2(kz * ph.y, -kz * ph.x);   // -i k_z phi
-                }
-            }
-            __syncthreads();
-            const float2 *O = fft_lines<true>(W1, W2, TX, 1, TX, lz, tw, true, make_fastdiv_dev(TX));
-            for (int e = threadIdx.x; e < nz * TX; e += blockDim.x) {
-                const int z = e / TX, c = e - z * TX, kx = kx0 + c;
-                if (kx >= g.nxh) continue;
-                const long long o = ((long long)z * g.ny + y) * g.hp + kx;
-                const float2 v = O[e];
-                if (pass == 0) {
-                    const float kxv = (g.nx % 2 == 0 && kx == g.nx / 2)
-                                          ? 0.f : (float)(ks.twopi_over_L[0] * signed_index(kx, g.nx));
-                    const float kyf = nyq_y ? 0.f : (float)kyv;
-                    Hg[(long long)(3 * f) * g.hstride + o] = make_float2(kxv * v.y, -kxv * v.x);
-                    Hg[(long long)(3 * f + 1) * g.hstride + o] = make_float2(kyf * v.y, -kyf * v.x);
-                } else {
-                    Hg[(long long)(3 * f + 2) * g.hstride + o] = v;
-                }
-            }
-            __syncthreads();
+    }
+    __syncthreads();
+    float2 *other = (Wk == Rho) ? S : Rho;
+    const float2 *O = fft_lines<true>(Wk, other, nf2 * TX, 1, nf2 * TX, lz, tw, true, make_fastdiv_dev(nf2 * TX));
+    const float kyf = nyq_y ? 0.f : (float)kyv;
+    for (int e = threadIdx.x; e < nz * TX; e += blockDim.x) {
+        const int z = e / TX, c = e - z * TX, kx = kx0 + c;
+        if (kx >= g.nxh) continue;
+        const long long o = ((long long)z * g.ny + y) * g.hp + kx;
+        const float kxv = (g.nx % 2 == 0 && kx == g.nx / 2) ? 0.f : (float)(ks.twopi_over_L[0] * signed_index(kx, g.nx));
+        for (int f = 0; f < ks.nfg; f++) {
+            const float2 v = O[z * pitch + (2 * f) * TX + c], w = O[z * pitch + (2 * f + 1) * TX + c];
+            Hg[(long long)(3 * f) * g.hstride + o] = make_float2(kxv * v.y, -kxv * v.x);
+            Hg[(long long)(3 * f + 1) * g.hstride + o] = make_float2(kyf * v.y, -kyf * v.x);
+            Hg[(long long)(3 * f + 2) * g.hstride + o] = w;
         }
     }
 }
@@ -662,14 +652,17 @@ __global__ void __launch_bounds__(256) k_xinv(Geom g, FftLine lx, int nfg, const
 
 // ---- plans and launchers ----
 constexpr int kTXy = 16;   // half-spectrum columns per y-pass block
-constexpr int kTXz = 8;    // half-spectrum columns per z-pass block
+constexpr int kTXz = 8;    // half-spectrum columns per structure-factor z block
+constexpr size_t kKspaceSmemMax = 220 * 1024;
 void init_fft_attributes()
 {
     set_max_smem(k_xfwd<true>, 200 * 1024);
     set_max_smem(k_xfwd<false>, 200 * 1024);
     set_max_smem(k_ypass<false, kTXy>, 200 * 1024);
     set_max_smem(k_ypass<true, kTXy>, 200 * 1024);
-    set_max_smem(k_kspace_z<kTXz>, 220 * 1024);
+    set_max_smem(k_kspace_z<8>, kKspaceSmemMax);
+    set_max_smem(k_kspace_z<4>, kKspaceSmemMax);
+    set_max_smem(k_kspace_z<2>, kKspaceSmemMax);
     set_max_smem(k_sk_z<kTXz>, 200 * 1024);
     set_max_smem(k_xinv, 200 * 1024);
 }
@@ -729,15 +722,31 @@ cudaError_t launch_ypass(const Geom &g, const FftLine &ly, int nfields, int inve
     return cudaGetLastError();
 }
 
+static size_t kspace_smem(const Geom &g, int nd, int nfg, int tx)
+{
+    const int ndb = nd < 2 ? 2 : nd;
+    const int nsets = ndb > 2 * nfg ? ndb : 2 * nfg;   // as in the kernel
+    return (size_t)(2 * nsets * g.nz * tx + g.nz) * sizeof(float2) + 8 * sizeof(double);
+}
+
+int kspace_tile_width(const Geom &g, int nd, int nfg)
+{
+    for (int tx : {4, 2})   // 4 columns: four blocks per SM at C2 sizes, better than 8 at two
+        if (kspace_smem(g, nd, nfg, tx) <= kKspaceSmemMax) return tx;
+    return 0;
+}
+
 cudaError_t launch_kspace_z(const Geom &g, const FftLine &lz, const KSpace &ks, const KSpace *ks_dev,
                             const float2 *H, const float *uk, float2 *Hg, double *epart, int energy, int forces,
                             int *nblocks_out, cudaStream_t st)
 {
-    constexpr int TX = kTXz;
-    const int ndb = ks.nd < 2 ? 2 : ks.nd;
-    dim3 grid((g.nxh + TX - 1) / TX, g.ny);
-    const size_t sm = (size_t)(2 * ndb * g.nz * TX + g.nz * TX + g.nz) * sizeof(float2) + 8 * sizeof(double);
-    k_kspace_z<TX><<<grid, 256, sm, st>>>(g, lz, ks_dev, H, uk, Hg, epart, energy, forces);
+    const int tx = kspace_tile_width(g, ks.nd, ks.nfg);
+    if (tx == 0) return cudaErrorInvalidConfiguration;
+    dim3 grid((g.nxh + tx - 1) / tx, g.ny);
+    const size_t sm = kspace_smem(g, ks.nd, ks.nfg, tx);
+    if (tx == 8) k_kspace_z<8><<<grid, 256, sm, st>>>(g, lz, ks_dev, H, uk, Hg, epart, energy, forces);
+    else if (tx == 4) k_kspace_z<4><<<grid, 256, sm, st>>>(g, lz, ks_dev, H, uk, Hg, epart, energy, forces);
+    else k_kspace_z<2><<<grid, 256, sm, st>>>(g, lz, ks_dev, H, uk, Hg, epart, energy, forces);
     if (nblocks_out) *nblocks_out = (int)(grid.x * grid.y);
     return cudaGetLastError();
 }
