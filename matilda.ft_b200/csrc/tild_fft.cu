@@ -754,7 +754,7 @@ cudaError_t launch_kspace_z(const Geom &g, const FftLine &lz, const KSpace &ks, 
 cudaError_t launch_xinv(const Geom &g, const FftLine &lx, int nfg, const float2 *Hg, float4 *rec, cudaStream_t st)
 {
     const int nf = 3 * nfg, npair = (nf + 1) / 2;
-    int L = (2560 + npair * g.nx - 1) / (npair * g.nx);   // about 2.5k complex points per block
+    int L = (4096 + npair * g.nx - 1) / (npair * g.nx);   // about 4k complex points per block
     L = L < 1 ? 1 : (L > 16 ? 16 : L);
     const long long nlines = (long long)g.ny * g.nz;
     const size_t bsz = (size_t)npair * L * g.nx, stsz = (size_t)nf * L * g.hp;
