@@ -100,6 +100,12 @@ int tild_box_set_particles(tild_box *box, int64_t n, const float *x, const int32
 int tild_box_set_bonds(tild_box *box, int64_t nbonds, const int64_t *pairs,
                        const int32_t *btype);
 
+/* Angles supplied as arrays (readDataConfig angles section,
+ * PS_Box_initialization.cu:933-993): triples[3*nangles] 0-based particle ids (i, middle
+ * j, k), atype[nangles] 0-based angle types (NULL = all type 0); each angle is stored on
+ * its three particles (at most MAXANGLES per particle).  Must precede endBox. */
+int tild_box_set_angles(tild_box *box, int64_t nangles, const int64_t *triples, const int32_t *atype);
+
 /* Options outside the reference grammar.  Keys:
  *   "rng"            0 = Philox4x32-10 (default), 1 = cuRAND XORWOW compatible mode
  *                    (same curand_init/curand_normal calls as device_utils.cu:465-472,
@@ -137,10 +143,12 @@ int tild_box_forces(tild_box *box, float *f_out);
 /* Thermodynamic terms at the current positions (PS_Box::computeThermoProps,
  * PS_Box.cu:282-317) in FP64: out[0] = Upe, out[1] = Ubond, out[2+i] = energy of
  * potential i (i < npot); then three 6-component tensors in the order xx, yy, zz, xy,
- * xz, yz: the bond virial sum_bonds dr_a f_b, the pair virial -dU_pair/d(strain_ab)
+ * xz, yz: the bonded virial (sum over bonds of dr_a f_b plus, over angles,
+ * r_ij,a f_i,b + r_kj,a f_k,b), the pair virial -dU_pair/d(strain_ab)
  * (= U_pair delta_ab + sum_k (du/dk / k) k_a k_b Re(rho_I* rho_J), the reference has no
- * counterpart), and the pressure tensor (N kT delta_ab + W_pair + W_bond) / V with kT = 1.
- * Writes min(nout, 2 + npot + 18) values; *nwritten (may be NULL) receives the count. */
+ * counterpart), and the pressure tensor (N kT delta_ab + W_pair + W_bonded) / V with
+ * kT = 1; last the angle energy Uangle (included in Upe, PS_Box.cu:296-315).
+ * Writes min(nout, 2 + npot + 19) values; *nwritten (may be NULL) receives the count. */
 int tild_box_thermo(tild_box *box, double *out, int nout, int *nwritten);
 
 /* Copy positions device -> host (x_out[n*Dim]) / host -> device.  Setting positions

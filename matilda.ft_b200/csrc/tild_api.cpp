@@ -134,6 +134,12 @@ int tild_box_set_bonds(tild_box *box, int64_t nbonds, const int64_t *pairs, cons
     return guarded([&] { box->impl->setBonds(nbonds, pairs, btype); });
 }
 
+int tild_box_set_angles(tild_box *box, int64_t nangles, const int64_t *triples, const int32_t *atype)
+{
+    NEED_BOX;
+    return guarded([&] { box->impl->setAngles(nangles, triples, atype); });
+}
+
 int tild_box_set_option(tild_box *box, const char *key, int64_t value)
 {
     NEED_BOX;
@@ -258,7 +264,7 @@ int tild_box_get_log(tild_box *box, double *out, int64_t *rows, int32_t *cols)
 {
     NEED_BOX;
     const auto &L = box->impl->logRows;
-    const int32_t c = 2 + (int32_t)box->impl->potentials.size();
+    const int32_t c = box->impl->logColumns();
     if (rows) *rows = (int64_t)L.size();
     if (cols) *cols = c;
     if (out)

@@ -205,12 +205,28 @@ void Box::parseWords(std::vector<std::string> &w, size_t &i)
         finishInitialization();
         return;
     }
-    if (fw == "angle") {
-        (void)inum(w, i, "angle type");
+    if (fw == "angle") {   // PS_Box_initialization.cu:83-106
+        const int at = (int)inum(w, i, "angle type");
+        if (at < 1 || at > kMaxAngleTypes) fail(TILD_ERR_UNSUPPORTED, "angle type out of range");
+        if (at > (int)angleK.size()) {
+            angleK.resize(at, 0.f);
+            angleTheq.resize(at, 0.f);
+            angleStyle.resize(at, 0);
+        }
         const std::string style = need(w, i, "angle style");
-        (void)dnum(w, i, "angle k");
-        if (style == "harmonic") (void)dnum(w, i, "angle theta");
-        else if (style != "wlc") fail(TILD_ERR_PARSE, "Angle style not supported!");
+        angleK[at - 1] = (float)dnum(w, i, "angle k");
+        if (style == "wlc") {
+            angleStyle[at - 1] = 0;
+        } else if (style == "harmonic") {
+            angleStyle[at - 1] = 1;
+            angleTheq[at - 1] = (float)(dnum(w, i, "angle theta") * (3.14159265358979323846 / 180.0));
+        } else {
+            fail(TILD_ERR_PARSE, "Angle style not supported!");
+        }
+    } else if (fw == "MAXANGLES") {
+        if (nstot > 0) fail(TILD_ERR_PARSE, "MAXANGLES must be set before defining any molecules");
+        MAXANGLES = (int)inum(w, i, "MAXANGLES");
+        if (MAXANGLES < 1 || MAXANGLES > 255) fail(TILD_ERR_PARSE, "MAXANGLES out of range");
     } else if (fw == "blocksize" || fw == "blockSize") {
         blockSize = (int)inum(w, i, "blockSize");
     } else if (fw == "bond") {
@@ -484,6 +500,10 @@ void Box::readDataConfig(const std::string &name)
     nBonds.assign(nstot, 0);
     bondedTo.assign(nstot * MAXBONDS, 0);
     bondType.assign(nstot * MAXBONDS, 0);
+    nAngles.assign(nstot, 0);
+    angleGroup.assign(nstot * MAXANGLES * 3, 0);
+    angleType.assign(nstot * MAXANGLES, 0);
+    nAnglesTot = 0;
     if (nbonds > 0) {
         if (!seek("Bonds")) fail(TILD_ERR_PARSE, "data file " + name + ": no Bonds section");
         std::vector<int64_t> pairs(2 * nbonds);
@@ -498,7 +518,21 @@ void Box::readDataConfig(const std::string &name)
         }
         setBonds(nbonds, pairs.data(), bt.data());
     }
-    nAnglesTot = (int)nangles;
+    if (nangles > 0) {   // :933-993
+        if (!seek("Angles")) fail(TILD_ERR_PARSE, "data file " + name + ": no Angles section");
+        std::vector<int64_t> tri(3 * nangles);
+        std::vector<int32_t> at(nangles);
+        for (int64_t a = 0; a < nangles; a++) {
+            std::istringstream iss(next_data());
+            long long id, t, i1, i2, i3;
+            if (!(iss >> id >> t >> i1 >> i2 >> i3)) fail(TILD_ERR_PARSE, "bad angle line in " + name);
+            tri[3 * a] = i1 - 1;
+            tri[3 * a + 1] = i2 - 1;
+            tri[3 * a + 2] = i3 - 1;
+            at[a] = (int32_t)(t - 1);
+        }
+        setAngles(nangles, tri.data(), at.data());
+    }
 }
 
 void Box::setParticles(int64_t n, const float *xin, const int32_t *type, const int32_t *mol, const float *q)
@@ -520,6 +554,37 @@ void Box::setParticles(int64_t n, const float *xin, const int32_t *type, const i
     nBonds.assign(nstot, 0);
     bondedTo.assign(nstot * MAXBONDS, 0);
     bondType.assign(nstot * MAXBONDS, 0);
+    nAngles.assign(nstot, 0);
+    angleGroup.assign(nstot * MAXANGLES * 3, 0);
+    angleType.assign(nstot * MAXANGLES, 0);
+}
+
+// Angles as 0-based particle triples (i1, i2 middle, i3) and 0-based types; the ends are
+// ordered i1 < i3 and the angle is stored on all three particles (:947-983).
+void Box::setAngles(int64_t na, const int64_t *tri, const int32_t *atype)
+{
+    if (ready) fail(TILD_ERR_STATE, "angles must be set before endBox");
+    if (nstot == 0) fail(TILD_ERR_STATE, "angles need particles");
+    if (na < 0 || (na > 0 && !tri)) fail(TILD_ERR_ARG, "bad angle arrays");
+    for (int64_t a = 0; a < na; a++) {
+        int64_t i1 = tri[3 * a], i2 = tri[3 * a + 1], i3 = tri[3 * a + 2];
+        if (i1 < 0 || i2 < 0 || i3 < 0 || i1 >= nstot || i2 >= nstot || i3 >= nstot)
+            fail(TILD_ERR_PARSE, "angle particle out of range");
+        if (i3 < i1) std::swap(i1, i3);
+        const int t = atype ? atype[a] : 0;
+        if (t < 0 || t >= kMaxAngleTypes) fail(TILD_ERR_PARSE, "angle type out of range");
+        for (int64_t p : {i1, i2, i3}) {
+            const int k = nAngles[p];
+            if (k >= MAXANGLES)
+                fail(TILD_ERR_PARSE, "a particle has more than MAXANGLES=" + std::to_string(MAXANGLES) + " angles");
+            angleGroup[(p * MAXANGLES + k) * 3 + 0] = (int)i1;
+            angleGroup[(p * MAXANGLES + k) * 3 + 1] = (int)i2;
+            angleGroup[(p * MAXANGLES + k) * 3 + 2] = (int)i3;
+            angleType[p * MAXANGLES + k] = t;
+            nAngles[p] = k + 1;
+        }
+    }
+    nAnglesTot += (int)na;
 }
 
 void Box::setBonds(int64_t nb, const int64_t *pairs, const int32_t *btype)
@@ -592,7 +657,11 @@ void Box::prepareHost()
         if (Nx[j] < pmeorder + 2)
             fail(TILD_ERR_UNSUPPORTED, "grid of " + std::to_string(Nx[j]) + " points is too small for pmeorder " +
                                            std::to_string(pmeorder) + " (needs at least pmeorder + 2)");
-    if (nAnglesTot > 0) fail(TILD_ERR_UNSUPPORTED, "angles are outside the TILD step");
+    for (int64_t p = 0; p < nstot && nAnglesTot > 0; p++)
+        for (int k = 0; k < nAngles[p]; k++)
+            if (angleType[p * MAXANGLES + k] >= (int)angleK.size())
+                fail(TILD_ERR_PARSE, "angle type " + std::to_string(angleType[p * MAXANGLES + k] + 1) +
+                                         " has no 'angle' command");
     if (integrators.empty()) fail(TILD_ERR_PARSE, "no integrator defined");
     if (species.size() > (size_t)kMaxTypes) fail(TILD_ERR_UNSUPPORTED, "too many species");
     gvol = 1.0;
@@ -673,9 +742,10 @@ int64_t Box::deviceBytesEstimate() const
     const int64_t perParticle = 12 * 4 + 4 + 4 + q + 1 + 5 * mb + rng + 12 + 1   // state, scratch, partials
                                 + 12 + 36 + q + 8 + 1 + 5 * mb + rng;         // sort keys and copies
     const int64_t nk = (int64_t)sort_key_count(geom);
+    const int64_t angles = nAnglesTot > 0 ? 2 * (1 + 13 * (int64_t)MAXANGLES) : 0;   // arrays and sort copies
     const int64_t grid = (deterministic ? 16 : 8) * npair * M + 8 * nd * hs + 24 * nfg * hs + 16 * nfg * M +
                          4 * std::max<int64_t>(1, (int64_t)potentials.size()) * hs + 8 * nk;
-    return N * perParticle + grid + (int64_t(4) << 20);   // + small arrays, alignment, graphs
+    return N * (perParticle + angles) + grid + (int64_t(4) << 20);   // + small arrays, alignment, graphs
 }
 
 void Box::buildPlan()
@@ -775,6 +845,12 @@ void Box::buildPlan()
     for (size_t k = 0; k < fgroups.size(); k++)
         if (psGroup[fgroups[k]].isCharges) pp.fg_qweighted |= 1u << k;
     pp.maxb = MAXBONDS;
+    pp.maxa = nAnglesTot > 0 ? MAXANGLES : 0;
+    for (size_t t = 0; t < angleK.size() && t < (size_t)kMaxAngleTypes; t++) {
+        pp.ak[t] = angleK[t];
+        pp.atheq[t] = angleTheq[t];
+        pp.astyle[t] = angleStyle[t];
+    }
     pp.nbtypes = nBondTypes;
     for (int t = 0; t < nBondTypes; t++) {
         pp.bk[t] = bondK[t];
@@ -816,6 +892,11 @@ void Box::allocDevice()
     dNb = dalloc<uint8_t>(N);
     dPartner = dalloc<int>(N * MAXBONDS);
     dBtype = dalloc<uint8_t>(N * MAXBONDS);
+    if (nAnglesTot > 0) {
+        dNa = dalloc<uint8_t>(N);
+        dAtype = dalloc<uint8_t>(N * MAXANGLES);
+        dAng = dalloc<int>(3 * N * MAXANGLES);
+    }
     if (rngCompat) dRng = dalloc<unsigned char>(N * rng_state_bytes());
     const int nd = std::max(1, (int)dfields.size()), nfg = std::max(1, (int)fgroups.size());
     const int npair = (nd + 1) / 2;
@@ -839,7 +920,7 @@ void Box::allocDevice()
     nblkZ = ((g.nxh + TXz - 1) / TXz) * g.ny;
     nblkP = (int)((N + 255) / 256);
     dEpart = dalloc<double>((size_t)nblkZ * (ksHost.neterms + 6));
-    dBpart = dalloc<double>((size_t)nblkP * 7);
+    dBpart = dalloc<double>((size_t)nblkP * 14);
     dRes = dalloc<double>(kResSize);
     dTmp = dalloc<float>(3 * N);
     if (sharedDevice) hKsPinned = new KSpace;   // pinned host memory would synchronise the device when freed
@@ -888,6 +969,9 @@ void Box::allocDevice()
     sortW.nb = dalloc<uint8_t>(N);
     sortW.btype = dalloc<uint8_t>(N * MAXBONDS);
     sortW.rng = rngCompat ? (void *)dalloc<unsigned char>(N * rng_state_bytes()) : nullptr;
+    sortW.na = nAnglesTot > 0 ? dalloc<uint8_t>(N) : nullptr;
+    sortW.atype = nAnglesTot > 0 ? dalloc<uint8_t>(N * MAXANGLES) : nullptr;
+    sortW.ang = nAnglesTot > 0 ? dalloc<int>(3 * N * MAXANGLES) : nullptr;
 }
 
 void Box::uploadParticles()
@@ -909,6 +993,14 @@ void Box::uploadParticles()
     ck(cudaMemcpy(dNb, nb8.data(), N, cudaMemcpyHostToDevice), "upload nb");
     ck(cudaMemcpy(dPartner, bondedTo.data(), 4 * N * MAXBONDS, cudaMemcpyHostToDevice), "upload partners");
     ck(cudaMemcpy(dBtype, bt8.data(), N * MAXBONDS, cudaMemcpyHostToDevice), "upload bond types");
+    if (dNa) {
+        std::vector<uint8_t> na8(N), at8(N * MAXANGLES);
+        for (int64_t p = 0; p < N; p++) na8[p] = (uint8_t)nAngles[p];
+        for (int64_t k = 0; k < N * MAXANGLES; k++) at8[k] = (uint8_t)angleType[k];
+        ck(cudaMemcpy(dNa, na8.data(), N, cudaMemcpyHostToDevice), "upload angle counts");
+        ck(cudaMemcpy(dAtype, at8.data(), N * MAXANGLES, cudaMemcpyHostToDevice), "upload angle types");
+        ck(cudaMemcpy(dAng, angleGroup.data(), 12 * N * MAXANGLES, cudaMemcpyHostToDevice), "upload angles");
+    }
     long long zero = 0;
     ck(cudaMemcpy(dStep, &zero, sizeof(zero), cudaMemcpyHostToDevice), "upload step");
     ck(cudaMemset(dRes, 0, sizeof(double) * kResSize), "zero results");
@@ -968,8 +1060,8 @@ std::vector<int> Box::slotOrder() const
 void Box::sortParticles()
 {
     const int64_t N = nstot;
-    PermIn in{dX[0], dX[1], dNoise, dQ, dFlags, dOrig, dPartner, dNb, dBtype, dRng, dStep};
-    ck(launch_sort(geom, (int)N, MAXBONDS, sortW, in, stream), "sort");
+    PermIn in{dX[0], dX[1], dNoise, dQ, dFlags, dOrig, dPartner, dNb, dBtype, dRng, dStep, dNa, dAtype, dAng};
+    ck(launch_sort(geom, (int)N, MAXBONDS, dNa ? MAXANGLES : 0, sortW, in, stream), "sort");
     auto cp = [&](void *dst, const void *src, size_t bytes) {
         ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, stream), "sort copy");
     };
@@ -983,6 +1075,11 @@ void Box::sortParticles()
     cp(dPartner, sortW.partner, 4 * N * MAXBONDS);
     cp(dBtype, sortW.btype, N * MAXBONDS);
     if (dRng) cp(dRng, sortW.rng, N * rng_state_bytes());
+    if (dNa) {
+        cp(dNa, sortW.na, N);
+        cp(dAtype, sortW.atype, N * MAXANGLES);
+        cp(dAng, sortW.ang, 12 * N * MAXANGLES);
+    }
     sinceSort = 0;
     sortedTiles = true;
 }
@@ -1036,14 +1133,16 @@ void Box::enqueueStep(bool energy, bool integrate, float *fout_dev)
             mark(STAGE_XINV);
         }
     }
-    ck(launch_particles(g, ppHost, dPp, dX[0], dX[1], dNoise, dFlags, dQ, dNb, dPartner, dBtype, dRec, dOrig, dRng,
+    ck(launch_particles(g, ppHost, dPp, dX[0], dX[1], dNoise, dFlags, dQ, dNb, dPartner, dBtype,
+                        AngleArrays{dNa, dAtype, dAng}, dRec, dOrig, dRng,
                         dStep, fout_dev, integrate ? 1 : 0, tileCfg(), st),
        "particles");
     mark(STAGE_PARTICLES);
     if (integrate) ck(launch_tick(dStep, st), "tick");
     if (energy) {
-        ck(launch_bond_energy(g, ppHost, dPp, dX[0], dX[1], dStep, dNb, dPartner, dBtype, dBpart, nullptr, st), "bond energy");
-        ck(launch_reduce_partials(dBpart, nblkP, 7, dRes + kResBond, st), "reduce bonds");
+        ck(launch_bond_energy(g, ppHost, dPp, dX[0], dX[1], dStep, dNb, dPartner, dBtype, AngleArrays{dNa, dAtype, dAng},
+                              dBpart, nullptr, st), "bond energy");
+        ck(launch_reduce_partials(dBpart, nblkP, 14, dRes + kResBond, st), "reduce bonds");
     }
 }
 
@@ -1064,8 +1163,9 @@ void Box::enqueueEnergyOnly()
         ck(launch_kspace_z(g, lz, ksHost, dKs, dH, dUk, dHg, dEpart, 1, 0, nullptr, st), "kspace energy");
         ck(launch_reduce_partials(dEpart, nblkZ, ksHost.neterms + 6, dRes, st), "reduce");
     }
-    ck(launch_bond_energy(g, ppHost, dPp, dX[0], dX[1], dStep, dNb, dPartner, dBtype, dBpart, nullptr, st), "bond energy");
-    ck(launch_reduce_partials(dBpart, nblkP, 7, dRes + kResBond, st), "reduce bonds");
+    ck(launch_bond_energy(g, ppHost, dPp, dX[0], dX[1], dStep, dNb, dPartner, dBtype, AngleArrays{dNa, dAtype, dAng},
+                              dBpart, nullptr, st), "bond energy");
+    ck(launch_reduce_partials(dBpart, nblkP, 14, dRes + kResBond, st), "reduce bonds");
 }
 
 std::vector<double> Box::readEnergies(bool)
@@ -1182,7 +1282,7 @@ void Box::NVT(int64_t nSteps)
     {   // writeData(-1) (PS_Box.cu:215)
         std::vector<double> t = thermo();
         std::vector<double> pe(t.begin() + 2, t.begin() + 2 + potentials.size());
-        writeData(-1, pe, t[1]);
+        writeData(-1, pe, t[1], t.back());
     }
     bool anyRamp = false;
     for (auto &p : potentials) anyRamp |= p.ramp;
@@ -1190,7 +1290,7 @@ void Box::NVT(int64_t nSteps)
     const int npot = (int)potentials.size();
     std::vector<double> ampUsed(npot);
     std::vector<double> lastPair(npot, 0.0);
-    double lastBond = 0.0;
+    double lastBond = 0.0, lastAngle = 0.0;
     for (int64_t i = 0; i < nSteps; i++) {
         const bool energy = (i % logFreq == 0) || (i == nSteps - 1);
         for (int k = 0; k < npot; k++) ampUsed[k] = potentials[k].amp_eff;
@@ -1205,17 +1305,18 @@ void Box::NVT(int64_t nSteps)
             for (int k = 0; k < npot; k++)   // CalcEnergy runs after update_prefactor (PS_Box.cu:159-172)
                 lastPair[k] = r[k] * (ampUsed[k] != 0.0 ? potentials[k].amp_eff / ampUsed[k] : 1.0);
             lastBond = 0.5 * r[kResBond];
-            if (i % logFreq == 0) writeData(i, lastPair, lastBond);
+            lastAngle = r[kResAngle] / 3.0;   // each angle summed on its three particles
+            if (i % logFreq == 0) writeData(i, lastPair, lastBond, lastAngle);
         }
     }
     ck(cudaStreamSynchronize(stream), "run");
-    if (nSteps > 0) writeData(nSteps, lastPair, lastBond);   // PS_Box.cu:227
+    if (nSteps > 0) writeData(nSteps, lastPair, lastBond, lastAngle);   // PS_Box.cu:227
     if (writeFiles) writeDataConfig("final.input.data");      // PS_Box.cu:230
 }
 
-void Box::writeData(int64_t step, const std::vector<double> &pairE, double ubond)
+void Box::writeData(int64_t step, const std::vector<double> &pairE, double ubond, double uangle)
 {
-    double upe = ubond;
+    double upe = ubond + uangle;
     for (size_t k = 0; k < pairE.size() && k < potentials.size(); k++) {
         potentials[k].energy = pairE[k];
         upe += pairE[k];
@@ -1223,6 +1324,7 @@ void Box::writeData(int64_t step, const std::vector<double> &pairE, double ubond
     std::vector<double> row;
     row.push_back((double)step);
     row.push_back(ubond);
+    if (nAnglesTot > 0) row.push_back(uangle);
     for (size_t k = 0; k < potentials.size(); k++) row.push_back(potentials[k].energy);
     logRows.push_back(row);
     std::ostringstream ln, echoLn;   // PS_Box.cu:339-370 (default stream formatting)
@@ -1231,6 +1333,10 @@ void Box::writeData(int64_t step, const std::vector<double> &pairE, double ubond
     if (nBondsTot > 0) {
         ln << " " << ubond;
         echoLn << " Ubond: " << ubond;
+    }
+    if (nAnglesTot > 0) {   // PS_Box.cu:356-359
+        ln << " " << uangle;
+        echoLn << " Uangle: " << uangle;
     }
     for (size_t k = 0; k < potentials.size(); k++) {
         ln << " " << potentials[k].energy;
@@ -1251,7 +1357,8 @@ std::vector<double> Box::thermo()
     std::vector<double> r = readEnergies(true);
     std::vector<double> out;
     const size_t np = potentials.size();
-    double ubond = 0.5 * r[kResBond], upe = ubond, upair = 0.0;
+    const double uangle = r[kResAngle] / 3.0;   // PS_Box.cu:296-305
+    double ubond = 0.5 * r[kResBond], upe = ubond + uangle, upair = 0.0;
     for (size_t k = 0; k < np; k++) upair += r[k];
     upe += upair;
     out.push_back(upe);
@@ -1259,7 +1366,8 @@ std::vector<double> Box::thermo()
     for (size_t k = 0; k < np; k++) out.push_back(r[k]);
     double wb[6], wp[6];
     for (int c = 0; c < 6; c++) {
-        wb[c] = 0.5 * r[kResBond + 1 + c];                    // bonds: sum over bonds of dr_a f_b
+        // bonded: sum over bonds of dr_a f_b, plus over angles of r_ij,a f_i,b + r_kj,a f_k,b
+        wb[c] = 0.5 * r[kResBond + 1 + c] + r[kResAngle + 1 + c] / 3.0;
         wp[c] = r[np + c] + (c < 3 ? upair : 0.0);            // pairs: -dU/d(strain_ab)
         out.push_back(wb[c]);
     }
@@ -1267,6 +1375,7 @@ std::vector<double> Box::thermo()
     for (int c = 0; c < 6; c++) out.push_back(wp[c]);
     const double V = (double)L[0] * L[1] * L[2];
     for (int c = 0; c < 6; c++) out.push_back(((c < 3 ? (double)nstot : 0.0) + wp[c] + wb[c]) / V);
+    out.push_back(uangle);
     return out;
 }
 
@@ -1493,7 +1602,10 @@ void Box::writeDataConfig(const std::string &name)   // PS_Box.cu:629-748
     for (int64_t p = 0; p < nstot; p++)
         for (int b = 0; b < nBonds[p]; b++) mx = std::max(mx, bondType[p * MAXBONDS + b]);
     out << mx + 1 << " bond types" << "\n";
-    out << 0 << " angle types" << "\n";
+    mx = -1;
+    for (int64_t p = 0; p < nstot && nAnglesTot > 0; p++)
+        for (int a = 0; a < nAngles[p]; a++) mx = std::max(mx, angleType[p * MAXANGLES + a]);
+    out << mx + 1 << " angle types" << "\n";
     out << "\n";
     out << "0.0 " << L[0] << " xlo xhi" << "\n";
     out << "0.0 " << L[1] << " ylo yhi" << "\n";
@@ -1520,6 +1632,19 @@ void Box::writeDataConfig(const std::string &name)   // PS_Box.cu:629-748
                 out << bc + 1 << " " << bondType[p * MAXBONDS + b] + 1 << " " << p + 1 << " " << bondedTo[p * MAXBONDS + b] + 1 << "\n";
                 bc++;
             }
+    if (nAnglesTot > 0) {   // PS_Box.cu:728-745: each angle once, from its first particle
+        out << "\nAngles\n" << "\n";
+        int64_t ac = 0;
+        for (int64_t p = 0; p < nstot; p++)
+            for (int a = 0; a < nAngles[p]; a++) {
+                const int *gq = &angleGroup[(p * MAXANGLES + a) * 3];
+                if (p == gq[0]) {
+                    out << ac + 1 << " " << angleType[p * MAXANGLES + a] + 1 << " " << gq[0] + 1 << " " << gq[1] + 1
+                        << " " << gq[2] + 1 << "\n";
+                    ac++;
+                }
+            }
+    }
 }
 
 std::string Box::describe() const
@@ -1538,7 +1663,8 @@ std::string Box::describe() const
       << ", \"grid\": [" << Nx[0] << ", " << Nx[1] << ", " << Nx[2] << "], \"L\": [" << L[0] << ", " << L[1] << ", "
       << L[2] << "], \"pmeorder\": " << pmeorder << ", \"randSeed\": " << RANDSEED << ", \"logFreq\": " << logFreq
       << ", \"doCharges\": " << (doCharges ? "true" : "false") << ", \"MAXBONDS\": " << MAXBONDS
-      << ", \"nBonds\": " << nBondsTot << ", \"datFileName\": " << q(datFileName) << ", \"species\": [";
+      << ", \"nBonds\": " << nBondsTot << ", \"nAngles\": " << nAnglesTot << ", \"MAXANGLES\": " << MAXANGLES
+      << ", \"datFileName\": " << q(datFileName) << ", \"species\": [";
     for (size_t t = 0; t < species.size(); t++)
         j << (t ? ", " : "") << "{\"label\": " << q(species[t].label) << ", \"mass\": " << species[t].mass
           << ", \"mobility\": " << species[t].mobility << "}";

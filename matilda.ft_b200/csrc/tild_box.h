@@ -78,6 +78,7 @@ public:
     void readDataConfig(const std::string &name);     // :787-997
     void setParticles(int64_t n, const float *x, const int32_t *type, const int32_t *mol, const float *q);
     void setBonds(int64_t nb, const int64_t *pairs, const int32_t *btype);
+    void setAngles(int64_t na, const int64_t *triples, const int32_t *atype);
     void setOption(const std::string &key, int64_t value);
     void setStream(cudaStream_t st);
     void setBaseDir(const std::string &d) { baseDir = d; }
@@ -117,6 +118,7 @@ public:
     int nDensityFields() const { return (int)dfields.size(); }
     int nForceGroups() const { return (int)fgroups.size(); }
     int64_t deviceBytes() const { return devBytes; }
+    int logColumns() const { return 2 + (nAnglesTot > 0 ? 1 : 0) + (int)potentials.size(); }
     bool echo = false;
 
 private:
@@ -127,7 +129,7 @@ private:
     int findSpeciesInteger(const std::string &name) const;
     void createDefaultGroups();
     void writeDataConfig(const std::string &name);
-    void writeData(int64_t step, const std::vector<double> &pairE, double ubond);
+    void writeData(int64_t step, const std::vector<double> &pairE, double ubond, double uangle);
     std::string resolve(const std::string &name) const;
 
     // device plan
@@ -170,6 +172,10 @@ private:
     std::vector<float> x, charges;
     std::vector<int> intSpecies, mID;
     std::vector<int> nBonds, bondedTo, bondType;   // [n], [n*MAXBONDS]
+    // angles (ps_deviceAngles.cu): every angle is stored on each of its three particles
+    std::vector<int> nAngles, angleGroup, angleType;   // [n], [n*MAXANGLES*3], [n*MAXANGLES]
+    std::vector<float> angleK, angleTheq;               // per angle type (theta in radians)
+    std::vector<int> angleStyle;                        // 0 wlc, 1 harmonic
 
     // derived plan
     struct DField { int group; int charge; };
@@ -199,6 +205,8 @@ private:
     float *dNoise = nullptr, *dQ = nullptr, *dF = nullptr;
     uint32_t *dFlags = nullptr;
     uint8_t *dNb = nullptr, *dBtype = nullptr;
+    uint8_t *dNa = nullptr, *dAtype = nullptr;   // angles (NULL when the box has none)
+    int *dAng = nullptr;
     int *dPartner = nullptr, *dOrig = nullptr;
     void *dRng = nullptr;
     float2 *dDep = nullptr, *dH = nullptr, *dHg = nullptr, *dTw = nullptr;

@@ -25,9 +25,11 @@ constexpr int kMaxTerms = 32;
 // the summed pair virial W_ab (xx, yy, zz, xy, xz, yz) right after them, the bond energy
 // and bond virial at kResBond
 constexpr int kResBond = kMaxPots + 6;
-constexpr int kResSize = kResBond + 8;
+constexpr int kResAngle = kResBond + 7;   // angle energy and virial (each angle on 3 particles)
+constexpr int kResSize = kResAngle + 8;
 constexpr int kMaxTypes = 16;
 constexpr int kMaxBondTypes = 16;
+constexpr int kMaxAngleTypes = 16;
 constexpr int kMaxStages = 20;
 constexpr int kNoIntegrator = 15;
 constexpr double kFixScale = 4294967296.0;  // deterministic deposit: 2^32 per unit weight
@@ -115,6 +117,9 @@ struct ParticleParams {
     int nbtypes;
     float bk[kMaxBondTypes], breq[kMaxBondTypes];
     int bstyle[kMaxBondTypes];
+    int maxa;                       // angle slots per particle (0: no angles)
+    float ak[kMaxAngleTypes], atheq[kMaxAngleTypes];
+    int astyle[kMaxAngleTypes];     // 0 wlc, 1 harmonic
     int integ_kind[4];              // 0 GJF, 1 EM per integrator slot
     float em_delt[4], em_noise[4];
     TypeCoef coef[4][kMaxTypes];
@@ -133,6 +138,11 @@ struct TileCfg {
     int box;      // deposit: shared-memory records of a tile's bounding box (estimate)
     int pbox;     // particle pass: records of the fixed tile box (odd pitches)
     int margin;   // particle pass: drift margin of the fixed box, cells per side
+};
+
+struct AngleArrays {        // angles in slot order (all NULL: the box has none)
+    const uint8_t *na, *atype;  // [n] angles per particle, [n*maxa] types
+    const int *ang;             // [n*maxa*3] slots of the angle's i, j (middle), k
 };
 
 // -------------------------------------------------------------------------------------
@@ -170,7 +180,7 @@ cudaError_t launch_xinv(const Geom &g, const FftLine &lx, int nfg, const float2 
 cudaError_t launch_particles(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd,
                              float *X0, float *X1, float *noise, const uint32_t *pflags,
                              const float *q, const uint8_t *nb, const int *partner,
-                             const uint8_t *btype, const float4 *rec, const int *orig_id,
+                             const uint8_t *btype, AngleArrays aa, const float4 *rec, const int *orig_id,
                              void *rng_states, const long long *d_step, float *fout,
                              int integrate, const TileCfg &tc, cudaStream_t st);
 void init_particle_attributes();
@@ -184,6 +194,8 @@ struct PermIn {             // current particle arrays (slot order)
     const uint8_t *nb, *btype;
     const void *rng;
     const long long *d_step;
+    const uint8_t *na, *atype;  // angles per particle and their types (may be NULL)
+    const int *ang;             // [n*maxa*3] particle slots of each angle
 };
 struct SortScratch {        // work arrays and the permuted copies
     uint32_t *key, *count, *totals, *start;
@@ -193,9 +205,12 @@ struct SortScratch {        // work arrays and the permuted copies
     int *orig, *partner;
     uint8_t *nb, *btype;
     void *rng;
+    uint8_t *na, *atype;
+    int *ang;
 };
 uint32_t sort_key_count(const Geom &g);
-cudaError_t launch_sort(const Geom &g, int N, int maxb, const SortScratch &w, const PermIn &in, cudaStream_t st);
+cudaError_t launch_sort(const Geom &g, int N, int maxb, int maxa, const SortScratch &w, const PermIn &in,
+                        cudaStream_t st);
 cudaError_t launch_unpermute_rows(int N, int width, const int *orig, const float *in, float *out,
                                   cudaStream_t st);
 cudaError_t launch_permute_rows(int N, int width, const int *orig, const float *in, float *out,
@@ -203,9 +218,10 @@ cudaError_t launch_permute_rows(int N, int width, const int *orig, const float *
 cudaError_t launch_rng_init(void *states, const int *orig_id, int n, unsigned long long seed,
                             cudaStream_t st);
 size_t rng_state_bytes();
+// per block: bond energy + virial (7 columns), then angle energy + virial (7 columns)
 cudaError_t launch_bond_energy(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd,
                                const float *X0, const float *X1, const long long *d_step,
-                               const uint8_t *nb, const int *partner, const uint8_t *btype,
+                               const uint8_t *nb, const int *partner, const uint8_t *btype, AngleArrays aa,
                                double *partials, int *nblocks_out, cudaStream_t st);
 cudaError_t launch_reduce_partials(const double *partials, int nblocks, int ncols, double *out,
                                    cudaStream_t st);

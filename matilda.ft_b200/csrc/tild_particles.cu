@@ -83,6 +83,86 @@ __device__ __forceinline__ void bond_force(const Geom &g, const ParticleParams &
     }
 }
 
+// One angle (ps_deviceAngles.cu:26-120): the two bond vectors from the middle particle j
+// (minimum image with Lh), cos(theta), and the forces fi on i and fk on k (the middle
+// particle takes -(fi + fk)); wlc U = k (1 + cos), harmonic U = k (theta - theta_eq)^2.
+// Returns false when the reference skips the angle (a bond shorter than 1e-2, or
+// |cos| > 1 for the harmonic style); e and the vectors are filled otherwise.
+__device__ __forceinline__ bool angle_terms(const Geom &g, const ParticleParams &pp, const float *__restrict__ X,
+                                            int ai, int aj, int ak, int atp, float *rij, float *rkj, float *fi,
+                                            float *fk, float &e)
+{
+    float mrij2 = 0.f, mrkj2 = 0.f;
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        rij[j] = X[3 * ai + j] - X[3 * aj + j];
+        if (rij[j] > g.Lh[j]) rij[j] -= g.L[j];
+        else if (rij[j] < -g.Lh[j]) rij[j] += g.L[j];
+        mrij2 = __fmaf_rn(rij[j], rij[j], mrij2);
+    }
+    if (mrij2 < 1.0e-4f) return false;
+    const float mrij = sqrtf(mrij2);
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        rkj[j] = X[3 * ak + j] - X[3 * aj + j];
+        if (rkj[j] > g.Lh[j]) rkj[j] -= g.L[j];
+        else if (rkj[j] < -g.Lh[j]) rkj[j] += g.L[j];
+        mrkj2 = __fmaf_rn(rkj[j], rkj[j], mrkj2);
+    }
+    if (mrkj2 < 1.0e-4f) return false;
+    const float mrkj = sqrtf(mrkj2);
+    float dot = 0.f;
+#pragma unroll
+    for (int j = 0; j < 3; j++) dot = __fmaf_rn(rij[j], rkj[j], dot);
+    const float cos_th = dot / mrij / mrkj;
+    const float kang = pp.ak[atp];
+    if (pp.astyle[atp] == 0) {   // wlc
+        e = kang * (1.0f + cos_th);
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            fi[j] = -kang * (rkj[j] / mrij / mrkj - cos_th * rij[j] / mrij2);
+            fk[j] = -kang * (rij[j] / mrkj / mrij - cos_th * rkj[j] / mrkj2);
+        }
+        return true;
+    }
+    if (cos_th < -1.f || cos_th > 1.f) return false;
+    const float theta = acosf(cos_th);
+    const float denom = sqrtf(1.f - cos_th * cos_th);
+    const float isin = denom > 1.0e-4f ? (float)(1.0 / (double)denom) : 0.f;
+    const float dtheta = theta - pp.atheq[atp];
+    const float du = 2.f * kang * dtheta;
+    e = kang * dtheta * dtheta;
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        fi[j] = du * isin * (rkj[j] / mrij / mrkj - cos_th * rij[j] / mrij2);
+        fk[j] = du * isin * (rij[j] / mrij / mrkj - cos_th * rkj[j] / mrkj2);
+    }
+    return true;
+}
+
+// Angle force on particle p summed over its angles, added after the bonds (the order of
+// d_bonds then d_angles, PS_Box.cu:245-254).
+__device__ __forceinline__ void angle_force(const Geom &g, const ParticleParams &pp, int p, const float *__restrict__ X,
+                                            const AngleArrays &aa, float *f)
+{
+    const int nap = aa.na[p];
+    float lf[3] = {0.f, 0.f, 0.f};
+    for (int i = 0; i < nap; i++) {
+        const int b = (p * pp.maxa + i) * 3;
+        const int ai = aa.ang[b], aj = aa.ang[b + 1], ak = aa.ang[b + 2];
+        float rij[3], rkj[3], fi[3], fk[3], e;
+        if (!angle_terms(g, pp, X, ai, aj, ak, aa.atype[p * pp.maxa + i], rij, rkj, fi, fk, e)) continue;
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            if (p == ai) lf[j] += fi[j];
+            else if (p == aj) lf[j] -= fi[j] + fk[j];
+            else if (p == ak) lf[j] += fk[j];
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 3; j++) f[j] += lf[j];
+}
+
 // GJF (ps_integratorGJF.cu:102-163) or EM (ps_integratorEM.cu:39-82) update of particle p;
 // x_{t-1} is read from Xn and replaced by x_{t+1}.
 __device__ __forceinline__ void integrate(const Geom &g, const ParticleParams &pp, int p, uint32_t fl,
@@ -197,7 +277,7 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
                                                       float *__restrict__ noise, const uint32_t *__restrict__ pflags,
                                                       const float *__restrict__ q, const uint8_t *__restrict__ nb,
                                                       const int *__restrict__ partner,
-                                                      const uint8_t *__restrict__ btype,
+                                                      const uint8_t *__restrict__ btype, AngleArrays aa,
                                                       const float4 *__restrict__ rec, const int *__restrict__ orig_id,
                                                       curandState *__restrict__ rng,
                                                       const long long *__restrict__ d_step, float *__restrict__ fout,
@@ -308,7 +388,10 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
         }
         // 4. bonds
         float f[3] = {0.f, 0.f, 0.f};
-        if (act) bond_force(g, pp, p, x, Xc, nb, partner, btype, f);
+        if (act) {
+            bond_force(g, pp, p, x, Xc, nb, partner, btype, f);
+            if (aa.na) angle_force(g, pp, p, Xc, aa, f);
+        }
         const int base = d[2] * E01 + d[1] * E0 + d[0];
         const float qp = (act && q) ? q[p] : 0.f;
         float Wx[P + 1], Wy[P + 1], Wz[P + 1];
@@ -401,20 +484,25 @@ __global__ void k_rng_init(curandState *st, const int *orig_id, int n, unsigned 
 }
 
 // Per-particle bond energy and virial (ps_deviceBonds.cu:85-171, including its
-// minimum-image threshold 0.5*Lh), summed per block in FP64: cols = e, vir[6].
+// minimum-image threshold 0.5*Lh) and angle energy and virial (ps_deviceAngles.cu:151-294,
+// every angle counted on each of its three particles), summed per block in FP64:
+// cols = bond e, vir[6], angle e, vir[6].
 __global__ void __launch_bounds__(256) k_bond_energy(Geom g, const ParticleParams *__restrict__ ppd, int N,
                                                      const float *__restrict__ X0, const float *__restrict__ X1,
                                                      const long long *__restrict__ d_step,
                                                      const uint8_t *__restrict__ nb,
                                                      const int *__restrict__ partner,
-                                                     const uint8_t *__restrict__ btype,
+                                                     const uint8_t *__restrict__ btype, AngleArrays aa,
                                                      double *__restrict__ partials)
 {
-    __shared__ double red[8][7];
+    constexpr int NC = 14;
+    __shared__ double red[8][NC];
     const ParticleParams &pp = *ppd;
     const float *__restrict__ X = (*d_step & 1) ? X1 : X0;
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    double acc[NC];
+#pragma unroll
+    for (int c = 0; c < NC; c++) acc[c] = 0.0;
     if (p < N && nb) {
         float e = 0.f, vir[6] = {0, 0, 0, 0, 0, 0};
         for (int b = 0; b < nb[p]; b++) {
@@ -449,17 +537,36 @@ __global__ void __launch_bounds__(256) k_bond_energy(Geom g, const ParticleParam
         acc[0] = e;
         for (int c = 0; c < 6; c++) acc[c + 1] = vir[c];
     }
+    if (p < N && aa.na) {
+        float e = 0.f, vir[6] = {0, 0, 0, 0, 0, 0};
+        for (int i = 0; i < aa.na[p]; i++) {
+            const int b = (p * pp.maxa + i) * 3;
+            float rij[3], rkj[3], fi[3], fk[3], ea;
+            if (!angle_terms(g, pp, X, aa.ang[b], aa.ang[b + 1], aa.ang[b + 2], aa.atype[p * pp.maxa + i], rij, rkj,
+                             fi, fk, ea))
+                continue;
+            e += ea;
+            vir[0] += fi[0] * rij[0] + fk[0] * rkj[0];
+            vir[1] += fi[1] * rij[1] + fk[1] * rkj[1];
+            vir[2] += fi[2] * rij[2] + fk[2] * rkj[2];
+            vir[3] += fi[0] * rij[1] + fk[0] * rkj[1];
+            vir[4] += fi[0] * rij[2] + fk[0] * rkj[2];
+            vir[5] += fi[1] * rij[2] + fk[1] * rkj[2];
+        }
+        acc[7] = e;
+        for (int c = 0; c < 6; c++) acc[8 + c] = vir[c];
+    }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int c = 0; c < 7; c++) {
+    for (int c = 0; c < NC; c++) {
         double v = acc[c];
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
         if (lane == 0) red[warp][c] = v;
     }
     __syncthreads();
-    if (threadIdx.x < 7) {
+    if (threadIdx.x < NC) {
         double s = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w][threadIdx.x];
-        partials[(long long)blockIdx.x * 7 + threadIdx.x] = s;
+        partials[(long long)blockIdx.x * NC + threadIdx.x] = s;
     }
 }
 
@@ -487,14 +594,14 @@ constexpr size_t kPartSmemMax = kPartBox * sizeof(float4);
 template <int P>
 static void part_launch(const Geom &g, const ParticleParams *ppd, int N, float *X0, float *X1, float *noise,
                         const uint32_t *pflags, const float *q, const uint8_t *nb, const int *partner,
-                        const uint8_t *btype, const float4 *rec, const int *orig_id, void *rng,
+                        const uint8_t *btype, AngleArrays aa, const float4 *rec, const int *orig_id, void *rng,
                         const long long *d_step, float *fout, int integrate, const TileCfg &tc, cudaStream_t st)
 {
     const int nbk = tc.start ? (tc.nkeys + tc.codes - 1) / tc.codes : (N + kPartWindow - 1) / kPartWindow;
     const int threads = tc.start ? tc.threads : 256;
     const int cap = tc.start ? std::min(tc.pbox, kPartBox) : 0;
     const size_t smem = (size_t)cap * sizeof(float4);
-    k_particles<P><<<nbk, threads, smem, st>>>(g, ppd, N, X0, X1, noise, pflags, q, nb, partner, btype, rec, orig_id,
+    k_particles<P><<<nbk, threads, smem, st>>>(g, ppd, N, X0, X1, noise, pflags, q, nb, partner, btype, aa, rec, orig_id,
                                                reinterpret_cast<curandState *>(rng), d_step, fout, integrate, tc, cap);
 }
 
@@ -509,12 +616,12 @@ void init_particle_attributes()
 
 cudaError_t launch_particles(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd, float *X0,
                              float *X1, float *noise, const uint32_t *pflags, const float *q, const uint8_t *nb,
-                             const int *partner, const uint8_t *btype, const float4 *rec, const int *orig_id,
-                             void *rng_states, const long long *d_step, float *fout, int integrate,
+                             const int *partner, const uint8_t *btype, AngleArrays aa, const float4 *rec,
+                             const int *orig_id, void *rng_states, const long long *d_step, float *fout, int integrate,
                              const TileCfg &tc, cudaStream_t st)
 {
     if (pp.N == 0) return cudaSuccess;
-#define TILD_PL(P) part_launch<P>(g, ppd, pp.N, X0, X1, noise, pflags, q, nb, partner, btype, rec, orig_id, \
+#define TILD_PL(P) part_launch<P>(g, ppd, pp.N, X0, X1, noise, pflags, q, nb, partner, btype, aa, rec, orig_id, \
                                   rng_states, d_step, fout, integrate, tc, st)
     switch (pp.order) {
         case 0: TILD_PL(0); break;
@@ -544,10 +651,11 @@ cudaError_t launch_rng_init(void *states, const int *orig_id, int n, unsigned lo
 
 cudaError_t launch_bond_energy(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd, const float *X0,
                                const float *X1, const long long *d_step, const uint8_t *nb, const int *partner,
-                               const uint8_t *btype, double *partials, int *nblocks_out, cudaStream_t st)
+                               const uint8_t *btype, AngleArrays aa, double *partials, int *nblocks_out,
+                               cudaStream_t st)
 {
     const int nbk = pp.N > 0 ? (pp.N + 255) / 256 : 1;
-    k_bond_energy<<<nbk, 256, 0, st>>>(g, ppd, pp.N, X0, X1, d_step, nb, partner, btype, partials);
+    k_bond_energy<<<nbk, 256, 0, st>>>(g, ppd, pp.N, X0, X1, d_step, nb, partner, btype, aa, partials);
     if (nblocks_out) *nblocks_out = nbk;
     return cudaGetLastError();
 }

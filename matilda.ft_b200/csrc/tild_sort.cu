@@ -128,14 +128,18 @@ struct PermArrays {
     const int *orig, *partner;
     const uint8_t *nb, *btype;
     const curandState *rng;
+    const uint8_t *na, *atype;
+    const int *ang;
     float *X0n, *X1n, *noisen, *qn;
     uint32_t *flagsn;
     int *orign, *partnern;
     uint8_t *nbn, *btypen;
     curandState *rngn;
+    uint8_t *nan, *atypen;
+    int *angn;
 };
 
-__global__ void k_permute(int N, int maxb, PermArrays a, const int *__restrict__ newpos)
+__global__ void k_permute(int N, int maxb, int maxa, PermArrays a, const int *__restrict__ newpos)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= N) return;
@@ -156,6 +160,15 @@ __global__ void k_permute(int N, int maxb, PermArrays a, const int *__restrict__
         a.btypen[s * maxb + b] = a.btype[p * maxb + b];
     }
     if (a.rng) a.rngn[s] = a.rng[p];
+    if (a.na) {   // angles: all three particle slots renumbered
+        const int nap = a.na[p];
+        a.nan[s] = (uint8_t)nap;
+        for (int k = 0; k < maxa; k++) {
+            for (int r = 0; r < 3; r++)
+                a.angn[(s * maxa + k) * 3 + r] = k < nap ? newpos[a.ang[(p * maxa + k) * 3 + r]] : 0;
+            a.atypen[s * maxa + k] = a.atype[p * maxa + k];
+        }
+    }
 }
 
 // out[orig[s]] = in[s] for rows of `width` floats (slot order -> original order)
@@ -186,7 +199,8 @@ uint32_t sort_key_count(const Geom &g)
     return 1u << (3 * bits);
 }
 
-cudaError_t launch_sort(const Geom &g, int N, int maxb, const SortScratch &w, const PermIn &in, cudaStream_t st)
+cudaError_t launch_sort(const Geom &g, int N, int maxb, int maxa, const SortScratch &w, const PermIn &in,
+                        cudaStream_t st)
 {
     if (N == 0) return cudaSuccess;
     const uint32_t nk = sort_key_count(g);
@@ -205,7 +219,13 @@ cudaError_t launch_sort(const Geom &g, int N, int maxb, const SortScratch &w, co
     a.X0n = w.X0; a.X1n = w.X1; a.noisen = w.noise; a.qn = w.q; a.flagsn = w.flags; a.orign = w.orig;
     a.partnern = w.partner; a.nbn = w.nb; a.btypen = w.btype;
     a.rngn = reinterpret_cast<curandState *>(w.rng);
-    k_permute<<<nbk, 256, 0, st>>>(N, maxb, a, w.newpos);
+    a.na = in.na;
+    a.atype = in.atype;
+    a.ang = in.ang;
+    a.nan = w.na;
+    a.atypen = w.atype;
+    a.angn = w.ang;
+    k_permute<<<nbk, 256, 0, st>>>(N, maxb, maxa, a, w.newpos);
     return cudaGetLastError();
 }
 

@@ -37,6 +37,7 @@ _SIGS = {
     "tild_box_set_particles": ([ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
                                 ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "tild_box_set_bonds": ([ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "tild_box_set_angles": ([ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "tild_box_set_option": ([ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int64], ctypes.c_int),
     "tild_box_describe": ([ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)],
                           ctypes.c_int),
@@ -169,6 +170,11 @@ class Box:
         b = None if btype is None else np.ascontiguousarray(btype, np.int32)
         _check(lib().tild_box_set_bonds(self._h, len(p), _ptr(p), _ptr(b)))
 
+    def set_angles(self, triples, atype=None):
+        t = np.ascontiguousarray(triples, np.int64).reshape(-1, 3)
+        a = None if atype is None else np.ascontiguousarray(atype, np.int32)
+        _check(lib().tild_box_set_angles(self._h, len(t), _ptr(t), _ptr(a)))
+
     # -- queries -------------------------------------------------------------------
     def describe(self) -> dict:
         need = ctypes.c_int64()
@@ -214,7 +220,7 @@ class Box:
         v = out[: n.value]
         return dict(Upe=float(v[0]), Ubond=float(v[1]), potentials=[float(e) for e in v[2:2 + npot]],
                     virial=v[2 + npot:2 + npot + 6].copy(), pair_virial=v[8 + npot:14 + npot].copy(),
-                    pressure=v[14 + npot:20 + npot].copy())
+                    pressure=v[14 + npot:20 + npot].copy(), Uangle=float(v[20 + npot]))
 
     def positions(self):
         x = np.zeros((self.N, 3), np.float32)
@@ -345,6 +351,10 @@ def box_from_spec(spec, device=0, options=None, steps_script=False):
     if len(spec.bonds):
         b.command("bond 1 harmonic %.9g %.9g" % (spec.bond_k, spec.bond_req))
         b.set_bonds(spec.bonds)
+    for line in spec.angle_commands():
+        b.command(line)
+    if len(spec.angles):
+        b.set_angles(spec.angles, spec.angle_types)
     for p in spec.potentials:
         if p["kind"] == "gaussian":
             b.command("potential gaussian %s %s %.9g %.9g" % (p["I"], p["J"], p["A"], p["sigma"]))

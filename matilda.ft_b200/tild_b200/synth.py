@@ -37,7 +37,8 @@ class SystemSpec:
 
     def __init__(self, name, L, grid, x, types, species, bonds, mol, charges=None,
                  potentials=(), order=3, delt=0.005, bond_k=1.5, bond_req=0.0, seed=1,
-                 dim=3, integrator="GJF", masses=None, mobility=None, log_freq=100):
+                 dim=3, integrator="GJF", masses=None, mobility=None, log_freq=100, angles=None,
+                 angle_types=None, angle_params=()):
         self.name = name
         self.L = np.asarray(L, np.float32)
         self.grid = np.asarray(grid, np.int32)
@@ -58,6 +59,21 @@ class SystemSpec:
         self.masses = masses or [1.0] * len(self.species)
         self.mobility = mobility or [1.0] * len(self.species)
         self.log_freq = log_freq
+        # angles (i, middle j, k), 0-based types, and per type dict(style="harmonic"|"wlc",
+        # k=..., theta=degrees)
+        self.angles = np.zeros((0, 3), np.int64) if angles is None else np.asarray(angles, np.int64).reshape(-1, 3)
+        self.angle_types = (np.zeros(len(self.angles), np.int32) if angle_types is None
+                            else np.asarray(angle_types, np.int32))
+        self.angle_params = list(angle_params)
+
+    def angle_commands(self):
+        out = []
+        for t, a in enumerate(self.angle_params):
+            if a["style"] == "harmonic":
+                out.append("angle %d harmonic %.9g %.9g" % (t + 1, a["k"], a["theta"]))
+            else:
+                out.append("angle %d wlc %.9g" % (t + 1, a["k"]))
+        return out
 
     @property
     def N(self):
@@ -73,9 +89,9 @@ class SystemSpec:
         N, D = self.N, self.dim
         nbt = 1 if len(self.bonds) else 0
         lines = ["Created by tild-b200 synth", "",
-                 "%d atoms" % N, "%d bonds" % len(self.bonds), "0 angles", "",
+                 "%d atoms" % N, "%d bonds" % len(self.bonds), "%d angles" % len(self.angles), "",
                  "%d atom types" % len(self.species), "%d bond types" % nbt,
-                 "0 angle types", "",
+                 "%d angle types" % len(self.angle_params), "",
                  "0.0 %.9g xlo xhi" % self.L[0], "0.0 %.9g ylo yhi" % self.L[1],
                  ("0.0 %.9g zlo zhi" % self.L[2]) if D > 2 else "0.0 1.0 zlo zhi", "",
                  "Masses", ""]
@@ -105,6 +121,11 @@ class SystemSpec:
                 b = np.column_stack([np.arange(1, len(self.bonds) + 1), np.ones(len(self.bonds)),
                                      self.bonds[:, 0] + 1, self.bonds[:, 1] + 1]).astype(np.int64)
                 np.savetxt(fh, b, fmt="%d %d %d %d")
+            if len(self.angles):
+                fh.write("\nAngles\n\n")
+                a = np.column_stack([np.arange(1, len(self.angles) + 1), self.angle_types + 1,
+                                     self.angles + 1]).astype(np.int64)
+                np.savetxt(fh, a, fmt="%d %d %d %d %d")
             fh.write("\n")
         del arr, body
 
@@ -122,6 +143,7 @@ class SystemSpec:
         s.append("readData %s" % data_name)
         if len(self.bonds):
             s.append("bond 1 harmonic %.9g %.9g" % (self.bond_k, self.bond_req))
+        s += self.angle_commands()
         for p in self.potentials:
             k = p["kind"]
             if k == "gaussian":
@@ -289,8 +311,17 @@ def config_c5_jobs(seed=5, njobs=40, nmin=2.0e4, nmax=2.0e5, smin=100, smax=400)
     return jobs
 
 
+def chain_angles(nchains, nper, offset=0):
+    """(i-1, i, i+1) triples along every chain."""
+    out = []
+    for c in range(nchains):
+        b = offset + c * nper
+        out += [(b + i - 1, b + i, b + i + 1) for i in range(1, nper - 1)]
+    return np.array(out, np.int64).reshape(-1, 3)
+
+
 def small_system(seed=0, n_chains=20, nper=8, L=6.0, grid=(12, 12, 12), order=3, charges=False,
-                 dim=3, pots=None, n_free=0):
+                 dim=3, pots=None, n_free=0, angle_params=None):
     """A tiny randomised system for oracle comparisons."""
     rng = np.random.default_rng(seed)
     Lv = np.array([L, L * 1.1, L * 0.9][:dim] + [1.0] * (3 - dim))
@@ -316,6 +347,11 @@ def small_system(seed=0, n_chains=20, nper=8, L=6.0, grid=(12, 12, 12), order=3,
         if charges:
             pots.append(dict(kind="charges", lB=1.0, sigma=0.5))
     grid = list(grid)[:dim] + [1] * (3 - dim)
+    ang, atyp = None, None
+    if angle_params:   # chain triples, types alternating over the given angle types
+        ang = chain_angles(n_chains, nper)
+        atyp = (np.arange(len(ang)) % len(angle_params)).astype(np.int32)
     return SystemSpec("small%d" % seed, Lv, grid, x[:, :dim] if dim == 2 else x, types, ["A", "B"],
                       chain_bonds(n_chains, nper), mol, charges=q, potentials=pots, order=order,
-                      seed=seed + 11, dim=dim)
+                      seed=seed + 11, dim=dim, angles=ang, angle_types=atyp,
+                      angle_params=angle_params or ())

@@ -81,6 +81,11 @@ class System:
     delt: float = 0.005
     integrator: str = "GJF"
     integ_group: str = "all"
+    angles: np.ndarray | None = None        # int[na, 3]: i, middle j, k (0-based)
+    angle_types: np.ndarray | None = None   # int[na]
+    angle_k: np.ndarray = field(default_factory=lambda: np.zeros(0, np.float64))
+    angle_theq: np.ndarray = field(default_factory=lambda: np.zeros(0, np.float64))   # radians
+    angle_style: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))    # 0 wlc, 1 harmonic
 
     @property
     def N(self):
@@ -328,6 +333,55 @@ def spectral_grid_forces(sysm: System, dens, prec=64):
     return gf
 
 
+def angle_terms(sysm: System, x=None):
+    """Per angle (FP64): forces fi on i and fk on k (the middle particle takes
+    -(fi + fk)), energy and virial r_ij,a f_i,b + r_kj,a f_k,b (xx, yy, zz, xy, xz, yz), as
+    ps_deviceAngles.cu:26-120 and 151-294 compute them: minimum image with L/2, angles with
+    a bond shorter than 1e-2 skipped, wlc U = k (1 + cos), harmonic U = k (theta - theta_eq)^2
+    (skipped for |cos| > 1, 1/sin taken as 0 below 1e-4)."""
+    x = np.asarray(sysm.x if x is None else x, np.float64)
+    a = np.asarray(sysm.angles, np.int64)
+    t = np.asarray(sysm.angle_types, np.int64)
+    L = np.asarray(sysm.L, np.float32).astype(np.float64)
+    Lh = (0.5 * np.asarray(sysm.L, np.float32)).astype(np.float64)
+
+    def mi(d):
+        return np.where(d > Lh, d - L, np.where(d < -Lh, d + L, d))
+
+    rij = mi(x[a[:, 0]] - x[a[:, 1]])
+    rkj = mi(x[a[:, 2]] - x[a[:, 1]])
+    m2i, m2k = (rij * rij).sum(1), (rkj * rkj).sum(1)
+    ok = (m2i >= 1e-4) & (m2k >= 1e-4)
+    mi_, mk = np.sqrt(m2i), np.sqrt(m2k)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        cos = (rij * rkj).sum(1) / mi_ / mk
+        k = np.asarray(sysm.angle_k, np.float64)[t]
+        wlc = np.asarray(sysm.angle_style)[t] == 0
+        dri = rkj / (mi_ * mk)[:, None] - (cos / m2i)[:, None] * rij
+        drk = rij / (mi_ * mk)[:, None] - (cos / m2k)[:, None] * rkj
+        theta = np.arccos(np.clip(cos, -1.0, 1.0))
+        den = np.sqrt(np.maximum(1.0 - cos * cos, 0.0))
+        isin = np.where(den > 1e-4, 1.0 / den, 0.0)
+        dth = theta - np.asarray(sysm.angle_theq, np.float64)[t]
+        coef = np.where(wlc, -k, 2.0 * k * dth * isin)
+        e = np.where(wlc, k * (1.0 + cos), k * dth * dth)
+        ok &= wlc | ((cos >= -1.0) & (cos <= 1.0))
+    fi = np.where(ok[:, None], coef[:, None] * dri, 0.0)
+    fk = np.where(ok[:, None], coef[:, None] * drk, 0.0)
+    e = np.where(ok, e, 0.0)
+    pairs = ((0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2))
+    vir = np.stack([fi[:, p] * rij[:, q] + fk[:, p] * rkj[:, q] for p, q in pairs], 1)
+    return fi, fk, e, vir
+
+
+def angle_energy(sysm: System, x=None):
+    """Uangle and the angle virial sum (FP64)."""
+    if sysm.angles is None or len(sysm.angles) == 0:
+        return 0.0, np.zeros(6)
+    _, _, e, vir = angle_terms(sysm, x)
+    return float(e.sum()), vir.sum(0)
+
+
 def forces(sysm: System, x=None, prec=64, include_bonds=True, include_grid=True):
     """Total force on every particle: bonds, then each force group's gather in the
     reference's group order (PS_Box.cu:240-270).  Returns f[N, Dim] (float64 for
@@ -344,6 +398,14 @@ def forces(sysm: System, x=None, prec=64, include_bonds=True, include_grid=True)
             ctypes.c_int(N), ctypes.c_int(Dim), _p(xs), _p(sysm.nb), _p(sysm.partner),
             _p(sysm.btype), ctypes.c_int(sysm.maxb), _p(sysm.bond_k.astype(real)),
             _p(sysm.bond_req.astype(real)), _p(sysm.bond_style.astype(np.int32)), _p(Lr), _p(f))
+    if include_bonds and sysm.angles is not None and len(sysm.angles):   # after the bonds (PS_Box.cu:245-254)
+        fi, fk, _, _ = angle_terms(sysm, x)
+        fa = np.zeros((N, Dim))
+        a = np.asarray(sysm.angles, np.int64)
+        np.add.at(fa, a[:, 0], fi)
+        np.add.at(fa, a[:, 1], -(fi + fk))
+        np.add.at(fa, a[:, 2], fk)
+        f += fa.reshape(-1).astype(real)
     inter = {}
     if include_grid:
         dens, inds, W = densities(sysm, x, prec)

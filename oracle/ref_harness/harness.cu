@@ -10,6 +10,7 @@
 //   rho_<group>.f32, rhoq_charges.f32   every group's density (PS_Box_initialization.cu:551-559)
 //   f0.f32                         d_f after cudaMemset(0) + PS_Box::forces()
 //   energies.f64                   Ubond, then CalcEnergy() of each potential
+//   uangle.f64                     Uangle
 //   x_final.f32                    d_x after <nsteps> doTimeStep calls
 // With time_steps > 0 it also times that many further doTimeStep calls with CUDA events
 // and prints "ms_per_step <value>".
@@ -88,6 +89,8 @@ int main(int argc, char** argv)
     e.push_back(b->Ubond);
     for (size_t k = 0; k < b->potentials.size(); k++) e.push_back(b->potentials[k]->energy);
     dump_host(out, "energies.f64", e.data(), e.size() * sizeof(double));
+    const double ua = b->Uangle;                            // PS_Box.cu:296-305
+    dump_host(out, "uangle.f64", &ua, sizeof(double));
     b->maxSteps = nsteps;
     for (int i = 0; i < nsteps; i++) b->doTimeStep(i);      // PS_Box.cu:210-234 loop
     cudaDeviceSynchronize();

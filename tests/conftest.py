@@ -26,7 +26,12 @@ def spec_to_system(spec, maxb=2, **kw):
         species=spec.species, charges=spec.charges, nb=nb, partner=partner, btype=btype,
         bond_k=np.array([spec.bond_k], np.float32), bond_req=np.array([spec.bond_req], np.float32),
         bond_style=np.array([0], np.int32), potentials=spec.potentials, delt=spec.delt,
-        integrator=spec.integrator, **kw)
+        integrator=spec.integrator, angles=spec.angles if len(spec.angles) else None,
+        angle_types=spec.angle_types,
+        angle_k=np.array([a["k"] for a in spec.angle_params], np.float32).astype(np.float64),
+        angle_theq=np.array([np.float32(a.get("theta", 0.0) * (np.pi / 180.0)) for a in spec.angle_params],
+                            np.float64),
+        angle_style=np.array([0 if a["style"] == "wlc" else 1 for a in spec.angle_params], np.int32), **kw)
 
 
 def force_error(f, fref):

@@ -41,6 +41,8 @@ def systems():
             dict(kind="erfG", I="B", J="B", A=0.3, Rp=0.8, sigma=0.5),
             dict(kind="gaussian", I="all", J="A", A=1.5, sigma=0.8)]),
         "c1": synth.config_c1(),
+        "angles_o3": synth.small_system(seed=37, order=3, charges=True, angle_params=[
+            dict(style="harmonic", k=3.0, theta=120.0), dict(style="wlc", k=2.0)]),
     }
 
 
@@ -92,6 +94,11 @@ def run(harness, name, spec, out, time_steps=0):
         for g in groups:
             res["rho_" + g] = ld("rho_%s.f32" % g, np.float32)
         res["potentials"] = np.array([repr(p) for p in spec.potentials])
+        if len(spec.angles):
+            res["angles"] = spec.angles.astype(np.int32)
+            res["angle_types"] = spec.angle_types.astype(np.int32)
+            res["angle_params"] = np.array([repr(a) for a in spec.angle_params])
+            res["uangle"] = ld("uangle.f64", np.float64)
         np.savez_compressed(os.path.join(out, "ref_%s.npz" % name), **res)
         return meta.get("ms_per_step")
 
@@ -101,9 +108,12 @@ def main():
     ap.add_argument("--harness", default=os.path.join(ROOT, "oracle", "_ref", "tild_ref_harness"))
     ap.add_argument("--out", required=True)
     ap.add_argument("--time", action="store_true", help="also time the reference on C1 and C2")
+    ap.add_argument("--only", nargs="*", help="generate only these systems")
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
     for name, spec in systems().items():
+        if a.only and name not in a.only:
+            continue
         ms = run(a.harness, name, spec, a.out, time_steps=200 if (a.time and name == "c1") else 0)
         print(name, "ok", "" if ms is None else "ms_per_step %s" % ms, flush=True)
     if a.time:

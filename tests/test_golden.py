@@ -44,6 +44,13 @@ def load(path):
                          species=["A", "B"], charges=q, nb=nb, partner=partner, btype=np.zeros_like(partner),
                          bond_k=np.array([1.5], np.float32), bond_req=np.array([0.0], np.float32),
                          bond_style=np.array([0], np.int32), potentials=pots, delt=float(z["delt"]))
+    if "angles" in z.files:
+        ap = [ast.literal_eval(a) for a in z["angle_params"]]
+        sysm.angles = z["angles"].astype(np.int64)
+        sysm.angle_types = z["angle_types"].astype(np.int64)
+        sysm.angle_k = np.array([a["k"] for a in ap], np.float32).astype(np.float64)
+        sysm.angle_theq = np.array([np.float32(a.get("theta", 0.0) * (np.pi / 180.0)) for a in ap], np.float64)
+        sysm.angle_style = np.array([0 if a["style"] == "wlc" else 1 for a in ap], np.int32)
     return z, sysm
 
 
@@ -79,6 +86,9 @@ def test_oracle_forces_and_energies_match_reference(path):
     assert abs(ref[0] - ub) <= 1e-5 * abs(ub)
     for a, b in zip(ref[1:], pe):
         assert abs(a - b) <= 1e-5 * max(abs(b), 1e-9), (a, b)
+    if "uangle" in z.files:
+        ua, _ = oracle.angle_energy(sysm)
+        assert abs(float(z["uangle"][0]) - ua) <= 1e-5 * abs(ua)
 
 
 def _box(z, sysm, **opts):
@@ -98,6 +108,11 @@ def _box(z, sysm, **opts):
     b.set_particles(z["x"], z["types"], z["mol"], sysm.charges)
     b.command("bond 1 harmonic 1.5 0.0")
     b.set_bonds(z["bonds"])
+    if "angles" in z.files:
+        for t, a in enumerate(ast.literal_eval(x) for x in z["angle_params"]):
+            b.command("angle %d harmonic %.9g %.9g" % (t + 1, a["k"], a["theta"]) if a["style"] == "harmonic"
+                      else "angle %d wlc %.9g" % (t + 1, a["k"]))
+        b.set_angles(z["angles"], z["angle_types"])
     for p in sysm.potentials:
         if p["kind"] == "gaussian":
             b.command("potential gaussian %s %s %.9g %.9g" % (p["I"], p["J"], p["A"], p["sigma"]))

@@ -233,3 +233,42 @@ def test_pair_virial_is_the_strain_derivative_of_the_energy(kind):
         sp[a], sm[a] = 1 + h, 1 - h
         fd = -(_energy_scaled(sysm, dens, sp) - _energy_scaled(sysm, dens, sm)) / (2 * h)
         assert abs(W[a] - fd) <= 1e-7 * abs(W[:3]).max(), (kind, a, W[a], fd)
+
+
+ANGLES = [dict(style="harmonic", k=3.0, theta=120.0), dict(style="wlc", k=2.0)]
+
+
+def test_angle_forces_are_the_energy_gradient():
+    """Oracle angle forces (ps_deviceAngles.cu formulas) = -grad of the angle energy, FP64
+    central differences on random chain geometries, both styles."""
+    spec = synth.small_system(seed=91, order=3, angle_params=ANGLES)
+    sysm = spec_to_system(spec)
+    fi, fk, _, _ = oracle.angle_terms(sysm)
+    a = np.asarray(sysm.angles)
+    f = np.zeros((sysm.N, 3))
+    np.add.at(f, a[:, 0], fi)
+    np.add.at(f, a[:, 1], -(fi + fk))
+    np.add.at(f, a[:, 2], fk)
+    x0 = sysm.x.astype(np.float64)
+    h = 1e-6
+    for p in (0, 1, 3, 7, 9, 40):
+        for d in range(3):
+            xp, xm = x0.copy(), x0.copy()
+            xp[p, d] += h
+            xm[p, d] -= h
+            g = (oracle.angle_energy(sysm, xp)[0] - oracle.angle_energy(sysm, xm)[0]) / (2 * h)
+            assert abs(-g - f[p, d]) <= 1e-6 * (1 + abs(f[p, d])), (p, d, -g, f[p, d])
+
+
+def test_angle_script_and_data_file_round_trip(tmp_path):
+    """angle words, the Angles section and MAXANGLES are read like readInput/readDataConfig."""
+    import tild_b200
+    spec = synth.small_system(seed=92, order=3, angle_params=ANGLES)
+    scr, data = spec.write(str(tmp_path), steps=0)
+    b = tild_b200.Box(base_dir=str(tmp_path), options={"write_files": 0})
+    for line in open(scr).read().split("endBox")[0].splitlines()[1:]:   # the words after "box ps"
+        if line.strip():
+            b.command(line)
+    d = b.describe()
+    assert d["nAngles"] == len(spec.angles)
+    b.close()
