@@ -90,6 +90,7 @@ double PS_Potential::T0() const
 Box::Box(int dev) : device(dev)
 {
     RANDSEED = (long long)time(nullptr);   // idum = RANDSEED = time(0) (:45)
+    idum = RANDSEED;
 }
 
 Box::~Box()
@@ -301,15 +302,16 @@ void Box::parseWords(std::vector<std::string> &w, size_t &i)
     } else if (fw == "logFreq" || fw == "logfreq") {
         logFreq = (int)inum(w, i, "logFreq");
         if (logFreq <= 0) fail(TILD_ERR_PARSE, "logFreq must be positive");
-    } else if (fw == "MAXANGLES") {
-        if (nstot > 0) fail(TILD_ERR_PARSE, "MAXANGLES must be set before defining any molecules");
-        MAXANGLES = (int)inum(w, i, "MAXANGLES");
     } else if (fw == "MAXBONDS") {
         if (nstot > 0) fail(TILD_ERR_PARSE, "MAXBONDS must be set before defining any molecules");
         MAXBONDS = (int)inum(w, i, "MAXBONDS");
         if (MAXBONDS < 1 || MAXBONDS > 255) fail(TILD_ERR_PARSE, "MAXBONDS out of range");
-    } else if (fw == "molecule") {
-        fail(TILD_ERR_UNSUPPORTED, "molecule builders are outside the TILD step; use readData");
+    } else if (fw == "molecule") {   // :239-251
+        const std::string kind = need(w, i, "molecule type");
+        if (kind == "linear") makeLinear(w, i);
+        else if (kind == "grafted" || kind == "sclc")
+            fail(TILD_ERR_UNSUPPORTED, "molecule " + kind + " is outside the TILD step; use readData");
+        else fail(TILD_ERR_PARSE, "PS_Box_init:readInput: invalid molecule type read");
     } else if (fw == "Nr") {
         Nr = (int)inum(w, i, "Nr");
     } else if (fw == "NSEXTRA" || fw == "nsextra") {
@@ -329,7 +331,8 @@ void Box::parseWords(std::vector<std::string> &w, size_t &i)
     } else if (fw == "neighbor_list") {
         fail(TILD_ERR_UNSUPPORTED, "neighbor_list is only used by DPD, outside the TILD step");
     } else if (fw == "randSeed" || fw == "RAND_SEED" || fw == "RANDSEED") {
-        RANDSEED = inum(w, i, "randSeed");
+        RANDSEED = inum(w, i, "randSeed");   // seeds both the host and the device generators (:291-293)
+        idum = RANDSEED;
     } else if (fw == "readData") {
         readDataConfig(need(w, i, "readData file"));
     } else if (fw == "rho0") {
@@ -557,6 +560,200 @@ void Box::setParticles(int64_t n, const float *xin, const int32_t *type, const i
     nAngles.assign(nstot, 0);
     angleGroup.assign(nstot * MAXANGLES * 3, 0);
     angleType.assign(nstot * MAXANGLES, 0);
+}
+
+// ---- host random numbers (random.cu) -------------------------------------------------
+// Uniform deviate in (0, 1): L'Ecuyer's (1988) combination of two multiplicative LCGs
+// (m1 = 2147483563, a1 = 40014; m2 = 2147483399, a2 = 40692; products by Schrage's
+// decomposition) passed through a Bays-Durham shuffle of 32 entries, results capped at
+// 1 - 1.2e-7.  A seed <= 0 fills the table first; a positive seed (what randSeed and the
+// time-based default give) starts from the empty table with the second generator at
+// 123456789, as the reference's static state does.
+double Box::ran2()
+{
+    constexpr int64_t M1 = 2147483563, M2 = 2147483399, A1 = 40014, A2 = 40692;
+    constexpr int64_t Q1 = 53668, Q2 = 52774, R1 = 12211, R2 = 3791;   // m = a q + r
+    constexpr int NT = 32;
+    constexpr int64_t NDIV = 1 + (M1 - 1) / NT;
+    constexpr double AM = 1.0 / M1, RNMX = 1.0 - 1.2e-7;
+    auto lcg1 = [&](int64_t &v) {
+        const int64_t k = v / Q1;
+        v = A1 * (v - k * Q1) - k * R1;
+        if (v < 0) v += M1;
+    };
+    if (idum <= 0) {
+        idum = (-idum < 1) ? 1 : -idum;
+        idum2 = idum;
+        for (int j = NT + 7; j >= 0; j--) {
+            lcg1(idum);
+            if (j < NT) iv[j] = idum;
+        }
+        iy = iv[0];
+    }
+    lcg1(idum);
+    const int64_t k = idum2 / Q2;
+    idum2 = A2 * (idum2 - k * Q2) - k * R2;
+    if (idum2 < 0) idum2 += M2;
+    const int j = (int)(iy / NDIV);
+    iy = iv[j] - idum2;
+    iv[j] = idum;
+    if (iy < 1) iy += M1 - 1;
+    const double t = AM * (double)iy;
+    return t > RNMX ? RNMX : t;
+}
+
+// Normal deviate by the polar Box-Muller method, two per accepted pair (the second kept
+// for the next call).
+double Box::gasdev2()
+{
+    if (gasIset) {
+        gasIset = 0;
+        return gasGset;
+    }
+    double v1, v2, rsq;
+    do {
+        v1 = 2.0 * ran2() - 1.0;
+        v2 = 2.0 * ran2() - 1.0;
+        rsq = v1 * v1 + v2 * v2;
+    } while (rsq >= 1.0 || rsq == 0.0);
+    const double fac = std::sqrt(-2.0 * std::log(rsq) / rsq);
+    gasGset = v1 * fac;
+    gasIset = 1;
+    return v2 * fac;
+}
+
+// Isotropic unit vector: normalised vector of normal deviates.
+void Box::randomUnitVec(double *v, int dim)
+{
+    double xi[3], m2 = 0.0;
+    for (int k = 0; k < dim; k++) {
+        xi[k] = gasdev2();
+        m2 += xi[k] * xi[k];
+    }
+    const double m = std::sqrt(m2);
+    for (int k = 0; k < dim; k++) v[k] = xi[k] / m;
+}
+
+// molecule linear {phi F | nmolecs n} nblocks (N_b species_b)... [charge q_b...]
+// [bondType t_b...] [angleType t_b...] [xrange lo hi] [yrange lo hi] [zrange lo hi]
+// (PS_Box_moleculeMakers.cu:15-311): chains whose first bead is uniform in the range and
+// whose next beads sit a unit step from the previous one (a fresh random direction per
+// step, or per chain when the chain carries angles), wrapped into the box; bonds along
+// the chain with the block's bond type on each side, angles on interior beads of blocks
+// with an angle type.
+void Box::makeLinear(std::vector<std::string> &w, size_t &i)
+{
+    if (rho0 < 0.0) fail(TILD_ERR_PARSE, "rho0 must be defined before molecules created!");
+    if (!readDimension) fail(TILD_ERR_PARSE, "Dim must be defined before molecules");
+    double phi = -1.0;
+    int64_t nmolecs = -1;
+    const std::string s1 = need(w, i, "molecule linear phi|nmolecs");
+    if (s1 == "phi") phi = dnum(w, i, "phi");
+    else if (s1 == "nmolecs") nmolecs = inum(w, i, "nmolecs");
+    else fail(TILD_ERR_PARSE, "invalid keyword after molecule linear. must be 'phi' or 'nmolecs'");
+    const int nblk = (int)inum(w, i, "number of blocks");
+    if (nblk < 1) fail(TILD_ERR_PARSE, "a linear molecule needs at least one block");
+    std::vector<int> nper(nblk), spec(nblk), bt(nblk, 1), at(nblk, 0);
+    std::vector<float> bq(nblk, 0.f);
+    int ntot = 0;
+    for (int b = 0; b < nblk; b++) {
+        nper[b] = (int)inum(w, i, "block length");
+        spec[b] = findSpeciesInteger(need(w, i, "block species"));
+        ntot += nper[b];
+    }
+    bool molQ = false, angles = false;
+    float rmin[3] = {0.f, 0.f, 0.f}, rmax[3] = {L[0], L[1], L[2]};
+    while (i < w.size()) {
+        const std::string o = w[i++];
+        if (o == "drude") {
+            fail(TILD_ERR_UNSUPPORTED, "drude oscillators not implemented!");
+        } else if (o == "charge") {
+            if (!doCharges) {   // enableCharges (PS_Box_initialization.cu:1000-1010)
+                doCharges = 1;
+                charges.assign(nstot, 0.f);
+            }
+            molQ = true;
+            for (int b = 0; b < nblk; b++) bq[b] = (float)dnum(w, i, "block charge");
+        } else if (o == "bondType" || o == "bondtype") {
+            for (int b = 0; b < nblk; b++) bt[b] = (int)inum(w, i, "block bond type");
+        } else if (o == "angleType" || o == "angletype") {
+            for (int b = 0; b < nblk; b++) at[b] = (int)inum(w, i, "block angle type");
+            angles = true;
+        } else if (o == "xrange" || o == "yrange" || o == "zrange") {
+            const int d = o[0] - 'x';
+            if (d == 2 && Dim != 3) fail(TILD_ERR_PARSE, "z-range defined for a non-3D simulation!");
+            rmin[d] = (float)dnum(w, i, "range low");
+            rmax[d] = (float)dnum(w, i, "range high");
+        } else {
+            fail(TILD_ERR_PARSE, "invalid keyword " + o + " in molecule linear");
+        }
+    }
+    double V = 1.0;   // as PS_Box_initialization.cu:143-146 accumulates it
+    for (int j = 0; j < Dim; j++) V *= L[j];
+    if (phi > 0.0) nmolecs = (int64_t)(int)(rho0 * V * phi / (double)(float)ntot);
+    if (nmolecs < 0) fail(TILD_ERR_PARSE, "molecule linear: no molecules to make");
+    const int64_t first = nstot, n = nstot + nmolecs * ntot;
+    x.resize(n * Dim, 0.f);
+    intSpecies.resize(n, 0);
+    mID.resize(n, 0);
+    if (doCharges) charges.resize(n, 0.f);
+    nBonds.resize(n, 0);
+    bondedTo.resize(n * MAXBONDS, 0);
+    bondType.resize(n * MAXBONDS, 0);
+    nAngles.resize(n, 0);
+    angleGroup.resize(n * MAXANGLES * 3, 0);
+    angleType.resize(n * MAXANGLES, 0);
+    nstot = n;
+    int mol = 0;   // starting molecule id: the largest so far (:140-146)
+    for (int64_t p = 0; p < first; p++) mol = std::max(mol, mID[p]);
+    int64_t ind = first;
+    for (int64_t m = 0; m < nmolecs; m++) {
+        double ru[3] = {0.0, 0.0, 0.0};
+        for (int b = 0; b < nblk; b++) {
+            for (int s = 0; s < nper[b]; s++) {
+                intSpecies[ind] = spec[b];
+                if (b == 0 && s == 0) {
+                    for (int a = 0; a < Dim; a++) x[ind * Dim + a] = (float)(ran2() * (rmax[a] - rmin[a]) + rmin[a]);
+                } else {
+                    if ((s == 1 && b == 0) || !angles) randomUnitVec(ru, Dim);
+                    for (int a = 0; a < Dim; a++) {
+                        float v = (float)(x[(ind - 1) * Dim + a] + ru[a]);
+                        if (v > L[a]) v -= L[a];
+                        else if (v < 0.0f) v += L[a];
+                        x[ind * Dim + a] = v;
+                    }
+                }
+                if (molQ) charges[ind] = bq[b];
+                nBonds[ind] = 0;
+                if (b != 0 || s != 0) {
+                    bondedTo[ind * MAXBONDS + nBonds[ind]] = (int)(ind - 1);
+                    bondType[ind * MAXBONDS + nBonds[ind]] = bt[b] - 1;
+                    nBonds[ind]++;
+                }
+                if (b != nblk - 1 || s != nper[b] - 1) {
+                    if (nBonds[ind] >= MAXBONDS) fail(TILD_ERR_PARSE, "MAXBONDS too small for linear molecules");
+                    bondedTo[ind * MAXBONDS + nBonds[ind]] = (int)(ind + 1);
+                    bondType[ind * MAXBONDS + nBonds[ind]] = bt[b] - 1;
+                    nBonds[ind]++;
+                }
+                if (at[b] != 0 && (b > 0 || s > 0) && (b < nblk - 1 || s < nper[b] - 1)) {
+                    const int64_t tri[3] = {ind - 1, ind, ind + 1};
+                    for (int64_t p : tri) {
+                        const int k = nAngles[p];
+                        if (k >= MAXANGLES)
+                            fail(TILD_ERR_PARSE, "a particle has more than MAXANGLES=" + std::to_string(MAXANGLES) + " angles");
+                        for (int r = 0; r < 3; r++) angleGroup[(p * MAXANGLES + k) * 3 + r] = (int)tri[r];
+                        angleType[p * MAXANGLES + k] = at[b] - 1;
+                        nAngles[p] = k + 1;
+                    }
+                    nAnglesTot++;
+                }
+                mID[ind] = mol;
+                ind++;
+            }
+        }
+        mol++;
+    }
 }
 
 // Angles as 0-based particle triples (i1, i2 middle, i3) and 0-based types; the ends are

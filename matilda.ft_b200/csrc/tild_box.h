@@ -154,6 +154,16 @@ private:
     int blockSize = 512, NSEXTRA = 0, MAXBONDS = 2, MAXANGLES = 3, Nr = 100;
     double rho0 = -1.0;
     long long RANDSEED = 0;
+    // the reference's host RNG (random.cu:27-106), one state per box: ran2's generator
+    // state and shuffle table, gasdev2's cached spare normal
+    int64_t idum = 0, idum2 = 123456789, iy = 0;
+    int64_t iv[32] = {0};
+    int gasIset = 0;
+    double gasGset = 0.0;
+    double ran2();
+    double gasdev2();
+    void randomUnitVec(double *v, int dim);
+    void makeLinear(std::vector<std::string> &w, size_t &i);   // PS_Box_moleculeMakers.cu:15-311
     int logFreq = 100;
     std::string datFileName = "ps_data.dat", initDataFileName = "init.input.data";
     bool doCharges = false;
