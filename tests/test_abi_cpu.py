@@ -94,7 +94,8 @@ def test_endbox_without_gpu_reports_cuda(tmp_path):
     (["Dim 3", "integrator all VV"], 6, "VV"),
     (["Dim 3", "integrator all XYZ"], 2, "not a valid Integrator"),
     (["Dim 3", "integrator all GJF dt 0.1"], 2, "Invalid keyword in Integrator"),
-    (["Dim 3", "molecule linear 10"], 6, "molecule"),
+    (["Dim 3", "molecule grafted 10"], 6, "molecule"),
+    (["Dim 3", "molecule linear nmolecs 2 1 4 A"], 2, "rho0 must be defined"),
     (["Dim 3", "readData does_not_exist.data"], 3, "Failed to open"),
     (["Dim 3", "species"], 2, "Missing label for species"),
     (["Dim 3", "pmeorder 7"], 2, "pmeorder"),
