@@ -113,7 +113,8 @@ int tild_box_set_angles(tild_box *box, int64_t nangles, const int64_t *triples, 
  *   "deterministic"  1 = deposit by exact fixed-point sums (bit-reproducible), 0 = fast
  *   "bspline4_exact" 1 = true quartic B-spline at pmeorder 4 instead of the
  *                    reference's weights (ps_grid_utils.cu:57)
- *   "write_files"    0 = do not write ps_data.dat / data files (default 1)
+ *   "write_files"    0 = write no files: ps_data.dat, init/final data files, and the
+ *                    run's lammpstrj, GSD and density-<group>.bin outputs (default 1)
  *   "sort_interval"  steps between spatial re-sorts of the particle arrays (0 = never)
  * Must precede endBox except "write_files". */
 int tild_box_set_option(tild_box *box, const char *key, int64_t value);

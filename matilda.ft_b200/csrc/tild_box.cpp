@@ -95,6 +95,7 @@ Box::Box(int dev) : device(dev)
 
 Box::~Box()
 {
+    releaseFrames();
     dropGraphs();
     freeDevice();
     if (hKsPinned) {
@@ -261,13 +262,23 @@ void Box::parseWords(std::vector<std::string> &w, size_t &i)
             doCharges = true;
             if (nstot > 0) charges.assign(nstot, 0.f);
         }
-    } else if (fw == "fieldFreq" || fw == "field_freq" || fw == "gsdFreq" || fw == "gsd_freq") {
-        (void)inum(w, i, fw.c_str());
+    } else if (fw == "fieldFreq" || fw == "field_freq") {   // PS_Box_initialization.cu:171-183
+        fieldFreq = (int)inum(w, i, fw.c_str());
         if (i < w.size()) {
             const std::string t = need(w, i, "logspace");
             if (t != "logspace" && t != "log_space" && t != "logSpace")
                 fail(TILD_ERR_PARSE, "invalid option to " + fw);
-            (void)dnum(w, i, "log scale");
+            logSpaceFields = true;
+            logScaleFields = fnum(w, i, "log scale");
+        }
+    } else if (fw == "gsdFreq" || fw == "gsd_freq") {   // PS_Box_initialization.cu:200-211
+        gsdFreq = (int)inum(w, i, fw.c_str());
+        if (i < w.size()) {
+            const std::string t = need(w, i, "logspace");
+            if (t != "logspace" && t != "log_space" && t != "logSpace")
+                fail(TILD_ERR_PARSE, "invalid option to " + fw);
+            logSpaceGSD = true;
+            logScaleGSD = fnum(w, i, "log scale");
         }
     } else if (fw == "grid") {
         if (!readDimension) fail(TILD_ERR_PARSE, "Dim must be defined before grid!");
@@ -283,8 +294,10 @@ void Box::parseWords(std::vector<std::string> &w, size_t &i)
             if (std::find(tids.begin(), tids.end(), intSpecies[p]) != tids.end()) g.siteList.push_back((int)p);
         g.inputCommand = "group " + g.name;
         psGroup.push_back(g);
-    } else if (fw == "gsdName" || fw == "gsd_name" || fw == "trajFileName") {
-        (void)need(w, i, fw.c_str());
+    } else if (fw == "gsdName" || fw == "gsd_name") {   // PS_Box_initialization.cu:213-215
+        gsdName = need(w, i, fw.c_str());
+    } else if (fw == "trajFileName") {   // PS_Box_initialization.cu:310-312
+        trajFileName = need(w, i, fw.c_str());
     } else if (fw == "integrator") {
         Integrator in;
         in.groupName = need(w, i, "integrator group");
@@ -349,8 +362,8 @@ void Box::parseWords(std::vector<std::string> &w, size_t &i)
         }
         if ((int)species.size() >= kMaxTypes) fail(TILD_ERR_UNSUPPORTED, "too many species");
         species.push_back(s);
-    } else if (fw == "trajFreq" || fw == "traj_freq") {
-        (void)inum(w, i, "trajFreq");
+    } else if (fw == "trajFreq" || fw == "traj_freq") {   // PS_Box_initialization.cu:314-316
+        trajFreq = (int)inum(w, i, "trajFreq");
     } else if (fw == "verbose") {
         verbose = inum(w, i, "verbose") != 0;
     } else {
@@ -507,6 +520,7 @@ void Box::readDataConfig(const std::string &name)
     angleGroup.assign(nstot * MAXANGLES * 3, 0);
     angleType.assign(nstot * MAXANGLES, 0);
     nAnglesTot = 0;
+    angleList.clear();
     if (nbonds > 0) {
         if (!seek("Bonds")) fail(TILD_ERR_PARSE, "data file " + name + ": no Bonds section");
         std::vector<int64_t> pairs(2 * nbonds);
@@ -560,6 +574,8 @@ void Box::setParticles(int64_t n, const float *xin, const int32_t *type, const i
     nAngles.assign(nstot, 0);
     angleGroup.assign(nstot * MAXANGLES * 3, 0);
     angleType.assign(nstot * MAXANGLES, 0);
+    nAnglesTot = 0;
+    angleList.clear();
 }
 
 // ---- host random numbers (random.cu) -------------------------------------------------
@@ -780,6 +796,7 @@ void Box::setAngles(int64_t na, const int64_t *tri, const int32_t *atype)
             angleType[p * MAXANGLES + k] = t;
             nAngles[p] = k + 1;
         }
+        angleList.insert(angleList.end(), {(uint32_t)t, (uint32_t)i1, (uint32_t)i2, (uint32_t)i3});
     }
     nAnglesTot += (int)na;
 }
@@ -901,6 +918,8 @@ void Box::prepareHost()
             psGroup[p.Jind].forceFlag = true;
         }
     }
+    if (writeFiles) writeGsdFrame(0, x.data());   // GSDinit + writeGSDtraj (PS_Box_initialization.cu:521-523)
+    if (writeFiles) initFieldFiles();
     if (writeFiles) { std::ofstream o(resolve(datFileName)); }   // :359-364, :543-544 truncate
     buildPlan();
     hostPrepared = true;
@@ -1488,10 +1507,17 @@ void Box::NVT(int64_t nSteps)
     std::vector<double> ampUsed(npot);
     std::vector<double> lastPair(npot, 0.0);
     double lastBond = 0.0, lastAngle = 0.0;
+    const bool files = writeFiles != 0;
+    if (files && !fieldFilesReady) initFieldFiles();   // write_files switched on after endBox
     for (int64_t i = 0; i < nSteps; i++) {
         const bool energy = (i % logFreq == 0) || (i == nSteps - 1);
+        const bool fieldDue = files && fieldFreq > 0 && i % fieldFreq == 0;
         for (int k = 0; k < npot; k++) ampUsed[k] = potentials[k].amp_eff;
         maybeSort();
+        // the group densities of step i come from the positions it starts from (PS_Box.cu:108-114);
+        // the last step's stay in the buffer for the final frame
+        if (files && (fieldDue || i == nSteps - 1)) computeFieldFrame();
+        if (fieldDue) enqueueFrame(0, i);
         if (anyRamp) enqueueStep(energy, true, nullptr);
         else ck(cudaGraphLaunch(energy ? gEnergy : gNorm, stream), "graph launch");
         totSteps++;
@@ -1505,10 +1531,248 @@ void Box::NVT(int64_t nSteps)
             lastAngle = r[kResAngle] / 3.0;   // each angle summed on its three particles
             if (i % logFreq == 0) writeData(i, lastPair, lastBond, lastAngle);
         }
+        // positions after the step (PS_Box.cu:180-194); the GSD frame carries the step count
+        // the box had before this step
+        const bool gsdDue = files && gsdFreq > 0 && i % gsdFreq == 0;
+        if (gsdDue) enqueueFrame(2, totSteps - 1);
+        if (gsdDue && i > 1 && logSpaceGSD) gsdFreq = (int)((float)gsdFreq * logScaleGSD);
+        if (files && trajFreq > 0 && i % trajFreq == 0) enqueueFrame(1, i);
+        if (fieldDue && i > 1 && logSpaceFields)   // PS_Box.cu:197-203
+            fieldFreq = (int)((float)fieldFreq * logScaleFields);
     }
     ck(cudaStreamSynchronize(stream), "run");
     if (nSteps > 0) writeData(nSteps, lastPair, lastBond, lastAngle);   // PS_Box.cu:227
-    if (writeFiles) writeDataConfig("final.input.data");      // PS_Box.cu:230
+    if (files) {   // writeFields (PS_Box.cu:228): the densities the last step started from
+        if (!fieldFrameValid) computeFieldFrame();
+        enqueueFrame(0, nSteps);
+        enqueueFrame(2, totSteps);                // writeGSDtraj (PS_Box.cu:229)
+        flushFrames(0);
+        writeDataConfig("final.input.data");      // PS_Box.cu:230
+    }
+}
+
+// ---- output frames ------------------------------------------------------------------
+
+// Box::initBinaryDataFile (Box.cu:552-570) for every group's density file
+// (PS_Box_initialization.cu:527-533): int Dim, int Nx[Dim], float L[Dim], native byte order.
+void Box::initFieldFiles()
+{
+    if ((int)psGroup.size() > kMaxFrameGroups)
+        fail(TILD_ERR_UNSUPPORTED, "density files support at most " + std::to_string(kMaxFrameGroups) + " groups");
+    nFrameGroups = (int)psGroup.size();
+    fieldFilesReady = true;
+    for (const PS_Group &g : psGroup) {
+        std::ofstream o(resolve("density-" + g.name + ".bin"), std::ios::binary);
+        if (!o.is_open()) fail(TILD_ERR_IO, "Failed to initialize output binary file!");
+        o.write(reinterpret_cast<const char *>(&Dim), sizeof(int));
+        o.write(reinterpret_cast<const char *>(Nx), Dim * sizeof(int));
+        o.write(reinterpret_cast<const char *>(L), Dim * sizeof(float));
+    }
+}
+
+// Every frame group's density at the current positions into dFieldFrame (one pass over
+// the particles, each adding its weights to the fields of the groups it belongs to).
+void Box::computeFieldFrame()
+{
+    const int64_t M = geom.M;
+    if (!dFieldFrame) {
+        std::vector<unsigned long long> mask(nstot, 0ull);
+        for (int g = 0; g < nFrameGroups; g++)
+            for (int p : psGroup[g].siteList) mask[p] |= 1ull << g;
+        dGroupMask = dalloc<unsigned long long>(nstot);
+        dFieldFrame = dalloc<float>((size_t)nFrameGroups * M);
+        ck(cudaMemcpyAsync(dGroupMask, mask.data(), 8 * nstot, cudaMemcpyHostToDevice, stream), "group masks");
+        ck(cudaStreamSynchronize(stream), "group masks");
+    }
+    ck(cudaMemsetAsync(dFieldFrame, 0, 4 * (size_t)nFrameGroups * M, stream), "clear field frame");
+    ck(launch_group_density_frames(geom, ppHost, dX[0], dX[1], dStep, dOrig, dGroupMask, (int)nstot, dFieldFrame,
+                                   stream),
+       "field frame");
+    fieldFrameValid = true;
+}
+
+float *Box::hostBuffer(size_t bytes)
+{
+    for (size_t k = 0; k < hostSpare.size(); k++)
+        if (hostSpare[k].first == bytes) {
+            float *h = hostSpare[k].second;
+            hostSpare.erase(hostSpare.begin() + k);
+            return h;
+        }
+    void *h = nullptr;
+    if (sharedDevice) h = ::operator new(bytes);   // cudaFreeHost would synchronise the shared device
+    else ck(cudaMallocHost(&h, bytes), "cudaMallocHost");
+    return static_cast<float *>(h);
+}
+
+// Queue a copy of a frame: kind 0 the field frame in dFieldFrame, kind 1 the positions
+// in original order.  The copy runs on the box's stream behind the queued steps; at most
+// two frames wait, the oldest written once its copy has landed.
+void Box::enqueueFrame(int kind, int64_t step)
+{
+    OutFrame f{kind, step, nullptr, 0, nullptr};
+    const float *src;
+    if (kind == 0) {
+        f.bytes = 4 * (size_t)nFrameGroups * geom.M;
+        src = dFieldFrame;
+    } else {   // lammpstrj and GSD frames: positions
+        f.bytes = 12 * (size_t)nstot;
+        ck(launch_snapshot_positions((int)nstot, dOrig, dX[0], dX[1], dStep, dTmp, stream), "position snapshot");
+        src = dTmp;
+    }
+    f.host = hostBuffer(f.bytes);
+    ck(cudaEventCreateWithFlags(&f.ev, cudaEventDisableTiming), "event");
+    outFrames.push_back(f);   // owned by the queue from here on
+    ck(cudaMemcpyAsync(f.host, src, f.bytes, cudaMemcpyDeviceToHost, stream), "frame copy");
+    ck(cudaEventRecord(f.ev, stream), "frame event");
+    flushFrames(2);
+}
+
+void Box::flushFrames(size_t keep)
+{
+    while (outFrames.size() > keep) {
+        OutFrame f = outFrames.front();
+        ck(cudaEventSynchronize(f.ev), "frame copy");
+        outFrames.pop_front();
+        cudaEventDestroy(f.ev);
+        hostSpare.push_back({f.bytes, f.host});
+        writeFrame(f);
+    }
+}
+
+void Box::writeFrame(const OutFrame &f)
+{
+    if (f.kind == 0) {   // PS_Group::writeDensityFieldBinary -> Box::writeBinaryData (Box.cu:573-583)
+        for (int g = 0; g < nFrameGroups; g++) {
+            std::ofstream o(resolve("density-" + psGroup[g].name + ".bin"), std::ios::app | std::ios::binary);
+            if (!o.is_open()) fail(TILD_ERR_IO, "Failed to open output binary file!");
+            o.write(reinterpret_cast<const char *>(f.host + (size_t)g * geom.M), 4 * geom.M);
+        }
+        return;
+    }
+    if (f.kind == 2) {
+        writeGsdFrame(f.step, f.host);
+        return;
+    }
+    // PS_Box::writeLammpsTraj (PS_Box.cu:750-795): one wrap into the box, the file
+    // truncated by the frame of step 0
+    const std::string name = resolve(trajFileName);
+    FILE *o = std::fopen(name.c_str(), f.step == 0 ? "w" : "a");
+    if (!o) fail(TILD_ERR_IO, "Failed to open " + name);
+    std::fprintf(o, "ITEM: TIMESTEP\n%d\nITEM: NUMBER OF ATOMS\n%d\n", (int)f.step, (int)nstot);
+    std::fprintf(o, "ITEM: BOX BOUNDS pp pp pp\n");
+    std::fprintf(o, "%f %f\n%f %f\n%f %f\n", 0.f, L[0], 0.f, L[1], 0.f, Dim == 3 ? L[2] : 1.f);
+    std::fprintf(o, "ITEM: ATOMS id type mol x y z\n");
+    std::vector<char> buf;
+    buf.reserve(1 << 20);
+    char line[160];
+    for (int64_t p = 0; p < nstot; p++) {
+        int n = std::snprintf(line, sizeof line, "%d %d %d  ", (int)p + 1, intSpecies[p] + 1, mID[p] + 1);
+        for (int j = 0; j < Dim; j++) {
+            float v = f.host[3 * p + j];
+            if (v > L[j]) v -= L[j];
+            else if (v < 0.0f) v += L[j];
+            n += std::snprintf(line + n, sizeof line - n, "%f ", v);
+        }
+        for (int j = Dim; j < 3; j++) n += std::snprintf(line + n, sizeof line - n, "%f", 0.f);
+        line[n++] = '\n';
+        buf.insert(buf.end(), line, line + n);
+        if (buf.size() > (1u << 20)) {
+            std::fwrite(buf.data(), 1, buf.size(), o);
+            buf.clear();
+        }
+    }
+    std::fwrite(buf.data(), 1, buf.size(), o);
+    std::fclose(o);
+}
+
+// PS_Box::writeGSDtraj (PS_Box_gsdUtils.cu:14-168) with the lists of GSDinit (:586-608).
+// At step 0 the file is created again with the topology chunks; later frames hold the step,
+// the positions shifted by -L/2 (not wrapped) and the charges.  Bonds are listed from their
+// lower-index particle in particle order (GSDinit); angles in the order they were read, ends
+// swapped so i1 < i3, as readDataConfig records them (:931-990) -- angles made by a molecule
+// builder are never recorded there and stay zero, as in the reference.  Types are named
+// type0..type<ntypes> in 10-byte rows.  Two reference defects are not reproduced: its
+// bond and angle totals count data-file bonds and angles twice (the header's count plus the
+// finishInit count, PS_Box_initialization.cu:430-445, 809-810), padding the lists with
+// zero rows, and it fills only the low 32 bits of the 64-bit step chunk.
+void Box::writeGsdFrame(int64_t step, const float *x_orig)
+{
+    const uint64_t N = (uint64_t)nstot;
+    const uint64_t st = (uint64_t)step;
+    if (step == 0 || !gsd.isOpen()) {
+        gsd.create(resolve(gsdName), "gpu-tild", "hoomd", GsdWriter::version(1, 4));
+        gsd.chunk("configuration/step", GSD_U64, 1, 1, &st);
+        const uint8_t dims = 3;
+        gsd.chunk("configuration/dimensions", GSD_U8, 1, 1, &dims);
+        float box[6] = {0, 0, 0, 0, 0, 0};
+        for (int j = 0; j < Dim; j++) box[j] = L[j];
+        if (Dim == 2) box[2] = 5.0f;
+        gsd.chunk("configuration/box", GSD_F32, 6, 1, box);
+        const uint32_t n32 = (uint32_t)N;
+        gsd.chunk("particles/N", GSD_U32, 1, 1, &n32);
+        std::vector<float> mass(N);
+        std::vector<uint32_t> typeid_(N), molid(N);
+        for (uint64_t p = 0; p < N; p++) {
+            mass[p] = species[intSpecies[p]].mass;
+            typeid_[p] = (uint32_t)(intSpecies[p] + 1);
+            molid[p] = (uint32_t)(mID[p] + 1);
+        }
+        gsd.chunk("particles/mass", GSD_F32, N, 1, mass.data());
+        gsd.chunk("particles/typeid", GSD_U32, N, 1, typeid_.data());
+        gsd.chunk("log/particles/moleculeid", GSD_U32, N, 1, molid.data());
+        const size_t nt = species.size() + 1;
+        std::vector<char> tn(nt * 10, 0);
+        for (size_t t = 0; t < nt; t++) {
+            const std::string nm = "type" + std::to_string(t);
+            std::memcpy(tn.data() + t * 10, nm.c_str(), std::min<size_t>(nm.size(), 9));
+        }
+        gsd.chunk("particles/types", GSD_I8, nt, 10, tn.data());
+        std::vector<uint32_t> btype, bgroup;
+        for (int64_t p = 0; p < nstot; p++)
+            for (int b = 0; b < nBonds[p]; b++)
+                if (bondedTo[p * MAXBONDS + b] > p) {
+                    bgroup.push_back((uint32_t)p);
+                    bgroup.push_back((uint32_t)bondedTo[p * MAXBONDS + b]);
+                    btype.push_back((uint32_t)bondType[p * MAXBONDS + b]);
+                }
+        const uint32_t nb = (uint32_t)btype.size(), na = (uint32_t)nAnglesTot;
+        gsd.chunk("bonds/N", GSD_U32, 1, 1, &nb);
+        gsd.chunk("bonds/typeid", GSD_U32, nb, 1, btype.data());
+        gsd.chunk("bonds/group", GSD_U32, nb, 2, bgroup.data());
+        std::vector<uint32_t> atype(na, 0u), agroup((size_t)na * 3, 0u);
+        for (size_t a = 0; a < angleList.size() / 4 && a < na; a++) {
+            atype[a] = angleList[4 * a];
+            for (int r = 0; r < 3; r++) agroup[3 * a + r] = angleList[4 * a + 1 + r];
+        }
+        gsd.chunk("angles/N", GSD_U32, 1, 1, &na);
+        gsd.chunk("angles/typeid", GSD_U32, na, 1, atype.data());
+        gsd.chunk("angles/group", GSD_U32, na, 3, agroup.data());
+    } else {
+        gsd.chunk("configuration/step", GSD_U64, 1, 1, &st);
+    }
+    std::vector<float> pos(3 * N, 0.f);
+    for (uint64_t p = 0; p < N; p++)
+        for (int j = 0; j < Dim; j++) pos[3 * p + j] = x_orig[3 * p + j] - Lh[j];
+    gsd.chunk("particles/position", GSD_F32, N, 3, pos.data());
+    if (doCharges) gsd.chunk("particles/charge", GSD_F32, N, 1, charges.data());
+    gsd.endFrame();
+}
+
+// Drop queued frames without writing them (error paths, destruction) and free the host buffers.
+void Box::releaseFrames()
+{
+    if (!outFrames.empty() && stream) cudaStreamSynchronize(stream);
+    for (OutFrame &f : outFrames) {
+        cudaEventDestroy(f.ev);
+        hostSpare.push_back({f.bytes, f.host});
+    }
+    outFrames.clear();
+    for (auto &h : hostSpare) {
+        if (sharedDevice) ::operator delete(h.second);
+        else cudaFreeHost(h.second);
+    }
+    hostSpare.clear();
 }
 
 void Box::writeData(int64_t step, const std::vector<double> &pairE, double ubond, double uangle)
@@ -1861,7 +2125,11 @@ std::string Box::describe() const
       << L[2] << "], \"pmeorder\": " << pmeorder << ", \"randSeed\": " << RANDSEED << ", \"logFreq\": " << logFreq
       << ", \"doCharges\": " << (doCharges ? "true" : "false") << ", \"MAXBONDS\": " << MAXBONDS
       << ", \"nBonds\": " << nBondsTot << ", \"nAngles\": " << nAnglesTot << ", \"MAXANGLES\": " << MAXANGLES
-      << ", \"datFileName\": " << q(datFileName) << ", \"species\": [";
+      << ", \"datFileName\": " << q(datFileName) << ", \"trajFreq\": " << trajFreq
+      << ", \"trajFileName\": " << q(trajFileName) << ", \"fieldFreq\": " << fieldFreq
+      << ", \"logScaleFields\": " << (logSpaceFields ? logScaleFields : 0.f) << ", \"gsdFreq\": " << gsdFreq
+      << ", \"logScaleGSD\": " << (logSpaceGSD ? logScaleGSD : 0.f) << ", \"gsdName\": " << q(gsdName)
+      << ", \"species\": [";
     for (size_t t = 0; t < species.size(); t++)
         j << (t ? ", " : "") << "{\"label\": " << q(species[t].label) << ", \"mass\": " << species[t].mass
           << ", \"mobility\": " << species[t].mobility << "}";

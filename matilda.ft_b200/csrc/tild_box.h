@@ -5,12 +5,14 @@
 // fused B200 pipeline of tild_device.h instead of per-object kernels.
 #pragma once
 #include <cstdint>
+#include <deque>
 #include <string>
 #include <vector>
 
 #include <cuda_runtime.h>
 
 #include "tild_device.h"
+#include "tild_gsd.h"
 
 namespace tild {
 
@@ -166,6 +168,22 @@ private:
     void makeLinear(std::vector<std::string> &w, size_t &i);   // PS_Box_moleculeMakers.cu:15-311
     int logFreq = 100;
     std::string datFileName = "ps_data.dat", initDataFileName = "init.input.data";
+    // output written during NVT (PS_Box.cu:166-205): lammpstrj frames every trajFreq
+    // steps, group density frames (density-<group>.bin) every fieldFreq steps with an
+    // optional geometric growth of the interval (logspace)
+    int trajFreq = 0, fieldFreq = 0;
+    std::string trajFileName = "traj.lammpstrj";
+    bool logSpaceFields = false;
+    float logScaleFields = 1.0f;
+    // GSD trajectory (PS_Box_gsdUtils.cu:14-168): a full frame when the box's step count is
+    // 0 (at set-up, and again at the first step of the first run), positions (and charges)
+    // every gsdFreq steps and at the end of every run
+    int gsdFreq = 0;
+    bool logSpaceGSD = false;
+    float logScaleGSD = 1.0f;
+    std::string gsdName = "traj.gsd";
+    GsdWriter gsd;
+    void writeGsdFrame(int64_t step, const float *x_orig);
     bool doCharges = false;
     bool verbose = false;
     int nAnglesTot = 0;
@@ -186,6 +204,7 @@ private:
     std::vector<int> nAngles, angleGroup, angleType;   // [n], [n*MAXANGLES*3], [n*MAXANGLES]
     std::vector<float> angleK, angleTheq;               // per angle type (theta in radians)
     std::vector<int> angleStyle;                        // 0 wlc, 1 harmonic
+    std::vector<uint32_t> angleList;   // (type, i1, i2, i3) per angle read or set, in input order
 
     // derived plan
     struct DField { int group; int charge; };
@@ -245,6 +264,29 @@ private:
     void sortParticles();
     void maybeSort();
     long long deviceStep() const;
+    // output snapshots: device work on the box's stream, copies into host buffers, each
+    // frame written to its file once its event has completed (frames stay in step order)
+    struct OutFrame {
+        int kind;          // 0 field frame (all groups), 1 lammpstrj frame, 2 GSD frame
+        int64_t step;
+        float *host;
+        size_t bytes;
+        cudaEvent_t ev;
+    };
+    std::deque<OutFrame> outFrames;
+    std::vector<std::pair<size_t, float *>> hostSpare;
+    unsigned long long *dGroupMask = nullptr;   // [N] group bits of each original particle id
+    float *dFieldFrame = nullptr;               // [nFrameGroups * M]
+    int nFrameGroups = 0;
+    bool fieldFrameValid = false;               // dFieldFrame holds the last step's densities
+    bool fieldFilesReady = false;               // density-<group>.bin headers written
+    void initFieldFiles();
+    void computeFieldFrame();
+    void enqueueFrame(int kind, int64_t step);
+    void flushFrames(size_t keep);
+    void writeFrame(const OutFrame &f);
+    float *hostBuffer(size_t bytes);
+    void releaseFrames();
     // per-kernel event timing (option "stage_timing")
     enum { STAGE_DEPOSIT, STAGE_XFWD, STAGE_YFWD, STAGE_KSPACE, STAGE_YINV, STAGE_XINV, STAGE_PARTICLES, STAGE_COUNT };
     bool timing = false;

@@ -230,6 +230,15 @@ cudaError_t launch_grid_weights(const Geom &g, int order, int quirk4, const floa
 cudaError_t launch_density_single(const Geom &g, const ParticleParams &pp, const float *X,
                                   const int *sites, int ns, const float *q, int charge,
                                   float *rho, cudaStream_t st);
+// Output snapshots, read from the current buffer of the (X0, X1) pair chosen by *d_step:
+// field frames rho[g*M + m] of every group g whose bit is set in mask[original id]
+// (group densities with the reference's weights), and positions in original order.
+constexpr int kMaxFrameGroups = 64;
+cudaError_t launch_group_density_frames(const Geom &g, const ParticleParams &pp, const float *X0, const float *X1,
+                                        const long long *d_step, const int *orig,
+                                        const unsigned long long *mask, int N, float *rho, cudaStream_t st);
+cudaError_t launch_snapshot_positions(int N, const int *orig, const float *X0, const float *X1,
+                                      const long long *d_step, float *out, cudaStream_t st);
 
 // Static device scratch of the allocation-free density read-back (tild_noalloc.cu):
 // kStaticScratchBytes in one file-scope __device__ array, address looked up once per device.

@@ -65,6 +65,35 @@ __global__ void k_density_single(Geom g, int quirk4, const float *X, const int *
 }
 
 
+// Field frames of every group at once (PS_Group::makeDensityField, ps_groups.cu:147-158,
+// written by writeDensityFieldBinary, :257-262): each particle computes its stencil once
+// and adds the reference weight (/gvol) to the field of every group in its mask.  The
+// 'charges' group's frame is its particle density d_rho, not the charge density.
+template <int P>
+__global__ void k_group_density_frames(Geom g, int quirk4, const float *X0, const float *X1,
+                                       const long long *d_step, const int *orig,
+                                       const unsigned long long *mask, int N, float *rho)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= N) return;
+    const unsigned long long bits = mask[orig[s]];
+    if (!bits) return;
+    const float *X = (*d_step & 1) ? X1 : X0;
+    float Wx[P + 1], Wy[P + 1], Wz[P + 1];
+    const int gx = stencil_axis<P>(X[3 * s], g.dxf[0], quirk4, Wx);
+    const int gy = stencil_axis<P>(X[3 * s + 1], g.dxf[1], quirk4, Wy);
+    const int gz = stencil_axis<P>(X[3 * s + 2], g.dxf[2], quirk4, Wz);
+    const float gvol = __fmul_rn(__fmul_rn(g.dxf[0], g.dxf[1]), g.dxf[2]);
+    for (int a = 0; a <= P; a++)
+        for (int b = 0; b <= P; b++)
+            for (int e = 0; e <= P; e++) {
+                const long long m = wrapi(gx + a, g.nx) + (long long)g.nx * (wrapi(gy + b, g.ny) + (long long)g.ny * wrapi(gz + e, g.nz));
+                const float w = __fdiv_rn(__fmul_rn(__fmul_rn(Wx[a], Wy[b]), Wz[e]), gvol);
+                for (unsigned long long r = bits; r; r &= r - 1)
+                    atomicAdd(rho + (long long)(__ffsll((long long)r) - 1) * g.M + m, w);
+            }
+}
+
 // ---- launchers ----
 cudaError_t launch_zero(void *p, size_t bytes, cudaStream_t st) { return cudaMemsetAsync(p, 0, bytes, st); }
 
@@ -405,6 +434,22 @@ __global__ void k_to_pairs(const float *__restrict__ rho, float2 *__restrict__ o
 {
     const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (m < M) out[m] = make_float2(rho[m], 0.f);
+}
+
+cudaError_t launch_group_density_frames(const Geom &g, const ParticleParams &pp, const float *X0, const float *X1,
+                                        const long long *d_step, const int *orig,
+                                        const unsigned long long *mask, int N, float *rho, cudaStream_t st)
+{
+    if (N == 0) return cudaSuccess;
+    const int nbk = (N + 255) / 256;
+    switch (pp.order) {
+        case 0: k_group_density_frames<0><<<nbk, 256, 0, st>>>(g, pp.quirk4, X0, X1, d_step, orig, mask, N, rho); break;
+        case 1: k_group_density_frames<1><<<nbk, 256, 0, st>>>(g, pp.quirk4, X0, X1, d_step, orig, mask, N, rho); break;
+        case 2: k_group_density_frames<2><<<nbk, 256, 0, st>>>(g, pp.quirk4, X0, X1, d_step, orig, mask, N, rho); break;
+        case 3: k_group_density_frames<3><<<nbk, 256, 0, st>>>(g, pp.quirk4, X0, X1, d_step, orig, mask, N, rho); break;
+        default: k_group_density_frames<4><<<nbk, 256, 0, st>>>(g, pp.quirk4, X0, X1, d_step, orig, mask, N, rho); break;
+    }
+    return cudaGetLastError();
 }
 
 cudaError_t launch_to_pairs(const float *rho, float2 *out, long long M, cudaStream_t st)

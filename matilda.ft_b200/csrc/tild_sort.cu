@@ -237,6 +237,27 @@ cudaError_t launch_unpermute_rows(int N, int width, const int *orig, const float
     return cudaGetLastError();
 }
 
+// positions of the current buffer (chosen by the step parity) in original order
+__global__ void k_snapshot_positions(int N, const int *__restrict__ orig, const float *__restrict__ X0,
+                                     const float *__restrict__ X1, const long long *__restrict__ d_step,
+                                     float *__restrict__ out)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 3LL * N) return;
+    const float *X = (*d_step & 1) ? X1 : X0;
+    const int s = (int)(i / 3), c = (int)(i - 3LL * s);
+    out[3LL * orig[s] + c] = X[i];
+}
+
+cudaError_t launch_snapshot_positions(int N, const int *orig, const float *X0, const float *X1,
+                                      const long long *d_step, float *out, cudaStream_t st)
+{
+    const long long n = 3LL * N;
+    if (n == 0) return cudaSuccess;
+    k_snapshot_positions<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(N, orig, X0, X1, d_step, out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_permute_rows(int N, int width, const int *orig, const float *in, float *out, cudaStream_t st)
 {
     const long long n = (long long)N * width;

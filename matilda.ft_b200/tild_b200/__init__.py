@@ -334,9 +334,10 @@ class Pool:
         return dict(zip(("queued", "running", "done", "failed", "bytes_in_use", "budget"), (int(a) for a in v)))
 
 
-def box_from_spec(spec, device=0, options=None, steps_script=False):
-    """Build a Box directly from a synth.SystemSpec (arrays instead of readData)."""
-    b = Box(device, options=options)
+def box_from_spec(spec, device=0, options=None, steps_script=False, base_dir=None):
+    """Build a Box directly from a synth.SystemSpec (arrays instead of readData); output
+    files (when the write_files option is on) go to base_dir."""
+    b = Box(device, base_dir=base_dir, options=options)
     D = spec.dim
     b.command("Dim %d" % D)
     b.command("boxLengths " + " ".join("%.9g" % v for v in spec.L[:D]))

@@ -2,7 +2,11 @@
 // the reference sources in place, see Makefile) and dumps what the reference computes,
 // so the oracle and the B200 path can be pinned against the reference's own CUDA build.
 //
-//   tild_ref_harness <script> <outdir> <nsteps> [time_steps]
+//   tild_ref_harness <script> <outdir> <nsteps> [time_steps] [nvt]
+//
+// With "nvt" the <nsteps> steps run through PS_Box::NVT (PS_Box.cu:210-234), which adds the
+// run's closing outputs (final writeData, writeFields, writeGSDtraj, final.input.data) to
+// the per-step ones doTimeStep writes at the script's frequencies.
 //
 // Runs in the current directory (readData paths are relative to it, as in main.cu).
 // Dumps (raw little-endian arrays + meta.txt) into <outdir>:
@@ -51,6 +55,7 @@ int main(int argc, char** argv)
     const std::string out = argv[2];
     const int nsteps = atoi(argv[3]);
     const int tsteps = argc > 4 ? atoi(argv[4]) : 0;
+    const bool nvt = argc > 5 && std::string(argv[5]) == "nvt";
     std::ifstream in(argv[1]);
     if (!in) { fprintf(stderr, "cannot open %s\n", argv[1]); return 1; }
     std::string line, word;
@@ -92,7 +97,9 @@ int main(int argc, char** argv)
     const double ua = b->Uangle;                            // PS_Box.cu:296-305
     dump_host(out, "uangle.f64", &ua, sizeof(double));
     b->maxSteps = nsteps;
-    for (int i = 0; i < nsteps; i++) b->doTimeStep(i);      // PS_Box.cu:210-234 loop
+    if (nvt) b->NVT(nsteps);
+    else
+        for (int i = 0; i < nsteps; i++) b->doTimeStep(i);  // PS_Box.cu:210-234 loop
     cudaDeviceSynchronize();
     dump(out, "x_final.f32", b->d_x, sizeof(float) * (size_t)N * D);
     if (tsteps > 0) {
