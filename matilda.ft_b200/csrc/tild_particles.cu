@@ -167,7 +167,7 @@ __device__ __forceinline__ void angle_force(const Geom &g, const ParticleParams 
 // x_{t-1} is read from Xn and replaced by x_{t+1}.
 __device__ __forceinline__ void integrate(const Geom &g, const ParticleParams &pp, int p, uint32_t fl,
                                           const float *xs, const float *fs, float *__restrict__ Xn,
-                                          float *__restrict__ noise, const int *__restrict__ orig_id,
+                                          float *__restrict__ noise, const float *xold, const float *nold, int oid,
                                           curandState *__restrict__ rng, long long step)
 {
     const int slot = (fl >> 16) & 0xfu;
@@ -185,7 +185,7 @@ __device__ __forceinline__ void integrate(const Geom &g, const ParticleParams &p
         nz3[2] = curand_normal(&st);
         rng[p] = st;
     } else {
-        philox_normals3(pp.seed, (uint32_t)step, (uint32_t)orig_id[p], nz3);
+        philox_normals3(pp.seed, (uint32_t)step, (uint32_t)oid, nz3);
     }
     if (pp.integ_kind[slot] == 0) {
         const int t = (fl >> 20) & 0xfu;
@@ -195,10 +195,10 @@ __device__ __forceinline__ void integrate(const Geom &g, const ParticleParams &p
             const int ai = 3 * p + j;
             const float nn = cf.noiseMag * nz3[j];
             const float xt = xs[j];
-            float xo = Xn[ai];
+            float xo = xold[j];
             if (xo - xt > g.L[j] / 2.0f) xo -= g.L[j];
             else if (xo - xt < -g.L[j] / 2.0f) xo += g.L[j];
-            float xv = 2.0f * cf.b * xt - cf.a * xo + cf.bdt2m * fs[j] + cf.bdt2m2 * (nn + noise[ai]);
+            float xv = 2.0f * cf.b * xt - cf.a * xo + cf.bdt2m * fs[j] + cf.bdt2m2 * (nn + nold[j]);
             noise[ai] = nn;
             if (xv > g.L[j]) xv -= g.L[j];
             else if (xv < 0.0f) xv += g.L[j];
@@ -214,6 +214,12 @@ __device__ __forceinline__ void integrate(const Geom &g, const ParticleParams &p
             Xn[3 * p + j] = xv;
         }
     }
+}
+
+__device__ __forceinline__ void cp_async4(void *smem_dst, const void *gsrc)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
 
 __device__ __forceinline__ void cp_async16p(void *smem_dst, const void *gsrc)
@@ -285,6 +291,8 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     float4 *box = reinterpret_cast<float4 *>(smraw);
+    // per-thread integrator operands (x_{t-1}[3], previous noise[3], particle id), planes of blockDim
+    float *iop = reinterpret_cast<float *>(box + box_cap);
     __shared__ TileShared ts;
     __shared__ float Ao[kPartOut][kMaxFGroups][3];
     __shared__ int outP[kPartOut];
@@ -326,15 +334,24 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
             fl = pflags[p];
             // operands of the bonds and of the integrator, needed only after the gathers:
             // start bringing them into L2 now
-            asm volatile("prefetch.global.L2 [%0];" ::"l"(Xn + 3 * p));
-            asm volatile("prefetch.global.L2 [%0];" ::"l"(noise + 3 * p));
+            // the integrator's operands go to shared memory now, so that their latency is
+            // hidden behind the gathers instead of stalling the integration at the end
+            if (integrate_flag) {
+                const unsigned T = blockDim.x;
+                cp_async4(iop + threadIdx.x, Xn + 3 * p);
+                cp_async4(iop + T + threadIdx.x, Xn + 3 * p + 1);
+                cp_async4(iop + 2 * T + threadIdx.x, Xn + 3 * p + 2);
+                cp_async4(iop + 3 * T + threadIdx.x, noise + 3 * p);
+                cp_async4(iop + 4 * T + threadIdx.x, noise + 3 * p + 1);
+                cp_async4(iop + 5 * T + threadIdx.x, noise + 3 * p + 2);
+                cp_async4(iop + 6 * T + threadIdx.x, orig_id + p);
+            }
             if (nb) {
                 asm volatile("prefetch.global.L2 [%0];" ::"l"(partner + p * pp.maxb));
                 asm volatile("prefetch.global.L2 [%0];" ::"l"(nb + p));
                 asm volatile("prefetch.global.L2 [%0];" ::"l"(btype + p * pp.maxb));
             }
             if (q) asm volatile("prefetch.global.L2 [%0];" ::"l"(q + p));
-            asm volatile("prefetch.global.L2 [%0];" ::"l"(orig_id + p));
         }
         const unsigned fm = (fl >> 8) & 0xffu;
         int gs[3] = {0, 0, 0};
@@ -420,7 +437,8 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
             if (!((fl >> (8 + fg)) & 1u)) continue;
             float a[3];
             if (inbox) {
-                float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+                float2 a01 = make_float2(0.f, 0.f);
+                float a2 = 0.f;
 #pragma unroll
                 for (int e = 0; e <= P; e++) {
 #pragma unroll
@@ -431,14 +449,13 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
                         for (int aa = 0; aa <= P; aa++) {
                             const float w = Wx[aa] * wyz;
                             const float4 r = box[row + aa];
-                            a0 = __fmaf_rn(r.x, w, a0);
-                            a1 = __fmaf_rn(r.y, w, a1);
+                            a01 = __ffma2_rn(make_float2(r.x, r.y), make_float2(w, w), a01);   // paired FP32 FMA
                             a2 = __fmaf_rn(r.z, w, a2);
                         }
                     }
                 }
-                a[0] = a0;
-                a[1] = a1;
+                a[0] = a01.x;
+                a[1] = a01.y;
                 a[2] = a2;
             } else if (slot >= 0 && slot < kPartOut) {
                 a[0] = Ao[slot][fg][0];
@@ -466,7 +483,12 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
             }
             if (integrate_flag) {
                 const float xr[3] = {Xc[3 * p], Xc[3 * p + 1], Xc[3 * p + 2]};
-                integrate(g, pp, p, fl, xr, f, Xn, noise, orig_id, rng, step);
+                asm volatile("cp.async.wait_group 0;\n" ::: "memory");   // this thread's operands (no-op when staged)
+                const unsigned T = blockDim.x;
+                const float xold[3] = {iop[threadIdx.x], iop[T + threadIdx.x], iop[2 * T + threadIdx.x]};
+                const float nold[3] = {iop[3 * T + threadIdx.x], iop[4 * T + threadIdx.x], iop[5 * T + threadIdx.x]};
+                const int oid = __float_as_int(iop[6 * T + threadIdx.x]);
+                integrate(g, pp, p, fl, xr, f, Xn, noise, xold, nold, oid, rng, step);
             }
         }
         __syncthreads();   // the box, nout and the helpers' results are reused by the next pass
@@ -589,7 +611,7 @@ __global__ void k_reduce_partials(const double *partials, int nblocks, int ncols
 }
 
 
-constexpr size_t kPartSmemMax = kPartBox * sizeof(float4);
+constexpr size_t kPartSmemMax = kPartBox * sizeof(float4) + 512 * 7 * sizeof(float);
 
 template <int P>
 static void part_launch(const Geom &g, const ParticleParams *ppd, int N, float *X0, float *X1, float *noise,
@@ -600,7 +622,7 @@ static void part_launch(const Geom &g, const ParticleParams *ppd, int N, float *
     const int nbk = tc.start ? (tc.nkeys + tc.codes - 1) / tc.codes : (N + kPartWindow - 1) / kPartWindow;
     const int threads = tc.start ? tc.threads : 256;
     const int cap = tc.start ? std::min(tc.pbox, kPartBox) : 0;
-    const size_t smem = (size_t)cap * sizeof(float4);
+    const size_t smem = (size_t)cap * sizeof(float4) + (size_t)threads * 7 * sizeof(float);
     k_particles<P><<<nbk, threads, smem, st>>>(g, ppd, N, X0, X1, noise, pflags, q, nb, partner, btype, aa, rec, orig_id,
                                                reinterpret_cast<curandState *>(rng), d_step, fout, integrate, tc, cap);
 }
