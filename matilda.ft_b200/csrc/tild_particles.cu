@@ -332,10 +332,9 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
             x[1] = Xc[3 * p + 1];
             x[2] = Xc[3 * p + 2];
             fl = pflags[p];
-            // operands of the bonds and of the integrator, needed only after the gathers:
-            // start bringing them into L2 now
-            // the integrator's operands go to shared memory now, so that their latency is
-            // hidden behind the gathers instead of stalling the integration at the end
+            // operands of the integrator go to shared memory now (their latency is then
+            // hidden behind the gathers instead of stalling the integration at the end);
+            // those of the bonds are brought into L2
             if (integrate_flag) {
                 const unsigned T = blockDim.x;
                 cp_async4(iop + threadIdx.x, Xn + 3 * p);
@@ -483,7 +482,9 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
             }
             if (integrate_flag) {
                 const float xr[3] = {Xc[3 * p], Xc[3 * p + 1], Xc[3 * p + 2]};
-                asm volatile("cp.async.wait_group 0;\n" ::: "memory");   // this thread's operands (no-op when staged)
+                // this thread's operands; wait_all also covers copies not yet committed to a
+                // group (tiles that stage no box)
+                asm volatile("cp.async.wait_all;\n" ::: "memory");
                 const unsigned T = blockDim.x;
                 const float xold[3] = {iop[threadIdx.x], iop[T + threadIdx.x], iop[2 * T + threadIdx.x]};
                 const float nold[3] = {iop[3 * T + threadIdx.x], iop[4 * T + threadIdx.x], iop[5 * T + threadIdx.x]};
@@ -491,6 +492,7 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
                 integrate(g, pp, p, fl, xr, f, Xn, noise, xold, nold, oid, rng, step);
             }
         }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");   // no copy outlives the pass
         __syncthreads();   // the box, nout and the helpers' results are reused by the next pass
     }
 }

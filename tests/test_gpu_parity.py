@@ -162,6 +162,25 @@ def test_trajectory_matches_oracle_100_steps(integ):
     assert d.max() <= 1e-3 and np.median(d) <= 1e-4, (d.max(), np.median(d))
 
 
+def test_tiles_without_grid_forces_integrate_like_the_oracle():
+    """Species B takes no grid force and fills half of the box, so whole tiles gather
+    nothing: their particles still integrate with their own x_{t-1}, noise and id."""
+    spec = synth.small_system(seed=19, order=3, n_chains=40, nper=8,
+                              pots=[dict(kind="gaussian", I="A", J="A", A=2.0, sigma=0.7)])
+    spec.types = (spec.x[:, 0] >= spec.L[0] / 2).astype(np.int32)
+    sysm = spec_to_system(spec)
+    traj = oracle.Trajectory(sysm, 64)
+    ids = np.arange(sysm.N)
+    with make_box(spec, sort_interval=5) as b:
+        b.step(30)
+        x = b.positions()
+    for step in range(30):
+        traj.step(oracle.philox_normals(spec.seed, step, ids))
+    d = np.abs(x - traj.positions())
+    d = np.minimum(d, spec.L - d)
+    assert d.max() <= 1e-3 and np.median(d) <= 1e-4, (d.max(), np.median(d))
+
+
 def test_forces_unchanged_by_forces_call_and_positions_round_trip():
     spec = synth.small_system(seed=14, order=3)
     # fast mode sums float atomics in scheduling order (like the reference); bitwise
