@@ -152,9 +152,10 @@ int tild_box_forces(tild_box *box, float *f_out);
  * Writes min(nout, 2 + npot + 19) values; *nwritten (may be NULL) receives the count. */
 int tild_box_thermo(tild_box *box, double *out, int nout, int *nwritten);
 
-/* Copy positions device -> host (x_out[n*Dim]) / host -> device.  Setting positions
- * also resets the GJF old positions to them (GJF::finishInitialization,
- * ps_integratorGJF.cu:48-51). */
+/* Copy positions device -> host (x_out[n*Dim]) / host -> device (x_in[n*Dim]).  Setting
+ * positions also resets the GJF old positions to them (GJF::finishInitialization,
+ * ps_integratorGJF.cu:48-51).  A 2-D box (Dim 2) runs as one grid plane: its particles
+ * stay at z = 0 and only x, y are read and written. */
 int tild_box_get_positions(tild_box *box, float *x_out);
 int tild_box_set_positions(tild_box *box, const float *x_in);
 
@@ -238,7 +239,7 @@ int tild_pool_submit(tild_pool *pool, tild_box *box, int64_t nsteps, int64_t *jo
 int tild_pool_status(tild_pool *pool, int64_t job_id, int32_t *state, int64_t *steps_done, double *times3);
 /* Blocks until the job is done; TILD_ERR_STATE with the job's error if it failed. */
 int tild_pool_wait(tild_pool *pool, int64_t job_id);
-/* Final positions x_out[n*3] (particle order, may be NULL) and up to nthermo values of
+/* Final positions x_out[n*Dim] (particle order, may be NULL) and up to nthermo values of
  * tild_box_thermo's layout at the last step. */
 int tild_pool_result(tild_pool *pool, int64_t job_id, float *x_out, double *thermo_out, int32_t nthermo,
                      int32_t *nwritten);

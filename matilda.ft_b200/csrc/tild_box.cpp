@@ -864,10 +864,14 @@ void Box::prepareHost()
 {
     if (hostPrepared) return;
     if (nstot == 0) fail(TILD_ERR_PARSE, "Box created with no particles?!?");
-    if (Dim != 3) fail(TILD_ERR_UNSUPPORTED, "the B200 TILD path runs 3-D boxes (Dim 3)");
-    for (int j = 0; j < 3; j++)
+    if (Dim != 2 && Dim != 3) fail(TILD_ERR_PARSE, "Dim must be 2 or 3");
+    if (Dim == 2) {   // a 2-D box runs as one plane of unit thickness at z = 0
+        Nx[2] = 1;
+        L[2] = 1.0f;
+    }
+    for (int j = 0; j < Dim; j++)
         if (Nx[j] <= 0) fail(TILD_ERR_PARSE, "grid must be given for every dimension");
-    for (int j = 0; j < 3; j++)   // the kernels wrap stencil indices with one add or subtract
+    for (int j = 0; j < Dim; j++)   // the kernels wrap stencil indices with one add or subtract
         if (Nx[j] < pmeorder + 2)
             fail(TILD_ERR_UNSUPPORTED, "grid of " + std::to_string(Nx[j]) + " points is too small for pmeorder " +
                                            std::to_string(pmeorder) + " (needs at least pmeorder + 2)");
@@ -883,6 +887,10 @@ void Box::prepareHost()
         dx[j] = (double)L[j] / (double)Nx[j];
         gvol *= dx[j];
         Lh[j] = 0.5f * L[j];
+    }
+    if (Dim == 2) {   // the plane's unit thickness: cell volume dx*dy*1, as the 2-D gvol
+        dx[2] = 1.0;
+        Lh[2] = 0.5f;
     }
     if (doCharges) {   // PS_Box_initialization.cu:398-412
         float qtot = 0.f, qneg = 0.f, qpos = 0.f;
@@ -918,7 +926,12 @@ void Box::prepareHost()
             psGroup[p.Jind].forceFlag = true;
         }
     }
-    if (writeFiles) writeGsdFrame(0, x.data());   // GSDinit + writeGSDtraj (PS_Box_initialization.cu:521-523)
+    if (writeFiles) {   // GSDinit + writeGSDtraj (PS_Box_initialization.cu:521-523)
+        std::vector<float> x3(3 * nstot, 0.f);
+        for (int64_t p = 0; p < nstot; p++)
+            for (int j = 0; j < Dim; j++) x3[3 * p + j] = x[p * Dim + j];
+        writeGsdFrame(0, x3.data());
+    }
     if (writeFiles) initFieldFiles();
     if (writeFiles) { std::ofstream o(resolve(datFileName)); }   // :359-364, :543-544 truncate
     buildPlan();
@@ -1089,6 +1102,7 @@ void Box::buildPlan()
     }
     pp.seed = (unsigned long long)RANDSEED;
     pp.rng_compat = rngCompat;
+    pp.dim = Dim;
 }
 
 void Box::allocDevice()
@@ -1145,7 +1159,7 @@ void Box::allocDevice()
     const uint32_t nk = sort_key_count(g);
     sortKeys = nk;
     {   // tile geometry: about one particle per thread, box sized for the tile plus drift
-        const double perCode = 64.0 * (double)N / (double)g.M;   // particles per 4^3-cell brick
+        const double perCode = 16.0 * std::min(4, g.nz) * (double)N / (double)g.M;   // particles per brick of 4^3 cells (4x4x1 in 2-D)
         int codes = 8;
         while (codes < 64 && perCode * codes * 2.0 <= 192.0) codes *= 2;
         const double e = perCode * codes;
@@ -1195,7 +1209,7 @@ void Box::uploadParticles()
     const int64_t N = nstot;
     std::vector<float> x3(3 * N);
     for (int64_t p = 0; p < N; p++)
-        for (int j = 0; j < 3; j++) x3[3 * p + j] = x[p * Dim + j];
+        for (int j = 0; j < 3; j++) x3[3 * p + j] = j < Dim ? x[p * Dim + j] : 0.f;
     ck(cudaMemcpy(dX[0], x3.data(), 12 * N, cudaMemcpyHostToDevice), "upload x");
     ck(cudaMemcpy(dX[1], x3.data(), 12 * N, cudaMemcpyHostToDevice), "upload xOld");   // GJF: xOld = x
     ck(cudaMemset(dNoise, 0, 12 * N), "zero noise");
@@ -1829,13 +1843,13 @@ std::vector<double> Box::thermo()
     for (int c = 0; c < 6; c++) {
         // bonded: sum over bonds of dr_a f_b, plus over angles of r_ij,a f_i,b + r_kj,a f_k,b
         wb[c] = 0.5 * r[kResBond + 1 + c] + r[kResAngle + 1 + c] / 3.0;
-        wp[c] = r[np + c] + (c < 3 ? upair : 0.0);            // pairs: -dU/d(strain_ab)
+        wp[c] = r[np + c] + (c < Dim ? upair : 0.0);          // pairs: -dU/d(strain_ab)
         out.push_back(wb[c]);
     }
     // pair virial, then the pressure tensor (N kT delta_ab + W_pair + W_bond) / V, kT = 1
     for (int c = 0; c < 6; c++) out.push_back(wp[c]);
     const double V = (double)L[0] * L[1] * L[2];
-    for (int c = 0; c < 6; c++) out.push_back(((c < 3 ? (double)nstot : 0.0) + wp[c] + wb[c]) / V);
+    for (int c = 0; c < 6; c++) out.push_back(((c < Dim ? (double)nstot : 0.0) + wp[c] + wb[c]) / V);
     out.push_back(uangle);
     return out;
 }
@@ -1846,8 +1860,22 @@ void Box::forces(float *f_out)
     ck(cudaSetDevice(device), "cudaSetDevice");
     enqueueStep(false, false, dF);
     ck(launch_unpermute_rows((int)nstot, 3, dOrig, dF, dTmp, stream), "unpermute forces");
-    ck(cudaMemcpyAsync(f_out, dTmp, 12 * nstot, cudaMemcpyDeviceToHost, stream), "read forces");
-    ck(cudaStreamSynchronize(stream), "forces");
+    readRows3(dTmp, f_out);
+}
+
+// dev[3n] (original order) -> host out[n*Dim], the reference's layout of x and f
+void Box::readRows3(const float *dev, float *out) const
+{
+    if (Dim == 3) {
+        ck(cudaMemcpyAsync(out, dev, 12 * nstot, cudaMemcpyDeviceToHost, stream), "read rows");
+        ck(cudaStreamSynchronize(stream), "read rows");
+        return;
+    }
+    std::vector<float> h(3 * nstot);
+    ck(cudaMemcpyAsync(h.data(), dev, 12 * nstot, cudaMemcpyDeviceToHost, stream), "read rows");
+    ck(cudaStreamSynchronize(stream), "read rows");
+    for (int64_t p = 0; p < nstot; p++)
+        for (int j = 0; j < Dim; j++) out[p * Dim + j] = h[3 * p + j];
 }
 
 TileCfg Box::tileCfg() const
@@ -1870,14 +1898,20 @@ void Box::getPositions(float *xo) const
     if (!ready) fail(TILD_ERR_STATE, "endBox has not been processed");
     const long long s = deviceStep();
     ck(launch_unpermute_rows((int)nstot, 3, dOrig, dX[s & 1], dTmp, stream), "unpermute positions");
-    ck(cudaMemcpyAsync(xo, dTmp, 12 * nstot, cudaMemcpyDeviceToHost, stream), "read positions");
-    ck(cudaStreamSynchronize(stream), "read positions");
+    readRows3(dTmp, xo);
 }
 
 void Box::setPositions(const float *xi)
 {
     if (!ready) fail(TILD_ERR_STATE, "endBox has not been processed");
     ck(cudaStreamSynchronize(stream), "sync");
+    std::vector<float> flat;
+    if (Dim == 2) {   // x_in[n*2]; the device rows keep z = 0 (the plane of a 2-D box)
+        flat.assign(3 * nstot, 0.f);
+        for (int64_t p = 0; p < nstot; p++)
+            for (int j = 0; j < 2; j++) flat[3 * p + j] = xi[2 * p + j];
+        xi = flat.data();
+    }
     ck(cudaMemcpyAsync(dTmp, xi, 12 * nstot, cudaMemcpyHostToDevice, stream), "set positions");
     ck(launch_permute_rows((int)nstot, 3, dOrig, dTmp, dX[0], stream), "permute positions");
     ck(cudaMemcpyAsync(dX[1], dX[0], 12 * nstot, cudaMemcpyDeviceToDevice, stream), "set positions");
@@ -1999,7 +2033,7 @@ void Box::gridWeights(int32_t *inds, float *w)
 {
     if (!ready) fail(TILD_ERR_STATE, "endBox has not been processed");
     const long long s = deviceStep();
-    const int G = (pmeorder + 1) * (pmeorder + 1) * (pmeorder + 1);
+    const int G = (pmeorder + 1) * (pmeorder + 1) * (Dim == 3 ? pmeorder + 1 : 1);
     int *dI = nullptr;
     float *dW = nullptr, *dO = nullptr;
     ck(cudaMalloc(&dI, 4 * nstot * G), "malloc");
@@ -2043,12 +2077,7 @@ void Box::modifyBox(const std::string &rest)
 void Box::writeDataConfig(const std::string &name)   // PS_Box.cu:629-748
 {
     std::vector<float> xs(x);
-    if (ready) {
-        std::vector<float> x3(3 * nstot);
-        getPositions(x3.data());
-        for (int64_t p = 0; p < nstot; p++)
-            for (int j = 0; j < Dim; j++) xs[p * Dim + j] = x3[3 * p + j];
-    }
+    if (ready) getPositions(xs.data());   // x[n*Dim]
     std::ofstream out(resolve(name));
     if (!out) fail(TILD_ERR_IO, "cannot write " + name);
     out << "Created by MATILDA.FT\n\n";

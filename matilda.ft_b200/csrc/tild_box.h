@@ -93,6 +93,7 @@ public:
     void forces(float *f_out);                         // PS_Box::forces at current x
     std::vector<double> thermo();                      // computeThermoProps (+ virial)
     void getPositions(float *x) const;
+    void readRows3(const float *dev, float *out) const;
     void setPositions(const float *x);
     void getDensity(const std::string &group, int charge, float *rho);
     void getDensityNoAlloc(const std::string &group, int charge, float *rho);

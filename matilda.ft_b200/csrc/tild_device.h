@@ -125,6 +125,7 @@ struct ParticleParams {
     TypeCoef coef[4][kMaxTypes];
     unsigned long long seed;
     int rng_compat;
+    int dim;                        // 2: z is one plane at z = 0 (no z noise), 3: full 3-D
 };
 
 // Work split of the particle kernels over a sorted particle order: a CTA of `threads`

@@ -15,7 +15,8 @@ namespace tild {
 // into the k-space constants.
 // =====================================================================================
 
-// Reference-exact stencil table (d_calcGridWeights, ps_grid_utils.cu:74-204), 3-D.
+// Reference-exact stencil table (d_calcGridWeights, ps_grid_utils.cu:74-204): (P+1)^3
+// entries per particle, or (P+1)^2 for a 2-D box (nz == 1; index n1*nx + n0, :139).
 template <int P>
 __global__ void k_grid_weights(Geom g, int quirk4, const float *X, int N, int *inds, float *W)
 {
@@ -24,15 +25,16 @@ __global__ void k_grid_weights(Geom g, int quirk4, const float *X, int N, int *i
     float Wx[P + 1], Wy[P + 1], Wz[P + 1];
     const int gx = stencil_axis<P>(X[3 * p], g.dxf[0], quirk4, Wx);
     const int gy = stencil_axis<P>(X[3 * p + 1], g.dxf[1], quirk4, Wy);
-    const int gz = stencil_axis<P>(X[3 * p + 2], g.dxf[2], quirk4, Wz);
+    const int gz = stencil_axis_z<P>(X[3 * p + 2], g.dxf[2], quirk4, Wz, g.nz);
     const float gvol = __fmul_rn(__fmul_rn(__fmul_rn(1.0f, g.dxf[0]), g.dxf[1]), g.dxf[2]);
-    constexpr int G = (P + 1) * (P + 1) * (P + 1);
+    const bool flat = g.nz == 1;
+    const int G = flat ? (P + 1) * (P + 1) : (P + 1) * (P + 1) * (P + 1), ez = flat ? 0 : P;
     int ct = 0;
     for (int a = 0; a <= P; a++) {
         const int n0 = wrapi(gx + a, g.nx);
         for (int b = 0; b <= P; b++) {
             const int n1 = wrapi(gy + b, g.ny);
-            for (int e = 0; e <= P; e++) {
+            for (int e = 0; e <= ez; e++) {
                 const int n2 = wrapi(gz + e, g.nz);
                 inds[(long long)p * G + ct] = n0 + (n1 + n2 * g.ny) * g.nx;
                 W[(long long)p * G + ct] = __fdiv_rn(__fmul_rn(__fmul_rn(Wx[a], Wy[b]), Wz[e]), gvol);
@@ -53,7 +55,7 @@ __global__ void k_density_single(Geom g, int quirk4, const float *X, const int *
     float Wx[P + 1], Wy[P + 1], Wz[P + 1];
     const int gx = stencil_axis<P>(X[3 * p], g.dxf[0], quirk4, Wx);
     const int gy = stencil_axis<P>(X[3 * p + 1], g.dxf[1], quirk4, Wy);
-    const int gz = stencil_axis<P>(X[3 * p + 2], g.dxf[2], quirk4, Wz);
+    const int gz = stencil_axis_z<P>(X[3 * p + 2], g.dxf[2], quirk4, Wz, g.nz);
     const float gvol = __fmul_rn(__fmul_rn(g.dxf[0], g.dxf[1]), g.dxf[2]);
     const float c = charge ? q[p] : 1.f;
     for (int a = 0; a <= P; a++)
@@ -82,7 +84,7 @@ __global__ void k_group_density_frames(Geom g, int quirk4, const float *X0, cons
     float Wx[P + 1], Wy[P + 1], Wz[P + 1];
     const int gx = stencil_axis<P>(X[3 * s], g.dxf[0], quirk4, Wx);
     const int gy = stencil_axis<P>(X[3 * s + 1], g.dxf[1], quirk4, Wy);
-    const int gz = stencil_axis<P>(X[3 * s + 2], g.dxf[2], quirk4, Wz);
+    const int gz = stencil_axis_z<P>(X[3 * s + 2], g.dxf[2], quirk4, Wz, g.nz);
     const float gvol = __fmul_rn(__fmul_rn(g.dxf[0], g.dxf[1]), g.dxf[2]);
     for (int a = 0; a <= P; a++)
         for (int b = 0; b <= P; b++)
@@ -208,7 +210,7 @@ __global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4
                 float Wx[P1], Wy[P1], Wz[P1];
                 const int gs[3] = {stencil_fast<P>(X[3 * p + 0], inv[0], quirk4, Wx),
                                    stencil_fast<P>(X[3 * p + 1], inv[1], quirk4, Wy),
-                                   stencil_fast<P>(X[3 * p + 2], inv[2], quirk4, Wz)};
+                                   stencil_fast_z<P>(X[3 * p + 2], inv[2], quirk4, Wz, g.nz)};
                 int d[3];
                 bool in = true;
 #pragma unroll
@@ -281,7 +283,7 @@ __global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4
             float Wx[P1], Wy[P1], Wz[P1];
             const int gx = stencil_fast<P>(X[3 * p + 0], inv[0], quirk4, Wx);
             const int gy = stencil_fast<P>(X[3 * p + 1], inv[1], quirk4, Wy);
-            const int gz = stencil_fast<P>(X[3 * p + 2], inv[2], quirk4, Wz);
+            const int gz = stencil_fast_z<P>(X[3 * p + 2], inv[2], quirk4, Wz, g.nz);
             const float qp = q ? q[p] : 0.f;
             int ix[P1], iy[P1], iz[P1];
 #pragma unroll

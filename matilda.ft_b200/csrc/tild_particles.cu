@@ -178,14 +178,15 @@ __device__ __forceinline__ void integrate(const Geom &g, const ParticleParams &p
         return;
     }
     float nz3[3];
-    if (pp.rng_compat) {
+    if (pp.rng_compat) {   // one normal per dimension, as the reference draws them
         curandState st = rng[p];
         nz3[0] = curand_normal(&st);
         nz3[1] = curand_normal(&st);
-        nz3[2] = curand_normal(&st);
+        nz3[2] = pp.dim == 3 ? curand_normal(&st) : 0.f;
         rng[p] = st;
     } else {
         philox_normals3(pp.seed, (uint32_t)step, (uint32_t)oid, nz3);
+        if (pp.dim == 2) nz3[2] = 0.f;   // z (always 0 in a 2-D box) takes no noise
     }
     if (pp.integ_kind[slot] == 0) {
         const int t = (fl >> 20) & 0xfu;
@@ -357,7 +358,7 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
         if (fm) {
             gs[0] = stencil_origin<P>(x[0], inv[0]);
             gs[1] = stencil_origin<P>(x[1], inv[1]);
-            gs[2] = stencil_origin<P>(x[2], inv[2]);
+            gs[2] = stencil_origin_z<P>(x[2], inv[2], g.nz);
         }
         if (threadIdx.x == 0) {
             nout = 0;
@@ -398,7 +399,7 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
             int hs[3];
             hs[0] = stencil_fast<P>(Xc[3 * ph], inv[0], pp.quirk4, Hx);
             hs[1] = stencil_fast<P>(Xc[3 * ph + 1], inv[1], pp.quirk4, Hy);
-            hs[2] = stencil_fast<P>(Xc[3 * ph + 2], inv[2], pp.quirk4, Hz);
+            hs[2] = stencil_fast_z<P>(Xc[3 * ph + 2], inv[2], pp.quirk4, Hz, g.nz);
             for (int h = 0; h < pp.nfg; h++)
                 if ((flh >> (8 + h)) & 1u) gather_global<P>(g, rec + (long long)h * g.M, hs, Hx, Hy, Hz, Ao[threadIdx.x][h]);
         }
@@ -414,7 +415,7 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
         if (fm) {
             stencil_fast<P>(x[0], inv[0], pp.quirk4, Wx);
             stencil_fast<P>(x[1], inv[1], pp.quirk4, Wy);
-            stencil_fast<P>(x[2], inv[2], pp.quirk4, Wz);
+            stencil_fast_z<P>(x[2], inv[2], pp.quirk4, Wz, g.nz);
         }
         // 5. gather each force group in group order
         bool first = true;

@@ -175,7 +175,7 @@ bool Pool::admit(Job *j)
 
 void Pool::harvest(Job *j)
 {
-    std::vector<float> x(3 * (size_t)j->N);
+    std::vector<float> x((size_t)j->box->Dim * j->N);
     std::vector<double> th;
     try {
         j->box->getPositions(x.data());

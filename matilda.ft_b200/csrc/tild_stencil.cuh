@@ -140,6 +140,35 @@ __device__ __forceinline__ int stencil_origin(float x, float inv_d)
     return g - P / 2;
 }
 
+// The z axis of a 2-D box is one plane (nz == 1, every particle at z = 0): its stencil is
+// the single point 0 with weight 1 (the z loops still run over P + 1 points, the others
+// with weight 0), so products Wx*Wy*Wz are exactly the 2-D weights Wx*Wy.
+template <int P>
+__device__ __forceinline__ int stencil_fast_z(float z, float inv_d, int quirk4, float *W, int nz)
+{
+    if (nz != 1) return stencil_fast<P>(z, inv_d, quirk4, W);
+    W[0] = 1.f;
+#pragma unroll
+    for (int k = 1; k <= P; k++) W[k] = 0.f;
+    return 0;
+}
+
+template <int P>
+__device__ __forceinline__ int stencil_axis_z(float z, float d, int quirk4, float *W, int nz)
+{
+    if (nz != 1) return stencil_axis<P>(z, d, quirk4, W);
+    W[0] = 1.f;
+#pragma unroll
+    for (int k = 1; k <= P; k++) W[k] = 0.f;
+    return 0;
+}
+
+template <int P>
+__device__ __forceinline__ int stencil_origin_z(float z, float inv_d, int nz)
+{
+    return nz == 1 ? 0 : stencil_origin<P>(z, inv_d);
+}
+
 // [b0, b1) of the CTA: a tile of sorted particles, or a fixed window of slots
 __device__ __forceinline__ void tile_range(const TileCfg &tc, int N, int window, int &b0, int &b1)
 {

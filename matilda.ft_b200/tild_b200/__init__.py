@@ -200,7 +200,7 @@ class Box:
         _check(lib().tild_box_step(self._h, int(nsteps)))
 
     def forces(self):
-        f = np.zeros((self.N, 3), np.float32)
+        f = np.zeros((self.N, int(self.info().dim)), np.float32)
         _check(lib().tild_box_forces(self._h, _ptr(f)))
         return f
 
@@ -223,7 +223,7 @@ class Box:
                     pressure=v[14 + npot:20 + npot].copy(), Uangle=float(v[20 + npot]))
 
     def positions(self):
-        x = np.zeros((self.N, 3), np.float32)
+        x = np.zeros((self.N, int(self.info().dim)), np.float32)
         _check(lib().tild_box_get_positions(self._h, _ptr(x)))
         return x
 
@@ -253,7 +253,7 @@ class Box:
 
     def grid_weights(self):
         i = self.info()
-        G = (i.pmeorder + 1) ** 3
+        G = (i.pmeorder + 1) ** int(i.dim)
         inds = np.zeros((self.N, G), np.int32)
         w = np.zeros((self.N, G), np.float32)
         _check(lib().tild_box_grid_weights(self._h, _ptr(inds), _ptr(w)))
@@ -318,8 +318,8 @@ class Pool:
     def wait(self, job: int):
         _check(lib().tild_pool_wait(self._h, int(job)))
 
-    def result(self, job: int, n: int):
-        x = np.zeros((n, 3), np.float32)
+    def result(self, job: int, n: int, dim: int = 3):
+        x = np.zeros((n, dim), np.float32)
         th = np.zeros(64, np.float64)
         nw = ctypes.c_int32()
         _check(lib().tild_pool_result(self._h, int(job), _ptr(x), _ptr(th), 64, ctypes.byref(nw)))

@@ -221,7 +221,8 @@ def pair_virial(sysm: System, dens):
     """Pair virial W_ab = -dU_pair/d(strain_ab) for an affine strain of the box and the
     positions (the grid follows the box, so the deposited weights do not change):
     U = C/V sum_k û(|k|) Re(rho_I* rho_J) gives W_ab = U delta_ab + C/V sum_k (û'(k)/k)
-    k_a k_b Re(rho_I* rho_J).  Components xx, yy, zz, xy, xz, yz (FP64)."""
+    k_a k_b Re(rho_I* rho_J).  Components xx, yy, zz, xy, xz, yz (FP64; those with z are 0
+    in a 2-D box)."""
     glist = groups(sysm)
     shape = _grid_shape(sysm)
     M = int(np.prod(sysm.Nx))
@@ -246,8 +247,9 @@ def pair_virial(sysm: System, dens):
         utot += c * float(np.sum(uk(pot, k2) * re))
         d = duk_over_k(pot, k2) * re
         for i, (a, b) in enumerate(pairs):
-            W[i] += c * float(np.sum(d * ks[a] * ks[b]))
-    W[:3] += utot
+            if a < sysm.Dim and b < sysm.Dim:   # a 2-D box has only xx, yy, xy
+                W[i] += c * float(np.sum(d * ks[a] * ks[b]))
+    W[:sysm.Dim] += utot
     return W
 
 
@@ -370,7 +372,9 @@ def angle_terms(sysm: System, x=None):
     fk = np.where(ok[:, None], coef[:, None] * drk, 0.0)
     e = np.where(ok, e, 0.0)
     pairs = ((0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2))
-    vir = np.stack([fi[:, p] * rij[:, q] + fk[:, p] * rkj[:, q] for p, q in pairs], 1)
+    D = rij.shape[1]   # components with z are 0 in a 2-D box
+    vir = np.stack([fi[:, p] * rij[:, q] + fk[:, p] * rkj[:, q] if p < D and q < D else np.zeros(len(e))
+                    for p, q in pairs], 1)
     return fi, fk, e, vir
 
 
@@ -606,7 +610,10 @@ class Trajectory:
         s, real, lib = self.s, self.real, _lib(self.prec)
         f, _ = forces(s, self.x.reshape(s.N, s.Dim), self.prec)
         f = np.ascontiguousarray(f, dtype=real).reshape(-1)
-        nz = np.ascontiguousarray(unit_noise, dtype=real).reshape(-1)
+        un = np.asarray(unit_noise)
+        if un.ndim == 2:   # (N, 3) draws: a 2-D box uses the first two of each particle
+            un = un[:, :s.Dim]
+        nz = np.ascontiguousarray(un, dtype=real).reshape(-1)
         Lr = np.ascontiguousarray(s.L, dtype=real)
         if s.integrator == "GJF":
             getattr(lib, "orc%d_gjf" % self.prec)(

@@ -43,6 +43,10 @@ def systems():
         "c1": synth.config_c1(),
         "angles_o3": synth.small_system(seed=37, order=3, charges=True, angle_params=[
             dict(style="harmonic", k=3.0, theta=120.0), dict(style="wlc", k=2.0)]),
+        # 2-D boxes (Dim 2): the plane's stencils, k-vectors, noise draws and gvol
+        "d2_o3": synth.small_system(seed=38, order=3, charges=True, dim=2, grid=(16, 18, 1)),
+        "d2_o4": synth.small_system(seed=39, order=4, dim=2, grid=(15, 12, 1), angle_params=[
+            dict(style="harmonic", k=2.0, theta=110.0)]),
     }
 
 

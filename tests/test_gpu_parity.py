@@ -4,7 +4,8 @@ Tolerances (written here, used below):
   * stencil indices: bit-exact with the FP32 restatement of d_calcGridWeights;
     weights: bit-exact as well (same IEEE operations, explicit FMAs);
   * densities: |drho| <= 1e-6 * max|rho| (FP32 atomics vs FP64 sums);
-  * forces: max_p |df_p| / max(|f_p|, f_rms) <= 1e-5 against the FP64 oracle;
+  * forces: max_p |df_p| / max(|f_p|, f_rms) <= 1e-5 against the FP64 oracle, raised by
+    2^-21/sin^2(theta) for the particles of a near-straight angle (FP32 conditioning);
   * energies: relative 1e-5 (pair terms) and 1e-6 (bond term);
   * 100-step GJF trajectories with identical Philox noise: max |dx| <= 2e-4.
 """
@@ -15,7 +16,7 @@ import pytest
 
 import oracle
 import tild_b200
-from conftest import force_error, spec_to_system
+from conftest import angle_force_tolerance, force_error, spec_to_system
 from tild_b200 import synth
 
 pytestmark = pytest.mark.gpu
@@ -51,6 +52,9 @@ SYSTEMS = {
     "prime_grid": lambda: synth.small_system(seed=13, order=1, grid=(22, 13, 11), charges=True),
     "angles": lambda: synth.small_system(seed=15, order=3, charges=True, angle_params=ANGLES),
     "free_particles": lambda: synth.small_system(seed=9, order=3, n_free=50, charges=True),
+    # 2-D boxes: one grid plane, particles at z = 0
+    "d2_charged": lambda: synth.small_system(seed=20, order=3, charges=True, dim=2, grid=(16, 18, 1)),
+    "d2_o4_angles": lambda: synth.small_system(seed=21, order=4, dim=2, grid=(15, 12, 1), angle_params=ANGLES),
 }
 
 
@@ -61,8 +65,8 @@ def test_forces_match_oracle(name):
     with make_box(spec) as b:
         f = b.forces()
     fref, _ = oracle.forces(sysm, prec=64)
-    err = force_error(f, fref)
-    assert err <= F_TOL, "%s: force error %.3g" % (name, err)
+    err = force_error(f, fref, angle_force_tolerance(sysm, F_TOL))
+    assert err <= 1.0, "%s: force error %.3g of the tolerance" % (name, err)
 
 
 @pytest.mark.parametrize("order", [0, 1, 2, 3, 4])
@@ -181,6 +185,29 @@ def test_tiles_without_grid_forces_integrate_like_the_oracle():
     assert d.max() <= 1e-3 and np.median(d) <= 1e-4, (d.max(), np.median(d))
 
 
+@pytest.mark.parametrize("name", ["d2_charged", "d2_o4_angles"])
+def test_2d_trajectory_energies_and_pressure_match_oracle(name):
+    spec = SYSTEMS[name]()
+    sysm = spec_to_system(spec)
+    dens, _, _ = oracle.densities(sysm)
+    ref = oracle.pair_energies(sysm, dens)
+    with make_box(spec) as b:
+        th = b.thermo()
+        for k, r in enumerate(ref):
+            assert abs(th["potentials"][k] - r) <= 1e-5 * max(abs(r), 1e-9)
+        assert th["pressure"][2] == 0.0   # zz: no kinetic or virial term in a plane
+        b.step(50)
+        x = b.positions()
+    assert x.shape == (spec.N, 2)
+    traj = oracle.Trajectory(sysm, 64)
+    ids = np.arange(sysm.N)
+    for step in range(50):
+        traj.step(oracle.philox_normals(spec.seed, step, ids))
+    d = np.abs(x - traj.positions())
+    d = np.minimum(d, np.asarray(spec.L[:2]) - d)
+    assert d.max() <= 1e-3 and np.median(d) <= 1e-4, (d.max(), np.median(d))
+
+
 def test_forces_unchanged_by_forces_call_and_positions_round_trip():
     spec = synth.small_system(seed=14, order=3)
     # fast mode sums float atomics in scheduling order (like the reference); bitwise
@@ -291,7 +318,7 @@ def test_full_size_c2_properties():
         assert (x >= 0).all() and (x <= spec.L).all()
 
 
-@pytest.mark.parametrize("name", ["diblock_o3", "charged_o3", "erf", "odd_grid"])
+@pytest.mark.parametrize("name", ["diblock_o3", "charged_o3", "erf", "odd_grid", "d2_charged"])
 def test_pair_virial_and_pressure_match_oracle(name):
     """FP64 pair virial W_ab against the oracle (relative 1e-5 of max |W|), and the pressure
     tensor equal to (N kT delta + W_pair + W_bond)/V with kT = 1."""
@@ -303,8 +330,9 @@ def test_pair_virial_and_pressure_match_oracle(name):
         t = b.thermo()
     W = t["pair_virial"]
     assert np.abs(W - Wref).max() <= 1e-5 * np.abs(Wref).max(), (W, Wref)
-    V = float(np.prod(np.asarray(spec.L, np.float64)))
-    P = (np.r_[np.full(3, spec.N), np.zeros(3)] + W + t["virial"]) / V
+    D = spec.dim
+    V = float(np.prod(np.asarray(spec.L[:D], np.float64)))   # a 2-D box: its area
+    P = (np.r_[np.full(D, spec.N), np.zeros(6 - D)] + W + t["virial"]) / V
     assert np.allclose(t["pressure"], P, rtol=1e-12, atol=0)
 
 
