@@ -1145,7 +1145,7 @@ void Box::allocDevice()
     dKs = dalloc<KSpace>(1);
     dUk = dalloc<float>((size_t)std::max<size_t>(1, potentials.size()) * g.hstride);
     dPp = dalloc<ParticleParams>(1);
-    const int TXz = kspace_tile_width(g, (int)dfields.size(), (int)fgroups.size());
+    const int TXz = kspace_tile_width(g, (int)dfields.size(), (int)fgroups.size(), (int)potentials.size());
     if (TXz == 0) fail(TILD_ERR_UNSUPPORTED, "the grid's z size is too large for the fused k-space pass with this many fields");
     nblkZ = ((g.nxh + TXz - 1) / TXz) * g.ny;
     nblkP = (int)((N + 255) / 256);

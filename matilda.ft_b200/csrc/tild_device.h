@@ -166,7 +166,7 @@ cudaError_t launch_kspace_z(const Geom &g, const FftLine &lz, const KSpace &ks, 
                             int *nblocks_out, cudaStream_t st);
 // half-spectrum columns per block of the k-space z pass (4, or 2 so that its shared
 // memory fits), 0 if even 2 do not fit
-int kspace_tile_width(const Geom &g, int nd, int nfg);
+int kspace_tile_width(const Geom &g, int nd, int nfg, int npots);
 // FP32 table of every potential's û(k) shape (amplitude 1) over the half spectrum
 cudaError_t launch_uk_table(const Geom &g, const KSpace *ks_dev, float *tab, cudaStream_t st);
 // S(|k|) of one real field given as float2 pairs (field in .x): x/y forward passes into

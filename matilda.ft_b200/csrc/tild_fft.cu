@@ -424,6 +424,12 @@ __global__ void k_uk_table(Geom g, const KSpace *__restrict__ ksp, float *__rest
         tab[(long long)p * g.hstride + o] = kx < g.nxh ? (float)uk_shape(ks.pots[p], k2) : 0.f;
 }
 
+__device__ __forceinline__ size_t kspace_uk_offset_dev(int nz, int nsets, int tx)
+{
+    const size_t b = (size_t)(2 * nsets * nz * tx + nz) * sizeof(float2) + 8 * sizeof(double);
+    return (b + 15) & ~(size_t)15;
+}
+
 // Fused z pass: forward z FFT of every density field, k-space combine, gradient and
 // inverse z FFT of each gradient field; FP64 energies on request.
 template <int TX>
@@ -445,6 +451,18 @@ __global__ void __launch_bounds__(256) k_kspace_z(Geom g, FftLine lz, const KSpa
     for (int d = 0; d < nd; d++)
         tile_load_async(Rho + d * TX, nd * TX, H + d * g.hstride + (long long)y * g.hp + kx0, (long long)g.ny * g.hp,
                         nz, TX, g.nxh - kx0);
+    // the u(k) rows of the block's columns, for the combine: whole rows of TX floats (the
+    // table's row pitch hp covers every block's TX columns)
+    const size_t ukoff = kspace_uk_offset_dev(nz, nsets, TX);
+    float *ukt = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(sm) + ukoff);
+    if (forces)
+        for (int e = threadIdx.x; e < ks.npots * nz; e += blockDim.x) {
+            const int pt = e / nz, z = e - pt * nz;
+            const float *src = uk + pt * g.hstride + ((long long)z * g.ny + y) * g.hp + kx0;
+            const unsigned s = (unsigned)__cvta_generic_to_shared(ukt + e * TX);
+            if (TX == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(src) : "memory");
+            else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(src) : "memory");
+        }
     cp_async_wait_all();
     __syncthreads();
     float2 *R = fft_lines<false>(Rho, S, nd * TX, 1, nd * TX, lz, tw, true, make_fastdiv_dev(nd * TX));
@@ -518,13 +536,12 @@ __global__ void __launch_bounds__(256) k_kspace_z(Geom g, FftLine lz, const KSpa
     for (int e = threadIdx.x; e < nz * TX; e += blockDim.x) {
         const int z = e / TX, c = e - z * TX, kx = kx0 + c;
         const float kz = (g.nz % 2 == 0 && z == g.nz / 2) ? 0.f : (float)(ks.twopi_over_L[2] * signed_index(z, g.nz));
-        const long long o = ((long long)z * g.ny + y) * g.hp + kx;
         for (int f = 0; f < ks.nfg; f++) {
             float px = 0.f, py = 0.f;
             if (kx < g.nxh) {
                 for (int t = 0; t < nterms; t++) {
                     if (tfg[t] != f) continue;
-                    const float u = tcoef[t] * __ldg(uk + tpot[t] * g.hstride + o);
+                    const float u = tcoef[t] * ukt[(tpot[t] * nz + z) * TX + c];
                     const float2 r = R[z * nd * TX + tdf[t] * TX + c];
                     px = fmaf(u, r.x, px);
                     py = fmaf(u, r.y, py);
@@ -722,17 +739,25 @@ cudaError_t launch_ypass(const Geom &g, const FftLine &ly, int nfields, int inve
     return cudaGetLastError();
 }
 
-static size_t kspace_smem(const Geom &g, int nd, int nfg, int tx)
+// two line-set buffers and the twiddles (float2), the reduction slots, then the staged
+// u(k) rows of every potential (float, 16-byte aligned)
+static size_t kspace_uk_offset(const Geom &g, int nsets, int tx)
+{
+    const size_t b = (size_t)(2 * nsets * g.nz * tx + g.nz) * sizeof(float2) + 8 * sizeof(double);
+    return (b + 15) & ~(size_t)15;
+}
+
+static size_t kspace_smem(const Geom &g, int nd, int nfg, int npots, int tx)
 {
     const int ndb = nd < 2 ? 2 : nd;
     const int nsets = ndb > 2 * nfg ? ndb : 2 * nfg;   // as in the kernel
-    return (size_t)(2 * nsets * g.nz * tx + g.nz) * sizeof(float2) + 8 * sizeof(double);
+    return kspace_uk_offset(g, nsets, tx) + (size_t)npots * g.nz * tx * sizeof(float);
 }
 
-int kspace_tile_width(const Geom &g, int nd, int nfg)
+int kspace_tile_width(const Geom &g, int nd, int nfg, int npots)
 {
     for (int tx : {4, 2})   // 4 columns: four blocks per SM at C2 sizes, better than 8 at two
-        if (kspace_smem(g, nd, nfg, tx) <= kKspaceSmemMax) return tx;
+        if (kspace_smem(g, nd, nfg, npots, tx) <= kKspaceSmemMax) return tx;
     return 0;
 }
 
@@ -740,10 +765,10 @@ cudaError_t launch_kspace_z(const Geom &g, const FftLine &lz, const KSpace &ks, 
                             const float2 *H, const float *uk, float2 *Hg, double *epart, int energy, int forces,
                             int *nblocks_out, cudaStream_t st)
 {
-    const int tx = kspace_tile_width(g, ks.nd, ks.nfg);
+    const int tx = kspace_tile_width(g, ks.nd, ks.nfg, ks.npots);
     if (tx == 0) return cudaErrorInvalidConfiguration;
     dim3 grid((g.nxh + tx - 1) / tx, g.ny);
-    const size_t sm = kspace_smem(g, ks.nd, ks.nfg, tx);
+    const size_t sm = kspace_smem(g, ks.nd, ks.nfg, ks.npots, tx);
     if (tx == 8) k_kspace_z<8><<<grid, 256, sm, st>>>(g, lz, ks_dev, H, uk, Hg, epart, energy, forces);
     else if (tx == 4) k_kspace_z<4><<<grid, 256, sm, st>>>(g, lz, ks_dev, H, uk, Hg, epart, energy, forces);
     else k_kspace_z<2><<<grid, 256, sm, st>>>(g, lz, ks_dev, H, uk, Hg, epart, energy, forces);
