@@ -15,12 +15,13 @@ namespace tild {
 // earlier radices: butterfly i reads i + q*n/R, twiddles by W_{pR}^{q*(i mod p)}, writes
 // (i - i mod p)*R + i mod p + q*p.  Returns the buffer holding the result.
 // =====================================================================================
+// complex arithmetic on paired FP32 instructions (FMUL2/FFMA2/FADD2 of sm_100)
 __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 {
-    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+    return __ffma2_rn(make_float2(a.y, a.y), make_float2(-b.y, b.x), __fmul2_rn(make_float2(a.x, a.x), b));
 }
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
 
 template <bool INV>
 __device__ __forceinline__ float2 twid(const float2 *tw, int t)
