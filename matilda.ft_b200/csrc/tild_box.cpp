@@ -404,8 +404,31 @@ void Box::addPotential(std::vector<std::string> &w, size_t &i)
         p.grpI = p.grpJ = "charges";
         p.LB = fnum(w, i, "Bjerrum length");
         p.sigma = fnum(w, i, "sigma");
+    } else if (p.word == "wall") {                // ps_potentialWall.cu:11-46
+        p.kind = POT_WALL;
+        p.grpI = p.grpJ = need(w, i, "wall group");
+        const std::string axis = need(w, i, "wall axis");
+        if (axis == "x" || axis == "X") p.wallAxis = 0;
+        else if (axis == "y" || axis == "Y") p.wallAxis = 1;
+        else if (axis == "z" || axis == "Z") p.wallAxis = 2;
+        else fail(TILD_ERR_PARSE, "ps_potentialWall.cu: axis must be x, y, or z (got '" + axis + "')");
+        if (p.wallAxis >= Dim)
+            fail(TILD_ERR_PARSE, "ps_potentialWall.cu: requested wall normal '" + axis + "' but box is only " +
+                                     std::to_string(Dim) + "-dimensional");
+        p.wallPos = fnum(w, i, "wall position");
+        p.wallSign = (int)inum(w, i, "wall side");
+        if (p.wallSign != 1 && p.wallSign != -1)
+            fail(TILD_ERR_PARSE, "ps_potentialWall.cu: dirSign must be +1 or -1 (got " + std::to_string(p.wallSign) + ")");
+        p.wallK = fnum(w, i, "wall k");
+        if (i < w.size()) {   // ramp_check_input(iss, -1)
+            if (w[i] == "ramp") fail(TILD_ERR_PARSE, "ramping applied on an unsupported potential!");
+            fail(TILD_ERR_PARSE, "Invalid keyword: " + w[i]);
+        }
+        int nw = 0;
+        for (auto &q : potentials) nw += q.kind == POT_WALL;
+        if (nw >= kMaxWalls) fail(TILD_ERR_UNSUPPORTED, "more than " + std::to_string(kMaxWalls) + " walls");
     } else if (p.word == "bias" || p.word == "bias_lc" || p.word == "Langevin" || p.word == "langevin" ||
-               p.word == "dpd" || p.word == "maiersaupe" || p.word == "wall") {
+               p.word == "dpd" || p.word == "maiersaupe") {
         fail(TILD_ERR_UNSUPPORTED, "potential " + p.word + " is outside the TILD step");
     } else {
         fail(TILD_ERR_PARSE, "ps_potential.cu: " + p.word + " is not a supported potential");
@@ -993,6 +1016,7 @@ void Box::buildPlan()
     std::vector<T> raw;
     for (size_t pi = 0; pi < potentials.size(); pi++) {
         const PS_Potential &p = potentials[pi];
+        if (p.kind == POT_WALL) continue;   // a per-particle force, in the particle pass
         if (p.kind == POT_CHARGES) {
             raw.push_back({p.Iind, (int)pi, dfield(p.Iind, 1), 1.0});
         } else {
@@ -1038,7 +1062,10 @@ void Box::buildPlan()
         d.lB = p.LB;
         ETerm &e = ks.eterms[pi];
         e.pot = (int)pi;
-        if (p.kind == POT_CHARGES) {
+        if (p.kind == POT_WALL) {   // no k-space energy: the particle reduction gives it
+            e.dI = e.dJ = 0;
+            e.fac = 0.0;
+        } else if (p.kind == POT_CHARGES) {
             e.dI = e.dJ = dfield(p.Iind, 1);
             e.fac = 0.5 * norm;
         } else {
@@ -1103,6 +1130,15 @@ void Box::buildPlan()
     pp.seed = (unsigned long long)RANDSEED;
     pp.rng_compat = rngCompat;
     pp.dim = Dim;
+    pp.nwall = 0;
+    for (const PS_Potential &p : potentials)
+        if (p.kind == POT_WALL) {
+            const int wi = pp.nwall++;
+            pp.wall_axis[wi] = p.wallAxis;
+            pp.wall_sign[wi] = p.wallSign;
+            pp.wall_pos[wi] = p.wallPos;
+            pp.wall_k[wi] = p.wallK;
+        }
 }
 
 void Box::allocDevice()
@@ -1150,7 +1186,7 @@ void Box::allocDevice()
     nblkZ = ((g.nxh + TXz - 1) / TXz) * g.ny;
     nblkP = (int)((N + 255) / 256);
     dEpart = dalloc<double>((size_t)nblkZ * (ksHost.neterms + 6));
-    dBpart = dalloc<double>((size_t)nblkP * 14);
+    dBpart = dalloc<double>((size_t)nblkP * kPartialCols);
     dRes = dalloc<double>(kResSize);
     dTmp = dalloc<float>(3 * N);
     if (sharedDevice) hKsPinned = new KSpace;   // pinned host memory would synchronise the device when freed
@@ -1258,6 +1294,12 @@ void Box::uploadFlags()
     for (size_t k = 0; k < fgroups.size(); k++)
         for (int64_t p = 0; p < N; p++)
             if (member[fgroups[k]][p]) fl[p] |= 1u << (8 + k);
+    int wi = 0;
+    for (const PS_Potential &p : potentials)
+        if (p.kind == POT_WALL) {
+            for (int s : psGroup[p.Iind].siteList) fl[s] |= 1u << (24 + wi);
+            wi++;
+        }
     std::vector<int> slot(N, kNoIntegrator);
     for (size_t s = 0; s < integrators.size(); s++)
         for (int p : psGroup[integrators[s].group_index].siteList) {
@@ -1371,8 +1413,8 @@ void Box::enqueueStep(bool energy, bool integrate, float *fout_dev)
     if (integrate) ck(launch_tick(dStep, st), "tick");
     if (energy) {
         ck(launch_bond_energy(g, ppHost, dPp, dX[0], dX[1], dStep, dNb, dPartner, dBtype, AngleArrays{dNa, dAtype, dAng},
-                              dBpart, nullptr, st), "bond energy");
-        ck(launch_reduce_partials(dBpart, nblkP, 14, dRes + kResBond, st), "reduce bonds");
+                              dFlags, dBpart, nullptr, st), "bond energy");
+        ck(launch_reduce_partials(dBpart, nblkP, kPartialCols, dRes + kResBond, st), "reduce bonds");
     }
 }
 
@@ -1394,8 +1436,8 @@ void Box::enqueueEnergyOnly()
         ck(launch_reduce_partials(dEpart, nblkZ, ksHost.neterms + 6, dRes, st), "reduce");
     }
     ck(launch_bond_energy(g, ppHost, dPp, dX[0], dX[1], dStep, dNb, dPartner, dBtype, AngleArrays{dNa, dAtype, dAng},
-                              dBpart, nullptr, st), "bond energy");
-    ck(launch_reduce_partials(dBpart, nblkP, 14, dRes + kResBond, st), "reduce bonds");
+                              dFlags, dBpart, nullptr, st), "bond energy");
+    ck(launch_reduce_partials(dBpart, nblkP, kPartialCols, dRes + kResBond, st), "reduce bonds");
 }
 
 std::vector<double> Box::readEnergies(bool)
@@ -1403,6 +1445,9 @@ std::vector<double> Box::readEnergies(bool)
     std::vector<double> r(kResSize, 0.0);
     ck(cudaStreamSynchronize(stream), "sync");
     ck(cudaMemcpy(r.data(), dRes, sizeof(double) * r.size(), cudaMemcpyDeviceToHost), "read energies");
+    int wi = 0;   // Wall::CalcEnergy (ps_potentialWall.cu:58-70) in the wall's potential slot
+    for (size_t k = 0; k < potentials.size(); k++)
+        if (potentials[k].kind == POT_WALL) r[k] = r[kResWall + wi++];
     return r;
 }
 
@@ -1833,9 +1878,9 @@ std::vector<double> Box::thermo()
     std::vector<double> out;
     const size_t np = potentials.size();
     const double uangle = r[kResAngle] / 3.0;   // PS_Box.cu:296-305
-    double ubond = 0.5 * r[kResBond], upe = ubond + uangle, upair = 0.0;
-    for (size_t k = 0; k < np; k++) upair += r[k];
-    upe += upair;
+    double ubond = 0.5 * r[kResBond], upe = ubond + uangle, upair = 0.0, uwall = 0.0;
+    for (size_t k = 0; k < np; k++) (potentials[k].kind == POT_WALL ? uwall : upair) += r[k];
+    upe += upair + uwall;
     out.push_back(upe);
     out.push_back(ubond);
     for (size_t k = 0; k < np; k++) out.push_back(r[k]);

@@ -44,6 +44,8 @@ struct PS_Potential {        // ps_potential.h:13-53 and the Gaussian/Erf2/ErfG/
     int Iind = -1, Jind = -1;
     float Ao = 0.f, sigma = 0.f, Rp = 0.f, LB = 0.f;
     bool ramp = false;
+    int wallAxis = 0, wallSign = 1;   // `wall` (ps_potentialWall.cu:11-46): normal axis, side
+    float wallPos = 0.f, wallK = 0.f;
     double Ao_initial = 0.0, Ao_final = 0.0;
     double amp_eff = 0.0;    // amplitude the k-space tables currently carry
     double energy = 0.0;     // last CalcEnergy value

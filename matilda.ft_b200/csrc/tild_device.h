@@ -26,7 +26,10 @@ constexpr int kMaxTerms = 32;
 // and bond virial at kResBond
 constexpr int kResBond = kMaxPots + 6;
 constexpr int kResAngle = kResBond + 7;   // angle energy and virial (each angle on 3 particles)
-constexpr int kResSize = kResAngle + 8;
+constexpr int kMaxWalls = 4;              // `potential wall` terms (per-particle, flag bits 24..27)
+constexpr int kResWall = kResAngle + 7;   // energy of each wall
+constexpr int kResSize = kResWall + kMaxWalls;
+constexpr int kPartialCols = 14 + kMaxWalls;   // per-block columns of the bond/angle/wall reduction
 constexpr int kMaxTypes = 16;
 constexpr int kMaxBondTypes = 16;
 constexpr int kMaxAngleTypes = 16;
@@ -34,7 +37,7 @@ constexpr int kMaxStages = 20;
 constexpr int kNoIntegrator = 15;
 constexpr double kFixScale = 4294967296.0;  // deterministic deposit: 2^32 per unit weight
 
-enum PotKind { POT_GAUSSIAN = 0, POT_ERF2 = 1, POT_ERFG = 2, POT_CHARGES = 3 };
+enum PotKind { POT_GAUSSIAN = 0, POT_ERF2 = 1, POT_ERFG = 2, POT_CHARGES = 3, POT_WALL = 4 };
 
 // Division by a runtime constant d through a multiply: exact for i * d < 2^32.
 struct FastDiv {
@@ -126,6 +129,11 @@ struct ParticleParams {
     unsigned long long seed;
     int rng_compat;
     int dim;                        // 2: z is one plane at z = 0 (no z noise), 3: full 3-D
+    // harmonic walls (ps_potentialWall.cu): on particles with flag bit 24 + w, a force
+    // k (pos - x_axis) along the axis while sign (pos - x_axis) > 0
+    int nwall;
+    int wall_axis[kMaxWalls], wall_sign[kMaxWalls];
+    float wall_pos[kMaxWalls], wall_k[kMaxWalls];
 };
 
 // Work split of the particle kernels over a sorted particle order: a CTA of `threads`
@@ -219,11 +227,12 @@ cudaError_t launch_permute_rows(int N, int width, const int *orig, const float *
 cudaError_t launch_rng_init(void *states, const int *orig_id, int n, unsigned long long seed,
                             cudaStream_t st);
 size_t rng_state_bytes();
-// per block: bond energy + virial (7 columns), then angle energy + virial (7 columns)
+// per block (kPartialCols columns): bond energy + virial (7), angle energy + virial (7),
+// then the energy of each wall (kMaxWalls)
 cudaError_t launch_bond_energy(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd,
                                const float *X0, const float *X1, const long long *d_step,
                                const uint8_t *nb, const int *partner, const uint8_t *btype, AngleArrays aa,
-                               double *partials, int *nblocks_out, cudaStream_t st);
+                               const uint32_t *pflags, double *partials, int *nblocks_out, cudaStream_t st);
 cudaError_t launch_reduce_partials(const double *partials, int nblocks, int ncols, double *out,
                                    cudaStream_t st);
 cudaError_t launch_grid_weights(const Geom &g, int order, int quirk4, const float *X, int N,

@@ -362,6 +362,7 @@ __global__ void __launch_bounds__(256) k_ypass(Geom g, FftLine ly, float2 *__res
 __device__ double uk_shape(const PotDev &p, double k2)
 {
     const double PI4 = 12.566370614359172953850573533118;
+    if (p.kind == POT_WALL) return 0.0;   // a per-particle term, nothing in k-space
     if (p.kind == POT_GAUSSIAN) return exp(-0.5 * k2 * p.sig2);
     if (p.kind == POT_CHARGES) return k2 > 0.0 ? PI4 * p.lB * exp(-k2 * p.sig2) / k2 : 0.0;
     const double R = p.Rp;
@@ -388,7 +389,7 @@ __device__ __forceinline__ double uk_eval(const PotDev &p, double k2) { return u
 // t'/k = 4 pi (R^2 sin(Rk)/k^3 - 3 (sin Rk - Rk cos Rk)/k^5).
 __device__ double uk_dk_over_k(const PotDev &p, double k2)
 {
-    if (k2 <= 0.0) return 0.0;
+    if (k2 <= 0.0 || p.kind == POT_WALL) return 0.0;
     if (p.kind == POT_GAUSSIAN) return -p.sig2 * uk_eval(p, k2);
     if (p.kind == POT_CHARGES) return uk_eval(p, k2) * (-2.0 * p.sig2 - 2.0 / k2);
     const double PI4 = 12.566370614359172953850573533118;

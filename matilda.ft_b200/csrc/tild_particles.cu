@@ -217,6 +217,21 @@ __device__ __forceinline__ void integrate(const Geom &g, const ParticleParams &p
     }
 }
 
+// Harmonic walls (d_wallHarmonicForce, ps_potentialWall.cu:92-108): k (pos - x_n) along
+// the wall's axis on the forbidden side sign (pos - x_n) > 0; e: the energy k disp^2 / 2.
+__device__ __forceinline__ void wall_terms(const ParticleParams &pp, uint32_t fl, const float *x, float *f, float *e)
+{
+    for (int w = 0; w < pp.nwall; w++) {
+        if (!((fl >> (24 + w)) & 1u)) continue;
+        const int a = pp.wall_axis[w];
+        const float disp = pp.wall_pos[w] - x[a];
+        if ((float)pp.wall_sign[w] * disp > 0.0f) {
+            if (f) f[a] += pp.wall_k[w] * disp;
+            if (e) e[w] = 0.5f * pp.wall_k[w] * disp * disp;
+        }
+    }
+}
+
 __device__ __forceinline__ void cp_async4(void *smem_dst, const void *gsrc)
 {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
@@ -408,6 +423,7 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
         if (act) {
             bond_force(g, pp, p, x, Xc, nb, partner, btype, f);
             if (aa.na) angle_force(g, pp, p, Xc, aa, f);
+            if (pp.nwall) wall_terms(pp, fl, x, f, nullptr);   // potentials' own forces, before the gathers
         }
         const int base = d[2] * E01 + d[1] * E0 + d[0];
         const float qp = (act && q) ? q[p] : 0.f;
@@ -518,9 +534,10 @@ __global__ void __launch_bounds__(256) k_bond_energy(Geom g, const ParticleParam
                                                      const uint8_t *__restrict__ nb,
                                                      const int *__restrict__ partner,
                                                      const uint8_t *__restrict__ btype, AngleArrays aa,
+                                                     const uint32_t *__restrict__ pflags,
                                                      double *__restrict__ partials)
 {
-    constexpr int NC = 14;
+    constexpr int NC = kPartialCols;
     __shared__ double red[8][NC];
     const ParticleParams &pp = *ppd;
     const float *__restrict__ X = (*d_step & 1) ? X1 : X0;
@@ -580,6 +597,13 @@ __global__ void __launch_bounds__(256) k_bond_energy(Geom g, const ParticleParam
         }
         acc[7] = e;
         for (int c = 0; c < 6; c++) acc[8 + c] = vir[c];
+    }
+    if (p < N && pp.nwall) {   // d_wallHarmonicEnergy (ps_potentialWall.cu:114-131)
+        const float xp[3] = {X[3 * p], X[3 * p + 1], X[3 * p + 2]};
+        float ew[kMaxWalls] = {0.f, 0.f, 0.f, 0.f};
+        wall_terms(pp, pflags[p], xp, nullptr, ew);
+#pragma unroll
+        for (int w = 0; w < kMaxWalls; w++) acc[14 + w] = ew[w];
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int c = 0; c < NC; c++) {
@@ -676,11 +700,11 @@ cudaError_t launch_rng_init(void *states, const int *orig_id, int n, unsigned lo
 
 cudaError_t launch_bond_energy(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd, const float *X0,
                                const float *X1, const long long *d_step, const uint8_t *nb, const int *partner,
-                               const uint8_t *btype, AngleArrays aa, double *partials, int *nblocks_out,
-                               cudaStream_t st)
+                               const uint8_t *btype, AngleArrays aa, const uint32_t *pflags, double *partials,
+                               int *nblocks_out, cudaStream_t st)
 {
     const int nbk = pp.N > 0 ? (pp.N + 255) / 256 : 1;
-    k_bond_energy<<<nbk, 256, 0, st>>>(g, ppd, pp.N, X0, X1, d_step, nb, partner, btype, aa, partials);
+    k_bond_energy<<<nbk, 256, 0, st>>>(g, ppd, pp.N, X0, X1, d_step, nb, partner, btype, aa, pflags, partials);
     if (nblocks_out) *nblocks_out = nbk;
     return cudaGetLastError();
 }

@@ -356,13 +356,9 @@ def box_from_spec(spec, device=0, options=None, steps_script=False, base_dir=Non
         b.command(line)
     if len(spec.angles):
         b.set_angles(spec.angles, spec.angle_types)
+    from . import synth
     for p in spec.potentials:
-        if p["kind"] == "gaussian":
-            b.command("potential gaussian %s %s %.9g %.9g" % (p["I"], p["J"], p["A"], p["sigma"]))
-        elif p["kind"] in ("erf2", "erfG"):
-            b.command("potential %s %s %s %.9g %.9g %.9g" % (p["kind"], p["I"], p["J"], p["A"], p["Rp"], p["sigma"]))
-        else:
-            b.command("potential charges %.9g %.9g" % (p["lB"], p["sigma"]))
+        b.command(synth.potential_command(p))
     b.command("integrator all %s delt %.9g" % (spec.integrator, spec.delt))
     b.command("logFreq %d" % spec.log_freq)
     return b

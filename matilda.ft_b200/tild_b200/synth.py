@@ -32,6 +32,20 @@ def chain_bonds(nchains, nper, offset=0):
     return np.stack([i, i + 1], axis=1)
 
 
+def potential_command(p):
+    """Script line of one potential spec (dict with kind and its parameters)."""
+    k = p["kind"]
+    if k == "gaussian":
+        return "potential gaussian %s %s %.9g %.9g" % (p["I"], p["J"], p["A"], p["sigma"])
+    if k in ("erf2", "erfG"):
+        return "potential %s %s %s %.9g %.9g %.9g" % (k, p["I"], p["J"], p["A"], p["Rp"], p["sigma"])
+    if k == "charges":
+        return "potential charges %.9g %.9g" % (p["lB"], p["sigma"])
+    if k == "wall":   # potential wall <group> <axis> <position> <side +1|-1> <k>
+        return "potential wall %s %s %.9g %d %.9g" % (p["I"], p["axis"], p["pos"], p["sign"], p["k"])
+    raise ValueError("unknown potential kind " + k)
+
+
 class SystemSpec:
     """Arrays + script parameters of one synthetic box."""
 
@@ -144,14 +158,7 @@ class SystemSpec:
         if len(self.bonds):
             s.append("bond 1 harmonic %.9g %.9g" % (self.bond_k, self.bond_req))
         s += self.angle_commands()
-        for p in self.potentials:
-            k = p["kind"]
-            if k == "gaussian":
-                s.append("potential gaussian %s %s %.9g %.9g" % (p["I"], p["J"], p["A"], p["sigma"]))
-            elif k in ("erf2", "erfG"):
-                s.append("potential %s %s %s %.9g %.9g %.9g" % (k, p["I"], p["J"], p["A"], p["Rp"], p["sigma"]))
-            elif k == "charges":
-                s.append("potential charges %.9g %.9g" % (p["lB"], p["sigma"]))
+        s += [potential_command(p) for p in self.potentials]
         s.append("integrator all %s delt %.9g" % (self.integrator, self.delt))
         s.append("logFreq %d" % self.log_freq)
         s += list(extra)

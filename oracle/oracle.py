@@ -232,7 +232,7 @@ def pair_virial(sysm: System, dens):
     W = np.zeros(6)
     utot = 0.0
     pairs = ((0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2))
-    for pot in sysm.potentials:
+    for pot in kspace_potentials(sysm):
         if pot["kind"] == "charges":
             rI = rJ = dens["charges"][1]
             fac = 0.5
@@ -313,7 +313,7 @@ def spectral_grid_forces(sysm: System, dens, prec=64):
     ks = kvectors(sysm, 64)
     k2 = sum(k * k for k in ks)
     gf = {}
-    for pot in sysm.potentials:
+    for pot in kspace_potentials(sysm):
         u = uk(pot, k2)
         if pot["kind"] == "charges":
             I = J = find_group(glist, "charges")
@@ -386,6 +386,29 @@ def angle_energy(sysm: System, x=None):
     return float(e.sum()), vir.sum(0)
 
 
+AXES = {"x": 0, "X": 0, "y": 1, "Y": 1, "z": 2, "Z": 2}
+
+
+def wall_terms(sysm: System, pot, x=None, real=np.float64):
+    """Harmonic wall (ps_potentialWall.cu:92-131) on group I: per site, the force
+    k (pos - x_axis) along the axis and the energy k disp^2 / 2 where sign (pos - x_axis) > 0.
+    Returns (sites, axis, force per site, energy per site)."""
+    x = sysm.x if x is None else x
+    glist = groups(sysm)
+    sites = glist[find_group(glist, pot["I"])][1]
+    a = AXES[pot["axis"]]
+    xs = np.asarray(x, real).reshape(sysm.N, sysm.Dim)[sites, a]
+    disp = real(pot["pos"]) - xs
+    on = real(pot["sign"]) * disp > 0
+    k = real(pot["k"])
+    return sites, a, np.where(on, k * disp, 0), np.where(on, real(0.5) * k * disp * disp, 0)
+
+
+def kspace_potentials(sysm: System):
+    """The potentials that act through the grid (every kind but the per-particle wall)."""
+    return [p for p in sysm.potentials if p["kind"] != "wall"]
+
+
 def forces(sysm: System, x=None, prec=64, include_bonds=True, include_grid=True):
     """Total force on every particle: bonds, then each force group's gather in the
     reference's group order (PS_Box.cu:240-270).  Returns f[N, Dim] (float64 for
@@ -410,6 +433,11 @@ def forces(sysm: System, x=None, prec=64, include_bonds=True, include_grid=True)
         np.add.at(fa, a[:, 1], -(fi + fk))
         np.add.at(fa, a[:, 2], fk)
         f += fa.reshape(-1).astype(real)
+    for pot in sysm.potentials:   # walls add to the forces before the gathers (PS_Box.cu:262-264)
+        if include_grid and pot["kind"] == "wall":
+            sites, ax, fw, _ = wall_terms(sysm, pot, x, real)
+            fv = f.reshape(N, Dim)
+            fv[sites, ax] += fw
     inter = {}
     if include_grid:
         dens, inds, W = densities(sysm, x, prec)
@@ -420,7 +448,7 @@ def forces(sysm: System, x=None, prec=64, include_bonds=True, include_grid=True)
         q = None if sysm.charges is None else np.ascontiguousarray(sysm.charges, dtype=real)
         # force flags: groups named by a non-charge potential, plus 'charges'
         flagged = set()
-        for pot in sysm.potentials:
+        for pot in kspace_potentials(sysm):
             if pot["kind"] != "charges":
                 flagged.add(find_group(glist, pot["I"]))
                 flagged.add(find_group(glist, pot["J"]))
@@ -438,7 +466,7 @@ def forces(sysm: System, x=None, prec=64, include_bonds=True, include_grid=True)
     return f.reshape(N, Dim), inter
 
 
-def pair_energies(sysm: System, dens):
+def pair_energies(sysm: System, dens, x=None):
     """Per-potential energy: gvol * sum rho_I (u*rho_J) (ps_potential.cu:133-178, no
     1/2 for I==J); charges 0.5*gvol*sum rhoq (u*rhoq) (ps_potentialCharges.cu:274-322)."""
     glist = groups(sysm)
@@ -449,6 +477,9 @@ def pair_energies(sysm: System, dens):
     _, _, gvol = grid_geometry(sysm)
     out = []
     for pot in sysm.potentials:
+        if pot["kind"] == "wall":   # Wall::CalcEnergy (ps_potentialWall.cu:58-70) at the positions
+            out.append(float(np.sum(wall_terms(sysm, pot, x)[3])))
+            continue
         u = uk(pot, k2)
         if pot["kind"] == "charges":
             rI = rJ = dens["charges"][1]
@@ -522,6 +553,8 @@ class CpuStep:
         self.M = int(np.prod(sysm.Nx))
         ks = kvectors(sysm, 32)
         k2 = sum(k.astype(np.float64) ** 2 for k in ks)
+        if any(p["kind"] == "wall" for p in sysm.potentials):
+            raise NotImplementedError("CpuStep times grid potentials only; Trajectory covers walls")
         self.fk = []
         for pot in sysm.potentials:   # host tables built once, FP32 complex (fk = -i k u)
             u = uk(pot, k2).astype(np.float32)

@@ -43,6 +43,11 @@ def systems():
         "c1": synth.config_c1(),
         "angles_o3": synth.small_system(seed=37, order=3, charges=True, angle_params=[
             dict(style="harmonic", k=3.0, theta=120.0), dict(style="wlc", k=2.0)]),
+        # harmonic walls (potential wall) beside grid potentials
+        "walls_o3": synth.small_system(seed=40, order=3, charges=True, pots=[
+            dict(kind="gaussian", I="A", J="B", A=2.0, sigma=0.7), dict(kind="charges", lB=1.0, sigma=0.5),
+            dict(kind="wall", I="A", axis="z", pos=2.0, sign=1, k=5.0),
+            dict(kind="wall", I="all", axis="x", pos=4.5, sign=-1, k=3.0)]),
         # 2-D boxes (Dim 2): the plane's stencils, k-vectors, noise draws and gvol
         "d2_o3": synth.small_system(seed=38, order=3, charges=True, dim=2, grid=(16, 18, 1)),
         "d2_o4": synth.small_system(seed=39, order=4, dim=2, grid=(15, 12, 1), angle_params=[

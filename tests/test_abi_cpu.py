@@ -89,6 +89,10 @@ def test_endbox_without_gpu_reports_cuda(tmp_path):
     (["Dim 3", "bond 1 quartic 1 1"], 2, "Bond type not supported"),
     (["Dim 3", "potential bias A 1"], 6, "outside the TILD step"),
     (["Dim 3", "potential morse A B 1"], 2, "not a supported potential"),
+    (["Dim 3", "potential wall A w 1.0 1 2.0"], 2, "axis must be x, y, or z"),
+    (["Dim 2", "potential wall A z 1.0 1 2.0"], 2, "box is only 2-dimensional"),
+    (["Dim 3", "potential wall A z 1.0 2 2.0"], 2, "dirSign must be +1 or -1"),
+    (["Dim 3", "potential wall A z 1.0 1 2.0 ramp 3.0"], 2, "ramping applied on an unsupported potential"),
     (["Dim 3", "potential gaussian A B 1.0 0.5 foo"], 2, "Invalid keyword: foo"),
     (["Dim 3", "potential gaussian A B 1.0 0.5 ramp"], 2, "no final prefactor"),
     (["Dim 3", "integrator all VV"], 6, "VV"),

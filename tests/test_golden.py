@@ -116,13 +116,9 @@ def _box(z, sysm, **opts):
             b.command("angle %d harmonic %.9g %.9g" % (t + 1, a["k"], a["theta"]) if a["style"] == "harmonic"
                       else "angle %d wlc %.9g" % (t + 1, a["k"]))
         b.set_angles(z["angles"], z["angle_types"])
+    from tild_b200 import synth
     for p in sysm.potentials:
-        if p["kind"] == "gaussian":
-            b.command("potential gaussian %s %s %.9g %.9g" % (p["I"], p["J"], p["A"], p["sigma"]))
-        elif p["kind"] in ("erf2", "erfG"):
-            b.command("potential %s %s %s %.9g %.9g %.9g" % (p["kind"], p["I"], p["J"], p["A"], p["Rp"], p["sigma"]))
-        else:
-            b.command("potential charges %.9g %.9g" % (p["lB"], p["sigma"]))
+        b.command(synth.potential_command(p))
     b.command("integrator all GJF delt %.9g" % float(z["delt"]))
     b.command("endBox")
     return b

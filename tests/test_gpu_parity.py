@@ -52,6 +52,11 @@ SYSTEMS = {
     "prime_grid": lambda: synth.small_system(seed=13, order=1, grid=(22, 13, 11), charges=True),
     "angles": lambda: synth.small_system(seed=15, order=3, charges=True, angle_params=ANGLES),
     "free_particles": lambda: synth.small_system(seed=9, order=3, n_free=50, charges=True),
+    # harmonic walls (per-particle potentials) beside grid potentials
+    "walls": lambda: synth.small_system(seed=22, order=3, charges=True, pots=[
+        dict(kind="gaussian", I="A", J="B", A=2.0, sigma=0.7), dict(kind="charges", lB=1.0, sigma=0.5),
+        dict(kind="wall", I="A", axis="z", pos=2.0, sign=1, k=5.0),
+        dict(kind="wall", I="all", axis="x", pos=4.5, sign=-1, k=3.0)]),
     # 2-D boxes: one grid plane, particles at z = 0
     "d2_charged": lambda: synth.small_system(seed=20, order=3, charges=True, dim=2, grid=(16, 18, 1)),
     "d2_o4_angles": lambda: synth.small_system(seed=21, order=4, dim=2, grid=(15, 12, 1), angle_params=ANGLES),
@@ -104,7 +109,7 @@ def test_densities_match_oracle():
                 assert np.abs(gq - rhoq).max() <= 1e-6 * np.abs(rhoq).max()
 
 
-@pytest.mark.parametrize("name", ["diblock_o3", "charged_o3", "erf", "odd_grid"])
+@pytest.mark.parametrize("name", ["diblock_o3", "charged_o3", "erf", "odd_grid", "walls"])
 def test_energies_match_oracle(name):
     spec = SYSTEMS[name]()
     sysm = spec_to_system(spec)
