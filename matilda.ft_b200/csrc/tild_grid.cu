@@ -254,25 +254,39 @@ __global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4
             }
             unsigned rem = __ballot_sync(full, dm != 0u);
             __syncwarp();
+            // four particles per round: their table reads in flight before the atomics
+            constexpr int U = 4;
             while (rem) {
-                const int j = __ffs(rem) - 1;
-                rem &= rem - 1;
-                const float *pj = wt + j * WREC;
-                const int offj = __float_as_int(pj[P1 + P1 * P1]);
-                float cf[NC];
+                int jj[U];
 #pragma unroll
-                for (int f = 0; f < NC; f++) cf[f] = pj[P1 + P1 * P1 + 1 + f];
-#pragma unroll
-                for (int k = 0; k < NPASS; k++) {
-                    if (lane + 32 * k >= G) break;
-                    // Wx * (Wy * Wz): the association of the unstaged path, so that the
-                    // deterministic mode's fixed-point values do not depend on staging
-                    const float w = pj[sa[k]] * pj[P1 + syz[k]];
-                    const int idx = offj + loff[k];
-#pragma unroll
-                    for (int f = 0; f < NC; f++)
-                        if (cf[f] != 0.f) smem_add<FIXED>(tf, tu, f * V + idx, cf[f] * w);
+                for (int u = 0; u < U; u++) {
+                    jj[u] = rem ? __ffs(rem) - 1 : -1;
+                    if (rem) rem &= rem - 1;
                 }
+                int offs[U];
+                float cfs[U][NC], ws[U][NPASS];
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const float *pj = wt + (jj[u] < 0 ? jj[0] : jj[u]) * WREC;
+                    offs[u] = __float_as_int(pj[P1 + P1 * P1]);
+#pragma unroll
+                    for (int f = 0; f < NC; f++) cfs[u][f] = jj[u] < 0 ? 0.f : pj[P1 + P1 * P1 + 1 + f];
+#pragma unroll
+                    for (int k = 0; k < NPASS; k++)
+                        // Wx * (Wy * Wz): the association of the unstaged path, so that the
+                        // deterministic mode's fixed-point values do not depend on staging
+                        ws[u][k] = (lane + 32 * k < G) ? pj[sa[k]] * pj[P1 + syz[k]] : 0.f;
+                }
+#pragma unroll
+                for (int u = 0; u < U; u++)
+#pragma unroll
+                    for (int k = 0; k < NPASS; k++) {
+                        if (lane + 32 * k >= G) break;
+                        const int idx = offs[u] + loff[k];
+#pragma unroll
+                        for (int f = 0; f < NC; f++)
+                            if (cfs[u][f] != 0.f) smem_add<FIXED>(tf, tu, f * V + idx, cfs[u][f] * ws[u][k]);
+                    }
             }
             __syncwarp();
         }
