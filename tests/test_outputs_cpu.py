@@ -192,3 +192,24 @@ def test_reader_on_the_reference_trajectory(tmp_path):
     assert [int(g.frame(f)["configuration/step"][0]) & 0xFFFFFFFF for f in range(4)] == [0, 5, 10, 12]
     if os.path.exists(GSD_DUMP):
         compare_with_reference_reader(path)
+
+
+def test_2d_box_outputs_at_endbox(tmp_path):
+    """A 2-D box: density headers carry Dim 2 with two grid sizes and lengths, and the GSD
+    frame has the reference's 2-D box (Lz = 5.0) and particles on the plane z = 0 - L/2
+    only through x and y (z written as 0)."""
+    s = synth.small_system(seed=24, dim=2, grid=(16, 18, 1), charges=True)
+    b = tild_b200.box_from_spec(s, options={"write_files": 1}, base_dir=str(tmp_path))
+    end_box(b)
+    b.close()
+    raw = open(os.path.join(tmp_path, "density-all.bin"), "rb").read()
+    assert np.frombuffer(raw[:4], np.int32)[0] == 2
+    assert list(np.frombuffer(raw[4:12], np.int32)) == [16, 18]
+    assert np.array_equal(np.frombuffer(raw[12:20], np.float32), np.asarray(s.L[:2], np.float32))
+    assert (len(raw) - 20) % (4 * 16 * 18) == 0
+    fr = gsd_reader.GsdFile(os.path.join(tmp_path, "traj.gsd")).frame(0)
+    assert np.array_equal(fr["configuration/box"], np.array([s.L[0], s.L[1], 5.0, 0, 0, 0], np.float32))
+    x = np.asarray(s.x, np.float32)
+    Lh = np.float32(0.5) * np.asarray(s.L[:2], np.float32)
+    pos = fr["particles/position"]
+    assert np.array_equal(pos[:, :2], (x - Lh).astype(np.float32)) and not pos[:, 2].any()
