@@ -85,19 +85,23 @@ def read_bin(path):
 
 
 def lammpstrj_text(step, x, s):
-    """PS_Box::writeLammpsTraj (PS_Box.cu:750-795) applied to positions x (float32)."""
+    """PS_Box::writeLammpsTraj (PS_Box.cu:750-795) applied to positions x (float32, N x Dim):
+    one wrap per coordinate, "%f " per dimension, then "%f" of 0 for a missing z."""
+    D = s.dim
     L = np.asarray(s.L, np.float32)
     out = ["ITEM: TIMESTEP\n%d\nITEM: NUMBER OF ATOMS\n%d\n" % (step, s.N), "ITEM: BOX BOUNDS pp pp pp\n",
-           "%f %f\n%f %f\n%f %f\n" % (0.0, L[0], 0.0, L[1], 0.0, L[2]), "ITEM: ATOMS id type mol x y z\n"]
+           "%f %f\n%f %f\n%f %f\n" % (0.0, L[0], 0.0, L[1], 0.0, L[2] if D == 3 else 1.0),
+           "ITEM: ATOMS id type mol x y z\n"]
     for p in range(s.N):
         row = "%d %d %d  " % (p + 1, s.types[p] + 1, s.mol[p] + 1)
-        for j in range(3):
+        for j in range(D):
             v = np.float32(x[p, j])
             if v > L[j]:
                 v = np.float32(v - L[j])
             elif v < np.float32(0.0):
                 v = np.float32(v + L[j])
             row += "%f " % v
+        row += "%f" % 0.0 * (3 - D)
         out.append(row + "\n")
     return "".join(out)
 
@@ -132,6 +136,15 @@ def test_lammpstrj_frames_match_reference_format(tmp_path):
     expect = "".join(lammpstrj_text(i, xs[i + 1], s) for i in range(n) if i % 3 == 0)
     got = open(os.path.join(tmp_path, "run.lammpstrj")).read()
     assert got == expect
+
+
+def test_lammpstrj_frames_of_a_2d_box(tmp_path):
+    s = synth.small_system(seed=25, order=3, dim=2, grid=(16, 18, 1), charges=True)
+    n = 4
+    run_with_outputs(s, tmp_path, ["trajFreq 2"], n)
+    xs = positions_by_step(s, n)
+    expect = "".join(lammpstrj_text(i, xs[i + 1], s) for i in range(n) if i % 2 == 0)
+    assert open(os.path.join(tmp_path, "traj.lammpstrj")).read() == expect
 
 
 def test_gsd_frames(tmp_path):
