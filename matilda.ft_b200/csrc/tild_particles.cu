@@ -293,7 +293,9 @@ constexpr int kPartOut = 32;   // particles per pass gathered from global memory
 // has drifted out of the box is gathered from global memory, before the staging wait, by a
 // helper thread (thread o for the pass's o-th such particle); its owner adds the result in
 // group order like any other, so the sums do not depend on which path served them.
-template <int P>
+// EXTRA: the box has angles or walls (compiled out of the common instantiation, whose
+// schedule the unused terms would otherwise disturb)
+template <int P, bool EXTRA>
 __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticleParams *__restrict__ ppd, int N,
                                                       float *__restrict__ X0, float *__restrict__ X1,
                                                       float *__restrict__ noise, const uint32_t *__restrict__ pflags,
@@ -422,8 +424,10 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
         float f[3] = {0.f, 0.f, 0.f};
         if (act) {
             bond_force(g, pp, p, x, Xc, nb, partner, btype, f);
-            if (aa.na) angle_force(g, pp, p, Xc, aa, f);
-            if (pp.nwall) wall_terms(pp, fl, x, f, nullptr);   // potentials' own forces, before the gathers
+            if (EXTRA) {
+                if (aa.na) angle_force(g, pp, p, Xc, aa, f);
+                if (pp.nwall) wall_terms(pp, fl, x, f, nullptr);   // potentials' own forces, before the gathers
+            }
         }
         const int base = d[2] * E01 + d[1] * E0 + d[0];
         const float qp = (act && q) ? q[p] : 0.f;
@@ -644,23 +648,34 @@ template <int P>
 static void part_launch(const Geom &g, const ParticleParams *ppd, int N, float *X0, float *X1, float *noise,
                         const uint32_t *pflags, const float *q, const uint8_t *nb, const int *partner,
                         const uint8_t *btype, AngleArrays aa, const float4 *rec, const int *orig_id, void *rng,
-                        const long long *d_step, float *fout, int integrate, const TileCfg &tc, cudaStream_t st)
+                        const long long *d_step, float *fout, int integrate, const TileCfg &tc, bool walls,
+                        cudaStream_t st)
 {
     const int nbk = tc.start ? (tc.nkeys + tc.codes - 1) / tc.codes : (N + kPartWindow - 1) / kPartWindow;
     const int threads = tc.start ? tc.threads : 256;
     const int cap = tc.start ? std::min(tc.pbox, kPartBox) : 0;
     const size_t smem = (size_t)cap * sizeof(float4) + (size_t)threads * 7 * sizeof(float);
-    k_particles<P><<<nbk, threads, smem, st>>>(g, ppd, N, X0, X1, noise, pflags, q, nb, partner, btype, aa, rec, orig_id,
+    const bool extra = aa.na != nullptr || walls;
+    if (extra)
+        k_particles<P, true><<<nbk, threads, smem, st>>>(g, ppd, N, X0, X1, noise, pflags, q, nb, partner, btype, aa, rec, orig_id,
+                                                     reinterpret_cast<curandState *>(rng), d_step, fout, integrate, tc, cap);
+    else
+        k_particles<P, false><<<nbk, threads, smem, st>>>(g, ppd, N, X0, X1, noise, pflags, q, nb, partner, btype, aa, rec, orig_id,
                                                reinterpret_cast<curandState *>(rng), d_step, fout, integrate, tc, cap);
 }
 
 void init_particle_attributes()
 {
-    cudaFuncSetAttribute(k_particles<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
-    cudaFuncSetAttribute(k_particles<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
-    cudaFuncSetAttribute(k_particles<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
-    cudaFuncSetAttribute(k_particles<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
-    cudaFuncSetAttribute(k_particles<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
+    cudaFuncSetAttribute(k_particles<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
+    cudaFuncSetAttribute(k_particles<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
+    cudaFuncSetAttribute(k_particles<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
+    cudaFuncSetAttribute(k_particles<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
+    cudaFuncSetAttribute(k_particles<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
+    cudaFuncSetAttribute(k_particles<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
+    cudaFuncSetAttribute(k_particles<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
+    cudaFuncSetAttribute(k_particles<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
+    cudaFuncSetAttribute(k_particles<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
+    cudaFuncSetAttribute(k_particles<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
 }
 
 cudaError_t launch_particles(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd, float *X0,
@@ -671,7 +686,7 @@ cudaError_t launch_particles(const Geom &g, const ParticleParams &pp, const Part
 {
     if (pp.N == 0) return cudaSuccess;
 #define TILD_PL(P) part_launch<P>(g, ppd, pp.N, X0, X1, noise, pflags, q, nb, partner, btype, aa, rec, orig_id, \
-                                  rng_states, d_step, fout, integrate, tc, st)
+                                  rng_states, d_step, fout, integrate, tc, pp.nwall > 0, st)
     switch (pp.order) {
         case 0: TILD_PL(0); break;
         case 1: TILD_PL(1); break;
