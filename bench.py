@@ -337,10 +337,11 @@ def run_ours(args):
     torch.cuda.set_device(local)
     spec = make_spec(args.scale)
     stream = torch.cuda.Stream(device=local)
-    box = tild_b200.box_from_spec(spec, device=local, options={"write_files": 0})
+    box = tild_b200.box_from_spec(spec, device=local, options={"write_files": 0, "autotune": 1})
     box.set_stream(stream.cuda_stream)
     box.command("endBox")
     info = box.info()
+    tiles = box.describe()["tiles"]
     for _ in range(args.warmup):
         box.step(1)
     torch.cuda.synchronize()
@@ -428,6 +429,7 @@ def run_ours(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (numpy seed 2)",
             "config": {"workload": WORKLOAD, "particles": spec.N, "grid": [int(v) for v in spec.grid],
                        "parallelism": "replicas" if world > 1 else "single", "rng": "philox",
+                       "tiles": {"bricks_per_cta": tiles["codes"], "threads": tiles["threads"], "autotuned": True},
                        "l2": "inputs larger than L2 (%.2f GB moved per step by the kernels' compulsory traffic)"
                              % (step_bytes / 1e9)},
             "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved, "peak": peak,

@@ -116,6 +116,8 @@ int tild_box_set_angles(tild_box *box, int64_t nangles, const int64_t *triples, 
  *   "write_files"    0 = write no files: ps_data.dat, init/final data files, and the
  *                    run's lammpstrj, GSD and density-<group>.bin outputs (default 1)
  *   "sort_interval"  steps between spatial re-sorts of the particle arrays (0 = never)
+ *   "autotune"       1 = at endBox, time the force evaluation with tiles of half, the
+ *                    same and twice the bricks per CTA and keep the fastest (default 0)
  * Must precede endBox except "write_files". */
 int tild_box_set_option(tild_box *box, const char *key, int64_t value);
 

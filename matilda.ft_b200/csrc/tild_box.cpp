@@ -180,6 +180,7 @@ void Box::setOption(const std::string &key, int64_t v)
     if (key == "rng") rngCompat = (int)v;
     else if (key == "deterministic") deterministic = (int)v;
     else if (key == "bspline4_exact") exact4 = (int)v;
+    else if (key == "autotune") autotune = v != 0;
     else if (key == "sort_interval") {
         if (v < 0) fail(TILD_ERR_ARG, "sort_interval must be >= 0");
         sortInterval = (int)v;
@@ -981,6 +982,7 @@ void Box::initDevice()
         sortParticles();
         ck(cudaStreamSynchronize(stream), "initial sort");
     }
+    if (autotune) autotuneTiles();
     ready = true;
 }
 
@@ -1194,30 +1196,11 @@ void Box::allocDevice()
     // sort scratch and the permuted copies
     const uint32_t nk = sort_key_count(g);
     sortKeys = nk;
-    {   // tile geometry: about one particle per thread, box sized for the tile plus drift
+    {   // tile geometry: about one particle per thread (the density decides the bricks)
         const double perCode = 16.0 * std::min(4, g.nz) * (double)N / (double)g.M;   // particles per brick of 4^3 cells (4x4x1 in 2-D)
         int codes = 8;
         while (codes < 64 && perCode * codes * 2.0 <= 192.0) codes *= 2;
-        const double e = perCode * codes;
-        int thr = (int)std::ceil((e + 2.0 * std::sqrt(e) + 8.0) / 32.0) * 32;
-        thr = std::max(64, std::min(512, thr));
-        int bits = 0;
-        while ((1 << bits) < codes) bits++;
-        const int cx = 4 << ((bits + 2) / 3), cy = 4 << ((bits + 1) / 3), cz = 4 << (bits / 3);
-        const int slack = pmeorder + 1 + 3;   // stencil width + drift between sorts
-        long long box = (long long)(((cx + slack) | 1) * (cy + slack) | 1) * (cz + slack);
-        box = std::min<long long>(box, 3072);
-        // particle pass: the tile's bricks widened by the stencil and one cell of drift per
-        // side (particles that drift further are gathered from global memory)
-        const int margin = 1, ev = (pmeorder % 2 == 0) ? 1 : 0;
-        auto edge = [&](int cells, int n) { return std::min(cells, n) - 1 + ev + 2 * margin + pmeorder + 1; };
-        const int ex = edge(cx, g.nx), ey = edge(cy, g.ny), ez = edge(cz, g.nz);
-        tiles.nkeys = (int)nk;
-        tiles.codes = codes;
-        tiles.threads = thr;
-        tiles.box = (int)box;
-        tiles.pbox = (((ex | 1) * ey) | 1) * ez;
-        tiles.margin = margin;
+        tiles = tileGeometry(codes);
     }
     sortW.key = dalloc<uint32_t>(N);
     sortW.rank = dalloc<int>(N);
@@ -1923,6 +1906,71 @@ void Box::readRows3(const float *dev, float *out) const
         for (int j = 0; j < Dim; j++) out[p * Dim + j] = h[3 * p + j];
 }
 
+// Tile of `codes` consecutive brick codes: threads for about one particle each (mean plus
+// two standard deviations), the deposit's box estimate, and the particle pass's fixed box
+// (the tile's bricks widened by the stencil and one cell of drift per side; particles that
+// drift further are gathered from global memory).
+TileCfg Box::tileGeometry(int codes) const
+{
+    const Geom &g = geom;
+    const double perCode = 16.0 * std::min(4, g.nz) * (double)nstot / (double)g.M;
+    const double e = perCode * codes;
+    int thr = (int)std::ceil((e + 2.0 * std::sqrt(e) + 8.0) / 32.0) * 32;
+    thr = std::max(64, std::min(512, thr));
+    int bits = 0;
+    while ((1 << bits) < codes) bits++;
+    const int cx = 4 << ((bits + 2) / 3), cy = 4 << ((bits + 1) / 3), cz = 4 << (bits / 3);
+    const int slack = pmeorder + 1 + 3;   // stencil width + drift between sorts
+    long long box = (long long)(((cx + slack) | 1) * (cy + slack) | 1) * (cz + slack);
+    box = std::min<long long>(box, 3072);
+    const int margin = 1, ev = (pmeorder % 2 == 0) ? 1 : 0;
+    auto edge = [&](int cells, int n) { return std::min(cells, n) - 1 + ev + 2 * margin + pmeorder + 1; };
+    const int ex = edge(cx, g.nx), ey = edge(cy, g.ny), ez = edge(cz, g.nz);
+    TileCfg t{};
+    t.nkeys = (int)sortKeys;
+    t.codes = codes;
+    t.threads = thr;
+    t.box = (int)box;
+    t.pbox = (((ex | 1) * ey) | 1) * ez;
+    t.margin = margin;
+    return t;
+}
+
+// Tile autotuner (option "autotune"): times the force evaluation (deposit, transforms,
+// force pass without integration) with tiles of half, the same and twice the bricks of
+// the density rule and keeps the fastest.  Positions, the step counter, the noise and
+// the RNG state are not touched.
+void Box::autotuneTiles()
+{
+    if (!sortedTiles) return;
+    std::vector<TileCfg> cands;
+    for (int c : {tiles.codes / 2, tiles.codes, tiles.codes * 2})
+        if (c >= 1 && c <= 64) cands.push_back(tileGeometry(c));
+    cudaEvent_t e0, e1;
+    ck(cudaEventCreate(&e0), "event");
+    ck(cudaEventCreate(&e1), "event");
+    float best = 1e30f;
+    TileCfg pick = tiles;
+    for (const TileCfg &t : cands) {
+        tiles = t;
+        enqueueStep(false, false, dF);   // warm-up
+        ck(cudaEventRecord(e0, stream), "event");
+        for (int r = 0; r < 3; r++) enqueueStep(false, false, dF);
+        ck(cudaEventRecord(e1, stream), "event");
+        ck(cudaEventSynchronize(e1), "autotune");
+        float ms = 0.f;
+        ck(cudaEventElapsedTime(&ms, e0, e1), "event");
+        if (ms < best) {
+            best = ms;
+            pick = t;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    tiles = pick;
+    tunedMs = best / 3.f;
+}
+
 TileCfg Box::tileCfg() const
 {
     TileCfg t = tiles;
@@ -2199,7 +2247,9 @@ std::string Box::describe() const
       << L[2] << "], \"pmeorder\": " << pmeorder << ", \"randSeed\": " << RANDSEED << ", \"logFreq\": " << logFreq
       << ", \"doCharges\": " << (doCharges ? "true" : "false") << ", \"MAXBONDS\": " << MAXBONDS
       << ", \"nBonds\": " << nBondsTot << ", \"nAngles\": " << nAnglesTot << ", \"MAXANGLES\": " << MAXANGLES
-      << ", \"datFileName\": " << q(datFileName) << ", \"trajFreq\": " << trajFreq
+      << ", \"datFileName\": " << q(datFileName) << ", \"tiles\": {\"codes\": " << tiles.codes
+      << ", \"threads\": " << tiles.threads << ", \"autotuned\": " << (autotune ? "true" : "false")
+      << ", \"tuned_ms\": " << tunedMs << "}, \"trajFreq\": " << trajFreq
       << ", \"trajFileName\": " << q(trajFileName) << ", \"fieldFreq\": " << fieldFreq
       << ", \"logScaleFields\": " << (logSpaceFields ? logScaleFields : 0.f) << ", \"gsdFreq\": " << gsdFreq
       << ", \"logScaleGSD\": " << (logSpaceGSD ? logScaleGSD : 0.f) << ", \"gsdName\": " << q(gsdName)

@@ -262,6 +262,10 @@ private:
     uint32_t sortKeys = 0;
     TileCfg tiles{};                // codes / threads / box chosen from the density
     TileCfg tileCfg() const;
+    TileCfg tileGeometry(int codes) const;
+    bool autotune = false;          // option "autotune": time tile sizes at endBox
+    float tunedMs = 0.f;            // force evaluation time of the chosen tiles
+    void autotuneTiles();
     void uploadFlags();
     std::vector<int> slotOrder() const;
     void sortParticles();

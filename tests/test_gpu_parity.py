@@ -138,6 +138,20 @@ def test_deterministic_mode_bit_reproducible_and_accurate():
     assert force_error(outs[0], fref) <= F_TOL
 
 
+def test_autotuned_tiles_are_invisible():
+    """The tile autotuner only changes the work split: in deterministic mode the forces and
+    a short trajectory are bit-identical with and without it."""
+    spec = synth.small_system(seed=26, order=3, charges=True, n_chains=120, nper=10, L=10.0, grid=(20, 20, 20))
+    outs = []
+    for tune in (0, 1):
+        with make_box(spec, deterministic=1, autotune=tune) as b:
+            outs.append((b.forces(), b.describe()["tiles"]))
+            b.step(5)
+            outs[-1] += (b.positions(),)
+    assert outs[1][1]["autotuned"] and outs[1][1]["tuned_ms"] > 0
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][2], outs[1][2])
+
+
 def test_spatial_sort_is_invisible():
     """Re-sorting the particle arrays changes only memory order: in deterministic mode the
     trajectory is bit-identical with no sort, a sort every 3 steps and every step."""
