@@ -163,6 +163,23 @@ def dist_setup(args):
     return world, rank, local, pg
 
 
+def max_over_ranks(dist, x, device):
+    """The largest x over all ranks, returned on every rank (x itself without a process
+    group): whole-job times are the slowest rank's."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, units_per_rank, ms):
+    """Units processed by all ranks per second, every rank doing units_per_rank in the
+    slowest rank's ms (replicas: the work per GPU is fixed as the GPU count grows)."""
+    return world * units_per_rank / (ms * 1e-3)
+
+
 def run_reference(args):
     world, rank, local, _ = (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
                              int(os.environ.get("LOCAL_RANK", "0")), None)
@@ -355,13 +372,10 @@ def run_ours(args):
         box.step(args.steps)
         e1.record(stream)
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(dist, e0.elapsed_time(e1), "cuda")
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
-    value = world * spec.N * args.steps / (ms * 1e-3)
+    value = whole_job_rate(world, spec.N * args.steps, ms)
 
     # end to end through the C ABI: pinned host positions -> S steps -> host positions
     S = args.e2e_steps
@@ -381,12 +395,8 @@ def run_ours(args):
     tild_b200._check(L.tild_box_get_positions(box._h, ctypes.c_void_p(hout.data_ptr())))
     f1.record(stream)
     torch.cuda.synchronize()
-    ems = f0.elapsed_time(f1)
-    if dist:
-        t = torch.tensor([ems], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ems = float(t.item())
-    e2e = world * spec.N * S / (ems * 1e-3)
+    ems = max_over_ranks(dist, f0.elapsed_time(f1), "cuda")
+    e2e = whole_job_rate(world, spec.N * S, ems)
 
     # per-kernel durations: instrumented launches (an event after every kernel)
     box.set_option("stage_timing", 1)
