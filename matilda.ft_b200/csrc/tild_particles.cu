@@ -254,8 +254,8 @@ template <int P>
 __device__ __forceinline__ void gather_global(const Geom &g, const float4 *__restrict__ rf, const int *gs,
                                               const float *Wx, const float *Wy, const float *Wz, float *acc)
 {
-    // stencil origins lie in [-P, n]: one conditional add or subtract wraps an index
-    auto wrap = [](int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); };
+    // a true modulo past one box length: a position outside [0, L) still reads the grid
+    auto wrap = [](int v, int n) { return wrapi(v, n); };
     float a0 = 0.f, a1 = 0.f, a2 = 0.f;
 #pragma unroll 1
     for (int e = 0; e <= P; e++) {
