@@ -439,7 +439,8 @@ def run_ours(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (numpy seed 2)",
             "config": {"workload": WORKLOAD, "particles": spec.N, "grid": [int(v) for v in spec.grid],
                        "parallelism": "replicas" if world > 1 else "single", "rng": "philox",
-                       "tiles": {"bricks_per_cta": tiles["codes"], "threads": tiles["threads"], "autotuned": True},
+                       "tiles": {"bricks_per_cta": tiles["codes"], "threads": tiles["threads"],
+                                 "gather": tiles["gather"], "autotuned": True},
                        "l2": "inputs larger than L2 (%.2f GB moved per step by the kernels' compulsory traffic)"
                              % (step_bytes / 1e9)},
             "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved, "peak": peak,

@@ -117,7 +117,10 @@ int tild_box_set_angles(tild_box *box, int64_t nangles, const int64_t *triples, 
  *                    run's lammpstrj, GSD and density-<group>.bin outputs (default 1)
  *   "sort_interval"  steps between spatial re-sorts of the particle arrays (0 = never)
  *   "autotune"       1 = at endBox, time the force evaluation with tiles of half, the
- *                    same and twice the bricks per CTA and keep the fastest (default 0)
+ *                    same and twice the bricks per CTA, each with a staged and a direct
+ *                    particle gather, and keep the fastest (default 0)
+ *   "direct_gather"  1 = the particle pass reads each stencil through L1/L2 instead of
+ *                    staging its tile's box in shared memory (default 0; same bits)
  * Must precede endBox except "write_files". */
 int tild_box_set_option(tild_box *box, const char *key, int64_t value);
 

@@ -181,6 +181,7 @@ void Box::setOption(const std::string &key, int64_t v)
     else if (key == "deterministic") deterministic = (int)v;
     else if (key == "bspline4_exact") exact4 = (int)v;
     else if (key == "autotune") autotune = v != 0;
+    else if (key == "direct_gather") directGather = v != 0;
     else if (key == "sort_interval") {
         if (v < 0) fail(TILD_ERR_ARG, "sort_interval must be >= 0");
         sortInterval = (int)v;
@@ -1200,7 +1201,7 @@ void Box::allocDevice()
         const double perCode = 16.0 * std::min(4, g.nz) * (double)N / (double)g.M;   // particles per brick of 4^3 cells (4x4x1 in 2-D)
         int codes = 8;
         while (codes < 64 && perCode * codes * 2.0 <= 192.0) codes *= 2;
-        tiles = tileGeometry(codes);
+        tiles = tileGeometry(codes, directGather);
     }
     sortW.key = dalloc<uint32_t>(N);
     sortW.rank = dalloc<int>(N);
@@ -1909,8 +1910,9 @@ void Box::readRows3(const float *dev, float *out) const
 // Tile of `codes` consecutive brick codes: threads for about one particle each (mean plus
 // two standard deviations), the deposit's box estimate, and the particle pass's fixed box
 // (the tile's bricks widened by the stencil and one cell of drift per side; particles that
-// drift further are gathered from global memory).
-TileCfg Box::tileGeometry(int codes) const
+// drift further are gathered from global memory).  direct: the particle pass stages no
+// box and reads every particle's stencil through L1/L2.
+TileCfg Box::tileGeometry(int codes, bool direct) const
 {
     const Geom &g = geom;
     const double perCode = 16.0 * std::min(4, g.nz) * (double)nstot / (double)g.M;
@@ -1932,20 +1934,23 @@ TileCfg Box::tileGeometry(int codes) const
     t.threads = thr;
     t.box = (int)box;
     t.pbox = (((ex | 1) * ey) | 1) * ez;
+    t.direct = direct ? 1 : 0;
     t.margin = margin;
     return t;
 }
 
 // Tile autotuner (option "autotune"): times the force evaluation (deposit, transforms,
 // force pass without integration) with tiles of half, the same and twice the bricks of
-// the density rule and keeps the fastest.  Positions, the step counter, the noise and
+// the density rule, each with the particle pass's staged box and with direct gathers,
+// and keeps the fastest.  Positions, the step counter, the noise and
 // the RNG state are not touched.
 void Box::autotuneTiles()
 {
     if (!sortedTiles) return;
     std::vector<TileCfg> cands;
     for (int c : {tiles.codes / 2, tiles.codes, tiles.codes * 2})
-        if (c >= 1 && c <= 64) cands.push_back(tileGeometry(c));
+        if (c >= 1 && c <= 64)
+            for (bool direct : {false, true}) cands.push_back(tileGeometry(c, direct));
     cudaEvent_t e0, e1;
     ck(cudaEventCreate(&e0), "event");
     ck(cudaEventCreate(&e1), "event");
@@ -2248,7 +2253,8 @@ std::string Box::describe() const
       << ", \"doCharges\": " << (doCharges ? "true" : "false") << ", \"MAXBONDS\": " << MAXBONDS
       << ", \"nBonds\": " << nBondsTot << ", \"nAngles\": " << nAnglesTot << ", \"MAXANGLES\": " << MAXANGLES
       << ", \"datFileName\": " << q(datFileName) << ", \"tiles\": {\"codes\": " << tiles.codes
-      << ", \"threads\": " << tiles.threads << ", \"autotuned\": " << (autotune ? "true" : "false")
+      << ", \"threads\": " << tiles.threads << ", \"gather\": \"" << (tiles.direct ? "direct" : "staged")
+      << "\", \"autotuned\": " << (autotune ? "true" : "false")
       << ", \"tuned_ms\": " << tunedMs << "}, \"trajFreq\": " << trajFreq
       << ", \"trajFileName\": " << q(trajFileName) << ", \"fieldFreq\": " << fieldFreq
       << ", \"logScaleFields\": " << (logSpaceFields ? logScaleFields : 0.f) << ", \"gsdFreq\": " << gsdFreq

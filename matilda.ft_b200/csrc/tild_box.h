@@ -262,8 +262,9 @@ private:
     uint32_t sortKeys = 0;
     TileCfg tiles{};                // codes / threads / box chosen from the density
     TileCfg tileCfg() const;
-    TileCfg tileGeometry(int codes) const;
+    TileCfg tileGeometry(int codes, bool direct) const;
     bool autotune = false;          // option "autotune": time tile sizes at endBox
+    bool directGather = false;      // option "direct_gather": particle pass reads L1/L2, no box
     float tunedMs = 0.f;            // force evaluation time of the chosen tiles
     void autotuneTiles();
     void uploadFlags();

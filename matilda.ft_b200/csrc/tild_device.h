@@ -147,6 +147,7 @@ struct TileCfg {
     int box;      // deposit: shared-memory records of a tile's bounding box (estimate)
     int pbox;     // particle pass: records of the fixed tile box (odd pitches)
     int margin;   // particle pass: drift margin of the fixed box, cells per side
+    int direct;   // particle pass: 1 = read every stencil through L1/L2 (no staged box)
 };
 
 struct AngleArrays {        // angles in slot order (all NULL: the box has none)

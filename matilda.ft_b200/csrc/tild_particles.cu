@@ -249,15 +249,16 @@ constexpr int kPartWindow = 256;   // slots per CTA when the particles are not s
 
 // Gather of one force group's records at a particle's stencil straight from global memory
 // (device_utils.cu:358-461), summed in the same order as the shared-memory gather so the
-// two paths give the same bits.
-template <int P>
+// two paths give the same bits.  UNROLL: all (P+1)^3 loads in flight at once (the direct
+// gathers of a whole CTA), else one plane at a time (the few helpers' gathers).
+template <int P, bool UNROLL>
 __device__ __forceinline__ void gather_global(const Geom &g, const float4 *__restrict__ rf, const int *gs,
                                               const float *Wx, const float *Wy, const float *Wz, float *acc)
 {
     // a true modulo past one box length: a position outside [0, L) still reads the grid
     auto wrap = [](int v, int n) { return wrapi(v, n); };
     float a0 = 0.f, a1 = 0.f, a2 = 0.f;
-#pragma unroll 1
+#pragma unroll(UNROLL ? P + 1 : 1)
     for (int e = 0; e <= P; e++) {
         const float wz = sel<P>(Wz, e);
         const float4 *rz = rf + (long long)g.nx * g.ny * wrap(gs[2] + e, g.nz);
@@ -418,7 +419,7 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
             hs[1] = stencil_fast<P>(Xc[3 * ph + 1], inv[1], pp.quirk4, Hy);
             hs[2] = stencil_fast_z<P>(Xc[3 * ph + 2], inv[2], pp.quirk4, Hz, g.nz);
             for (int h = 0; h < pp.nfg; h++)
-                if ((flh >> (8 + h)) & 1u) gather_global<P>(g, rec + (long long)h * g.M, hs, Hx, Hy, Hz, Ao[threadIdx.x][h]);
+                if ((flh >> (8 + h)) & 1u) gather_global<P, false>(g, rec + (long long)h * g.M, hs, Hx, Hy, Hz, Ao[threadIdx.x][h]);
         }
         // 4. bonds
         float f[3] = {0.f, 0.f, 0.f};
@@ -482,7 +483,7 @@ __global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticlePara
                 a[1] = Ao[slot][fg][1];
                 a[2] = Ao[slot][fg][2];
             } else {
-                gather_global<P>(g, rf, gs, Wx, Wy, Wz, a);
+                gather_global<P, true>(g, rf, gs, Wx, Wy, Wz, a);
             }
             if ((pp.fg_qweighted >> fg) & 1u) {
                 f[0] = __fmaf_rn(a[0], qp, f[0]);
@@ -653,7 +654,7 @@ static void part_launch(const Geom &g, const ParticleParams *ppd, int N, float *
 {
     const int nbk = tc.start ? (tc.nkeys + tc.codes - 1) / tc.codes : (N + kPartWindow - 1) / kPartWindow;
     const int threads = tc.start ? tc.threads : 256;
-    const int cap = tc.start ? std::min(tc.pbox, kPartBox) : 0;
+    const int cap = (tc.start && !tc.direct) ? std::min(tc.pbox, kPartBox) : 0;
     const size_t smem = (size_t)cap * sizeof(float4) + (size_t)threads * 7 * sizeof(float);
     const bool extra = aa.na != nullptr || walls;
     if (extra)

@@ -152,6 +152,21 @@ def test_autotuned_tiles_are_invisible():
     assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][2], outs[1][2])
 
 
+@pytest.mark.parametrize("order", [2, 3, 4])
+def test_direct_gather_is_invisible(order):
+    """Reading every stencil through L1/L2 instead of the tile's staged box changes only
+    where the records come from: forces and a short trajectory are bit-identical."""
+    spec = synth.small_system(seed=27, order=order, charges=True, n_chains=120, nper=10, L=10.0, grid=(20, 20, 20))
+    outs = []
+    for direct in (0, 1):
+        with make_box(spec, deterministic=1, direct_gather=direct) as b:
+            outs.append((b.forces(), b.describe()["tiles"]["gather"]))
+            b.step(5)
+            outs[-1] += (b.positions(),)
+    assert [o[1] for o in outs] == ["staged", "direct"]
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][2], outs[1][2])
+
+
 def test_spatial_sort_is_invisible():
     """Re-sorting the particle arrays changes only memory order: in deterministic mode the
     trajectory is bit-identical with no sort, a sort every 3 steps and every step."""
