@@ -297,7 +297,7 @@ constexpr int kPartOut = 32;   // particles per pass gathered from global memory
 // EXTRA: the box has angles or walls (compiled out of the common instantiation, whose
 // schedule the unused terms would otherwise disturb)
 template <int P, bool EXTRA>
-__global__ void __launch_bounds__(512, 2) k_particles(Geom g, const ParticleParams *__restrict__ ppd, int N,
+__global__ void __launch_bounds__(448, 2) k_particles(Geom g, const ParticleParams *__restrict__ ppd, int N,
                                                       float *__restrict__ X0, float *__restrict__ X1,
                                                       float *__restrict__ noise, const uint32_t *__restrict__ pflags,
                                                       const float *__restrict__ q, const uint8_t *__restrict__ nb,
