@@ -354,7 +354,7 @@ def run_ours(args):
     torch.cuda.set_device(local)
     spec = make_spec(args.scale)
     stream = torch.cuda.Stream(device=local)
-    box = tild_b200.box_from_spec(spec, device=local, options={"write_files": 0, "autotune": 1})
+    box = tild_b200.box_from_spec(spec, device=local, options={"write_files": 0, "autotune": 0 if args.no_autotune else 1})
     box.set_stream(stream.cuda_stream)
     box.command("endBox")
     info = box.info()
@@ -440,7 +440,7 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "particles": spec.N, "grid": [int(v) for v in spec.grid],
                        "parallelism": "replicas" if world > 1 else "single", "rng": "philox",
                        "tiles": {"bricks_per_cta": tiles["codes"], "threads": tiles["threads"],
-                                 "gather": tiles["gather"], "autotuned": True},
+                                 "gather": tiles["gather"], "autotuned": not args.no_autotune},
                        "l2": "inputs larger than L2 (%.2f GB moved per step by the kernels' compulsory traffic)"
                              % (step_bytes / 1e9)},
             "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved, "peak": peak,
@@ -480,6 +480,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched (C3) and served (C5) runs")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the density rule's tiles (profiling: fewer launches before the steps)")
     ap.add_argument("--c3-replicas", type=int, default=64)
     ap.add_argument("--c3-steps", type=int, default=500)
     ap.add_argument("--c5-jobs", type=int, default=40)
