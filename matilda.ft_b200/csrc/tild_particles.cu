@@ -282,6 +282,9 @@ __device__ __forceinline__ void gather_global(const Geom &g, const float4 *__res
 }
 
 constexpr int kPartOut = 32;   // particles per pass gathered from global memory by helpers
+// threads of a particle-pass CTA at most: the launch bound that caps registers at 72
+// (a tile with more particles takes more than one pass)
+constexpr int kPartThreadsMax = 448;
 
 // Particle pass over one Morton tile of particles (or a window of slots), one particle
 // per thread and pass: bonds, then per force group the gather (device_utils.cu:358-461),
@@ -297,7 +300,7 @@ constexpr int kPartOut = 32;   // particles per pass gathered from global memory
 // EXTRA: the box has angles or walls (compiled out of the common instantiation, whose
 // schedule the unused terms would otherwise disturb)
 template <int P, bool EXTRA>
-__global__ void __launch_bounds__(448, 2) k_particles(Geom g, const ParticleParams *__restrict__ ppd, int N,
+__global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const ParticleParams *__restrict__ ppd, int N,
                                                       float *__restrict__ X0, float *__restrict__ X1,
                                                       float *__restrict__ noise, const uint32_t *__restrict__ pflags,
                                                       const float *__restrict__ q, const uint8_t *__restrict__ nb,
@@ -643,7 +646,7 @@ __global__ void k_reduce_partials(const double *partials, int nblocks, int ncols
 }
 
 
-constexpr size_t kPartSmemMax = kPartBox * sizeof(float4) + 512 * 7 * sizeof(float);
+constexpr size_t kPartSmemMax = kPartBox * sizeof(float4) + kPartThreadsMax * 7 * sizeof(float);
 
 template <int P>
 static void part_launch(const Geom &g, const ParticleParams *ppd, int N, float *X0, float *X1, float *noise,
@@ -653,7 +656,7 @@ static void part_launch(const Geom &g, const ParticleParams *ppd, int N, float *
                         cudaStream_t st)
 {
     const int nbk = tc.start ? (tc.nkeys + tc.codes - 1) / tc.codes : (N + kPartWindow - 1) / kPartWindow;
-    const int threads = tc.start ? tc.threads : 256;
+    const int threads = tc.start ? std::min(tc.threads, kPartThreadsMax) : 256;
     const int cap = (tc.start && !tc.direct) ? std::min(tc.pbox, kPartBox) : 0;
     const size_t smem = (size_t)cap * sizeof(float4) + (size_t)threads * 7 * sizeof(float);
     const bool extra = aa.na != nullptr || walls;
