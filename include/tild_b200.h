@@ -33,7 +33,9 @@ enum tild_status {
     TILD_ERR_CUDA = 4,        /* a CUDA runtime call or kernel failed                */
     TILD_ERR_STATE = 5,       /* call out of order (e.g. step before endBox)         */
     TILD_ERR_UNSUPPORTED = 6, /* a script feature outside the TILD hot path          */
-    TILD_ERR_DEVICE = 7       /* device-side check failed (error flag set by a kernel)*/
+    TILD_ERR_DEVICE = 7       /* device-side check failed: a kernel counted particles whose
+                                 position is not finite (the run blew up); reported when
+                                 energies are read (log rows, thermo) */
 };
 
 typedef struct tild_box tild_box;

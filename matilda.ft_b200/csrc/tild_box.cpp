@@ -1429,6 +1429,9 @@ std::vector<double> Box::readEnergies(bool)
     std::vector<double> r(kResSize, 0.0);
     ck(cudaStreamSynchronize(stream), "sync");
     ck(cudaMemcpy(r.data(), dRes, sizeof(double) * r.size(), cudaMemcpyDeviceToHost), "read energies");
+    if (r[kResNonFinite] > 0.0)   // the run has blown up: stop instead of logging NaN
+        fail(TILD_ERR_DEVICE, std::to_string((long long)r[kResNonFinite]) +
+                                  " particle(s) with a non-finite position at step " + std::to_string(deviceStep()));
     int wi = 0;   // Wall::CalcEnergy (ps_potentialWall.cu:58-70) in the wall's potential slot
     for (size_t k = 0; k < potentials.size(); k++)
         if (potentials[k].kind == POT_WALL) r[k] = r[kResWall + wi++];

@@ -28,8 +28,9 @@ constexpr int kResBond = kMaxPots + 6;
 constexpr int kResAngle = kResBond + 7;   // angle energy and virial (each angle on 3 particles)
 constexpr int kMaxWalls = 4;              // `potential wall` terms (per-particle, flag bits 24..27)
 constexpr int kResWall = kResAngle + 7;   // energy of each wall
-constexpr int kResSize = kResWall + kMaxWalls;
-constexpr int kPartialCols = 14 + kMaxWalls;   // per-block columns of the bond/angle/wall reduction
+constexpr int kResNonFinite = kResWall + kMaxWalls;   // particles whose position is not finite
+constexpr int kResSize = kResNonFinite + 1;
+constexpr int kPartialCols = 15 + kMaxWalls;   // per-block columns of the bond/angle/wall reduction
 constexpr int kMaxTypes = 16;
 constexpr int kMaxBondTypes = 16;
 constexpr int kMaxAngleTypes = 16;
@@ -229,7 +230,8 @@ cudaError_t launch_rng_init(void *states, const int *orig_id, int n, unsigned lo
                             cudaStream_t st);
 size_t rng_state_bytes();
 // per block (kPartialCols columns): bond energy + virial (7), angle energy + virial (7),
-// then the energy of each wall (kMaxWalls)
+// the energy of each wall (kMaxWalls), then the count of particles whose position is not
+// finite
 cudaError_t launch_bond_energy(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd,
                                const float *X0, const float *X1, const long long *d_step,
                                const uint8_t *nb, const int *partner, const uint8_t *btype, AngleArrays aa,

@@ -560,6 +560,7 @@ __global__ void __launch_bounds__(256) k_bond_energy(Geom g, const ParticleParam
             float dr[3], mdr2 = 0.f, mf = 0.f;
             for (int j = 0; j < 3; j++) {
                 dr[j] = X[3 * p + j] - X[3 * o + j];
+                // the reference's threshold of 0.5*Lh here (ps_deviceBonds.cu:132-133)
                 if (dr[j] > 0.5f * g.Lh[j]) dr[j] -= g.L[j];
                 else if (dr[j] < -0.5f * g.Lh[j]) dr[j] += g.L[j];
                 mdr2 = __fmaf_rn(dr[j], dr[j], mdr2);
@@ -613,6 +614,9 @@ __global__ void __launch_bounds__(256) k_bond_energy(Geom g, const ParticleParam
 #pragma unroll
         for (int w = 0; w < kMaxWalls; w++) acc[14 + w] = ew[w];
     }
+    // blow-up check: a particle whose position is not finite (NaN or inf) is counted
+    if (p < N && !(isfinite(X[3 * p]) && isfinite(X[3 * p + 1]) && isfinite(X[3 * p + 2])))
+        acc[14 + kMaxWalls] = 1.0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int c = 0; c < NC; c++) {
         double v = acc[c];

@@ -167,6 +167,28 @@ def test_direct_gather_is_invisible(order):
     assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][2], outs[1][2])
 
 
+def test_blown_up_positions_are_reported_as_err_device():
+    """A position that is NaN or infinite (a run that blew up) is counted on the device and
+    reported as ERR_DEVICE when the energies are read, instead of logging NaN; the box
+    stays usable once the positions are finite again.  Every index stays on the grid for
+    such positions: stencil origins and sort cells are wrapped or clamped."""
+    spec = synth.small_system(seed=31, order=3, charges=True, n_chains=40, nper=10, L=10.0, grid=(20, 20, 20))
+    with make_box(spec) as b:
+        x = b.positions()
+        ok = b.thermo()
+        for bad in (np.nan, np.inf):
+            y = x.copy()
+            y[7, 1] = bad
+            y[123, 2] = bad
+            b.set_positions(y)
+            with pytest.raises(tild_b200.TildError) as ei:
+                b.thermo()
+            assert ei.value.code == 7 and "2 particle(s) with a non-finite position" in str(ei.value)
+        b.set_positions(x)
+        again = b.thermo()
+        assert np.allclose(again["potentials"], ok["potentials"], rtol=1e-6)
+
+
 def test_spatial_sort_is_invisible():
     """Re-sorting the particle arrays changes only memory order: in deterministic mode the
     trajectory is bit-identical with no sort, a sort every 3 steps and every step."""
