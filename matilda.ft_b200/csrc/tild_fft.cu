@@ -173,37 +173,39 @@ __device__ __forceinline__ void fft_stage(const float2 *__restrict__ src, float2
     }
 }
 
-// Generic radix stage: b_q = sum_s a_s W_{pR}^{s k} W_R^{q s}.
+// Generic radix stage: b_q = sum_s a_s W_{pR}^{s k} W_R^{q s}.  One thread per output
+// (butterfly, q), so that a prime line (one butterfly of radix n) still spreads over n
+// threads; each output sums its R terms in order s = 0..R-1.
 template <bool INV>
 __device__ void fft_stage_generic(const float2 *__restrict__ src, float2 *__restrict__ dst, int L, int lp, int ls,
                                   int n, int R, int p, const FastDiv &dp, const FastDiv &dsplit, bool line_fast,
                                   const float2 *tw)
 {
-    const int nb = n / R, stride = n / (p * R), nR = n / R;
-    for (int w = threadIdx.x; w < L * nb; w += blockDim.x) {
+    const int nb = n / R, stride = n / (p * R), nR = n / R, items = L * nb;
+    for (int w = threadIdx.x; w < items * R; w += blockDim.x) {
+        const int qq = w / items, wi = w - qq * items;
         int l, i;
         if (line_fast) {
-            i = (int)fdiv((unsigned)w, dsplit);
-            l = w - i * L;
+            i = (int)fdiv((unsigned)wi, dsplit);
+            l = wi - i * L;
         } else {
-            l = (int)fdiv((unsigned)w, dsplit);
-            i = w - l * nb;
+            l = (int)fdiv((unsigned)wi, dsplit);
+            i = wi - l * nb;
         }
         const int k = i - p * (int)fdiv((unsigned)i, dp);
         const float2 *s = src + l * lp;
-        float2 *d = dst + l * lp;
         const int j = (i - k) * R + k;
-        for (int qq = 0; qq < R; qq++) {
-            float2 acc = make_float2(0.f, 0.f);
-            for (int ss = 0; ss < R; ss++) {
-                float2 v = s[(i + ss * nb) * ls];
-                if (k && ss) v = cmul(v, twid<INV>(tw, ss * k * stride));
-                const int e = (qq * ss) % R;
-                if (e) v = cmul(v, twid<INV>(tw, e * nR));
-                acc = cadd(acc, v);
-            }
-            d[(j + qq * p) * ls] = acc;
+        float2 acc = make_float2(0.f, 0.f);
+        int e = 0;   // (qq * ss) mod R
+        for (int ss = 0; ss < R; ss++) {
+            float2 v = s[(i + ss * nb) * ls];
+            if (k && ss) v = cmul(v, twid<INV>(tw, ss * k * stride));
+            if (e) v = cmul(v, twid<INV>(tw, e * nR));
+            acc = cadd(acc, v);
+            e += qq;
+            if (e >= R) e -= R;
         }
+        dst[l * lp + (j + qq * p) * ls] = acc;
     }
 }
 

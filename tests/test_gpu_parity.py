@@ -50,6 +50,8 @@ SYSTEMS = {
     # radix-7 stages on every axis, and generic prime radices 11 and 13
     "radix7_grid": lambda: synth.small_system(seed=12, order=2, grid=(21, 14, 28), L=7.0, charges=True),
     "prime_grid": lambda: synth.small_system(seed=13, order=1, grid=(22, 13, 11), charges=True),
+    # whole prime lines (one generic butterfly of radix n per line) on every axis
+    "prime_lines": lambda: synth.small_system(seed=14, order=3, grid=(31, 37, 29), L=11.0, charges=True),
     "angles": lambda: synth.small_system(seed=15, order=3, charges=True, angle_params=ANGLES),
     "free_particles": lambda: synth.small_system(seed=9, order=3, n_free=50, charges=True),
     # harmonic walls (per-particle potentials) beside grid potentials
@@ -109,7 +111,7 @@ def test_densities_match_oracle():
                 assert np.abs(gq - rhoq).max() <= 1e-6 * np.abs(rhoq).max()
 
 
-@pytest.mark.parametrize("name", ["diblock_o3", "charged_o3", "erf", "odd_grid", "walls"])
+@pytest.mark.parametrize("name", ["diblock_o3", "charged_o3", "erf", "odd_grid", "prime_lines", "walls"])
 def test_energies_match_oracle(name):
     spec = SYSTEMS[name]()
     sysm = spec_to_system(spec)
