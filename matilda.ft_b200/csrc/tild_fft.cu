@@ -173,16 +173,18 @@ __device__ __forceinline__ void fft_stage(const float2 *__restrict__ src, float2
     }
 }
 
-// Generic radix stage: b_q = sum_s a_s W_{pR}^{s k} W_R^{q s}.  One thread per output
-// (butterfly, q), so that a prime line (one butterfly of radix n) still spreads over n
-// threads; each output sums its R terms in order s = 0..R-1.
+// Generic radix stage: b_q = sum_s a_s W_{pR}^{s k} W_R^{q s}, R an odd prime (11, 13,
+// ...: the plan takes 2, 3, 5 and 7 first).  One thread per output pair (q, R - q) of a
+// butterfly, so that a prime line (one butterfly of radix n) still spreads over (n+1)/2
+// threads: W_R^{(R-q) s} = conj W_R^{q s}, so both outputs share each term's loads and
+// products; each sums its R terms in order s = 0..R-1.
 template <bool INV>
 __device__ void fft_stage_generic(const float2 *__restrict__ src, float2 *__restrict__ dst, int L, int lp, int ls,
                                   int n, int R, int p, const FastDiv &dp, const FastDiv &dsplit, bool line_fast,
                                   const float2 *tw)
 {
-    const int nb = n / R, stride = n / (p * R), nR = n / R, items = L * nb;
-    for (int w = threadIdx.x; w < items * R; w += blockDim.x) {
+    const int nb = n / R, stride = n / (p * R), nR = n / R, items = L * nb, half = (R + 1) / 2;
+    for (int w = threadIdx.x; w < items * half; w += blockDim.x) {
         const int qq = w / items, wi = w - qq * items;
         int l, i;
         if (line_fast) {
@@ -195,17 +197,27 @@ __device__ void fft_stage_generic(const float2 *__restrict__ src, float2 *__rest
         const int k = i - p * (int)fdiv((unsigned)i, dp);
         const float2 *s = src + l * lp;
         const int j = (i - k) * R + k;
-        float2 acc = make_float2(0.f, 0.f);
+        float2 acc = make_float2(0.f, 0.f), acm = make_float2(0.f, 0.f);   // b_q, b_{R-q}
         int e = 0;   // (qq * ss) mod R
         for (int ss = 0; ss < R; ss++) {
             float2 v = s[(i + ss * nb) * ls];
             if (k && ss) v = cmul(v, twid<INV>(tw, ss * k * stride));
-            if (e) v = cmul(v, twid<INV>(tw, e * nR));
-            acc = cadd(acc, v);
+            if (e) {
+                const float2 t = twid<INV>(tw, e * nR);
+                const float xr = v.x * t.x, yi = v.y * t.y, xi = v.x * t.y, yr = v.y * t.x;
+                acc.x += xr - yi;
+                acc.y += xi + yr;
+                acm.x += xr + yi;
+                acm.y += yr - xi;
+            } else {
+                acc = cadd(acc, v);
+                acm = cadd(acm, v);
+            }
             e += qq;
             if (e >= R) e -= R;
         }
         dst[l * lp + (j + qq * p) * ls] = acc;
+        if (qq) dst[l * lp + (j + (R - qq) * p) * ls] = acm;
     }
 }
 
