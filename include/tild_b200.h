@@ -140,6 +140,13 @@ int tild_box_get_info(const tild_box *box, tild_box_info *out);
  * then the final writeData and final.input.data. */
 int tild_box_run_nvt(tild_box *box, int64_t nsteps);
 
+/* A top-level `modify` line after endBox, without the word `modify`: PS_Box::modifyBox
+ * (PS_Box.cu:848-870).  "potential remove i" (or "delete") drops the i-th potential,
+ * counted from 1 in script order; positions, the integrators' state, the noise streams and
+ * the particle order are kept, so the next run continues the same trajectory.  Like the
+ * reference, an out-of-range index or another word changes nothing. */
+int tild_box_modify(tild_box *box, const char *rest);
+
 /* nsteps time steps with no I/O and no thermo (PS_Box::doTimeStep, PS_Box.cu:73-162,
  * without the I/O branch :168-205).  Runs as replays of a captured CUDA graph. */
 int tild_box_step(tild_box *box, int64_t nsteps);
@@ -169,6 +176,13 @@ int tild_box_set_positions(tild_box *box, const float *x_in);
 /* Density field of group `group` at the current positions (PS_Group::d_rho, or d_rhoq
  * when charge_channel != 0), rho_out[M] in the reference's x-fastest order. */
 int tild_box_get_density(tild_box *box, const char *group, int charge_channel, float *rho_out);
+
+/* Grid force of group `group` from the last force evaluation (tild_box_forces or a
+ * step): PS_Group::d_gridForce after the potentials' CalcForces (ps_potential.cu:41-125,
+ * ps_groups.cu:164-179), gf_out[M*Dim] interleaved per grid point in the reference's
+ * x-fastest order and units (the particle force is sum_m gf[m] W_m).  A group that takes
+ * no grid force reads zeros. */
+int tild_box_get_grid_force(tild_box *box, const char *group, float *gf_out);
 
 /* No counterpart in the reference.  tild_box_get_density for callers that cannot
  * allocate device memory: a host program whose pool allocator has reserved the device's
@@ -202,8 +216,9 @@ int tild_box_structure_factor(tild_box *box, const char *group, int charge_chann
  * same order and float arithmetic as the reference (weights divided by gvol). */
 int tild_box_grid_weights(tild_box *box, int32_t *inds_out, float *w_out);
 
-/* Energies recorded by the last run (one row per logged step: step, Ubond, pot...)
- * copied to out[rows*cols]; rows and cols report the shape.  Pass out=NULL to query. */
+/* Energies recorded by the runs so far (one row per logged step: step, Ubond, pot...)
+ * copied to out[rows*cols]; rows and cols report the shape (the widest row; rows logged
+ * while fewer potentials existed end in zeros).  Pass out=NULL to query. */
 int tild_box_get_log(tild_box *box, double *out, int64_t *rows, int32_t *cols);
 
 /* Execute a whole MATILDA.FT input script file (main.cu:21-156): `box ps` blocks,
@@ -231,7 +246,7 @@ int tild_box_stage_times(tild_box *box, double *out, int nmax, int *n);
  * job finishes, its positions and thermo are copied to the host and its device memory is
  * freed, so queued jobs enter while others are still running (continuous batching). */
 typedef struct tild_pool tild_pool;
-enum { TILD_JOB_QUEUED = 0, TILD_JOB_RUNNING = 1, TILD_JOB_DONE = 2, TILD_JOB_FAILED = 3 };
+enum { TILD_JOB_QUEUED = 0, TILD_JOB_RUNNING = 1, TILD_JOB_DONE = 2, TILD_JOB_FAILED = 3, TILD_JOB_CANCELLED = 4 };
 
 int tild_pool_create(int device, int64_t mem_budget_bytes, int32_t max_active, tild_pool **out);
 /* Cancels queued jobs, waits for running ones, frees everything. */
@@ -244,15 +259,27 @@ int tild_pool_submit(tild_pool *pool, tild_box *box, int64_t nsteps, int64_t *jo
 /* state: TILD_JOB_*; times3 (may be NULL): submit, admission and completion times in
  * seconds since the pool was created (0 until reached). */
 int tild_pool_status(tild_pool *pool, int64_t job_id, int32_t *state, int64_t *steps_done, double *times3);
-/* Blocks until the job is done; TILD_ERR_STATE with the job's error if it failed. */
+/* Blocks until the job is done; TILD_ERR_STATE with the job's error if it failed or was
+ * cancelled. */
 int tild_pool_wait(tild_pool *pool, int64_t job_id);
+/* Cancels a queued or running job.  A queued job leaves the queue at once; a running one
+ * stops taking new chunks of steps, its chunks already on the GPU finish, and then its
+ * device memory is freed and its state becomes TILD_JOB_CANCELLED (tild_pool_wait
+ * returns then, with TILD_ERR_STATE).  Other jobs are not disturbed.  TILD_ERR_STATE for a
+ * job that has already finished, failed or been cancelled. */
+int tild_pool_cancel(tild_pool *pool, int64_t job_id);
+/* Changes the memory budget.  It applies to admissions from now on: running jobs keep
+ * their memory and run to completion, queued jobs enter once the running set fits the new
+ * budget, and queued jobs larger than the whole new budget fail (TILD_JOB_FAILED). */
+int tild_pool_set_budget(tild_pool *pool, int64_t mem_budget_bytes);
 /* Final positions x_out[n*Dim] (particle order, may be NULL) and up to nthermo values of
  * tild_box_thermo's layout at the last step. */
 int tild_pool_result(tild_pool *pool, int64_t job_id, float *x_out, double *thermo_out, int32_t nthermo,
                      int32_t *nwritten);
-/* Forgets a finished or failed job. */
+/* Forgets a finished, failed or cancelled job. */
 int tild_pool_release(tild_pool *pool, int64_t job_id);
-/* out[0..5]: queued, running, done, failed, device bytes reserved by running jobs, budget. */
+/* out[0..6]: queued, running, done, failed, device bytes reserved by running jobs, budget,
+ * cancelled. */
 int tild_pool_stats(tild_pool *pool, int64_t *out, int32_t nout);
 
 #ifdef __cplusplus

@@ -1,5 +1,6 @@
 // tild_api.cpp -- extern "C" boundary of the B200 TILD library (declared in
 // include/tild_b200.h).  Converts C++ exceptions into status codes; never exits.
+#include <algorithm>
 #include <cstring>
 #include <fstream>
 #include <sstream>
@@ -238,6 +239,20 @@ int tild_box_get_density(tild_box *box, const char *group, int charge_channel, f
     return guarded([&] { box->impl->getDensity(group, charge_channel, rho_out); });
 }
 
+int tild_box_modify(tild_box *box, const char *rest)
+{
+    NEED_BOX;
+    if (!rest) return fail(TILD_ERR_ARG, "NULL argument");
+    return guarded([&] { box->impl->modifyBox(rest); });
+}
+
+int tild_box_get_grid_force(tild_box *box, const char *group, float *gf_out)
+{
+    NEED_BOX;
+    if (!group || !gf_out) return fail(TILD_ERR_ARG, "NULL argument");
+    return guarded([&] { box->impl->getGridForce(group, gf_out); });
+}
+
 int tild_box_get_density_noalloc(tild_box *box, const char *group, int charge_channel, float *rho_out)
 {
     NEED_BOX;
@@ -264,7 +279,8 @@ int tild_box_get_log(tild_box *box, double *out, int64_t *rows, int32_t *cols)
 {
     NEED_BOX;
     const auto &L = box->impl->logRows;
-    const int32_t c = box->impl->logColumns();
+    int32_t c = box->impl->logColumns();   // rows logged before a `modify` can be wider
+    for (const auto &r : L) c = std::max(c, (int32_t)r.size());
     if (rows) *rows = (int64_t)L.size();
     if (cols) *cols = c;
     if (out)
@@ -395,6 +411,18 @@ int tild_pool_result(tild_pool *pool, int64_t job_id, float *x_out, double *ther
         pool->impl->result(job_id, x_out, thermo_out, nthermo, &n);
         if (nwritten) *nwritten = n;
     });
+}
+
+int tild_pool_cancel(tild_pool *pool, int64_t job_id)
+{
+    NEED_POOL;
+    return guarded([&] { pool->impl->cancel(job_id); });
+}
+
+int tild_pool_set_budget(tild_pool *pool, int64_t mem_budget_bytes)
+{
+    NEED_POOL;
+    return guarded([&] { pool->impl->setBudget(mem_budget_bytes); });
 }
 
 int tild_pool_release(tild_pool *pool, int64_t job_id)

@@ -1044,6 +1044,8 @@ void Box::buildPlan()
     g.hstride = (long long)g.nz * g.ny * g.hp;
     for (int j = 0; j < 3; j++) {
         g.dxf[j] = (float)dx[j];
+        g.dlo[j] = (float)(dx[j] - (double)g.dxf[j]);
+        g.inv[j] = 1.0f / g.dxf[j];
         g.L[j] = L[j];
         g.Lh[j] = Lh[j];
     }
@@ -2043,6 +2045,38 @@ void Box::getDensity(const std::string &group, int charge, float *rho)
     cudaFree(dSites);
     cudaFree(dRho);
     ck(e, "density");
+}
+
+// Grid force of a group from the last force evaluation (tild_box_forces or a step), in the
+// reference's layout and units: gf[m*Dim + d] = -d/dx_d of the group's summed potential
+// field, as PS_Group::d_gridForce holds it after CalcForces (ps_potential.cu:41-125,
+// ps_groups.cu:164-179).  The records keep it scaled by the gather's gvol / gvol_f32 (the
+// particle pass takes unscaled weights), which is divided out here.  A group that takes
+// no grid force reads zeros, as its zeroed field would.
+void Box::getGridForce(const std::string &group, float *gf)
+{
+    if (!ready) fail(TILD_ERR_STATE, "endBox has not been processed");
+    const int gi = findGroupInteger(group);
+    const long long M = geom.M;
+    int k = -1;
+    for (size_t i = 0; i < fgroups.size(); i++)
+        if (fgroups[i] == gi) k = (int)i;
+    if (k < 0) {
+        std::fill(gf, gf + M * Dim, 0.f);
+        return;
+    }
+    std::vector<float4> h((size_t)M);
+    ck(cudaSetDevice(device), "cudaSetDevice");
+    ck(cudaMemcpyAsync(h.data(), dRec + (size_t)k * M, sizeof(float4) * M, cudaMemcpyDeviceToHost, stream),
+       "read grid force");
+    ck(cudaStreamSynchronize(stream), "read grid force");
+    const double gvf = (double)((1.0f * geom.dxf[0]) * geom.dxf[1] * geom.dxf[2]);
+    const double scale = gvf / gvol;
+    for (long long m = 0; m < M; m++) {
+        gf[m * Dim] = (float)(h[m].x * scale);
+        gf[m * Dim + 1] = (float)(h[m].y * scale);
+        if (Dim == 3) gf[m * Dim + 2] = (float)(h[m].z * scale);
+    }
 }
 
 // getDensity without any allocation: the accumulator rho[M], the slot-of-particle table

@@ -98,6 +98,7 @@ public:
     void readRows3(const float *dev, float *out) const;
     void setPositions(const float *x);
     void getDensity(const std::string &group, int charge, float *rho);
+    void getGridForce(const std::string &group, float *gf);   // PS_Group::d_gridForce
     void getDensityNoAlloc(const std::string &group, int charge, float *rho);
     void structureFactor(const std::string &group, int charge, int nbins, double kmax, double *k_out,
                          double *sk_out, double *count_out);

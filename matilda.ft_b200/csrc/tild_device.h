@@ -67,6 +67,8 @@ struct Geom {
     long long M;               // nx*ny*nz
     long long hstride;         // elements per half-spectrum field = nz*ny*hp
     float dxf[3];              // (float)(L/Nx)
+    float dlo[3];              // (float)(L/Nx - dxf): the FP32 remainder of the cell width
+    float inv[3];              // 1.f / dxf (IEEE FP32 division)
     float L[3];
     float Lh[3];
 };

@@ -156,7 +156,6 @@ __global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ TileShared ts;
     const float *__restrict__ X = (*d_step & 1) ? X1 : X0;
-    const float inv[3] = {1.f / g.dxf[0], 1.f / g.dxf[1], 1.f / g.dxf[2]};
     int b0, b1;
     tile_range(tc, N, kDepPB, b0, b1);
     if (b1 <= b0) return;
@@ -208,9 +207,9 @@ __global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4
             float *mine = wt + lane * WREC;
             if (dm) {
                 float Wx[P1], Wy[P1], Wz[P1];
-                const int gs[3] = {stencil_fast<P>(X[3 * p + 0], inv[0], quirk4, Wx),
-                                   stencil_fast<P>(X[3 * p + 1], inv[1], quirk4, Wy),
-                                   stencil_fast_z<P>(X[3 * p + 2], inv[2], quirk4, Wz, g.nz)};
+                const int gs[3] = {stencil_fast<P>(X[3 * p + 0], g, 0, quirk4, Wx),
+                                   stencil_fast<P>(X[3 * p + 1], g, 1, quirk4, Wy),
+                                   stencil_fast_z<P>(X[3 * p + 2], g, quirk4, Wz)};
                 int d[3];
                 bool in = true;
 #pragma unroll
@@ -295,9 +294,9 @@ __global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4
             const uint32_t dm = pflags[p] & 0xffu;
             if (!dm) continue;
             float Wx[P1], Wy[P1], Wz[P1];
-            const int gx = stencil_fast<P>(X[3 * p + 0], inv[0], quirk4, Wx);
-            const int gy = stencil_fast<P>(X[3 * p + 1], inv[1], quirk4, Wy);
-            const int gz = stencil_fast_z<P>(X[3 * p + 2], inv[2], quirk4, Wz, g.nz);
+            const int gx = stencil_fast<P>(X[3 * p + 0], g, 0, quirk4, Wx);
+            const int gy = stencil_fast<P>(X[3 * p + 1], g, 1, quirk4, Wy);
+            const int gz = stencil_fast_z<P>(X[3 * p + 2], g, quirk4, Wz);
             const float qp = q ? q[p] : 0.f;
             int ix[P1], iy[P1], iz[P1];
 #pragma unroll

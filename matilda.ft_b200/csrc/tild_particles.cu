@@ -51,6 +51,10 @@ __device__ __forceinline__ void philox_normals3(unsigned long long seed, uint32_
 
 // Bond force on particle p (ps_deviceBonds.cu:7-79): minimum image with Lh, skipped for
 // r^2 <= 1e-4, harmonic mf = 2k(r - req)/r or FENE; f -= mf * dr over every stored partner.
+// A bond across the periodic boundary is measured as (x_p - L) - x_o or x_p - (x_o - L):
+// the coordinate above L/2 is shifted first, which is exact in FP32, so the short image
+// vector is rounded once at its own magnitude instead of at the box length's (the
+// reference's x_p - x_o then -L loses up to half an ulp of L, ~2e-6 at L = 60).
 __device__ __forceinline__ void bond_force(const Geom &g, const ParticleParams &pp, int p, const float *x,
                                            const float *__restrict__ Xc, const uint8_t *__restrict__ nb,
                                            const int *__restrict__ partner, const uint8_t *__restrict__ btype,
@@ -60,12 +64,14 @@ __device__ __forceinline__ void bond_force(const Geom &g, const ParticleParams &
     for (int b = 0; b < nbp; b++) {
         const int o = partner[p * pp.maxb + b];
         const int t = btype[p * pp.maxb + b];
-        float dr[3] = {x[0] - Xc[3 * o], x[1] - Xc[3 * o + 1], x[2] - Xc[3 * o + 2]};
+        float dr[3];
         float mdr2 = 0.f;
 #pragma unroll
         for (int j = 0; j < 3; j++) {
-            if (dr[j] > g.Lh[j]) dr[j] -= g.L[j];
-            else if (dr[j] < -g.Lh[j]) dr[j] += g.L[j];
+            const float xo = Xc[3 * o + j];
+            dr[j] = x[j] - xo;
+            if (dr[j] > g.Lh[j]) dr[j] = (x[j] - g.L[j]) - xo;
+            else if (dr[j] < -g.Lh[j]) dr[j] = x[j] - (xo - g.L[j]);
             mdr2 = __fmaf_rn(dr[j], dr[j], mdr2);
         }
         float mf = 0.f;
@@ -323,7 +329,6 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
     const long long step = *d_step;
     const float *__restrict__ Xc = (step & 1) ? X1 : X0;   // x_t
     float *__restrict__ Xn = (step & 1) ? X0 : X1;         // x_{t-1} in, x_{t+1} out
-    const float inv[3] = {1.f / g.dxf[0], 1.f / g.dxf[1], 1.f / g.dxf[2]};
     const int nn[3] = {g.nx, g.ny, g.nz};
     int r0, r1;
     tile_range(tc, N, kPartWindow, r0, r1);
@@ -377,9 +382,9 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
         const unsigned fm = (fl >> 8) & 0xffu;
         int gs[3] = {0, 0, 0};
         if (fm) {
-            gs[0] = stencil_origin<P>(x[0], inv[0]);
-            gs[1] = stencil_origin<P>(x[1], inv[1]);
-            gs[2] = stencil_origin_z<P>(x[2], inv[2], g.nz);
+            gs[0] = stencil_origin<P>(x[0], g, 0);
+            gs[1] = stencil_origin<P>(x[1], g, 1);
+            gs[2] = stencil_origin_z<P>(x[2], g);
         }
         if (threadIdx.x == 0) {
             nout = 0;
@@ -418,9 +423,9 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
             const uint32_t flh = pflags[ph];
             float Hx[P + 1], Hy[P + 1], Hz[P + 1];
             int hs[3];
-            hs[0] = stencil_fast<P>(Xc[3 * ph], inv[0], pp.quirk4, Hx);
-            hs[1] = stencil_fast<P>(Xc[3 * ph + 1], inv[1], pp.quirk4, Hy);
-            hs[2] = stencil_fast_z<P>(Xc[3 * ph + 2], inv[2], pp.quirk4, Hz, g.nz);
+            hs[0] = stencil_fast<P>(Xc[3 * ph], g, 0, pp.quirk4, Hx);
+            hs[1] = stencil_fast<P>(Xc[3 * ph + 1], g, 1, pp.quirk4, Hy);
+            hs[2] = stencil_fast_z<P>(Xc[3 * ph + 2], g, pp.quirk4, Hz);
             for (int h = 0; h < pp.nfg; h++)
                 if ((flh >> (8 + h)) & 1u) gather_global<P, false>(g, rec + (long long)h * g.M, hs, Hx, Hy, Hz, Ao[threadIdx.x][h]);
         }
@@ -437,9 +442,9 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
         const float qp = (act && q) ? q[p] : 0.f;
         float Wx[P + 1], Wy[P + 1], Wz[P + 1];
         if (fm) {
-            stencil_fast<P>(x[0], inv[0], pp.quirk4, Wx);
-            stencil_fast<P>(x[1], inv[1], pp.quirk4, Wy);
-            stencil_fast_z<P>(x[2], inv[2], pp.quirk4, Wz, g.nz);
+            stencil_fast<P>(x[0], g, 0, pp.quirk4, Wx);
+            stencil_fast<P>(x[1], g, 1, pp.quirk4, Wy);
+            stencil_fast_z<P>(x[2], g, pp.quirk4, Wz);
         }
         // 5. gather each force group in group order
         bool first = true;

@@ -20,10 +20,10 @@ Pool::~Pool()
         std::lock_guard<std::mutex> lk(mu);
         stop = true;
         for (Job *j : queue) {   // never admitted: cancelled
-            j->state = JOB_FAILED;
+            j->state = JOB_CANCELLED;
             j->err = "cancelled: the pool was destroyed";
             j->box.reset();
-            nFailed++;
+            nCancelled++;
         }
         queue.clear();
     }
@@ -55,9 +55,6 @@ int64_t Pool::submit(Box *box, int64_t nsteps)
     if (box->initialized()) fail(TILD_ERR_STATE, "submit a box before endBox: the pool allocates it on admission");
     box->prepareHost();   // script checks and the plan; nothing on the device yet
     const int64_t bytes = box->deviceBytesEstimate();
-    if (bytes > budget)
-        fail(TILD_ERR_ARG, "the job needs about " + std::to_string(bytes) + " bytes of device memory; the pool's budget is " +
-                               std::to_string(budget));
     auto j = std::make_unique<Job>();
     j->N = box->nstot;
     j->nsteps = nsteps;
@@ -68,6 +65,9 @@ int64_t Pool::submit(Box *box, int64_t nsteps)
     {
         std::lock_guard<std::mutex> lk(mu);
         if (stop) fail(TILD_ERR_STATE, "the pool is shutting down");
+        if (bytes > budget)
+            fail(TILD_ERR_ARG, "the job needs about " + std::to_string(bytes) +
+                                   " bytes of device memory; the pool's budget is " + std::to_string(budget));
         id = nextId++;
         j->id = id;
         j->box.reset(box);   // adopted: nothing below can fail
@@ -97,8 +97,66 @@ void Pool::wait(int64_t id)
 {
     std::unique_lock<std::mutex> lk(mu);
     Job *j = find(id);
-    cvDone.wait(lk, [&] { return j->state == JOB_DONE || j->state == JOB_FAILED; });
+    cvDone.wait(lk, [&] { return j->state == JOB_DONE || j->state == JOB_FAILED || j->state == JOB_CANCELLED; });
     if (j->state == JOB_FAILED) fail(TILD_ERR_STATE, "job " + std::to_string(id) + " failed: " + j->err);
+    if (j->state == JOB_CANCELLED) fail(TILD_ERR_STATE, "job " + std::to_string(id) + " was cancelled");
+}
+
+void Pool::cancel(int64_t id)
+{
+    std::unique_ptr<Box> drop;   // a queued job's box, freed after the lock (host memory only)
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        Job *j = find(id);
+        if (j->state == JOB_DONE || j->state == JOB_FAILED || j->state == JOB_CANCELLED)
+            fail(TILD_ERR_STATE, "job " + std::to_string(id) + " has already finished");
+        auto it = std::find(queue.begin(), queue.end(), j);
+        if (it != queue.end()) {   // never admitted: nothing on the device yet
+            queue.erase(it);
+            drop = std::move(j->box);
+            j->state = JOB_CANCELLED;
+            j->err = "cancelled";
+            j->tDone = now();
+            nCancelled++;
+            cvDone.notify_all();
+        } else {
+            // being admitted or running: the scheduler thread drains its in-flight chunks,
+            // frees its arena and reports it cancelled
+            j->cancel = true;
+        }
+    }
+    cvWork.notify_all();
+}
+
+void Pool::setBudget(int64_t bytes)
+{
+    if (bytes < 0) fail(TILD_ERR_ARG, "the budget must be >= 0");
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        budget = bytes;
+        failOversizedLocked();
+    }
+    cvWork.notify_all();
+}
+
+// Queued jobs that can never fit the budget fail now instead of blocking the queue.
+void Pool::failOversizedLocked()
+{
+    for (auto it = queue.begin(); it != queue.end();) {
+        Job *j = *it;
+        if (j->bytes > budget) {
+            j->state = JOB_FAILED;
+            j->err = "the job needs about " + std::to_string(j->bytes) + " bytes of device memory; the pool's budget is now " +
+                     std::to_string(budget);
+            j->tDone = now();
+            j->box.reset();
+            nFailed++;
+            it = queue.erase(it);
+        } else {
+            ++it;
+        }
+    }
+    cvDone.notify_all();
 }
 
 void Pool::result(int64_t id, float *x, double *thermo, int nthermo, int *nwritten)
@@ -117,7 +175,8 @@ void Pool::release(int64_t id)
 {
     std::lock_guard<std::mutex> lk(mu);
     Job *j = find(id);
-    if (j->state != JOB_DONE && j->state != JOB_FAILED) fail(TILD_ERR_STATE, "job " + std::to_string(id) + " is still in the pool");
+    if (j->state != JOB_DONE && j->state != JOB_FAILED && j->state != JOB_CANCELLED)
+        fail(TILD_ERR_STATE, "job " + std::to_string(id) + " is still in the pool");
     jobs.erase(id);
 }
 
@@ -126,7 +185,7 @@ void Pool::stats(std::vector<int64_t> &out) const
     std::lock_guard<std::mutex> lk(mu);
     int64_t running = 0;
     for (auto &kv : jobs) running += kv.second->state == JOB_RUNNING;
-    out = {(int64_t)queue.size(), running, nDone, nFailed, inUse, budget};
+    out = {(int64_t)queue.size(), running, nDone, nFailed, inUse, budget, nCancelled};
 }
 
 // ---- scheduler thread ----
@@ -141,6 +200,22 @@ void Pool::failJob(Job *j, const std::string &msg)
     j->state = JOB_FAILED;
     j->tDone = now();
     nFailed++;
+    cvDone.notify_all();
+}
+
+// A running job whose cancel was requested: let its in-flight chunks finish (each is a
+// bounded number of captured steps), then free its arena like a finished job's.
+void Pool::finishCancel(Job *j)
+{
+    cudaStreamSynchronize(j->box->cudaStreamHandle());
+    dropEvents(j);
+    j->box.reset();
+    std::lock_guard<std::mutex> lk(mu);
+    inUse -= j->bytes;
+    j->err = "cancelled";
+    j->state = JOB_CANCELLED;
+    j->tDone = now();
+    nCancelled++;
     cvDone.notify_all();
 }
 
@@ -243,6 +318,7 @@ void Pool::run()
         {
             std::unique_lock<std::mutex> lk(mu);
             if (stop && queue.empty() && active.empty()) break;
+            failOversizedLocked();
             // at most two admissions per pass, so the running jobs keep getting work while
             // new ones are set up
             while (!queue.empty() && toAdmit.size() < 2 && (int)(active.size() + toAdmit.size()) < maxActive &&
@@ -262,6 +338,12 @@ void Pool::run()
         bool progressed = !toAdmit.empty();
         for (size_t i = 0; i < active.size();) {
             Job *j = active[i];
+            if (j->cancel) {
+                finishCancel(j);
+                active.erase(active.begin() + i);
+                progressed = true;
+                continue;
+            }
             bool finished = false;
             try {
                 pump(j, progressed);

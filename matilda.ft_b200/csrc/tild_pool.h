@@ -11,6 +11,7 @@
 // queued job can enter at once.
 #pragma once
 
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -25,14 +26,16 @@
 
 namespace tild {
 
-enum JobState { JOB_QUEUED = 0, JOB_RUNNING = 1, JOB_DONE = 2, JOB_FAILED = 3 };
+enum JobState { JOB_QUEUED = 0, JOB_RUNNING = 1, JOB_DONE = 2, JOB_FAILED = 3, JOB_CANCELLED = 4 };
 
 struct Job {
     int64_t id = 0;
     std::unique_ptr<Box> box;
-    int64_t nsteps = 0, issued = 0, done = 0;
+    int64_t nsteps = 0, issued = 0;       // issued: scheduler thread only
+    std::atomic<int64_t> done{0};         // steps finished on the GPU (read by status())
+    std::atomic<bool> cancel{false};      // a cancel request for a running job
     int64_t bytes = 0, N = 0, chunk = 1;
-    int state = JOB_QUEUED;
+    int state = JOB_QUEUED;               // written under the pool's mutex
     double tSubmit = 0.0, tAdmit = 0.0, tDone = 0.0;   // seconds since the pool was created
     std::deque<std::pair<cudaEvent_t, int64_t>> inflight;   // chunk end events and their steps
     std::vector<cudaEvent_t> spare;
@@ -50,7 +53,10 @@ public:
     void wait(int64_t id);
     void result(int64_t id, float *x, double *thermo, int nthermo, int *nwritten);
     void release(int64_t id);
-    void stats(std::vector<int64_t> &out) const;   // queued, running, done, failed, bytes in use, budget
+    void cancel(int64_t id);                       // queued: dropped; running: drained, then freed
+    void setBudget(int64_t bytes);                 // admissions from now on; running jobs stay
+    // queued, running, done, failed, bytes in use, budget, cancelled
+    void stats(std::vector<int64_t> &out) const;
 
 private:
     void run();
@@ -58,6 +64,8 @@ private:
     void pump(Job *j, bool &progressed);
     void harvest(Job *j);
     void failJob(Job *j, const std::string &msg);
+    void finishCancel(Job *j);
+    void failOversizedLocked();
     void dropEvents(Job *j);
     double now() const;
     Job *find(int64_t id) const;
@@ -71,7 +79,7 @@ private:
     std::deque<Job *> queue;
     std::vector<Job *> active;   // touched by the scheduler thread only
     int64_t inUse = 0, nextId = 1;
-    int nDone = 0, nFailed = 0;
+    int nDone = 0, nFailed = 0, nCancelled = 0;
     bool stop = false;
     cudaMemPool_t memPool = nullptr;   // arenas of the jobs; keeps freed memory up to the budget
     std::chrono::steady_clock::time_point t0;

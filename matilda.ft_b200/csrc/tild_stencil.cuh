@@ -60,24 +60,31 @@ __device__ __forceinline__ int stencil_axis(float x, float d, int quirk4, float 
     return g - P / 2;
 }
 
-// Fast stencil for the deposit and the gather: same cell choice and the same spline
+// Fast stencil for the deposit and the gather: the reference's cell choice and spline
 // polynomials, evaluated with a reciprocal multiply and Horner FMAs instead of IEEE
-// divisions.  Weights differ from the reference's by rounding only (the splines are
-// continuous across cell edges, so a different cell pick at an edge moves nothing).
+// divisions.  The cell is picked from t = x / d; the offset inside it is then taken from
+// x - c d with d split into its FP32 value and the FP32 remainder of L / Nx (g.dxf, g.dlo),
+// each product folded in by one FMA, so the offset carries an error of a few units in the
+// last place of d instead of t's rounding (which grows with x: about 1e-5 of a cell at
+// x / d = 160).  Weights therefore differ from exact B-spline weights at the FP64 position
+// by rounding only, and from the reference's by its own rounding (the splines are continuous
+// across cell edges, so a different cell pick at an edge moves nothing).
 // Returns the first stencil index; W[0..P] are the 1-D weights (unscaled, sum 1).
 template <int P>
-__device__ __forceinline__ int stencil_fast(float x, float inv_d, int quirk4, float *W)
+__device__ __forceinline__ int stencil_fast(float x, const Geom &g, int j, int quirk4, float *W)
 {
+    const float inv_d = g.inv[j];
     const float t = x * inv_d;
-    int g;
-    float s;
+    int g0;
+    float c;
     if (P % 2 == 0) {
-        g = (int)(t + 0.5f);
-        s = t - (float)g;
+        g0 = (int)(t + 0.5f);
+        c = (float)g0;
     } else {
-        g = (int)t;
-        s = t - (float)g - 0.5f;
+        g0 = (int)t;
+        c = (float)g0 + 0.5f;
     }
+    const float s = __fmaf_rn(-c, g.dlo[j], __fmaf_rn(-c, g.dxf[j], x)) * inv_d;
     if (P == 0) {
         W[0] = 1.f;
     } else if (P == 1) {
@@ -101,7 +108,7 @@ __device__ __forceinline__ int stencil_fast(float x, float inv_d, int quirk4, fl
         W[3] = (19.f + 44.f * s + 24.f * s2 - 16.f * s3 - 16.f * s4) * (1.f / 96.f);
         W[4] = (1.f + 8.f * s + 24.f * s2 + 32.f * s3 + 16.f * s4) * (1.f / 384.f);
     }
-    return g - P / 2;
+    return g0 - P / 2;
 }
 
 // -------------------------------------------------------------------------------------
@@ -131,22 +138,22 @@ __device__ __forceinline__ int unwrap_delta(int d, int n)
     return t;
 }
 
-// first stencil index of the fast stencil (same arithmetic as stencil_fast)
+// first stencil index of the fast stencil (same cell choice as stencil_fast)
 template <int P>
-__device__ __forceinline__ int stencil_origin(float x, float inv_d)
+__device__ __forceinline__ int stencil_origin(float x, const Geom &g, int j)
 {
-    const float t = x * inv_d;
-    const int g = (P % 2 == 0) ? (int)(t + 0.5f) : (int)t;
-    return g - P / 2;
+    const float t = x * g.inv[j];
+    const int g0 = (P % 2 == 0) ? (int)(t + 0.5f) : (int)t;
+    return g0 - P / 2;
 }
 
 // The z axis of a 2-D box is one plane (nz == 1, every particle at z = 0): its stencil is
 // the single point 0 with weight 1 (the z loops still run over P + 1 points, the others
 // with weight 0), so products Wx*Wy*Wz are exactly the 2-D weights Wx*Wy.
 template <int P>
-__device__ __forceinline__ int stencil_fast_z(float z, float inv_d, int quirk4, float *W, int nz)
+__device__ __forceinline__ int stencil_fast_z(float z, const Geom &g, int quirk4, float *W)
 {
-    if (nz != 1) return stencil_fast<P>(z, inv_d, quirk4, W);
+    if (g.nz != 1) return stencil_fast<P>(z, g, 2, quirk4, W);
     W[0] = 1.f;
 #pragma unroll
     for (int k = 1; k <= P; k++) W[k] = 0.f;
@@ -164,9 +171,9 @@ __device__ __forceinline__ int stencil_axis_z(float z, float d, int quirk4, floa
 }
 
 template <int P>
-__device__ __forceinline__ int stencil_origin_z(float z, float inv_d, int nz)
+__device__ __forceinline__ int stencil_origin_z(float z, const Geom &g)
 {
-    return nz == 1 ? 0 : stencil_origin<P>(z, inv_d);
+    return g.nz == 1 ? 0 : stencil_origin<P>(z, g, 2);
 }
 
 // [b0, b1) of the CTA: a tile of sorted particles, or a fixed window of slots

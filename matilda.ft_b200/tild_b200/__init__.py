@@ -50,6 +50,8 @@ _SIGS = {
     "tild_box_get_positions": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "tild_box_set_positions": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "tild_box_get_density": ([ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+    "tild_box_modify": ([ctypes.c_void_p, ctypes.c_char_p], ctypes.c_int),
+    "tild_box_get_grid_force": ([ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p], ctypes.c_int),
     "tild_box_get_density_noalloc": ([ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p],
                                      ctypes.c_int),
     "tild_box_grid_weights": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
@@ -71,6 +73,8 @@ _SIGS = {
     "tild_pool_result": ([ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                           ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
     "tild_pool_release": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
+    "tild_pool_cancel": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
+    "tild_pool_set_budget": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
     "tild_pool_stats": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32], ctypes.c_int),
 }
 
@@ -237,6 +241,18 @@ class Box:
         _check(lib().tild_box_get_density(self._h, group.encode(), int(bool(charge)), _ptr(rho)))
         return rho
 
+    def modify(self, rest: str):
+        """A top-level `modify` line (without the word), e.g. "potential remove 1"."""
+        _check(lib().tild_box_modify(self._h, rest.encode()))
+
+    def grid_force(self, group: str):
+        """PS_Group::d_gridForce of the last force evaluation, shape (M, Dim), x fastest."""
+        i = self.info()
+        D = int(i.dim)
+        gf = np.zeros((int(i.nx[0]) * int(i.nx[1]) * int(i.nx[2]), D), np.float32)
+        _check(lib().tild_box_get_grid_force(self._h, group.encode(), _ptr(gf)))
+        return gf
+
     def density_noalloc(self, group: str, charge=False):
         """density() through the allocation-free entry point (static device scratch)."""
         i = self.info()
@@ -272,7 +288,7 @@ def run_script_file(path: str, device: int = 0):
     _check(lib().tild_run_script_file(path.encode(), int(device)))
 
 
-JOB_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed"}
+JOB_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
 
 
 class Pool:
@@ -328,10 +344,19 @@ class Pool:
     def release(self, job: int):
         _check(lib().tild_pool_release(self._h, int(job)))
 
+    def cancel(self, job: int):
+        """Cancel a queued or running job (running: its in-flight chunks finish first)."""
+        _check(lib().tild_pool_cancel(self._h, int(job)))
+
+    def set_budget(self, mem_budget_bytes: int):
+        """New memory budget for admissions from now on."""
+        _check(lib().tild_pool_set_budget(self._h, int(mem_budget_bytes)))
+
     def stats(self) -> dict:
-        v = np.zeros(6, np.int64)
-        _check(lib().tild_pool_stats(self._h, _ptr(v), 6))
-        return dict(zip(("queued", "running", "done", "failed", "bytes_in_use", "budget"), (int(a) for a in v)))
+        v = np.zeros(7, np.int64)
+        _check(lib().tild_pool_stats(self._h, _ptr(v), 7))
+        return dict(zip(("queued", "running", "done", "failed", "bytes_in_use", "budget", "cancelled"),
+                        (int(a) for a in v)))
 
 
 def box_from_spec(spec, device=0, options=None, steps_script=False, base_dir=None):

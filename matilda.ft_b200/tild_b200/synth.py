@@ -35,10 +35,11 @@ def chain_bonds(nchains, nper, offset=0):
 def potential_command(p):
     """Script line of one potential spec (dict with kind and its parameters)."""
     k = p["kind"]
+    ramp = (" ramp %.9g" % p["ramp"]) if "ramp" in p else ""
     if k == "gaussian":
-        return "potential gaussian %s %s %.9g %.9g" % (p["I"], p["J"], p["A"], p["sigma"])
+        return "potential gaussian %s %s %.9g %.9g" % (p["I"], p["J"], p["A"], p["sigma"]) + ramp
     if k in ("erf2", "erfG"):
-        return "potential %s %s %s %.9g %.9g %.9g" % (k, p["I"], p["J"], p["A"], p["Rp"], p["sigma"])
+        return "potential %s %s %s %.9g %.9g %.9g" % (k, p["I"], p["J"], p["A"], p["Rp"], p["sigma"]) + ramp
     if k == "charges":
         return "potential charges %.9g %.9g" % (p["lB"], p["sigma"])
     if k == "wall":   # potential wall <group> <axis> <position> <side +1|-1> <k>
@@ -52,7 +53,7 @@ class SystemSpec:
     def __init__(self, name, L, grid, x, types, species, bonds, mol, charges=None,
                  potentials=(), order=3, delt=0.005, bond_k=1.5, bond_req=0.0, seed=1,
                  dim=3, integrator="GJF", masses=None, mobility=None, log_freq=100, angles=None,
-                 angle_types=None, angle_params=()):
+                 angle_types=None, angle_params=(), bond_style="harmonic"):
         self.name = name
         self.L = np.asarray(L, np.float32)
         self.grid = np.asarray(grid, np.int32)
@@ -67,6 +68,7 @@ class SystemSpec:
         self.delt = delt
         self.bond_k = bond_k
         self.bond_req = bond_req
+        self.bond_style = bond_style   # "harmonic" or "fene" (ps_deviceBonds.cu:54-62)
         self.seed = seed
         self.dim = dim
         self.integrator = integrator
@@ -143,8 +145,12 @@ class SystemSpec:
             fh.write("\n")
         del arr, body
 
-    def script(self, data_name, steps=100, extra=()):
-        """Current-grammar input script (PS_Box_initialization.cu:68-339)."""
+    def bond_command(self):
+        return "bond 1 %s %.9g %.9g" % (self.bond_style, self.bond_k, self.bond_req)
+
+    def script(self, data_name, steps=100, extra=(), tail=None):
+        """Current-grammar input script (PS_Box_initialization.cu:68-339).  After endBox:
+        `run nvt <steps>`, or the top-level lines ``tail`` (run / modify, main.cu:96-151)."""
         D = self.dim
         s = ["box ps", "Dim %d" % D,
              "boxLengths " + " ".join("%.9g" % v for v in self.L[:D]),
@@ -156,23 +162,23 @@ class SystemSpec:
             s.append("species %s mass %.9g mobility %.9g" % (lb, self.masses[t], self.mobility[t]))
         s.append("readData %s" % data_name)
         if len(self.bonds):
-            s.append("bond 1 harmonic %.9g %.9g" % (self.bond_k, self.bond_req))
+            s.append(self.bond_command())
         s += self.angle_commands()
         s += [potential_command(p) for p in self.potentials]
         s.append("integrator all %s delt %.9g" % (self.integrator, self.delt))
         s.append("logFreq %d" % self.log_freq)
         s += list(extra)
         s.append("endBox")
-        s.append("run nvt %d" % steps)
+        s += ["run nvt %d" % steps] if tail is None else list(tail)
         return "\n".join(s) + "\n"
 
-    def write(self, directory, steps=100, extra=()):
+    def write(self, directory, steps=100, extra=(), tail=None):
         os.makedirs(directory, exist_ok=True)
         data = os.path.join(directory, self.name + ".data")
         self.write_data(data)
         scr = os.path.join(directory, self.name + ".in")
         with open(scr, "w") as fh:
-            fh.write(self.script(os.path.basename(data), steps, extra))
+            fh.write(self.script(os.path.basename(data), steps, extra, tail))
         return scr, data
 
     # -- compact partner lists (both directions, like readDataConfig :897-926) ------
@@ -328,14 +334,15 @@ def chain_angles(nchains, nper, offset=0):
 
 
 def small_system(seed=0, n_chains=20, nper=8, L=6.0, grid=(12, 12, 12), order=3, charges=False,
-                 dim=3, pots=None, n_free=0, angle_params=None):
-    """A tiny randomised system for oracle comparisons."""
+                 dim=3, pots=None, n_free=0, angle_params=None, bond_rms=1.0, **spec_kw):
+    """A tiny randomised system for oracle comparisons.  spec_kw go to SystemSpec
+    (integrator, bond_style, bond_k, bond_req, ...)."""
     rng = np.random.default_rng(seed)
     Lv = np.array([L, L * 1.1, L * 0.9][:dim] + [1.0] * (3 - dim))
     if dim == 3:
-        x = random_walk_chains(rng, n_chains, nper, Lv)
+        x = random_walk_chains(rng, n_chains, nper, Lv, bond_rms)
     else:
-        x3 = random_walk_chains(rng, n_chains, nper, np.r_[Lv[:2], 1.0])
+        x3 = random_walk_chains(rng, n_chains, nper, np.r_[Lv[:2], 1.0], bond_rms)
         x = x3
     if n_free:
         x = np.concatenate([x, rng.uniform(0, 1, size=(n_free, 3)) * Lv])
@@ -361,4 +368,4 @@ def small_system(seed=0, n_chains=20, nper=8, L=6.0, grid=(12, 12, 12), order=3,
     return SystemSpec("small%d" % seed, Lv, grid, x[:, :dim] if dim == 2 else x, types, ["A", "B"],
                       chain_bonds(n_chains, nper), mol, charges=q, potentials=pots, order=order,
                       seed=seed + 11, dim=dim, angles=ang, angle_types=atyp,
-                      angle_params=angle_params or ())
+                      angle_params=angle_params or (), **spec_kw)

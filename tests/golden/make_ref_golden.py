@@ -11,6 +11,13 @@ in place), and pack the inputs plus what the reference computed into DIR/ref_<na
   f0                            PS_Box::forces() at the initial positions
   energies                      [Ubond, CalcEnergy() of each potential]
   x100                          positions after 100 doTimeStep calls (cuRAND XORWOW noise)
+  energies_final                [Ubond, CalcEnergy() of each remaining potential] at the end
+  bond_cmd, integrator          the bond and integrator words of the script
+Systems with RUNS below execute their script's top-level lines instead (`run nvt N` through
+PS_Box::NVT, `modify potential remove i` through PS_Box::modifyBox, main.cu:96-151); they add
+  tail                          those lines
+  ps_data                       the ps_data.dat the runs wrote (text)
+and x100 then holds the positions after the last run.
 The committed fixtures under tests/golden/ were produced by this script.
 """
 import argparse
@@ -52,7 +59,27 @@ def systems():
         "d2_o3": synth.small_system(seed=38, order=3, charges=True, dim=2, grid=(16, 18, 1)),
         "d2_o4": synth.small_system(seed=39, order=4, dim=2, grid=(15, 12, 1), angle_params=[
             dict(style="harmonic", k=2.0, theta=110.0)]),
+        # Euler-Maruyama (ps_integratorEM.cu:39-82: noise sqrt(2 dt), mass and mobility unused)
+        "em_o3": synth.small_system(seed=45, order=3, charges=True, integrator="EM"),
+        # FENE bonds (ps_deviceBonds.cu:60-62), chains with shorter bonds than r0
+        "fene_o3": synth.small_system(seed=42, order=3, bond_rms=0.8, bond_style="fene", bond_k=1.5,
+                                      bond_req=2.5),
+        # ramped amplitudes (ps_potential.cu:227-248): the table is rescaled to
+        # A(t) / Re u(0), which for erf2 and erfG is not A (run through NVT, maxSteps = 100)
+        "ramp_o3": synth.small_system(seed=43, order=3, pots=[
+            dict(kind="erf2", I="A", J="B", A=0.05, Rp=1.0, sigma=0.5, ramp=0.4),
+            dict(kind="erfG", I="B", J="B", A=0.3, Rp=0.8, sigma=0.5, ramp=0.05),
+            dict(kind="gaussian", I="A", J="A", A=1.0, sigma=0.7, ramp=3.0)]),
+        # modify potential remove between two runs (PS_Box.cu:848-870)
+        "modify_o3": synth.small_system(seed=44, order=3, charges=True),
     }
+
+
+# systems whose script's top-level lines run (main.cu:96-151) instead of NSTEPS doTimeStep calls
+RUNS = {
+    "ramp_o3": ["run nvt %d" % NSTEPS],
+    "modify_o3": ["run nvt 40", "modify potential remove 1", "run nvt 60"],
+}
 
 
 def read_data_positions(path, n, dim, charges):
@@ -70,12 +97,15 @@ def read_data_positions(path, n, dim, charges):
 
 def run(harness, name, spec, out, time_steps=0):
     with tempfile.TemporaryDirectory() as d:
-        spec.log_freq = 1000000
-        scr, data = spec.write(d, steps=NSTEPS)
+        tail = RUNS.get(name)
+        spec.log_freq = 1000000 if tail is None else 10
+        scr, data = spec.write(d, steps=NSTEPS, tail=tail)
         dump = os.path.join(d, "dump")
         os.makedirs(dump)
-        r = subprocess.run([os.path.abspath(harness), os.path.basename(scr), dump, str(NSTEPS), str(time_steps)],
-                           cwd=d, capture_output=True, text=True, timeout=1800)
+        cmd = [os.path.abspath(harness), os.path.basename(scr), dump, str(NSTEPS), str(time_steps)]
+        if tail is not None:
+            cmd.append("script")
+        r = subprocess.run(cmd, cwd=d, capture_output=True, text=True, timeout=1800)
         if r.returncode != 0:
             raise RuntimeError("%s: harness failed rc=%d\n%s" % (name, r.returncode, r.stderr[-2000:]))
         meta = {}
@@ -96,7 +126,12 @@ def run(harness, name, spec, out, time_steps=0):
             W=ld("gridW.f32", np.float32).reshape(N, G)[:NSTENCIL],
             f0=ld("f0.f32", np.float32).reshape(N, D), energies=ld("energies.f64", np.float64),
             x100=ld("x_final.f32", np.float32).reshape(N, D), gvol=np.float64(meta["gvol"]),
+            energies_final=ld("energies_final.f64", np.float64), bond_cmd=np.array(spec.bond_command()),
+            integrator=np.array(spec.integrator),
             groups=np.array(groups), cuda_error=np.array(meta.get("cuda_error", "")))
+        if tail is not None:
+            res["tail"] = np.array(tail)
+            res["ps_data"] = np.array(open(os.path.join(d, "ps_data.dat")).read())
         if spec.charges is not None:
             res["q"] = spec.charges
             res["rhoq"] = ld("rhoq_charges.f32", np.float32)

@@ -50,3 +50,24 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys):
     args = bench.argparse.Namespace(scale=1.0, steps=3, warmup=3, ref_budget=1.0)
     assert bench.run_reference(args) == 0
     assert capsys.readouterr().out == ""
+
+
+def test_reference_arm_line_matches_ours_without_the_reference_build(monkeypatch, capsys, tmp_path):
+    """Where oracle/_ref holds no reference build the arm falls back to the host port and
+    says so; its config carries the same keys as our arm's."""
+    import json
+    monkeypatch.setenv("WORLD_SIZE", "1")
+    monkeypatch.setenv("RANK", "0")
+    monkeypatch.setattr(bench, "harness_path", lambda: str(tmp_path / "absent"))
+    args = bench.argparse.Namespace(scale=1.0 / 256, steps=1, warmup=0, ref_budget=5.0, gpus=1, no_batch=True)
+    assert bench.run_reference(args) == 0
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["cpu_baseline"]["kind"] == "port"
+    assert "absent" in line["cpu_baseline"]["sample"]
+    assert set(line["config"]) == set(bench.bench_config(bench.make_spec(1.0), 1))
+    assert line["e2e"]["value"] == line["value"]
+
+
+def test_every_kth_spreads_the_sample():
+    assert bench.every_kth(list(range(64)), 16) == list(range(0, 64, 4))
+    assert bench.every_kth([1, 2, 3], 8) == [1, 2, 3]

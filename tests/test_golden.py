@@ -9,7 +9,11 @@ Tolerances: stencil indices and weights bit-exact (FP32 restatement with the ref
 FMA contractions); densities 1e-5 * max (the reference sums ~20 FP32 terms per point in atomic order); forces 1e-5 (per-particle metric, conftest);
 energies 1e-5 relative; 100-step trajectories in cuRAND-compatible mode max |dx| <= 2e-3,
 median <= 1e-4 (FP32 rounding of two different FFTs grows chaotically; the FP32
-restatement itself drifts 4.7e-4 from FP64 over 100 steps).
+restatement itself drifts 4.7e-4 from FP64 over 100 steps); energies at the end of the
+trajectory and the ps_data.dat rows logged along it 1e-4 relative (the same drift).
+
+Fixtures with a `tail` ran their script's top-level lines (`run nvt N`, `modify potential
+remove i`) through PS_Box::NVT and PS_Box::modifyBox; the GPU test replays those lines.
 """
 import ast
 import glob
@@ -40,12 +44,15 @@ def load(path):
     pots = [ast.literal_eval(s) for s in z["potentials"]]
     q = z["q"] if "q" in z.files else None
     D = z["x"].shape[1]
+    bw = str(z["bond_cmd"]).split() if "bond_cmd" in z.files else ["bond", "1", "harmonic", "1.5", "0.0"]
     sysm = oracle.System(Dim=D, L=z["L"][:D].astype(np.float32), Nx=z["grid"][:D].astype(np.int32),
                          order=int(z["order"]),
                          x=z["x"], types=z["types"], mass=np.ones(2, np.float32), mobility=np.ones(2, np.float32),
                          species=["A", "B"], charges=q, nb=nb, partner=partner, btype=np.zeros_like(partner),
-                         bond_k=np.array([1.5], np.float32), bond_req=np.array([0.0], np.float32),
-                         bond_style=np.array([0], np.int32), potentials=pots, delt=float(z["delt"]))
+                         bond_k=np.array([float(bw[3])], np.float32), bond_req=np.array([float(bw[4])], np.float32),
+                         bond_style=np.array([0 if bw[2] == "harmonic" else 1], np.int32), potentials=pots,
+                         delt=float(z["delt"]),
+                         integrator=str(z["integrator"]) if "integrator" in z.files else "GJF")
     if "angles" in z.files:
         ap = [ast.literal_eval(a) for a in z["angle_params"]]
         sysm.angles = z["angles"].astype(np.int64)
@@ -109,7 +116,7 @@ def _box(z, sysm, **opts):
     b.command("species A")
     b.command("species B")
     b.set_particles(z["x"], z["types"], z["mol"], sysm.charges)
-    b.command("bond 1 harmonic 1.5 0.0")
+    b.command(str(z["bond_cmd"]) if "bond_cmd" in z.files else "bond 1 harmonic 1.5 0.0")
     b.set_bonds(z["bonds"])
     if "angles" in z.files:
         for t, a in enumerate(ast.literal_eval(x) for x in z["angle_params"]):
@@ -119,7 +126,10 @@ def _box(z, sysm, **opts):
     from tild_b200 import synth
     for p in sysm.potentials:
         b.command(synth.potential_command(p))
-    b.command("integrator all GJF delt %.9g" % float(z["delt"]))
+    b.command("integrator all %s delt %.9g" % (str(z["integrator"]) if "integrator" in z.files else "GJF",
+                                                float(z["delt"])))
+    if "tail" in z.files:
+        b.command("logFreq 10")
     b.command("endBox")
     return b
 
@@ -142,8 +152,31 @@ def test_gpu_forces_match_reference(path):
 def test_gpu_curand_compatible_trajectory_matches_reference(path):
     z, sysm = load(path)
     with _box(z, sysm, rng=1) as b:
-        b.step(100)
+        if "tail" in z.files:   # the script's own runs (main.cu:96-151)
+            for line in z["tail"]:
+                w = str(line).split()
+                if w[0] == "run":
+                    b.run_nvt(int(w[2]))
+                elif w[0] == "modify":
+                    b.modify(" ".join(w[1:]))
+        else:
+            b.step(100)
         x = b.positions()
+        th = b.thermo() if "energies_final" in z.files else None
+        log = b.log() if "ps_data" in z.files else None
     d = np.abs(x - z["x100"])
     d = np.minimum(d, z["L"][: d.shape[1]] - d)
     assert d.max() <= 2e-3 and np.median(d) <= 1e-4, (d.max(), np.median(d))
+    if th is not None:   # Ubond and every remaining potential's energy after the run
+        ref = z["energies_final"]
+        assert abs(th["Ubond"] - ref[0]) <= 1e-4 * abs(ref[0])
+        assert len(th["potentials"]) == len(ref) - 1
+        for a, r in zip(th["potentials"], ref[1:]):
+            assert abs(a - r) <= 1e-4 * abs(r) + 1e-9, (a, r)
+    if log is not None:   # ps_data.dat rows: step, Ubond, each potential (PS_Box.cu:339-370)
+        rows = [list(map(float, ln.split())) for ln in str(z["ps_data"]).splitlines() if ln.strip()]
+        assert [r[0] for r in rows] == list(log[:, 0])
+        for got, ref in zip(log, rows):
+            n = len(ref)
+            assert not np.any(got[n:]), "columns of a removed potential"
+            assert np.allclose(got[1:n], ref[1:], rtol=1e-4, atol=1e-9), (got, ref)

@@ -100,3 +100,110 @@ def test_pool_refuses_a_job_larger_than_its_budget():
         b.step(2)
         assert np.isfinite(b.positions()).all()
         b.close()
+
+
+def _submit(pool, spec, nsteps, **opts):
+    o = {"write_files": 0, "sort_interval": 3, "deterministic": 1}
+    o.update(opts)
+    b = tild_b200.box_from_spec(spec, options=o)
+    jid = pool.submit(b, nsteps)
+    b.close()
+    return jid
+
+
+def _wait_until(pred, timeout=60.0):
+    import time
+    t0 = time.time()
+    while not pred():
+        assert time.time() - t0 < timeout, "condition not reached"
+        time.sleep(0.005)
+
+
+def test_cancel_a_running_job_frees_it_and_leaves_the_others_alone():
+    spec = SPECS["diblock_o3"]()
+    other = SPECS["charged_o4"]()
+    with tild_b200.Pool(mem_budget_bytes=8 << 30) as pool:
+        long_job = _submit(pool, spec, 10 ** 7)          # would run for minutes
+        keep = _submit(pool, other, NSTEPS)
+        _wait_until(lambda: pool.status(long_job)["steps_done"] > 0)
+        pool.cancel(long_job)
+        with pytest.raises(tild_b200.TildError, match="cancelled"):
+            pool.wait(long_job)
+        st = pool.status(long_job)
+        assert st["state"] == "cancelled" and 0 < st["steps_done"] < 10 ** 7
+        with pytest.raises(tild_b200.TildError, match="already finished"):
+            pool.cancel(long_job)
+        pool.wait(keep)
+        x, th = pool.result(keep, other.N)
+        s = pool.stats()
+        assert s["cancelled"] == 1 and s["done"] == 1 and s["bytes_in_use"] == 0 and s["running"] == 0
+        pool.release(long_job)
+    xa, tha = alone(other, deterministic=1)
+    assert np.array_equal(xa, x) and np.array_equal(tha[: len(th)], th)
+
+
+def test_cancel_a_queued_job():
+    with tild_b200.Pool(mem_budget_bytes=8 << 30, max_active=1) as pool:
+        running = _submit(pool, SPECS["diblock_o3"](), 10 ** 7)
+        queued = _submit(pool, SPECS["erf_o2"](), NSTEPS)
+        _wait_until(lambda: pool.status(running)["state"] == "running")
+        assert pool.status(queued)["state"] == "queued"
+        pool.cancel(queued)
+        st = pool.status(queued)
+        assert st["state"] == "cancelled" and st["steps_done"] == 0 and st["admit_s"] == 0.0
+        pool.cancel(running)
+        with pytest.raises(tild_b200.TildError, match="cancelled"):
+            pool.wait(running)
+        assert pool.stats()["cancelled"] == 2 and pool.stats()["bytes_in_use"] == 0
+
+
+def test_a_stalled_producer_does_not_hold_back_running_jobs():
+    """Jobs submitted with long pauses between them: the first runs to completion while
+    the producer is stalled, and each result equals the job run alone."""
+    import time
+    specs = [SPECS["diblock_o3"](), SPECS["charged_o4"]()]
+    with tild_b200.Pool(mem_budget_bytes=8 << 30) as pool:
+        first = _submit(pool, specs[0], NSTEPS)
+        _wait_until(lambda: pool.status(first)["state"] == "done")   # no further submit meanwhile
+        time.sleep(0.2)
+        second = _submit(pool, specs[1], NSTEPS)
+        pool.wait(second)
+        s1, s2 = pool.status(first), pool.status(second)
+        assert s1["done_s"] < s2["submit_s"]
+        for jid, spec in ((first, specs[0]), (second, specs[1])):
+            x, _ = pool.result(jid, spec.N)
+            assert np.array_equal(x, alone(spec, deterministic=1)[0])
+
+
+def test_budget_lowered_below_the_running_set():
+    """Running jobs keep their memory and finish; a queued job enters only once the
+    running set fits the new budget; a queued job larger than the new budget fails."""
+    spec = SPECS["diblock_o3"]()
+    with tild_b200.Pool(mem_budget_bytes=8 << 30) as pool:
+        a = _submit(pool, spec, 20000)   # long enough to still run when the budget drops
+        b = _submit(pool, spec, 20000)
+        _wait_until(lambda: pool.stats()["running"] == 2)
+        per_job = pool.stats()["bytes_in_use"] // 2
+        pool.set_budget(per_job + per_job // 2)   # below the two running jobs
+        c = _submit(pool, spec, NSTEPS)
+        assert pool.status(c)["state"] == "queued"
+        pool.wait(a)
+        pool.wait(b)
+        pool.wait(c)
+        sa, sb, sc = pool.status(a), pool.status(b), pool.status(c)
+        assert sa["steps_done"] == sb["steps_done"] == 20000 and sc["steps_done"] == NSTEPS
+        assert sc["admit_s"] >= min(sa["done_s"], sb["done_s"])   # entered after one had left
+        with pytest.raises(tild_b200.TildError, match="budget"):
+            pool.submit(tild_b200.box_from_spec(SPECS["bigger_o3"](), options={"write_files": 0}), 5)
+    with tild_b200.Pool(mem_budget_bytes=8 << 30, max_active=1) as pool:
+        r = _submit(pool, spec, 10 ** 7)
+        q = _submit(pool, SPECS["bigger_o3"](), NSTEPS)
+        _wait_until(lambda: pool.status(r)["state"] == "running")
+        pool.set_budget(pool.stats()["bytes_in_use"])   # the running job still fits; the queued one cannot
+        st = pool.status(q)
+        assert st["state"] == "failed"
+        with pytest.raises(tild_b200.TildError, match="budget"):
+            pool.wait(q)
+        pool.cancel(r)
+        with pytest.raises(tild_b200.TildError, match="cancelled"):
+            pool.wait(r)

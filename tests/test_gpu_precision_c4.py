@@ -3,11 +3,12 @@ f_A = 0.5, chi = 1.5, rho0 = 5) on a 160^3 grid with Gaussian and erf2 (Rp = 1.0
 sigma = 0.5) potentials.  FP32 deposit, FFT and interpolation against the FP64 oracle,
 FP64 GPU reductions for the energies, the pair virial and S(k):
 
-  * forces at step 0, per particle |df_p| / max(|f_p|, f_rms): 99 % of particles within
-    1e-5 and every one within 3e-5 (measured: median 1.3e-6, 99 % 6.5e-6, 99.9 % 9.1e-6,
-    max 1.6e-5; over a million particles the FP32 transforms of a 160^3 grid, whose
-    rounding the FP64 oracle does not share, reach past 1e-5 at a few; the FP32
-    restatement of the reference's arithmetic with FP64 transforms stays within 7.3e-6);
+  * forces at step 0, per particle |df_p| / max(|f_p|, f_rms) <= 1e-5 for every particle
+    (measured on B200: median 2.0e-7, 99.9 % 6.2e-7, max 9.9e-7.  The stencil offset of a
+    particle is taken as x - c (d_hi + d_lo) with two FMAs, so it does not carry the
+    rounding of x / d, which at x / d ~ 160 is ~1e-5 of a cell and, through the deposit,
+    gave a max error of 1.6e-5; bonds across the boundary shift the coordinate above L/2
+    first, which is exact);
   * every potential's energy: relative 1e-5; pair virial: 1e-5 of max |W|;
   * S(k) of group A in 60 shells up to k = 6: per shell |dS| <= 1e-5 S + 1e-7 max S;
   * 5,000 steps with the FP64 thermo sampled every 50 steps (ps_data rows): every sample
@@ -45,7 +46,7 @@ def test_c4_forces_energies_virial_and_sk_match_the_fp64_oracle(c4):
     den = np.maximum(mag, np.sqrt(np.mean(mag ** 2)))
     err = np.linalg.norm(f - fref, axis=1) / den
     print("c4 force error percentiles 50/99/99.9/max:", np.percentile(err, [50, 99, 99.9]), err.max())
-    assert np.percentile(err, 99) <= 1e-5 and err.max() <= 3e-5
+    assert err.max() <= 1e-5
     for e, r in zip(th["potentials"], oracle.pair_energies(sysm, dens)):
         assert abs(e - r) <= 1e-5 * abs(r), (e, r)
     W = oracle.pair_virial(sysm, dens)

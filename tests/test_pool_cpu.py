@@ -74,3 +74,30 @@ def test_emptied_box_cannot_be_submitted_twice():
             pool.submit(b, 1)
         b.close()
     assert np.isfinite(1.0)
+
+
+def test_cancel_and_budget_argument_errors():
+    with tild_b200.Pool(mem_budget_bytes=1 << 30) as pool:
+        with pytest.raises(tild_b200.TildError, match="no job"):
+            pool.cancel(777)
+        with pytest.raises(tild_b200.TildError, match="budget"):
+            pool.set_budget(-1)
+        pool.set_budget(1 << 20)
+        assert pool.stats()["budget"] == 1 << 20 and pool.stats()["cancelled"] == 0
+        b = configured_box()
+        with pytest.raises(tild_b200.TildError, match="budget"):   # checked against the new budget
+            pool.submit(b, 5)
+        b.close()
+
+
+@pytest.mark.skipif(gpu_visible(), reason="checks the failure path of a machine without a GPU")
+def test_cancel_after_failure_is_refused():
+    with tild_b200.Pool(mem_budget_bytes=1 << 30) as pool:
+        b = configured_box()
+        job = pool.submit(b, 5)
+        with pytest.raises(tild_b200.TildError):
+            pool.wait(job)
+        with pytest.raises(tild_b200.TildError, match="already finished") as e:
+            pool.cancel(job)
+        assert e.value.code == 5   # TILD_ERR_STATE
+        b.close()
