@@ -14,8 +14,10 @@ with CUDA events on the box's stream, max over ranks.  The per-step working set
 is needed between steps.
 e2e: the same metric through the C ABI for one job of S steps: positions uploaded from
 pinned host memory, S steps, positions read back; copies inside the timed region.
---impl reference: the reference's step restated on the host cores (oracle CpuStep,
-FP32, all threads), same workload and metric, rank 0 only.
+--impl reference: MATILDA.FT's own CUDA build (the unmodified sources compiled into
+oracle/_ref by oracle/ref_harness/Makefile) on the same workload, GPU and metric, rank 0
+only, plus its plain per-job form on samples of the batched and served job lists; when
+that build is absent, the reference's step restated on the host cores (oracle CpuStep).
 """
 import argparse
 import json
@@ -180,15 +182,98 @@ def whole_job_rate(world, units_per_rank, ms):
     return world * units_per_rank / (ms * 1e-3)
 
 
+def harness_path():
+    return os.path.join(ROOT, "oracle", "_ref", "tild_ref_harness")
+
+
+def reference_step_ms(spec, warmup, steps, workdir):
+    """ms per step of the reference's own CUDA build (the unmodified MATILDA.FT sources built
+    in place into oracle/_ref by oracle/ref_harness/Makefile) on `spec`: the harness reads
+    the same data file and script as `matilda.ft -in`, sets the box up (finishInitialization),
+    runs `warmup` doTimeStep calls, then times `steps` more with CUDA events.  Also returns
+    the process wall time (set-up included)."""
+    spec.log_freq = 1 << 30
+    scr, _ = spec.write(workdir, steps=0)
+    t0 = time.perf_counter()
+    r = subprocess.run([harness_path(), os.path.basename(scr), "-", str(max(1, warmup)), str(steps)], cwd=workdir,
+                       capture_output=True, text=True, timeout=3000)
+    wall = time.perf_counter() - t0
+    if r.returncode != 0:
+        raise RuntimeError("reference harness rc=%d: %s" % (r.returncode, r.stderr[-500:]))
+    ms = [float(ln.split()[1]) for ln in r.stdout.splitlines() if ln.startswith("ms_per_step")][0]
+    return ms, wall
+
+
+def reference_plain_jobs(jobs, time_steps, workdir):
+    """Plain per-job form of the reference build on a job list [(spec, steps)]: one process
+    per job, one after another, each job's time = its process wall time with the timed
+    steps replaced by its own step count at the measured ms per step (set-up counted once,
+    as a `matilda.ft -in job.in` run would)."""
+    work, total, steady = 0.0, 0.0, 0.0
+    for spec, steps in jobs:
+        ms, wall = reference_step_ms(spec, 1, time_steps, workdir)
+        total += wall - time_steps * ms * 1e-3 + steps * ms * 1e-3
+        steady += steps * ms * 1e-3
+        work += float(spec.N) * steps
+    return {"value": work / total, "steady_state_value": work / steady, "unit": METRIC, "jobs": len(jobs),
+            "particle_steps": work}
+
+
+def every_kth(items, n):
+    """n items spread evenly over the list (the whole list when n >= its length)."""
+    if n >= len(items):
+        return list(items)
+    return [items[int(i * len(items) / n)] for i in range(n)]
+
+
 def run_reference(args):
-    world, rank, local, _ = (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
-                             int(os.environ.get("LOCAL_RANK", "0")), None)
+    """The reference arm: MATILDA.FT's own CUDA build (unmodified, through the harness) on
+    this GPU, same workload and metric; rank 0 only.  Also times its plain per-job form on
+    samples of the batched (C3) and served (C5) job lists that our arm runs."""
+    rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    import tempfile
+    from tild_b200 import synth
+    spec = make_spec(args.scale)
+    base = {"impl": "reference", "metric": METRIC, "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (numpy seed 2)", "config": bench_config(spec, args.gpus)}
+    if not os.path.exists(harness_path()):
+        return run_reference_port(args, base, "the reference build (oracle/_ref/tild_ref_harness) is absent")
+    with tempfile.TemporaryDirectory() as d:
+        ms, wall = reference_step_ms(spec, args.warmup, args.steps, d)
+        value = spec.N / (ms * 1e-3)
+        line = dict(base, value=value, ms_per_step=ms)
+        line["cpu_baseline"] = {
+            "value": value, "unit": METRIC, "cores": 1, "kind": "reference",
+            "sample": "%d steps (after %d warm-up) of the full workload through MATILDA.FT's own CUDA build "
+                      "(unmodified sources compiled for sm_100, PS_Box::doTimeStep driven by the harness, "
+                      "CUDA events; one host thread drives it), on this B200; process wall %.1f s with set-up"
+                      % (args.steps, args.warmup, wall)}
+        line["e2e"] = {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+        if not args.no_batch:
+            c3 = [(s, args.c3_steps) for s in synth.config_c3(replicas=args.c3_replicas)]
+            c3s = every_kth(c3, args.ref_jobs_c3)
+            line["batched_reference"] = dict(
+                reference_plain_jobs(c3s, args.ref_time_steps, d),
+                workload="c3 plain per-job form of the reference build: %d of the %d replicas (every %gth), "
+                         "%d steps each, one process per job" % (len(c3s), len(c3), len(c3) / len(c3s), args.c3_steps))
+            c5 = c5_jobs(synth, args)
+            c5s = every_kth(c5, args.ref_jobs_c5)
+            line["served_reference"] = dict(
+                reference_plain_jobs(c5s, args.ref_time_steps, d),
+                workload="c5 plain per-job form of the reference build: %d of the %d jobs, one process per job "
+                         "back to back" % (len(c5s), len(c5)))
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_reference_port(args, base, why):
+    """Fallback reference arm when the reference build is absent: the reference's
+    algorithm restated on the host (oracle CpuStep, FP32, every host core) on a scaled
+    replica of the workload sized to --ref-budget seconds."""
     threads = os.cpu_count() or 1
-    # Each step is a bounded sample: a scaled replica of the workload (same density,
-    # chain length, charge fractions and grid spacing) sized so that W + K steps take
-    # about `--ref-budget` seconds on the host cores.
     probe = make_spec(args.scale / 64.0)
     _, t_probe = cpu_sample(probe, threads, 1, warmup=1)
     per_step_full = t_probe * 64.0
@@ -196,20 +281,29 @@ def run_reference(args):
     s = max(s, 1.0 / 512.0)
     spec = make_spec(args.scale * s)
     value, sec = cpu_sample(spec, threads, args.steps, warmup=args.warmup)
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "particles": spec.N, "grid": [int(v) for v in spec.grid]},
-            "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
-                             "sample": "%d steps (after %d warm-up) of a scaled replica of the workload (%d particles, "
-                                       "%s grid, same density and composition) with the reference's algorithm "
-                                       "restated on the host (stencil tables, deposit of every group, FP32 C2C "
-                                       "FFTs); full-size step estimated at %.1f s"
-                                       % (args.steps, args.warmup, spec.N, "x".join(str(int(v)) for v in spec.grid),
-                                          per_step_full)},
-            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    what = ("the full workload" if s >= 1.0 else
+            "a replica of the workload scaled to %d particles, %s grid (same density and composition)"
+            % (spec.N, "x".join(str(int(v)) for v in spec.grid)))
+    line = dict(base, value=value, ms_per_step=sec * 1e3)
+    line["cpu_baseline"] = {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
+                            "sample": "%d steps (after %d warm-up) of %s with the reference's algorithm restated "
+                                      "on the host (stencil tables, deposit of every group, FP32 C2C FFTs); %s"
+                                      % (args.steps, args.warmup, what, why)}
+    line["e2e"] = {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def bench_config(spec, world):
+    return {"workload": WORKLOAD, "particles": spec.N, "grid": [int(v) for v in spec.grid],
+            "parallelism": "replicas" if world > 1 else "single",
+            "l2": "inputs larger than L2 (every kernel's operands exceed the 126 MB L2)"}
+
+
+def c5_jobs(synth, args):
+    """The served job list: BASELINE's size and length distribution (N log-uniform in
+    [2e4, 1e6], 500-5,000 steps), --c5-jobs of them."""
+    return synth.config_c5_jobs(njobs=args.c5_jobs, nmin=2.0e4, nmax=1.0e6, smin=500, smax=5000)
 
 
 def cufft_times(torch, spec, nd, nfg, reps=20):
@@ -300,7 +394,7 @@ def run_served(tild_b200, synth, args):
     pool's throughput on the same job mix (measured first, all jobs submitted at once),
     admitted by the pool as memory frees up; latency = completion - arrival.  The same
     jobs run alone give the plain per-job service times."""
-    jobs = synth.config_c5_jobs(njobs=args.c5_jobs)
+    jobs = c5_jobs(synth, args)
     work = np.array([s.N * n for s, n in jobs], np.float64)
     capacity = pool_capacity(tild_b200, args, jobs)
     boxes = [job_box(tild_b200, s) for s, _ in jobs]
@@ -437,12 +531,11 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (numpy seed 2)",
-            "config": {"workload": WORKLOAD, "particles": spec.N, "grid": [int(v) for v in spec.grid],
-                       "parallelism": "replicas" if world > 1 else "single", "rng": "philox",
-                       "tiles": {"bricks_per_cta": tiles["codes"], "threads": tiles["threads"],
-                                 "gather": tiles["gather"], "autotuned": not args.no_autotune},
-                       "l2": "inputs larger than L2 (%.2f GB moved per step by the kernels' compulsory traffic)"
-                             % (step_bytes / 1e9)},
+            "config": bench_config(spec, world),
+            "rng": "philox",
+            "tiles": {"bricks_per_cta": tiles["codes"], "threads": tiles["threads"], "gather": tiles["gather"],
+                      "autotuned": not args.no_autotune},
+            "step_algorithmic_gb": step_bytes / 1e9,
             "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic, "algorithmic_bytes": ab[dom],
@@ -483,11 +576,14 @@ def main():
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the density rule's tiles (profiling: fewer launches before the steps)")
     ap.add_argument("--c3-replicas", type=int, default=64)
-    ap.add_argument("--c3-steps", type=int, default=500)
-    ap.add_argument("--c5-jobs", type=int, default=40)
+    ap.add_argument("--c3-steps", type=int, default=2000)
+    ap.add_argument("--c5-jobs", type=int, default=24, help="served jobs (the stated stream has 2,000)")
     ap.add_argument("--c5-load", type=float, default=0.8)
-    ap.add_argument("--pool-budget-gb", type=int, default=120)
-    ap.add_argument("--ref-budget", type=float, default=150.0, help="seconds for the reference arm")
+    ap.add_argument("--pool-budget-gb", type=int, default=150)
+    ap.add_argument("--ref-budget", type=float, default=150.0, help="seconds for the host-port fallback arm")
+    ap.add_argument("--ref-jobs-c3", type=int, default=16, help="C3 replicas the reference arm times")
+    ap.add_argument("--ref-jobs-c5", type=int, default=8, help="C5 jobs the reference arm times")
+    ap.add_argument("--ref-time-steps", type=int, default=30, help="timed steps per reference job")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
