@@ -198,7 +198,9 @@ int tild_box_get_grid_force(tild_box *box, const char *group, float *gf_out);
  * the array, which keeps the last call's contents; the call clears the part that must
  * start at zero (the density accumulator) itself.  Calls that overlap on one device
  * (two boxes, or two host threads) race on the array.  The call returns after the copy
- * to rho_out[M] has finished. */
+ * to rho_out[M] has finished.  The looked-up address is kept for the life of the
+ * process: do not call this entry point on a device after cudaDeviceReset (or any reset
+ * of its primary context) in the same process. */
 #define TILD_NOALLOC_SCRATCH_BYTES (16u << 20)
 int tild_box_get_density_noalloc(tild_box *box, const char *group, int charge_channel, float *rho_out);
 

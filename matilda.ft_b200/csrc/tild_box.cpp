@@ -1404,7 +1404,9 @@ void Box::enqueueStep(bool energy, bool integrate, float *fout_dev)
     }
 }
 
-void Box::enqueueEnergyOnly()
+// lastStepStart: deposit from the other position buffer, which after a step holds the
+// positions that step started from (GJF keeps x_{t-1} there, EM leaves x_t there).
+void Box::enqueueEnergyOnly(bool lastStepStart)
 {
     const Geom &g = geom;
     cudaStream_t st = stream;
@@ -1415,7 +1417,8 @@ void Box::enqueueEnergyOnly()
             ck(launch_zero(dDepFix, sizeof(unsigned long long) * 2 * npair * g.M, st), "zero");
         else
             ck(launch_zero(dDep, sizeof(float2) * npair * g.M, st), "zero");
-        ck(launch_deposit(g, ppHost, dX[0], dX[1], dStep, dFlags, dQ, dDep, dDepFix, deterministic, tileCfg(), st), "deposit");
+        float *xa = lastStepStart ? dX[1] : dX[0], *xb = lastStepStart ? dX[0] : dX[1];
+        ck(launch_deposit(g, ppHost, xa, xb, dStep, dFlags, dQ, dDep, dDepFix, deterministic, tileCfg(), st), "deposit");
         ck(launch_xfwd(g, lx, npair, nd, dDep, deterministic ? dDepFix : nullptr, dH, st), "fft x forward");
         ck(launch_ypass(g, ly, nd, 0, dH, st), "fft y forward");
         ck(launch_kspace_z(g, lz, ksHost, dKs, dH, dUk, dHg, dEpart, 1, 0, nullptr, st), "kspace energy");
@@ -1543,8 +1546,9 @@ void Box::NVT(int64_t nSteps)
 {
     if (!ready) fail(TILD_ERR_STATE, "run nvt before endBox");
     ck(cudaSetDevice(device), "cudaSetDevice");
-    {   // writeData(-1) (PS_Box.cu:215)
-        std::vector<double> t = thermo();
+    {   // writeData(-1) (PS_Box.cu:215): computeThermoProps reads the groups' densities,
+        // which after earlier steps are those the last step started from
+        std::vector<double> t = thermo(totSteps > 0);
         std::vector<double> pe(t.begin() + 2, t.begin() + 2 + potentials.size());
         writeData(-1, pe, t[1], t.back());
     }
@@ -1858,11 +1862,11 @@ void Box::writeData(int64_t step, const std::vector<double> &pairE, double ubond
     if (echo) std::cout << echoLn.str() << std::endl;
 }
 
-std::vector<double> Box::thermo()
+std::vector<double> Box::thermo(bool lastStepStart)
 {
     if (!ready) fail(TILD_ERR_STATE, "endBox has not been processed");
     ck(cudaSetDevice(device), "cudaSetDevice");
-    enqueueEnergyOnly();
+    enqueueEnergyOnly(lastStepStart);
     std::vector<double> r = readEnergies(true);
     std::vector<double> out;
     const size_t np = potentials.size();

