@@ -929,9 +929,12 @@ void Box::prepareHost()
                                      "total negative: " + std::to_string(qneg) + ", positive: " + std::to_string(qpos));
     }
     nBondsTot = 0;
-    for (int64_t p = 0; p < nstot; p++)
+    nBondEntries = 0;   // both directions: the length of the device's CSR bond list
+    for (int64_t p = 0; p < nstot; p++) {
+        nBondEntries += nBonds[p];
         for (int b = 0; b < nBonds[p]; b++)
             if (bondedTo[p * MAXBONDS + b] > p) nBondsTot++;
+    }
     for (int64_t p = 0; p < nstot; p++)
         for (int b = 0; b < nBonds[p]; b++)
             if (bondType[p * MAXBONDS + b] >= nBondTypes)
@@ -992,15 +995,16 @@ int64_t Box::deviceBytesEstimate() const
     if (!hostPrepared) fail(TILD_ERR_STATE, "the box has not been prepared");
     const int64_t N = nstot, M = geom.M, hs = geom.hstride;
     const int64_t nd = std::max<int64_t>(1, (int64_t)dfields.size()), nfg = std::max<int64_t>(1, (int64_t)fgroups.size());
-    const int64_t npair = (nd + 1) / 2, mb = MAXBONDS;
+    const int64_t npair = (nd + 1) / 2;
     const int64_t rng = rngCompat ? (int64_t)rng_state_bytes() : 0, q = doCharges ? 4 : 0;
-    const int64_t perParticle = 12 * 4 + 4 + 4 + q + 1 + 5 * mb + rng + 12 + 1   // state, scratch, partials
-                                + 12 + 36 + q + 8 + 1 + 5 * mb + rng;         // sort keys and copies
+    const int64_t perParticle = 12 * 4 + 4 + 4 + q + rng + 12 + 1   // state, scratch, partials
+                                + 12 + 36 + q + 8 + rng + 1;        // sort keys, copies, scan totals
+    const int64_t bonds = nBondEntries > 0 ? 2 * (4 * (N + 1) + 5 * nBondEntries) : 0;   // CSR + its sort copy
     const int64_t nk = (int64_t)sort_key_count(geom);
     const int64_t angles = nAnglesTot > 0 ? 2 * (1 + 13 * (int64_t)MAXANGLES) : 0;   // arrays and sort copies
     const int64_t grid = (deterministic ? 16 : 8) * npair * M + 8 * nd * hs + 24 * nfg * hs + 16 * nfg * M +
                          4 * std::max<int64_t>(1, (int64_t)potentials.size()) * hs + 8 * nk;
-    return N * (perParticle + angles) + grid + (int64_t(4) << 20);   // + small arrays, alignment, graphs
+    return N * (perParticle + angles) + bonds + grid + (int64_t(4) << 20);   // + small arrays, alignment, graphs
 }
 
 void Box::buildPlan()
@@ -1103,6 +1107,16 @@ void Box::buildPlan()
     for (size_t k = 0; k < dfields.size(); k++)
         if (dfields[k].charge) pp.dchan_charge |= 1u << k;
     pp.nfg = ks.nfg;
+    {   // int32 fixed-point tile sums (2^24 per unit): a grid point of a tile receives at
+        // most (particles) x (largest stencil weight) x (largest |q|)
+        const double w1[5] = {1.0, 1.0, 0.75, 2.0 / 3.0, 115.0 / 192.0};   // max 1-D weight per order
+        double wmax = 1.0;
+        for (int j = 0; j < Dim; j++) wmax *= w1[std::min(std::max(pmeorder, 0), 4)];
+        double qmax = 1.0;
+        if (doCharges)
+            for (int64_t p = 0; p < nstot; p++) qmax = std::max(qmax, (double)std::fabs(charges[p]));
+        pp.int_tile_max = (int)std::floor(0.9 * 2147483647.0 / (16777216.0 * wmax * qmax));
+    }
     for (size_t k = 0; k < fgroups.size(); k++)
         if (psGroup[fgroups[k]].isCharges) pp.fg_qweighted |= 1u << k;
     pp.maxb = MAXBONDS;
@@ -1160,9 +1174,12 @@ void Box::allocDevice()
     dFlags = dalloc<uint32_t>(N);
     dOrig = dalloc<int>(N);
     if (doCharges) dQ = dalloc<float>(N);
-    dNb = dalloc<uint8_t>(N);
-    dPartner = dalloc<int>(N * MAXBONDS);
-    dBtype = dalloc<uint8_t>(N * MAXBONDS);
+    const int64_t nnz = nBondEntries;   // CSR bond list, both directions
+    if (nnz > 0) {
+        dBrow = dalloc<int>(N + 1);
+        dPartner = dalloc<int>(nnz);
+        dBtype = dalloc<uint8_t>(nnz);
+    }
     if (nAnglesTot > 0) {
         dNa = dalloc<uint8_t>(N);
         dAtype = dalloc<uint8_t>(N * MAXANGLES);
@@ -1217,9 +1234,10 @@ void Box::allocDevice()
     sortW.q = doCharges ? dalloc<float>(N) : nullptr;
     sortW.flags = dalloc<uint32_t>(N);
     sortW.orig = dalloc<int>(N);
-    sortW.partner = dalloc<int>(N * MAXBONDS);
-    sortW.nb = dalloc<uint8_t>(N);
-    sortW.btype = dalloc<uint8_t>(N * MAXBONDS);
+    sortW.brow = nnz > 0 ? dalloc<int>(N + 1) : nullptr;
+    sortW.partner = nnz > 0 ? dalloc<int>(nnz) : nullptr;
+    sortW.btype = nnz > 0 ? dalloc<uint8_t>(nnz) : nullptr;
+    sortW.totalsN = dalloc<uint32_t>(N / 1024 + 2);
     sortW.rng = rngCompat ? (void *)dalloc<unsigned char>(N * rng_state_bytes()) : nullptr;
     sortW.na = nAnglesTot > 0 ? dalloc<uint8_t>(N) : nullptr;
     sortW.atype = nAnglesTot > 0 ? dalloc<uint8_t>(N * MAXANGLES) : nullptr;
@@ -1239,12 +1257,22 @@ void Box::uploadParticles()
     std::iota(orig.begin(), orig.end(), 0);
     ck(cudaMemcpy(dOrig, orig.data(), 4 * N, cudaMemcpyHostToDevice), "upload ids");
     if (doCharges) ck(cudaMemcpy(dQ, charges.data(), 4 * N, cudaMemcpyHostToDevice), "upload q");
-    std::vector<uint8_t> nb8(N), bt8(N * MAXBONDS);
-    for (int64_t p = 0; p < N; p++) nb8[p] = (uint8_t)nBonds[p];
-    for (int64_t k = 0; k < N * MAXBONDS; k++) bt8[k] = (uint8_t)bondType[k];
-    ck(cudaMemcpy(dNb, nb8.data(), N, cudaMemcpyHostToDevice), "upload nb");
-    ck(cudaMemcpy(dPartner, bondedTo.data(), 4 * N * MAXBONDS, cudaMemcpyHostToDevice), "upload partners");
-    ck(cudaMemcpy(dBtype, bt8.data(), N * MAXBONDS, cudaMemcpyHostToDevice), "upload bond types");
+    if (dBrow) {   // the padded partner lists of the data file as a CSR list
+        std::vector<int> row(N + 1, 0), col;
+        std::vector<uint8_t> bt;
+        for (int64_t p = 0; p < N; p++) {
+            for (int b = 0; b < nBonds[p]; b++) {
+                col.push_back(bondedTo[p * MAXBONDS + b]);
+                bt.push_back((uint8_t)bondType[p * MAXBONDS + b]);
+            }
+            row[p + 1] = (int)col.size();
+        }
+        if ((int64_t)col.size() != nBondEntries) fail(TILD_ERR_STATE, "bond list changed after set-up");
+        ck(cudaMemcpy(dBrow, row.data(), 4 * (N + 1), cudaMemcpyHostToDevice), "upload bond rows");
+        ck(cudaMemcpy(sortW.brow + N, row.data() + N, 4, cudaMemcpyHostToDevice), "upload bond rows");
+        ck(cudaMemcpy(dPartner, col.data(), 4 * col.size(), cudaMemcpyHostToDevice), "upload partners");
+        ck(cudaMemcpy(dBtype, bt.data(), bt.size(), cudaMemcpyHostToDevice), "upload bond types");
+    }
     if (dNa) {
         std::vector<uint8_t> na8(N), at8(N * MAXANGLES);
         for (int64_t p = 0; p < N; p++) na8[p] = (uint8_t)nAngles[p];
@@ -1318,8 +1346,8 @@ std::vector<int> Box::slotOrder() const
 void Box::sortParticles()
 {
     const int64_t N = nstot;
-    PermIn in{dX[0], dX[1], dNoise, dQ, dFlags, dOrig, dPartner, dNb, dBtype, dRng, dStep, dNa, dAtype, dAng};
-    ck(launch_sort(geom, (int)N, MAXBONDS, dNa ? MAXANGLES : 0, sortW, in, stream), "sort");
+    PermIn in{dX[0], dX[1], dNoise, dQ, dFlags, dOrig, dBrow, dPartner, dBtype, dRng, dStep, dNa, dAtype, dAng};
+    ck(launch_sort(geom, (int)N, dNa ? MAXANGLES : 0, sortW, in, stream), "sort");
     auto cp = [&](void *dst, const void *src, size_t bytes) {
         ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, stream), "sort copy");
     };
@@ -1329,9 +1357,12 @@ void Box::sortParticles()
     cp(dFlags, sortW.flags, 4 * N);
     cp(dOrig, sortW.orig, 4 * N);
     if (dQ) cp(dQ, sortW.q, 4 * N);
-    cp(dNb, sortW.nb, N);
-    cp(dPartner, sortW.partner, 4 * N * MAXBONDS);
-    cp(dBtype, sortW.btype, N * MAXBONDS);
+    if (dBrow) {   // brow[N] (the entry count) never changes
+        const int64_t nnz = nBondEntries;
+        cp(dBrow, sortW.brow, 4 * N);
+        cp(dPartner, sortW.partner, 4 * nnz);
+        cp(dBtype, sortW.btype, nnz);
+    }
     if (dRng) cp(dRng, sortW.rng, N * rng_state_bytes());
     if (dNa) {
         cp(dNa, sortW.na, N);
@@ -1391,14 +1422,14 @@ void Box::enqueueStep(bool energy, bool integrate, float *fout_dev)
             mark(STAGE_XINV);
         }
     }
-    ck(launch_particles(g, ppHost, dPp, dX[0], dX[1], dNoise, dFlags, dQ, dNb, dPartner, dBtype,
+    ck(launch_particles(g, ppHost, dPp, dX[0], dX[1], dNoise, dFlags, dQ, dBrow, dPartner, dBtype,
                         AngleArrays{dNa, dAtype, dAng}, dRec, dOrig, dRng,
                         dStep, fout_dev, integrate ? 1 : 0, tileCfg(), st),
        "particles");
     mark(STAGE_PARTICLES);
     if (integrate) ck(launch_tick(dStep, st), "tick");
     if (energy) {
-        ck(launch_bond_energy(g, ppHost, dPp, dX[0], dX[1], dStep, dNb, dPartner, dBtype, AngleArrays{dNa, dAtype, dAng},
+        ck(launch_bond_energy(g, ppHost, dPp, dX[0], dX[1], dStep, dBrow, dPartner, dBtype, AngleArrays{dNa, dAtype, dAng},
                               dFlags, dBpart, nullptr, st), "bond energy");
         ck(launch_reduce_partials(dBpart, nblkP, kPartialCols, dRes + kResBond, st), "reduce bonds");
     }
@@ -1424,7 +1455,7 @@ void Box::enqueueEnergyOnly(bool lastStepStart)
         ck(launch_kspace_z(g, lz, ksHost, dKs, dH, dUk, dHg, dEpart, 1, 0, nullptr, st), "kspace energy");
         ck(launch_reduce_partials(dEpart, nblkZ, ksHost.neterms + 6, dRes, st), "reduce");
     }
-    ck(launch_bond_energy(g, ppHost, dPp, dX[0], dX[1], dStep, dNb, dPartner, dBtype, AngleArrays{dNa, dAtype, dAng},
+    ck(launch_bond_energy(g, ppHost, dPp, dX[0], dX[1], dStep, dBrow, dPartner, dBtype, AngleArrays{dNa, dAtype, dAng},
                               dFlags, dBpart, nullptr, st), "bond energy");
     ck(launch_reduce_partials(dBpart, nblkP, kPartialCols, dRes + kResBond, st), "reduce bonds");
 }

@@ -119,6 +119,7 @@ public:
     double gvol = 0.0;
     int pmeorder = 1;
     int64_t nBondsTot = 0;
+    int64_t nBondEntries = 0;   // stored partner entries (each bond twice)
     int nBondTypes = 0;
     int64_t totSteps = 0;
     std::vector<PS_Group> psGroup;
@@ -240,7 +241,8 @@ private:
     float *dX[2] = {nullptr, nullptr};
     float *dNoise = nullptr, *dQ = nullptr, *dF = nullptr;
     uint32_t *dFlags = nullptr;
-    uint8_t *dNb = nullptr, *dBtype = nullptr;
+    int *dBrow = nullptr;                        // CSR bond rows [N+1] (NULL without bonds)
+    uint8_t *dBtype = nullptr;
     uint8_t *dNa = nullptr, *dAtype = nullptr;   // angles (NULL when the box has none)
     int *dAng = nullptr;
     int *dPartner = nullptr, *dOrig = nullptr;

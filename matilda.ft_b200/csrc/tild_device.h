@@ -6,7 +6,8 @@
 //   pflags[N]      uint32  bits 0-7 density-field membership, 8-15 force-group
 //                          membership, 16-19 integrator slot (15 = none), 20-23 type
 //   q[N]           float   charges (only with doCharges)
-//   nb[N], partner[N*maxb], btype[N*maxb]   bonds, both directions (readDataConfig)
+//   brow[N+1], partner[nnz], btype[nnz]     bonds in CSR, both directions (readDataConfig);
+//                          particle p's partners are partner[brow[p] .. brow[p+1])
 //   dep[npair][M]  float2  deposit target: field 2i in .x, 2i+1 in .y
 //   H[D][Nz][Ny][hp]  float2  density half spectra (kx in [0, Nx/2])
 //   Hg[3F][Nz][Ny][hp] float2 gradient half spectra
@@ -117,6 +118,7 @@ struct ParticleParams {
     int nd;                         // density fields
     int npair;
     unsigned dchan_charge;          // bit i set: field i is a charge-weighted channel
+    int int_tile_max;               // deposit: tiles of at most this many particles sum in int32 fixed point
     int nfg;
     unsigned fg_qweighted;          // bit f set: force group f gathers q-weighted
     int maxb;
@@ -192,7 +194,7 @@ cudaError_t launch_xinv(const Geom &g, const FftLine &lx, int nfg, const float2 
                         cudaStream_t st);
 cudaError_t launch_particles(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd,
                              float *X0, float *X1, float *noise, const uint32_t *pflags,
-                             const float *q, const uint8_t *nb, const int *partner,
+                             const float *q, const int *brow, const int *partner,
                              const uint8_t *btype, AngleArrays aa, const float4 *rec, const int *orig_id,
                              void *rng_states, const long long *d_step, float *fout,
                              int integrate, const TileCfg &tc, cudaStream_t st);
@@ -203,8 +205,9 @@ cudaError_t launch_tick(long long *d_step, cudaStream_t st);
 struct PermIn {             // current particle arrays (slot order)
     const float *X0, *X1, *noise, *q;
     const uint32_t *flags;
-    const int *orig, *partner;
-    const uint8_t *nb, *btype;
+    const int *orig;
+    const int *brow, *partner;  // bonds in CSR: row p = [brow[p], brow[p+1]) of partner/btype
+    const uint8_t *btype;       // (NULL brow: no bonds)
     const void *rng;
     const long long *d_step;
     const uint8_t *na, *atype;  // angles per particle and their types (may be NULL)
@@ -212,18 +215,19 @@ struct PermIn {             // current particle arrays (slot order)
 };
 struct SortScratch {        // work arrays and the permuted copies
     uint32_t *key, *count, *totals, *start;
+    uint32_t *totalsN;          // per-block totals of the scan of the N bond counts
     int *rank, *newpos;
     float *X0, *X1, *noise, *q;
     uint32_t *flags;
-    int *orig, *partner;
-    uint8_t *nb, *btype;
+    int *orig;
+    int *brow, *partner;
+    uint8_t *btype;
     void *rng;
     uint8_t *na, *atype;
     int *ang;
 };
 uint32_t sort_key_count(const Geom &g);
-cudaError_t launch_sort(const Geom &g, int N, int maxb, int maxa, const SortScratch &w, const PermIn &in,
-                        cudaStream_t st);
+cudaError_t launch_sort(const Geom &g, int N, int maxa, const SortScratch &w, const PermIn &in, cudaStream_t st);
 cudaError_t launch_unpermute_rows(int N, int width, const int *orig, const float *in, float *out,
                                   cudaStream_t st);
 cudaError_t launch_permute_rows(int N, int width, const int *orig, const float *in, float *out,
@@ -236,7 +240,7 @@ size_t rng_state_bytes();
 // finite
 cudaError_t launch_bond_energy(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd,
                                const float *X0, const float *X1, const long long *d_step,
-                               const uint8_t *nb, const int *partner, const uint8_t *btype, AngleArrays aa,
+                               const int *brow, const int *partner, const uint8_t *btype, AngleArrays aa,
                                const uint32_t *pflags, double *partials, int *nblocks_out, cudaStream_t st);
 cudaError_t launch_reduce_partials(const double *partials, int nblocks, int ncols, double *out,
                                    cudaStream_t st);

@@ -1,6 +1,8 @@
 // tild_grid.cu -- density deposit and reference-exact stencil tables (sm_100a).
 #include "tild_stencil.cuh"
 
+#include <type_traits>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -120,10 +122,18 @@ __device__ __forceinline__ float field_coef(uint32_t dm, unsigned dq, int f, flo
     return ((dm >> f) & 1u) ? (((dq >> f) & 1u) ? qp : 1.f) : 0.f;
 }
 
+// Shared-memory accumulation of one contribution.  Deterministic mode: 64-bit fixed
+// point (kFixScale), exact and order-independent.  Fast mode: 32-bit fixed point
+// (kTileFix per unit, integer shared atomics, about 1.2x the speed of FP32 ones) in tiles
+// whose particle count keeps every sum inside int32 (`ia`), else FP32 atomics.  A
+// contribution is rounded once to 2^-24 (3e-8 absolute), below the FP32 rounding of a
+// running sum of order one.
+constexpr float kTileFix = 16777216.f;   // 2^24 per unit weight
 template <bool FIXED>
-__device__ __forceinline__ void smem_add(float *tf, unsigned long long *tu, int i, float v)
+__device__ __forceinline__ void smem_add(float *tf, unsigned long long *tu, int i, float v, bool ia)
 {
     if (FIXED) atomicAdd(tu + i, (unsigned long long)__double2ll_rn((double)v * kFixScale));
+    else if (ia) atomicAdd(reinterpret_cast<int *>(tf) + i, __float2int_rn(v * kTileFix));
     else atomicAdd(tf + i, v);
 }
 
@@ -147,7 +157,7 @@ __global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4
                                                        const uint32_t *__restrict__ pflags,
                                                        const float *__restrict__ q, float2 *__restrict__ dep,
                                                        unsigned long long *__restrict__ depfix, int cap_bytes,
-                                                       TileCfg tc)
+                                                       TileCfg tc, int int_tile_max)
 {
     constexpr int P1 = P + 1, G = P1 * P1 * P1, NPASS = (G + 31) / 32;
     constexpr int NC = NF ? NF : kMaxFields;
@@ -170,6 +180,7 @@ __global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4
     const bool staged = tc.start && E[0] <= kMaxBoxEdge && E[1] <= kMaxBoxEdge && E[2] <= kMaxBoxEdge &&
                         Vl * nfields * (long long)esz <= cap_bytes;
     const int V = staged ? (int)Vl : 0, E0 = E[0], E01 = E[0] * E[1];
+    const bool ia = !FIXED && staged && (b1 - b0) <= int_tile_max;   // int32 fixed-point box
     float *tf = reinterpret_cast<float *>(smraw);
     unsigned long long *tu = reinterpret_cast<unsigned long long *>(smraw);
     if (staged) {
@@ -276,16 +287,22 @@ __global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4
                         // deterministic mode's fixed-point values do not depend on staging
                         ws[u][k] = (lane + 32 * k < G) ? pj[sa[k]] * pj[P1 + syz[k]] : 0.f;
                 }
+                // the box's number type is fixed for the tile: one branch per round
+                auto atomics = [&](auto int_box) {
 #pragma unroll
-                for (int u = 0; u < U; u++)
+                    for (int u = 0; u < U; u++)
 #pragma unroll
-                    for (int k = 0; k < NPASS; k++) {
-                        if (lane + 32 * k >= G) break;
-                        const int idx = offs[u] + loff[k];
+                        for (int k = 0; k < NPASS; k++) {
+                            if (lane + 32 * k >= G) break;
+                            const int idx = offs[u] + loff[k];
 #pragma unroll
-                        for (int f = 0; f < NC; f++)
-                            if (cfs[u][f] != 0.f) smem_add<FIXED>(tf, tu, f * V + idx, cfs[u][f] * ws[u][k]);
-                    }
+                            for (int f = 0; f < NC; f++)
+                                if (cfs[u][f] != 0.f)
+                                    smem_add<FIXED>(tf, tu, f * V + idx, cfs[u][f] * ws[u][k], decltype(int_box)::value);
+                        }
+                };
+                if (ia) atomics(std::true_type{});
+                else atomics(std::false_type{});
             }
             __syncwarp();
         }
@@ -336,8 +353,12 @@ __global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4
             }
         } else {
             for (int t = 0; t < npair; t++) {
-                const float a0 = tf[(2 * t) * V + v];
-                const float a1 = (2 * t + 1 < nfields) ? tf[(2 * t + 1) * V + v] : 0.f;
+                float a0 = tf[(2 * t) * V + v];
+                float a1 = (2 * t + 1 < nfields) ? tf[(2 * t + 1) * V + v] : 0.f;
+                if (ia) {
+                    a0 = (float)__float_as_int(a0) * (1.f / kTileFix);
+                    a1 = (float)__float_as_int(a1) * (1.f / kTileFix);
+                }
                 if (a0 != 0.f && a1 != 0.f) atomicAdd(dep + t * g.M + m, make_float2(a0, a1));
                 else if (a0 != 0.f) atomicAdd(&dep[t * g.M + m].x, a0);
                 else if (a1 != 0.f) atomicAdd(&dep[t * g.M + m].y, a1);
@@ -361,10 +382,12 @@ static void dep_launch_nf(int nb, int threads, const Geom &g, const ParticlePara
     const size_t table = (size_t)(threads / 32) * 32 * WREC * sizeof(float);
     if (depfix)
         k_deposit_tiled<P, NF, true><<<nb, threads, cap + table, st>>>(g, pp.N, pp.quirk4, pp.nd, pp.dchan_charge, X0,
-                                                                       X1, d_step, pflags, q, dep, depfix, cap, tc);
+                                                                       X1, d_step, pflags, q, dep, depfix, cap, tc,
+                                                                       pp.int_tile_max);
     else
         k_deposit_tiled<P, NF, false><<<nb, threads, cap + table, st>>>(g, pp.N, pp.quirk4, pp.nd, pp.dchan_charge, X0,
-                                                                        X1, d_step, pflags, q, dep, depfix, cap, tc);
+                                                                        X1, d_step, pflags, q, dep, depfix, cap, tc,
+                                                                        pp.int_tile_max);
 }
 
 template <int P>

@@ -51,19 +51,22 @@ __device__ __forceinline__ void philox_normals3(unsigned long long seed, uint32_
 
 // Bond force on particle p (ps_deviceBonds.cu:7-79): minimum image with Lh, skipped for
 // r^2 <= 1e-4, harmonic mf = 2k(r - req)/r or FENE; f -= mf * dr over every stored partner.
+// The reference keeps a padded [N x MAXBONDS] partner list; here the partners form a CSR
+// list (row offsets brow[N+1]), renumbered and re-packed by every spatial sort, so a
+// branched molecule's high-degree particles cost no padding for all the others.
 // A bond across the periodic boundary is measured as (x_p - L) - x_o or x_p - (x_o - L):
 // the coordinate above L/2 is shifted first, which is exact in FP32, so the short image
 // vector is rounded once at its own magnitude instead of at the box length's (the
 // reference's x_p - x_o then -L loses up to half an ulp of L, ~2e-6 at L = 60).
 __device__ __forceinline__ void bond_force(const Geom &g, const ParticleParams &pp, int p, const float *x,
-                                           const float *__restrict__ Xc, const uint8_t *__restrict__ nb,
+                                           const float *__restrict__ Xc, const int *__restrict__ brow,
                                            const int *__restrict__ partner, const uint8_t *__restrict__ btype,
                                            float *f)
 {
-    const int nbp = nb ? nb[p] : 0;
-    for (int b = 0; b < nbp; b++) {
-        const int o = partner[p * pp.maxb + b];
-        const int t = btype[p * pp.maxb + b];
+    const int k0 = brow ? brow[p] : 0, k1 = brow ? brow[p + 1] : 0;
+    for (int k = k0; k < k1; k++) {   // this particle's row of the CSR bond list
+        const int o = partner[k];
+        const int t = btype[k];
         float dr[3];
         float mdr2 = 0.f;
 #pragma unroll
@@ -309,7 +312,7 @@ template <int P, bool EXTRA>
 __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const ParticleParams *__restrict__ ppd, int N,
                                                       float *__restrict__ X0, float *__restrict__ X1,
                                                       float *__restrict__ noise, const uint32_t *__restrict__ pflags,
-                                                      const float *__restrict__ q, const uint8_t *__restrict__ nb,
+                                                      const float *__restrict__ q, const int *__restrict__ brow,
                                                       const int *__restrict__ partner,
                                                       const uint8_t *__restrict__ btype, AngleArrays aa,
                                                       const float4 *__restrict__ rec, const int *__restrict__ orig_id,
@@ -325,6 +328,7 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
     __shared__ float Ao[kPartOut][kMaxFGroups][3];
     __shared__ int outP[kPartOut];
     __shared__ int nout;
+    __shared__ int deal_src[kPartThreadsMax];   // per warp: the lane whose particle a lane gathers
     const ParticleParams &pp = *ppd;
     const long long step = *d_step;
     const float *__restrict__ Xc = (step & 1) ? X1 : X0;   // x_t
@@ -372,11 +376,7 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
                 cp_async4(iop + 5 * T + threadIdx.x, noise + 3 * p + 2);
                 cp_async4(iop + 6 * T + threadIdx.x, orig_id + p);
             }
-            if (nb) {
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(partner + p * pp.maxb));
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(nb + p));
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(btype + p * pp.maxb));
-            }
+            if (brow) asm volatile("prefetch.global.L2 [%0];" ::"l"(brow + p));
             if (q) asm volatile("prefetch.global.L2 [%0];" ::"l"(q + p));
         }
         const unsigned fm = (fl >> 8) & 0xffu;
@@ -432,7 +432,7 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
         // 4. bonds
         float f[3] = {0.f, 0.f, 0.f};
         if (act) {
-            bond_force(g, pp, p, x, Xc, nb, partner, btype, f);
+            bond_force(g, pp, p, x, Xc, brow, partner, btype, f);
             if (EXTRA) {
                 if (aa.na) angle_force(g, pp, p, Xc, aa, f);
                 if (pp.nwall) wall_terms(pp, fl, x, f, nullptr);   // potentials' own forces, before the gathers
@@ -445,6 +445,45 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
             stencil_fast<P>(x[0], g, 0, pp.quirk4, Wx);
             stencil_fast<P>(x[1], g, 1, pp.quirk4, Wy);
             stencil_fast_z<P>(x[2], g, pp.quirk4, Wz);
+        }
+        // 4b. deal the box gathers of the warp over its lanes by bank group.  A float4
+        // record gather of a quarter warp takes one shared-memory wavefront only when its
+        // eight lanes start at eight distinct 16-byte bank groups (record offset mod 8);
+        // particles of a warp start at random offsets.  So the warp orders its particles
+        // by that offset (class 8: nothing to gather from the box) and lane 8q + a takes
+        // the particle at position 4a + q of the order: the eight lanes of a quarter warp
+        // get positions four apart, which spreads them over the bank groups.  The lane
+        // gathers for that particle with its stencil (shuffled in) and sends the result
+        // back to the particle's own lane, which keeps every other access coalesced.
+        const unsigned full = 0xffffffffu;
+        const int lane = threadIdx.x & 31;
+        int tp = lane, src = lane;
+        if (staged) {
+            const int r = inbox ? (base & 7) : 8;
+            int below = 0;
+#pragma unroll
+            for (int v = 0; v < 8; v++) {
+                const unsigned bl = __ballot_sync(full, r == v);
+                below += v < r ? __popc(bl) : 0;
+            }
+            const int j = below + __popc(__match_any_sync(full, r) & ((1u << lane) - 1u));
+            tp = ((j & 3) << 3) | (j >> 2);
+            deal_src[(threadIdx.x & ~31) + tp] = lane;
+            __syncwarp();
+            src = deal_src[threadIdx.x];
+            __syncwarp();
+        }
+        int bsrc = base;
+        uint32_t flsrc = 0u;   // the groups this lane gathers from the box
+        if (staged) {
+            bsrc = __shfl_sync(full, base, src);
+            flsrc = __shfl_sync(full, inbox ? fl : 0u, src);
+#pragma unroll
+            for (int i = 0; i <= P; i++) {
+                Wx[i] = __shfl_sync(full, Wx[i], src);
+                Wy[i] = __shfl_sync(full, Wy[i], src);
+                Wz[i] = __shfl_sync(full, Wz[i], src);
+            }
         }
         // 5. gather each force group in group order
         bool first = true;
@@ -463,17 +502,15 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
                 __syncthreads();   // the helpers' results are visible
             }
             first = false;
-            if (!((fl >> (8 + fg)) & 1u)) continue;
-            float a[3];
-            if (inbox) {
-                float2 a01 = make_float2(0.f, 0.f);
-                float a2 = 0.f;
+            float2 a01 = make_float2(0.f, 0.f);
+            float a2 = 0.f;
+            if ((flsrc >> (8 + fg)) & 1u) {   // the box gather of the particle dealt to this lane
 #pragma unroll
                 for (int e = 0; e <= P; e++) {
 #pragma unroll
                     for (int b = 0; b <= P; b++) {
                         const float wyz = Wy[b] * Wz[e];
-                        const int row = base + e * E01 + b * E0;
+                        const int row = bsrc + e * E01 + b * E0;
 #pragma unroll
                         for (int aa = 0; aa <= P; aa++) {
                             const float w = Wx[aa] * wyz;
@@ -483,13 +520,21 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
                         }
                     }
                 }
-                a[0] = a01.x;
-                a[1] = a01.y;
-                a[2] = a2;
+            }
+            float a[3] = {__shfl_sync(full, a01.x, tp), __shfl_sync(full, a01.y, tp), __shfl_sync(full, a2, tp)};
+            if (!((fl >> (8 + fg)) & 1u)) continue;
+            if (inbox) {
+                // a[] holds this particle's box gather
             } else if (slot >= 0 && slot < kPartOut) {
                 a[0] = Ao[slot][fg][0];
                 a[1] = Ao[slot][fg][1];
                 a[2] = Ao[slot][fg][2];
+            } else if (staged) {   // own stencil again (the registers hold the dealt particle's)
+                float Ux[P + 1], Uy[P + 1], Uz[P + 1];
+                stencil_fast<P>(x[0], g, 0, pp.quirk4, Ux);
+                stencil_fast<P>(x[1], g, 1, pp.quirk4, Uy);
+                stencil_fast_z<P>(x[2], g, pp.quirk4, Uz);
+                gather_global<P, true>(g, rf, gs, Ux, Uy, Uz, a);
             } else {
                 gather_global<P, true>(g, rf, gs, Wx, Wy, Wz, a);
             }
@@ -544,7 +589,7 @@ __global__ void k_rng_init(curandState *st, const int *orig_id, int n, unsigned 
 __global__ void __launch_bounds__(256) k_bond_energy(Geom g, const ParticleParams *__restrict__ ppd, int N,
                                                      const float *__restrict__ X0, const float *__restrict__ X1,
                                                      const long long *__restrict__ d_step,
-                                                     const uint8_t *__restrict__ nb,
+                                                     const int *__restrict__ brow,
                                                      const int *__restrict__ partner,
                                                      const uint8_t *__restrict__ btype, AngleArrays aa,
                                                      const uint32_t *__restrict__ pflags,
@@ -558,10 +603,10 @@ __global__ void __launch_bounds__(256) k_bond_energy(Geom g, const ParticleParam
     double acc[NC];
 #pragma unroll
     for (int c = 0; c < NC; c++) acc[c] = 0.0;
-    if (p < N && nb) {
+    if (p < N && brow) {
         float e = 0.f, vir[6] = {0, 0, 0, 0, 0, 0};
-        for (int b = 0; b < nb[p]; b++) {
-            const int o = partner[p * pp.maxb + b], t = btype[p * pp.maxb + b];
+        for (int k = brow[p]; k < brow[p + 1]; k++) {
+            const int o = partner[k], t = btype[k];
             float dr[3], mdr2 = 0.f, mf = 0.f;
             for (int j = 0; j < 3; j++) {
                 dr[j] = X[3 * p + j] - X[3 * o + j];
@@ -659,7 +704,7 @@ constexpr size_t kPartSmemMax = kPartBox * sizeof(float4) + kPartThreadsMax * 7 
 
 template <int P>
 static void part_launch(const Geom &g, const ParticleParams *ppd, int N, float *X0, float *X1, float *noise,
-                        const uint32_t *pflags, const float *q, const uint8_t *nb, const int *partner,
+                        const uint32_t *pflags, const float *q, const int *brow, const int *partner,
                         const uint8_t *btype, AngleArrays aa, const float4 *rec, const int *orig_id, void *rng,
                         const long long *d_step, float *fout, int integrate, const TileCfg &tc, bool walls,
                         cudaStream_t st)
@@ -670,10 +715,10 @@ static void part_launch(const Geom &g, const ParticleParams *ppd, int N, float *
     const size_t smem = (size_t)cap * sizeof(float4) + (size_t)threads * 7 * sizeof(float);
     const bool extra = aa.na != nullptr || walls;
     if (extra)
-        k_particles<P, true><<<nbk, threads, smem, st>>>(g, ppd, N, X0, X1, noise, pflags, q, nb, partner, btype, aa, rec, orig_id,
+        k_particles<P, true><<<nbk, threads, smem, st>>>(g, ppd, N, X0, X1, noise, pflags, q, brow, partner, btype, aa, rec, orig_id,
                                                      reinterpret_cast<curandState *>(rng), d_step, fout, integrate, tc, cap);
     else
-        k_particles<P, false><<<nbk, threads, smem, st>>>(g, ppd, N, X0, X1, noise, pflags, q, nb, partner, btype, aa, rec, orig_id,
+        k_particles<P, false><<<nbk, threads, smem, st>>>(g, ppd, N, X0, X1, noise, pflags, q, brow, partner, btype, aa, rec, orig_id,
                                                reinterpret_cast<curandState *>(rng), d_step, fout, integrate, tc, cap);
 }
 
@@ -692,13 +737,13 @@ void init_particle_attributes()
 }
 
 cudaError_t launch_particles(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd, float *X0,
-                             float *X1, float *noise, const uint32_t *pflags, const float *q, const uint8_t *nb,
+                             float *X1, float *noise, const uint32_t *pflags, const float *q, const int *brow,
                              const int *partner, const uint8_t *btype, AngleArrays aa, const float4 *rec,
                              const int *orig_id, void *rng_states, const long long *d_step, float *fout, int integrate,
                              const TileCfg &tc, cudaStream_t st)
 {
     if (pp.N == 0) return cudaSuccess;
-#define TILD_PL(P) part_launch<P>(g, ppd, pp.N, X0, X1, noise, pflags, q, nb, partner, btype, aa, rec, orig_id, \
+#define TILD_PL(P) part_launch<P>(g, ppd, pp.N, X0, X1, noise, pflags, q, brow, partner, btype, aa, rec, orig_id, \
                                   rng_states, d_step, fout, integrate, tc, pp.nwall > 0, st)
     switch (pp.order) {
         case 0: TILD_PL(0); break;
@@ -727,12 +772,12 @@ cudaError_t launch_rng_init(void *states, const int *orig_id, int n, unsigned lo
 }
 
 cudaError_t launch_bond_energy(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd, const float *X0,
-                               const float *X1, const long long *d_step, const uint8_t *nb, const int *partner,
+                               const float *X1, const long long *d_step, const int *brow, const int *partner,
                                const uint8_t *btype, AngleArrays aa, const uint32_t *pflags, double *partials,
                                int *nblocks_out, cudaStream_t st)
 {
     const int nbk = pp.N > 0 ? (pp.N + 255) / 256 : 1;
-    k_bond_energy<<<nbk, 256, 0, st>>>(g, ppd, pp.N, X0, X1, d_step, nb, partner, btype, aa, pflags, partials);
+    k_bond_energy<<<nbk, 256, 0, st>>>(g, ppd, pp.N, X0, X1, d_step, brow, partner, btype, aa, pflags, partials);
     if (nblocks_out) *nblocks_out = nbk;
     return cudaGetLastError();
 }

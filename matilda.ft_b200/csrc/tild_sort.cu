@@ -125,21 +125,20 @@ __global__ void k_newpos(int N, const uint32_t *__restrict__ key, const int *__r
 struct PermArrays {
     const float *X0, *X1, *noise, *q;
     const uint32_t *flags;
-    const int *orig, *partner;
-    const uint8_t *nb, *btype;
+    const int *orig, *brow;
     const curandState *rng;
     const uint8_t *na, *atype;
     const int *ang;
     float *X0n, *X1n, *noisen, *qn;
     uint32_t *flagsn;
-    int *orign, *partnern;
-    uint8_t *nbn, *btypen;
+    int *orign;
+    uint32_t *degn;   // bond count of every new slot (the CSR rows' lengths in the new order)
     curandState *rngn;
     uint8_t *nan, *atypen;
     int *angn;
 };
 
-__global__ void k_permute(int N, int maxb, int maxa, PermArrays a, const int *__restrict__ newpos)
+__global__ void k_permute(int N, int maxa, PermArrays a, const int *__restrict__ newpos)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= N) return;
@@ -153,12 +152,7 @@ __global__ void k_permute(int N, int maxb, int maxa, PermArrays a, const int *__
     a.flagsn[s] = a.flags[p];
     a.orign[s] = a.orig[p];
     if (a.q) a.qn[s] = a.q[p];
-    const int nbp = a.nb[p];
-    a.nbn[s] = (uint8_t)nbp;
-    for (int b = 0; b < maxb; b++) {
-        a.partnern[s * maxb + b] = b < nbp ? newpos[a.partner[p * maxb + b]] : 0;
-        a.btypen[s * maxb + b] = a.btype[p * maxb + b];
-    }
+    if (a.brow) a.degn[s] = (uint32_t)(a.brow[p + 1] - a.brow[p]);
     if (a.rng) a.rngn[s] = a.rng[p];
     if (a.na) {   // angles: all three particle slots renumbered
         const int nap = a.na[p];
@@ -168,6 +162,21 @@ __global__ void k_permute(int N, int maxb, int maxa, PermArrays a, const int *__
                 a.angn[(s * maxa + k) * 3 + r] = k < nap ? newpos[a.ang[(p * maxa + k) * 3 + r]] : 0;
             a.atypen[s * maxa + k] = a.atype[p * maxa + k];
         }
+    }
+}
+
+// CSR bond rows in the new slot order: row p moves to the new row of slot newpos[p]
+// (offsets from the scan of the new order's bond counts), its partners renumbered.
+__global__ void k_permute_bonds(int N, const int *__restrict__ brow, const int *__restrict__ partner,
+                                const uint8_t *__restrict__ btype, const int *__restrict__ newpos,
+                                const int *__restrict__ brown, int *__restrict__ partnern, uint8_t *__restrict__ btypen)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    const int k0 = brow[p], k1 = brow[p + 1], d = brown[newpos[p]];
+    for (int k = k0; k < k1; k++) {
+        partnern[d + k - k0] = newpos[partner[k]];
+        btypen[d + k - k0] = btype[k];
     }
 }
 
@@ -199,8 +208,7 @@ uint32_t sort_key_count(const Geom &g)
     return 1u << (3 * bits);
 }
 
-cudaError_t launch_sort(const Geom &g, int N, int maxb, int maxa, const SortScratch &w, const PermIn &in,
-                        cudaStream_t st)
+cudaError_t launch_sort(const Geom &g, int N, int maxa, const SortScratch &w, const PermIn &in, cudaStream_t st)
 {
     if (N == 0) return cudaSuccess;
     const uint32_t nk = sort_key_count(g);
@@ -214,10 +222,11 @@ cudaError_t launch_sort(const Geom &g, int N, int maxb, int maxa, const SortScra
     k_newpos<<<nbk, 256, 0, st>>>(N, w.key, w.rank, w.start, w.newpos);
     PermArrays a;
     a.X0 = in.X0; a.X1 = in.X1; a.noise = in.noise; a.q = in.q; a.flags = in.flags; a.orig = in.orig;
-    a.partner = in.partner; a.nb = in.nb; a.btype = in.btype;
+    a.brow = in.brow;
     a.rng = reinterpret_cast<const curandState *>(in.rng);
     a.X0n = w.X0; a.X1n = w.X1; a.noisen = w.noise; a.qn = w.q; a.flagsn = w.flags; a.orign = w.orig;
-    a.partnern = w.partner; a.nbn = w.nb; a.btypen = w.btype;
+    // the ranks are spent once the new slots exist: their array takes the new bond counts
+    a.degn = reinterpret_cast<uint32_t *>(w.rank);
     a.rngn = reinterpret_cast<curandState *>(w.rng);
     a.na = in.na;
     a.atype = in.atype;
@@ -225,7 +234,14 @@ cudaError_t launch_sort(const Geom &g, int N, int maxb, int maxa, const SortScra
     a.nan = w.na;
     a.atypen = w.atype;
     a.angn = w.ang;
-    k_permute<<<nbk, 256, 0, st>>>(N, maxb, maxa, a, w.newpos);
+    k_permute<<<nbk, 256, 0, st>>>(N, maxa, a, w.newpos);
+    if (in.brow) {   // new CSR rows: exclusive scan of the counts (brow[N] never changes), then the rows
+        const int nsn = (N + kScanBlock - 1) / kScanBlock;
+        k_scan_totals<<<nsn, kScanBlock, 0, st>>>(a.degn, N, w.totalsN);
+        k_scan_partials<<<1, kScanBlock, 0, st>>>(w.totalsN, nsn);
+        k_scan_apply<<<nsn, kScanBlock, 0, st>>>(a.degn, N, w.totalsN, reinterpret_cast<uint32_t *>(w.brow));
+        k_permute_bonds<<<nbk, 256, 0, st>>>(N, in.brow, in.partner, in.btype, w.newpos, w.brow, w.partner, w.btype);
+    }
     return cudaGetLastError();
 }
 

@@ -371,11 +371,13 @@ def box_from_spec(spec, device=0, options=None, steps_script=False, base_dir=Non
     b.command("randSeed %d" % spec.seed)
     if spec.charges is not None:
         b.command("doCharges")
+    if getattr(spec, "max_bonds", None):
+        b.command("MAXBONDS %d" % spec.max_bonds)
     for t, lb in enumerate(spec.species):
         b.command("species %s mass %.9g mobility %.9g" % (lb, spec.masses[t], spec.mobility[t]))
     b.set_particles(spec.x, spec.types, spec.mol, spec.charges)
     if len(spec.bonds):
-        b.command("bond 1 harmonic %.9g %.9g" % (spec.bond_k, spec.bond_req))
+        b.command(spec.bond_command())
         b.set_bonds(spec.bonds)
     for line in spec.angle_commands():
         b.command(line)

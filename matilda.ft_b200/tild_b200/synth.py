@@ -53,7 +53,7 @@ class SystemSpec:
     def __init__(self, name, L, grid, x, types, species, bonds, mol, charges=None,
                  potentials=(), order=3, delt=0.005, bond_k=1.5, bond_req=0.0, seed=1,
                  dim=3, integrator="GJF", masses=None, mobility=None, log_freq=100, angles=None,
-                 angle_types=None, angle_params=(), bond_style="harmonic"):
+                 angle_types=None, angle_params=(), bond_style="harmonic", max_bonds=None):
         self.name = name
         self.L = np.asarray(L, np.float32)
         self.grid = np.asarray(grid, np.int32)
@@ -69,6 +69,7 @@ class SystemSpec:
         self.bond_k = bond_k
         self.bond_req = bond_req
         self.bond_style = bond_style   # "harmonic" or "fene" (ps_deviceBonds.cu:54-62)
+        self.max_bonds = max_bonds     # MAXBONDS word (None: the reference's default of 2)
         self.seed = seed
         self.dim = dim
         self.integrator = integrator
@@ -158,6 +159,8 @@ class SystemSpec:
              "pmeorder %d" % self.order, "randSeed %d" % self.seed]
         if self.charges is not None:
             s.append("doCharges")
+        if self.max_bonds:
+            s.append("MAXBONDS %d" % self.max_bonds)
         for t, lb in enumerate(self.species):
             s.append("species %s mass %.9g mobility %.9g" % (lb, self.masses[t], self.mobility[t]))
         s.append("readData %s" % data_name)
@@ -369,3 +372,61 @@ def small_system(seed=0, n_chains=20, nper=8, L=6.0, grid=(12, 12, 12), order=3,
                       chain_bonds(n_chains, nper), mol, charges=q, potentials=pots, order=order,
                       seed=seed + 11, dim=dim, angles=ang, angle_types=atyp,
                       angle_params=angle_params or (), **spec_kw)
+
+
+def branched_system(seed=0, L=7.0, grid=(14, 14, 14), order=3, charges=True):
+    """Branched molecules for the bond list: combs (a 12-bead backbone with 3-bead side
+    chains on beads 2, 6 and 10: degree 3) and stars (a centre with five 4-bead arms:
+    degree 5), plus free beads; MAXBONDS 5."""
+    rng = np.random.default_rng(seed)
+    xs, bonds, mol = [], [], []
+    def walk(start, n):
+        pts = [start]
+        for _ in range(n - 1):
+            pts.append(pts[-1] + rng.normal(0.0, 1.0 / math.sqrt(3.0), 3))
+        return pts
+    n = 0
+    for c in range(6):   # combs
+        back = walk(rng.uniform(0, L, 3), 12)
+        ids = list(range(n, n + 12))
+        xs += back
+        bonds += [(ids[i], ids[i + 1]) for i in range(11)]
+        mol += [c] * 12
+        n += 12
+        for b in (2, 6, 10):
+            side = walk(back[b] + rng.normal(0.0, 0.6, 3), 3)
+            xs += side
+            bonds += [(ids[b], n)] + [(n + i, n + i + 1) for i in range(2)]
+            mol += [c] * 3
+            n += 3
+    for s_ in range(5):   # stars
+        centre = rng.uniform(0, L, 3)
+        xs.append(centre)
+        c0 = n
+        mol.append(6 + s_)
+        n += 1
+        for a in range(5):
+            arm = walk(centre + rng.normal(0.0, 0.6, 3), 4)
+            xs += arm
+            bonds += [(c0, n)] + [(n + i, n + i + 1) for i in range(3)]
+            mol += [6 + s_] * 4
+            n += 4
+    for f in range(30):   # free beads
+        xs.append(rng.uniform(0, L, 3))
+        mol.append(11 + f)
+        n += 1
+    x = np.mod(np.array(xs), L)
+    N = x.shape[0]
+    types = rng.integers(0, 2, size=N).astype(np.int32)
+    q = None
+    if charges:
+        q = rng.choice([-1.0, 0.0, 1.0], size=N).astype(np.float32)
+        s = q.sum()
+        idx = np.nonzero(q == (1.0 if s > 0 else -1.0))[0]
+        q[idx[: int(abs(s))]] = 0.0
+    pots = [dict(kind="gaussian", I="A", J="B", A=2.5, sigma=0.7),
+            dict(kind="gaussian", I="all", J="all", A=1.0, sigma=0.7)]
+    if charges:
+        pots.append(dict(kind="charges", lB=1.0, sigma=0.5))
+    return SystemSpec("branched%d" % seed, [L, L, L], list(grid), x, types, ["A", "B"], np.array(bonds), mol,
+                      charges=q, potentials=pots, order=order, seed=seed + 11, max_bonds=5)

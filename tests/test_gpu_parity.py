@@ -54,6 +54,8 @@ SYSTEMS = {
     "prime_lines": lambda: synth.small_system(seed=14, order=3, grid=(31, 37, 29), L=11.0, charges=True),
     "angles": lambda: synth.small_system(seed=15, order=3, charges=True, angle_params=ANGLES),
     "free_particles": lambda: synth.small_system(seed=9, order=3, n_free=50, charges=True),
+    # combs (degree 3) and stars (degree 5): rows of every length in the CSR bond list
+    "branched": lambda: synth.branched_system(seed=3),
     # harmonic walls (per-particle potentials) beside grid potentials
     "walls": lambda: synth.small_system(seed=22, order=3, charges=True, pots=[
         dict(kind="gaussian", I="A", J="B", A=2.0, sigma=0.7), dict(kind="charges", lB=1.0, sigma=0.5),
@@ -74,6 +76,27 @@ def test_forces_match_oracle(name):
     fref, _ = oracle.forces(sysm, prec=64)
     err = force_error(f, fref, angle_force_tolerance(sysm, F_TOL))
     assert err <= 1.0, "%s: force error %.3g of the tolerance" % (name, err)
+
+
+@pytest.mark.parametrize("name", ["charged_o3", "erf", "odd_grid", "prime_lines", "radix7_grid"])
+def test_grid_forces_match_oracle(name):
+    """The spectral stage alone (cufftWrapperSingle + CalcForces, Box.cu:107-127,
+    ps_potential.cu:41-125): every force group's grid force (PS_Group::d_gridForce) after
+    a force evaluation against the oracle's FP64 transforms of the FP64 densities, within
+    1e-5 of the field's largest value, and zeros for a group without grid force."""
+    spec = SYSTEMS[name]()
+    sysm = spec_to_system(spec)
+    _, inter = oracle.forces(sysm, prec=64)
+    glist = oracle.groups(sysm)
+    with make_box(spec) as b:
+        b.forces()
+        for gi, (gname, _, _) in enumerate(glist):
+            gf = b.grid_force(gname)
+            if gi not in inter["gridforce"]:
+                assert not gf.any(), gname
+                continue
+            ref = inter["gridforce"][gi].T
+            assert np.abs(gf - ref).max() <= 1e-5 * np.abs(ref).max(), gname
 
 
 @pytest.mark.parametrize("order", [0, 1, 2, 3, 4])
@@ -111,7 +134,7 @@ def test_densities_match_oracle():
                 assert np.abs(gq - rhoq).max() <= 1e-6 * np.abs(rhoq).max()
 
 
-@pytest.mark.parametrize("name", ["diblock_o3", "charged_o3", "erf", "odd_grid", "prime_lines", "walls"])
+@pytest.mark.parametrize("name", ["diblock_o3", "charged_o3", "erf", "odd_grid", "prime_lines", "walls", "branched"])
 def test_energies_match_oracle(name):
     spec = SYSTEMS[name]()
     sysm = spec_to_system(spec)
@@ -204,6 +227,36 @@ def test_spatial_sort_is_invisible():
     for o in outs[1:]:
         for a, r in zip(o, outs[0]):
             assert np.array_equal(a, r)
+
+
+def test_branched_bonds_sorted_and_integrated_like_the_oracle():
+    """The CSR bond list under re-sorting: combs and stars (rows of 0 to 5 partners) keep
+    bit-identical trajectories with no sort and a sort every step (deterministic mode),
+    their bond energy matches the oracle after the steps, and 100 Philox steps follow the
+    FP64 oracle fed the same noise (the drift bar of the linear chains)."""
+    spec = synth.branched_system(seed=4)
+    outs = []
+    for interval in (0, 1):
+        with make_box(spec, deterministic=1, sort_interval=interval) as b:
+            b.step(20)
+            outs.append((b.positions(), b.forces(), b.thermo()["Ubond"]))
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+    assert outs[0][2] == outs[1][2]
+    sysm = spec_to_system(spec)
+    sysm.x = outs[0][0].astype(np.float32)
+    ub, _ = oracle.bond_energy(sysm)
+    assert abs(outs[0][2] - ub) <= 1e-6 * abs(ub)
+    sysm = spec_to_system(spec)
+    traj = oracle.Trajectory(sysm, 64)
+    ids = np.arange(sysm.N)
+    with make_box(spec, sort_interval=1) as b:
+        b.step(100)
+        x = b.positions()
+    for step in range(100):
+        traj.step(oracle.philox_normals(spec.seed, step, ids))
+    d = np.abs(x - traj.positions())
+    d = np.minimum(d, spec.L - d)
+    assert d.max() <= 1e-3 and np.median(d) <= 1e-4, (d.max(), np.median(d))
 
 
 @pytest.mark.parametrize("integ", ["GJF", "EM"])
