@@ -1210,6 +1210,8 @@ void Box::allocDevice()
     dEpart = dalloc<double>((size_t)nblkZ * (ksHost.neterms + 6));
     dBpart = dalloc<double>((size_t)nblkP * kPartialCols);
     dRes = dalloc<double>(kResSize);
+    dErr = dalloc<int>(1);
+    ck(cudaMemsetAsync(dErr, 0, sizeof(int), stream), "zero error flag");
     dTmp = dalloc<float>(3 * N);
     if (sharedDevice) hKsPinned = new KSpace;   // pinned host memory would synchronise the device when freed
     else ck(cudaMallocHost(&hKsPinned, sizeof(KSpace)), "cudaMallocHost");
@@ -1424,7 +1426,7 @@ void Box::enqueueStep(bool energy, bool integrate, float *fout_dev)
     }
     ck(launch_particles(g, ppHost, dPp, dX[0], dX[1], dNoise, dFlags, dQ, dBrow, dPartner, dBtype,
                         AngleArrays{dNa, dAtype, dAng}, dRec, dOrig, dRng,
-                        dStep, fout_dev, integrate ? 1 : 0, tileCfg(), st),
+                        dStep, fout_dev, integrate ? 1 : 0, tileCfg(), recordMap(), dErr, st),
        "particles");
     mark(STAGE_PARTICLES);
     if (integrate) ck(launch_tick(dStep, st), "tick");
@@ -1465,6 +1467,7 @@ std::vector<double> Box::readEnergies(bool)
     std::vector<double> r(kResSize, 0.0);
     ck(cudaStreamSynchronize(stream), "sync");
     ck(cudaMemcpy(r.data(), dRes, sizeof(double) * r.size(), cudaMemcpyDeviceToHost), "read energies");
+    checkDeviceErrors();
     if (r[kResNonFinite] > 0.0)   // the run has blown up: stop instead of logging NaN
         fail(TILD_ERR_DEVICE, std::to_string((long long)r[kResNonFinite]) +
                                   " particle(s) with a non-finite position at step " + std::to_string(deviceStep()));
@@ -1930,6 +1933,7 @@ void Box::forces(float *f_out)
     enqueueStep(false, false, dF);
     ck(launch_unpermute_rows((int)nstot, 3, dOrig, dF, dTmp, stream), "unpermute forces");
     readRows3(dTmp, f_out);
+    checkDeviceErrors();
 }
 
 // dev[3n] (original order) -> host out[n*Dim], the reference's layout of x and f
@@ -1976,6 +1980,12 @@ TileCfg Box::tileGeometry(int codes, bool direct) const
     t.pbox = (((ex | 1) * ey) | 1) * ez;
     t.direct = direct ? 1 : 0;
     t.margin = margin;
+    if (g.nz > 1 && !direct) {   // TMA box: odd x and y edges keep the dense pitches odd
+        t.te[0] = ex | 1;
+        t.te[1] = ey | 1;
+        t.te[2] = ez;
+        t.pbox = std::max(t.pbox, t.te[0] * t.te[1] * t.te[2]);
+    }
     return t;
 }
 
@@ -2014,6 +2024,31 @@ void Box::autotuneTiles()
     cudaEventDestroy(e1);
     tiles = pick;
     tunedMs = best / 3.f;
+}
+
+// TMA descriptor of the force records for the current tiles' box (rebuilt when the tiles
+// change); NULL where none can be built, and the particle pass stages with cp.async.
+const CUtensorMap *Box::recordMap()
+{
+    if (tiles.te[0] <= 0 || !dRec) return nullptr;
+    if (!recMapOk || std::memcmp(recMapTe, tiles.te, sizeof(recMapTe)) != 0) {
+        recMapOk = build_record_map(&recMap, dRec, geom, std::max(1, (int)fgroups.size()), tiles.te);
+        std::memcpy(recMapTe, tiles.te, sizeof(recMapTe));
+    }
+    return recMapOk ? &recMap : nullptr;
+}
+
+// Device-side failures the kernels record instead of faulting (a staging wait that ran
+// out): reported once as TILD_ERR_DEVICE, then cleared.
+void Box::checkDeviceErrors()
+{
+    int e = 0;
+    ck(cudaMemcpyAsync(&e, dErr, sizeof(int), cudaMemcpyDeviceToHost, stream), "read error flag");
+    ck(cudaStreamSynchronize(stream), "read error flag");
+    if (e) {
+        ck(cudaMemsetAsync(dErr, 0, sizeof(int), stream), "clear error flag");
+        fail(TILD_ERR_DEVICE, std::to_string(e) + " staging wait(s) of the particle pass ran out of time");
+    }
 }
 
 TileCfg Box::tileCfg() const
@@ -2237,6 +2272,7 @@ void Box::modifyBox(const std::string &rest)
                 buildPlan();
                 if ((int)dfields.size() > std::max(1, ndOld) || (int)fgroups.size() > std::max(1, nfOld))
                     fail(TILD_ERR_STATE, "plan grew after removing a potential");
+                recMapOk = false;   // the record descriptor follows the force-group count
                 uploadFlags();
                 ck(cudaDeviceSynchronize(), "modify");
             }

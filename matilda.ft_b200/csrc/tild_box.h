@@ -149,6 +149,8 @@ private:
     void uploadParticles();
     void enqueueStep(bool energy, bool integrate, float *fout_dev);
     void enqueueEnergyOnly(bool lastStepStart = false);
+    const CUtensorMap *recordMap();
+    void checkDeviceErrors();
     void updateRamps(int64_t step, int64_t maxSteps);
     void captureGraphs();
     void dropGraphs();
@@ -242,6 +244,10 @@ private:
     float *dNoise = nullptr, *dQ = nullptr, *dF = nullptr;
     uint32_t *dFlags = nullptr;
     int *dBrow = nullptr;                        // CSR bond rows [N+1] (NULL without bonds)
+    int *dErr = nullptr;                         // failures the kernels record (see checkDeviceErrors)
+    CUtensorMap recMap;                          // TMA descriptor of dRec for the tiles' box
+    int recMapTe[3] = {0, 0, 0};
+    bool recMapOk = false;
     uint8_t *dBtype = nullptr;
     uint8_t *dNa = nullptr, *dAtype = nullptr;   // angles (NULL when the box has none)
     int *dAng = nullptr;

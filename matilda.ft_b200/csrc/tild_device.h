@@ -14,6 +14,7 @@
 //   rec[F][M]      float4  grid force of each force group (x, y, z, 0)
 #pragma once
 #include <cstdint>
+#include <cuda.h>            // CUtensorMap (a host-built TMA descriptor; no driver library linked)
 #include <cuda_runtime.h>
 
 namespace tild {
@@ -153,7 +154,12 @@ struct TileCfg {
     int pbox;     // particle pass: records of the fixed tile box (odd pitches)
     int margin;   // particle pass: drift margin of the fixed box, cells per side
     int direct;   // particle pass: 1 = read every stencil through L1/L2 (no staged box)
+    int te[3];    // particle pass: edges of the TMA box of force records (0: stage with cp.async)
 };
+
+// TMA descriptor of the force records rec[F][nz][ny][nx] (float4) for boxes of te[] points:
+// false where it cannot be built (the particle pass then stages with cp.async).
+bool build_record_map(CUtensorMap *map, const float4 *rec, const Geom &g, int nfg, const int *te);
 
 struct AngleArrays {        // angles in slot order (all NULL: the box has none)
     const uint8_t *na, *atype;  // [n] angles per particle, [n*maxa] types
@@ -197,7 +203,8 @@ cudaError_t launch_particles(const Geom &g, const ParticleParams &pp, const Part
                              const float *q, const int *brow, const int *partner,
                              const uint8_t *btype, AngleArrays aa, const float4 *rec, const int *orig_id,
                              void *rng_states, const long long *d_step, float *fout,
-                             int integrate, const TileCfg &tc, cudaStream_t st);
+                             int integrate, const TileCfg &tc, const CUtensorMap *rec_map, int *err,
+                             cudaStream_t st);
 void init_particle_attributes();
 cudaError_t launch_tick(long long *d_step, cudaStream_t st);
 

@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 
 namespace tild {
 
@@ -253,6 +254,42 @@ __device__ __forceinline__ void cp_async16p(void *smem_dst, const void *gsrc)
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
 
+// ---- TMA staging of the force-record box (cp.async.bulk.tensor with an mbarrier) ----
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long *mb)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(mb)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+
+// One thread: the box of force group f whose first point is grid point (x, y, z)
+// (unwrapped; points outside the grid arrive as zeros) into dst, completing on mb.
+__device__ __forceinline__ void tma_load_records(float4 *dst, const CUtensorMap *map, int x, int y, int z, int f,
+                                                 unsigned long long *mb, unsigned bytes)
+{
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");   // earlier reads of dst come first
+    asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n"
+                 ::"r"(smem_u32(mb)), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];\n"
+                 ::"r"(smem_u32(dst)), "l"(map), "r"(0), "r"(x), "r"(y), "r"(z), "r"(f), "r"(smem_u32(mb))
+                 : "memory");
+}
+
+// Bounded wait for phase `phase` of mb: false if it did not complete within the limit.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *mb, unsigned phase)
+{
+    for (int i = 0; i < (1 << 22); i++) {
+        unsigned ok;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                     " selp.u32 %0, 1, 0, p;\n}\n"
+                     : "=r"(ok) : "r"(smem_u32(mb)), "r"(phase) : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
 constexpr int kPartBox = 4096;     // float4 records staged per force group (64 KB)
 constexpr int kPartWindow = 256;   // slots per CTA when the particles are not sorted
 
@@ -308,7 +345,9 @@ constexpr int kPartThreadsMax = 448;
 // group order like any other, so the sums do not depend on which path served them.
 // EXTRA: the box has angles or walls (compiled out of the common instantiation, whose
 // schedule the unused terms would otherwise disturb)
-template <int P, bool EXTRA>
+// TMA: sorted tiles stage their boxes with one TMA load (the host selects this instantiation
+// when it holds a descriptor for the tiles' box); else with per-thread cp.async copies.
+template <int P, bool EXTRA, bool TMA>
 __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const ParticleParams *__restrict__ ppd, int N,
                                                       float *__restrict__ X0, float *__restrict__ X1,
                                                       float *__restrict__ noise, const uint32_t *__restrict__ pflags,
@@ -318,10 +357,12 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
                                                       const float4 *__restrict__ rec, const int *__restrict__ orig_id,
                                                       curandState *__restrict__ rng,
                                                       const long long *__restrict__ d_step, float *__restrict__ fout,
-                                                      int integrate_flag, TileCfg tc, int box_cap)
+                                                      int integrate_flag, TileCfg tc, int box_cap,
+                                                      const __grid_constant__ CUtensorMap rmap, int *__restrict__ err)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
-    float4 *box = reinterpret_cast<float4 *>(smraw);
+    // the box starts on a 128-byte boundary of the shared window (a TMA destination)
+    float4 *box = reinterpret_cast<float4 *>(smraw + ((128u - (smem_u32(smraw) & 127u)) & 127u));
     // per-thread integrator operands (x_{t-1}[3], previous noise[3], particle id), planes of blockDim
     float *iop = reinterpret_cast<float *>(box + box_cap);
     __shared__ TileShared ts;
@@ -329,6 +370,7 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
     __shared__ int outP[kPartOut];
     __shared__ int nout;
     __shared__ int deal_src[kPartThreadsMax];   // per warp: the lane whose particle a lane gathers
+    __shared__ __align__(8) unsigned long long tma_bar;   // completion of a TMA box load
     const ParticleParams &pp = *ppd;
     const long long step = *d_step;
     const float *__restrict__ Xc = (step & 1) ? X1 : X0;   // x_t
@@ -344,15 +386,58 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
         staged = E[0] <= kMaxBoxEdge && E[1] <= kMaxBoxEdge && E[2] <= kMaxBoxEdge &&
                  (long long)((((E[0] | 1) * E[1]) | 1)) * E[2] <= box_cap;
     }
-    const int E0 = E[0] | 1, E01 = (E0 * E[1]) | 1;   // odd pitches (16-byte records)
+    // The box arrives by one TMA load of the fixed box te[] (odd edges, so the dense
+    // pitches stay odd), or by per-thread cp.async copies with odd pitches.  A box that
+    // leaves the grid gets its periodic images by cp.async after the TMA load.
+    const bool use_tma = TMA && staged;
+    const int E0 = TMA ? tc.te[0] : (E[0] | 1);
+    const int E01 = TMA ? tc.te[0] * tc.te[1] : ((E0 * E[1]) | 1);
+    const bool wraps = use_tma && (lo[0] < 0 || lo[1] < 0 || lo[2] < 0 || lo[0] + tc.te[0] > g.nx ||
+                                   lo[1] + tc.te[1] > g.ny || lo[2] + tc.te[2] > g.nz);
+    unsigned tphase = 0u;
     if (staged) {
         if (threadIdx.x < 3) {
             ts.ref[threadIdx.x] = lo[threadIdx.x];
             ts.lo[threadIdx.x] = 0;
         }
+        if (use_tma && threadIdx.x == 0) mbar_init(&tma_bar);
         __syncthreads();
-        tile_tables(ts, g.nx, g.ny, g.nz, E);
+        tile_tables(ts, g.nx, g.ny, g.nz, use_tma ? tc.te : E);
     }
+    const int te[3] = {tc.te[0], tc.te[1], tc.te[2]};
+    const unsigned tbytes = (unsigned)(E01 * te[2]) * 16u;
+// start the copy of force group f's box (every thread calls it)
+#define TILD_STAGE(f)                                                                                      \
+    do {                                                                                                   \
+        if (TMA) {                                                                                         \
+            if (threadIdx.x == 0) tma_load_records(box, &rmap, lo[0], lo[1], lo[2], (f), &tma_bar, tbytes); \
+        } else {                                                                                           \
+            const float4 *rf_ = rec + (long long)(f) * g.M;                                                \
+            tile_for_each(ts, E, E0, E01, [&](int v, int m) { cp_async16p(box + v, rf_ + m); });           \
+            asm volatile("cp.async.commit_group;\n" ::: "memory");                                         \
+        }                                                                                                  \
+    } while (0)
+// wait for it; a TMA box that leaves the grid then gets its periodic images by cp.async
+#define TILD_STAGE_WAIT(f)                                                                                 \
+    do {                                                                                                   \
+        if (TMA) {                                                                                         \
+            if (!mbar_wait(&tma_bar, tphase)) { /* record the failure, wait once more for the copy */      \
+                if (threadIdx.x == 0) atomicAdd(err, 1);                                                   \
+                mbar_wait(&tma_bar, tphase);                                                               \
+            }                                                                                              \
+            tphase ^= 1u;                                                                                  \
+            if (wraps) {                                                                                   \
+                const float4 *rf_ = rec + (long long)(f) * g.M;                                            \
+                const int l0 = lo[0], l1 = lo[1], l2 = lo[2];                                              \
+                tile_for_each_xyz(ts, te, E0, E01, [=](int v, int m, int lx, int ly, int lz) {             \
+                    if ((unsigned)(l0 + lx) >= (unsigned)g.nx || (unsigned)(l1 + ly) >= (unsigned)g.ny ||  \
+                        (unsigned)(l2 + lz) >= (unsigned)g.nz)                                             \
+                        cp_async16p(box + v, rf_ + m);                                                     \
+                });                                                                                        \
+            }                                                                                              \
+        }                                                                                                  \
+        asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");                    \
+    } while (0)
     for (int c0 = r0; c0 < r1; c0 += blockDim.x) {
         const int p = c0 + threadIdx.x;
         const bool act = p < r1;
@@ -412,11 +497,7 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
         int fg = 0;
         while (fg < pp.nfg && !((fmall >> fg) & 1u)) fg++;
         // 2. start staging the first force group's box
-        if (staged && fg < pp.nfg) {
-            const float4 *rf = rec + (long long)fg * g.M;
-            tile_for_each(ts, E, E0, E01, [&](int v, int m) { cp_async16p(box + v, rf + m); });
-            asm volatile("cp.async.commit_group;\n" ::: "memory");
-        }
+        if (staged && fg < pp.nfg) TILD_STAGE(fg);
         // 3. helpers gather the out-of-box particles of every group from global memory
         if (threadIdx.x < nhelp) {
             const int ph = outP[threadIdx.x];
@@ -493,10 +574,9 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
             if (staged) {
                 if (!first) {
                     __syncthreads();   // every gather from the previous group's box is done
-                    tile_for_each(ts, E, E0, E01, [&](int v, int m) { cp_async16p(box + v, rf + m); });
-                    asm volatile("cp.async.commit_group;\n" ::: "memory");
+                    TILD_STAGE(fg);
                 }
-                asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+                TILD_STAGE_WAIT(fg);
                 __syncthreads();   // every thread's copies have landed (and the helpers' results)
             } else if (first) {
                 __syncthreads();   // the helpers' results are visible
@@ -571,6 +651,9 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
         __syncthreads();   // the box, nout and the helpers' results are reused by the next pass
     }
 }
+
+#undef TILD_STAGE
+#undef TILD_STAGE_WAIT
 
 __global__ void k_tick(long long *d_step) { *d_step += 1; }
 
@@ -700,51 +783,95 @@ __global__ void k_reduce_partials(const double *partials, int nblocks, int ncols
 }
 
 
-constexpr size_t kPartSmemMax = kPartBox * sizeof(float4) + kPartThreadsMax * 7 * sizeof(float);
+constexpr size_t kPartSmemMax = 128 + kPartBox * sizeof(float4) + kPartThreadsMax * 7 * sizeof(float);
 
 template <int P>
 static void part_launch(const Geom &g, const ParticleParams *ppd, int N, float *X0, float *X1, float *noise,
                         const uint32_t *pflags, const float *q, const int *brow, const int *partner,
                         const uint8_t *btype, AngleArrays aa, const float4 *rec, const int *orig_id, void *rng,
-                        const long long *d_step, float *fout, int integrate, const TileCfg &tc, bool walls,
-                        cudaStream_t st)
+                        const long long *d_step, float *fout, int integrate, const TileCfg &tc0, bool walls,
+                        const CUtensorMap *rec_map, int *err, cudaStream_t st)
 {
+    TileCfg tc = tc0;
+    CUtensorMap none;
+    std::memset(&none, 0, sizeof(none));
+    if (!rec_map || tc.direct) tc.te[0] = tc.te[1] = tc.te[2] = 0;   // no TMA descriptor: cp.async staging
+    const CUtensorMap &rm = rec_map ? *rec_map : none;
     const int nbk = tc.start ? (tc.nkeys + tc.codes - 1) / tc.codes : (N + kPartWindow - 1) / kPartWindow;
     const int threads = tc.start ? std::min(tc.threads, kPartThreadsMax) : 256;
     const int cap = (tc.start && !tc.direct) ? std::min(tc.pbox, kPartBox) : 0;
-    const size_t smem = (size_t)cap * sizeof(float4) + (size_t)threads * 7 * sizeof(float);
+    // the box first (moved up to a 128-byte boundary), then the integrator operands
+    const size_t smem = 128 + (size_t)cap * sizeof(float4) + (size_t)threads * 7 * sizeof(float);
     const bool extra = aa.na != nullptr || walls;
-    if (extra)
-        k_particles<P, true><<<nbk, threads, smem, st>>>(g, ppd, N, X0, X1, noise, pflags, q, brow, partner, btype, aa, rec, orig_id,
-                                                     reinterpret_cast<curandState *>(rng), d_step, fout, integrate, tc, cap);
-    else
-        k_particles<P, false><<<nbk, threads, smem, st>>>(g, ppd, N, X0, X1, noise, pflags, q, brow, partner, btype, aa, rec, orig_id,
-                                               reinterpret_cast<curandState *>(rng), d_step, fout, integrate, tc, cap);
+    // TMA staging needs the descriptor and the whole fixed box inside the shared-memory box
+    const bool tma = tc.start && tc.te[0] > 0 && (long long)tc.te[0] * tc.te[1] * tc.te[2] <= cap;
+    curandState *rs = reinterpret_cast<curandState *>(rng);
+#define TILD_PK(EX, TM) \
+    k_particles<P, EX, TM><<<nbk, threads, smem, st>>>(g, ppd, N, X0, X1, noise, pflags, q, brow, partner, btype, aa, rec, \
+                                                     orig_id, rs, d_step, fout, integrate, tc, cap, rm, err)
+    if (extra) {
+        if (tma) TILD_PK(true, true);
+        else TILD_PK(true, false);
+    } else {
+        if (tma) TILD_PK(false, true);
+        else TILD_PK(false, false);
+    }
+#undef TILD_PK
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no driver library link).
+bool build_record_map(CUtensorMap *map, const float4 *rec, const Geom &g, int nfg, const int *te)
+{
+    typedef CUresult (*EncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                    const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static EncodeTiled fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult qr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &qr) != cudaSuccess ||
+            qr != cudaDriverEntryPointSuccess || !p) {
+            cudaGetLastError();
+            return false;
+        }
+        fn = reinterpret_cast<EncodeTiled>(p);
+    }
+    if (te[0] <= 0 || te[0] > 256 || te[1] > 256 || te[2] > 256 || g.nz < 2) return false;
+    // float4 records as 4 floats: (component, x, y, z, group); a box is one group's te[] points
+    const cuuint64_t dims[5] = {4, (cuuint64_t)g.nx, (cuuint64_t)g.ny, (cuuint64_t)g.nz, (cuuint64_t)nfg};
+    // byte strides of dimensions 1..4 (the components are contiguous)
+    const cuuint64_t st[4] = {16, 16ull * g.nx, 16ull * g.nx * g.ny, 16ull * (cuuint64_t)g.M};
+    const cuuint32_t box[5] = {4, (cuuint32_t)te[0], (cuuint32_t)te[1], (cuuint32_t)te[2], 1};
+    const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, const_cast<float4 *>(rec), dims, st, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 void init_particle_attributes()
 {
-    cudaFuncSetAttribute(k_particles<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
-    cudaFuncSetAttribute(k_particles<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
-    cudaFuncSetAttribute(k_particles<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
-    cudaFuncSetAttribute(k_particles<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
-    cudaFuncSetAttribute(k_particles<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
-    cudaFuncSetAttribute(k_particles<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
-    cudaFuncSetAttribute(k_particles<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
-    cudaFuncSetAttribute(k_particles<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
-    cudaFuncSetAttribute(k_particles<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
-    cudaFuncSetAttribute(k_particles<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);
+#define TILD_PA(P)                                                                                        \
+    cudaFuncSetAttribute(k_particles<P, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax); \
+    cudaFuncSetAttribute(k_particles<P, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);  \
+    cudaFuncSetAttribute(k_particles<P, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);  \
+    cudaFuncSetAttribute(k_particles<P, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax)
+    TILD_PA(0);
+    TILD_PA(1);
+    TILD_PA(2);
+    TILD_PA(3);
+    TILD_PA(4);
+#undef TILD_PA
 }
 
 cudaError_t launch_particles(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd, float *X0,
                              float *X1, float *noise, const uint32_t *pflags, const float *q, const int *brow,
                              const int *partner, const uint8_t *btype, AngleArrays aa, const float4 *rec,
                              const int *orig_id, void *rng_states, const long long *d_step, float *fout, int integrate,
-                             const TileCfg &tc, cudaStream_t st)
+                             const TileCfg &tc, const CUtensorMap *rec_map, int *err, cudaStream_t st)
 {
     if (pp.N == 0) return cudaSuccess;
 #define TILD_PL(P) part_launch<P>(g, ppd, pp.N, X0, X1, noise, pflags, q, brow, partner, btype, aa, rec, orig_id, \
-                                  rng_states, d_step, fout, integrate, tc, pp.nwall > 0, st)
+                                  rng_states, d_step, fout, integrate, tc, pp.nwall > 0, rec_map, err, st)
     switch (pp.order) {
         case 0: TILD_PL(0); break;
         case 1: TILD_PL(1); break;

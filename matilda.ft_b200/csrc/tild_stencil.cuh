@@ -263,6 +263,31 @@ __device__ __forceinline__ void tile_for_each(const TileShared &ts, const int *E
     }
 }
 
+// tile_for_each that also passes the element's box coordinates: f(v, m, lx, ly, lz).
+template <typename F>
+__device__ __forceinline__ void tile_for_each_xyz(const TileShared &ts, const int *E, int p1, int p2, F f)
+{
+    const int E0 = E[0], E1 = E[1], rows = E1 * E[2];
+    const int xw = E0 <= 32 ? E0 : 32;
+    const int rpp = blockDim.x / xw;
+    if ((int)threadIdx.x >= rpp * xw) return;
+    int row = threadIdx.x / xw;
+    const int lx0 = threadIdx.x - row * xw;
+    int lz = row / E1, ly = row - lz * E1;
+    const int dz = rpp / E1, dy = rpp - dz * E1;
+    for (; row < rows; row += rpp) {
+        const int rb = ts.zb[lz] + ts.yb[ly];
+        const int vb = lz * p2 + ly * p1;
+        for (int lx = lx0; lx < E0; lx += xw) f(vb + lx, rb + ts.xi[lx], lx, ly, lz);
+        lz += dz;
+        ly += dy;
+        if (ly >= E1) {
+            ly -= E1;
+            lz++;
+        }
+    }
+}
+
 // (g + i - shift + N) % N in the reference; a true modulo here so that positions the
 // reference would send out of bounds still land on the grid.
 __device__ __forceinline__ int wrapi(int v, int n)
