@@ -306,7 +306,7 @@ def c5_jobs(synth, args):
     return synth.config_c5_jobs(njobs=args.c5_jobs, nmin=2.0e4, nmax=1.0e6, smin=500, smax=5000)
 
 
-def cufft_times(torch, spec, nd, nfg, reps=10):
+def cufft_times(torch, spec, nd, nfg, reps=20):
     """The spectral stage done with cuFFT (through torch.fft) and torch elementwise
     kernels, device-timed on the same grid and field counts:
       chain: what our five passes do -- R2C of the nd density fields, phi_f = u(k) rho_f,
@@ -351,7 +351,7 @@ def cufft_times(torch, spec, nd, nfg, reps=10):
     for name, fn in (("chain", chain), ("reference_form", reference_form),
                      ("forward", lambda: torch.fft.rfftn(rho, dim=(1, 2, 3))),
                      ("inverse", lambda: torch.fft.irfftn(spec_b, s=(nz, ny, nx), dim=(1, 2, 3)))):
-        for _ in range(2):
+        for _ in range(5):   # plans and the caching allocator settle first
             fn()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
