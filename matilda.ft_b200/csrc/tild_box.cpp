@@ -182,6 +182,10 @@ void Box::setOption(const std::string &key, int64_t v)
     else if (key == "bspline4_exact") exact4 = (int)v;
     else if (key == "autotune") autotune = v != 0;
     else if (key == "direct_gather") directGather = v != 0;
+    else if (key == "deposit_codes") {
+        if (v != 0 && (v < 8 || v > 64 || (v & (v - 1)))) fail(TILD_ERR_ARG, "deposit_codes must be 0 or a power of two in [8, 64]");
+        depositCodes = (int)v;
+    }
     else if (key == "sort_interval") {
         if (v < 0) fail(TILD_ERR_ARG, "sort_interval must be >= 0");
         sortInterval = (int)v;
@@ -1223,6 +1227,7 @@ void Box::allocDevice()
         int codes = 8;
         while (codes < 64 && perCode * codes * 2.0 <= 192.0) codes *= 2;
         tiles = tileGeometry(codes, directGather);
+        dtiles = tileGeometry(depositCodes ? depositCodes : codes, true);
     }
     sortW.key = dalloc<uint32_t>(N);
     sortW.rank = dalloc<int>(N);
@@ -1408,7 +1413,7 @@ void Box::enqueueStep(bool energy, bool integrate, float *fout_dev)
             ck(launch_zero(dDepFix, sizeof(unsigned long long) * 2 * npair * g.M, st), "zero");
         else
             ck(launch_zero(dDep, sizeof(float2) * npair * g.M, st), "zero");
-        ck(launch_deposit(g, ppHost, dX[0], dX[1], dStep, dFlags, dQ, dDep, dDepFix, deterministic, tileCfg(), st), "deposit");
+        ck(launch_deposit(g, ppHost, dX[0], dX[1], dStep, dFlags, dQ, dDep, dDepFix, deterministic, depTileCfg(), st), "deposit");
         mark(STAGE_DEPOSIT);
         ck(launch_xfwd(g, lx, npair, nd, dDep, deterministic ? dDepFix : nullptr, dH, st), "fft x forward");
         mark(STAGE_XFWD);
@@ -1451,7 +1456,7 @@ void Box::enqueueEnergyOnly(bool lastStepStart)
         else
             ck(launch_zero(dDep, sizeof(float2) * npair * g.M, st), "zero");
         float *xa = lastStepStart ? dX[1] : dX[0], *xb = lastStepStart ? dX[0] : dX[1];
-        ck(launch_deposit(g, ppHost, xa, xb, dStep, dFlags, dQ, dDep, dDepFix, deterministic, tileCfg(), st), "deposit");
+        ck(launch_deposit(g, ppHost, xa, xb, dStep, dFlags, dQ, dDep, dDepFix, deterministic, depTileCfg(), st), "deposit");
         ck(launch_xfwd(g, lx, npair, nd, dDep, deterministic ? dDepFix : nullptr, dH, st), "fft x forward");
         ck(launch_ypass(g, ly, nd, 0, dH, st), "fft y forward");
         ck(launch_kspace_z(g, lz, ksHost, dKs, dH, dUk, dHg, dEpart, 1, 0, nullptr, st), "kspace energy");
@@ -1992,8 +1997,9 @@ TileCfg Box::tileGeometry(int codes, bool direct) const
 // Tile autotuner (option "autotune"): times the force evaluation (deposit, transforms,
 // force pass without integration) with tiles of half, the same and twice the bricks of
 // the density rule, each with the particle pass's staged box and with direct gathers,
-// and keeps the fastest.  Positions, the step counter, the noise and
-// the RNG state are not touched.
+// and keeps the fastest; then the deposit's own tiles from the particle pass's up to
+// eight times its bricks.  Positions, the step counter, the noise and the RNG state are
+// not touched.
 void Box::autotuneTiles()
 {
     if (!sortedTiles) return;
@@ -2020,9 +2026,30 @@ void Box::autotuneTiles()
             pick = t;
         }
     }
+    tiles = pick;
+    // the deposit's tiles: the same, twice, four and eight times the bricks (a larger tile
+    // zeroes and flushes fewer halo points per particle, but sums in FP32 once its particle
+    // count leaves the int32 range of the fixed-point box)
+    if (!depositCodes) {
+        TileCfg dpick = dtiles;
+        for (int c = tiles.codes; c <= std::min(64, 8 * tiles.codes); c *= 2) {
+            dtiles = tileGeometry(c, true);
+            enqueueStep(false, false, dF);   // warm-up
+            ck(cudaEventRecord(e0, stream), "event");
+            for (int r = 0; r < 3; r++) enqueueStep(false, false, dF);
+            ck(cudaEventRecord(e1, stream), "event");
+            ck(cudaEventSynchronize(e1), "autotune");
+            float ms = 0.f;
+            ck(cudaEventElapsedTime(&ms, e0, e1), "event");
+            if (ms < best) {
+                best = ms;
+                dpick = dtiles;
+            }
+        }
+        dtiles = dpick;
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    tiles = pick;
     tunedMs = best / 3.f;
 }
 
@@ -2054,6 +2081,13 @@ void Box::checkDeviceErrors()
 TileCfg Box::tileCfg() const
 {
     TileCfg t = tiles;
+    t.start = sortedTiles ? sortW.start : nullptr;
+    return t;
+}
+
+TileCfg Box::depTileCfg() const
+{
+    TileCfg t = dtiles;
     t.start = sortedTiles ? sortW.start : nullptr;
     return t;
 }
@@ -2362,7 +2396,7 @@ std::string Box::describe() const
       << ", \"nBonds\": " << nBondsTot << ", \"nAngles\": " << nAnglesTot << ", \"MAXANGLES\": " << MAXANGLES
       << ", \"datFileName\": " << q(datFileName) << ", \"tiles\": {\"codes\": " << tiles.codes
       << ", \"threads\": " << tiles.threads << ", \"gather\": \"" << (tiles.direct ? "direct" : "staged")
-      << "\", \"autotuned\": " << (autotune ? "true" : "false")
+      << "\", \"deposit_codes\": " << dtiles.codes << ", \"autotuned\": " << (autotune ? "true" : "false")
       << ", \"tuned_ms\": " << tunedMs << "}, \"trajFreq\": " << trajFreq
       << ", \"trajFileName\": " << q(trajFileName) << ", \"fieldFreq\": " << fieldFreq
       << ", \"logScaleFields\": " << (logSpaceFields ? logScaleFields : 0.f) << ", \"gsdFreq\": " << gsdFreq

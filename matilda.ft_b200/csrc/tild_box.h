@@ -273,7 +273,11 @@ private:
     bool sortedTiles = false;       // sortW.start holds the tile ranges of the current order
     uint32_t sortKeys = 0;
     TileCfg tiles{};                // codes / threads / box chosen from the density
+    TileCfg dtiles{};               // the deposit's tiles (its own brick count: a larger tile
+                                    // zeroes and flushes fewer halo points per particle)
+    int depositCodes = 0;           // option "deposit_codes": fixed deposit tile bricks (0: chosen)
     TileCfg tileCfg() const;
+    TileCfg depTileCfg() const;
     TileCfg tileGeometry(int codes, bool direct) const;
     bool autotune = false;          // option "autotune": time tile sizes at endBox
     bool directGather = false;      // option "direct_gather": particle pass reads L1/L2, no box

@@ -111,10 +111,8 @@ cudaError_t launch_zero(void *p, size_t bytes, cudaStream_t st) { return cudaMem
 constexpr int kDepPB = 512;
 // float pointer to field f of the packed pair array (field 2t in .x, 2t+1 in .y of pair t)
 #define FIELD_PTR(dep, f, M) (reinterpret_cast<float *>((dep) + ((f) >> 1) * (M)) + ((f) & 1))
-constexpr int kDepSmemFast = 64 * 1024;
+constexpr int kDepSmemFast = 96 * 1024;   // a box of 21^3 points x 2 fields (64-brick tiles)
 constexpr int kDepSmemFixed = 128 * 1024;
-// largest warp table: 16 warps x 32 particles x (5 + 25 + 1 + kMaxFields) floats (order 4)
-constexpr int kDepTableMax = 16 * 32 * (5 + 25 + 1 + kMaxFields) * 4;
 
 // Coefficient of field f for a particle: membership bit, charge channel -> q.
 __device__ __forceinline__ float field_coef(uint32_t dm, unsigned dq, int f, float qp)
@@ -137,6 +135,30 @@ __device__ __forceinline__ void smem_add(float *tf, unsigned long long *tu, int 
     else atomicAdd(tf + i, v);
 }
 
+// The contribution v to every field f with sgn[f] != 0, as sgn[f] * v: one conversion to
+// fixed point for all of them (exact: the conversions round to nearest even, so the value
+// of -v is minus that of v).
+template <bool FIXED, bool IB, int NC>
+__device__ __forceinline__ void smem_add_signed(float *tf, unsigned long long *tu, int V, int i, float v,
+                                                const int *sgn)
+{
+    if (FIXED) {
+        const long long k = __double2ll_rn((double)v * kFixScale);
+#pragma unroll
+        for (int f = 0; f < NC; f++)
+            if (sgn[f]) atomicAdd(tu + f * V + i, (unsigned long long)(sgn[f] > 0 ? k : -k));
+    } else if (IB) {
+        const int k = __float2int_rn(v * kTileFix);
+#pragma unroll
+        for (int f = 0; f < NC; f++)
+            if (sgn[f]) atomicAdd(reinterpret_cast<int *>(tf) + f * V + i, sgn[f] > 0 ? k : -k);
+    } else {
+#pragma unroll
+        for (int f = 0; f < NC; f++)
+            if (sgn[f]) atomicAdd(tf + f * V + i, sgn[f] > 0 ? v : -v);
+    }
+}
+
 template <bool FIXED>
 __device__ __forceinline__ void global_add(float2 *dep, unsigned long long *depfix, long long M, int f, long long m,
                                            float v)
@@ -146,9 +168,10 @@ __device__ __forceinline__ void global_add(float2 *dep, unsigned long long *depf
 }
 
 // Deposit of one tile of sorted particles (or a window of slots).  The box of grid points
-// is accumulated in shared memory by warp-cooperative atomics: a warp takes one particle
-// at a time and its lanes cover the particle's (P+1)^3 stencil points, so the addresses
-// of one atomic instruction form a compact block.  Each touched point is flushed once.
+// is accumulated in shared memory, each thread adding its particle's (P+1)^3 points with
+// shared-memory atomics (the atomics have throughput to spare; what bounds the deposit
+// is instruction issue, so a particle's stencil is computed once, by its own thread, and
+// converted to fixed point once per point).  Each touched point is flushed once.
 // NF: number of density fields when 1 or 2 (unrolled), 0 = any.
 template <int P, int NF, bool FIXED>
 __global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4, int nd, unsigned dq,
@@ -159,10 +182,8 @@ __global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4
                                                        unsigned long long *__restrict__ depfix, int cap_bytes,
                                                        TileCfg tc, int int_tile_max)
 {
-    constexpr int P1 = P + 1, G = P1 * P1 * P1, NPASS = (G + 31) / 32;
+    constexpr int P1 = P + 1;
     constexpr int NC = NF ? NF : kMaxFields;
-    // per-particle record of the warp table: Wx, Wy*Wz, box offset, field coefficients
-    constexpr int WREC = P1 + P1 * P1 + 1 + NC;
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ TileShared ts;
     const float *__restrict__ X = (*d_step & 1) ? X1 : X0;
@@ -199,25 +220,22 @@ __global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     if (staged) {
-        // this lane's stencil points: s = lane + 32*pass -> (a, b, e), x fastest; its box
-        // offset and its Wy*Wz index are fixed for the whole tile
-        int sa[NPASS], syz[NPASS], loff[NPASS];
-#pragma unroll
-        for (int k = 0; k < NPASS; k++) {
-            const int s = lane + 32 * k;
-            const int a = s % P1, bb = (s / P1) % P1, e = s / (P1 * P1);
-            sa[k] = a;
-            syz[k] = e * P1 + bb;
-            loff[k] = e * E01 + bb * E0 + a;
-        }
-        float *wt = reinterpret_cast<float *>(smraw + (size_t)cap_bytes) + (threadIdx.x >> 5) * 32 * WREC;
+        // One particle per thread, all its (P+1)^3 points.  A particle's field coefficients
+        // are c0 (its first non-zero one) times s_f in {-1, 0, +1} (a density field and a
+        // charge channel of charge +-1, or one field of each block of a copolymer), so one
+        // conversion per stencil point serves every field: the fixed-point value of
+        // -c0 * w is minus that of c0 * w (round to nearest even is symmetric).  A warp
+        // holding a particle with any other coefficients converts per field.
         for (int base = b0 + (threadIdx.x & ~31); base < b1; base += blockDim.x) {
             const int p = base + lane;
-            uint32_t dm = 0u;
-            if (p < b1) dm = pflags[p] & 0xffu;
-            float *mine = wt + lane * WREC;
+            uint32_t dm = p < b1 ? (pflags[p] & 0xffu) : 0u;
+            float Wx[P1], Wy[P1], Wz[P1], cf[NC];
+            int o = 0;
+#pragma unroll
+            for (int i = 0; i < P1; i++) Wx[i] = Wy[i] = Wz[i] = 0.f;
+#pragma unroll
+            for (int f = 0; f < NC; f++) cf[f] = 0.f;
             if (dm) {
-                float Wx[P1], Wy[P1], Wz[P1];
                 const int gs[3] = {stencil_fast<P>(X[3 * p + 0], g, 0, quirk4, Wx),
                                    stencil_fast<P>(X[3 * p + 1], g, 1, quirk4, Wy),
                                    stencil_fast_z<P>(X[3 * p + 2], g, quirk4, Wz)};
@@ -248,63 +266,52 @@ __global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4
                             }
                         }
                     }
-                    dm = 0u;
                 } else {
+                    o = d[2] * E01 + d[1] * E0 + d[0];
 #pragma unroll
-                    for (int i = 0; i < P1; i++) mine[i] = Wx[i];
-#pragma unroll
-                    for (int e = 0; e < P1; e++)
-#pragma unroll
-                        for (int bb = 0; bb < P1; bb++) mine[P1 + e * P1 + bb] = Wy[bb] * Wz[e];
-                    mine[P1 + P1 * P1] = __int_as_float(d[2] * E01 + d[1] * E0 + d[0]);
-#pragma unroll
-                    for (int f = 0; f < NC; f++)
-                        mine[P1 + P1 * P1 + 1 + f] = f < nfields ? field_coef(dm, dq, f, qp) : 0.f;
+                    for (int f = 0; f < NC; f++) cf[f] = f < nfields ? field_coef(dm, dq, f, qp) : 0.f;
                 }
             }
-            unsigned rem = __ballot_sync(full, dm != 0u);
-            __syncwarp();
-            // four particles per round: their table reads in flight before the atomics
-            constexpr int U = 4;
-            while (rem) {
-                int jj[U];
+            float c0 = 0.f;
+            int sgn[NC];
+            bool general = false;
 #pragma unroll
-                for (int u = 0; u < U; u++) {
-                    jj[u] = rem ? __ffs(rem) - 1 : -1;
-                    if (rem) rem &= rem - 1;
-                }
-                int offs[U];
-                float cfs[U][NC], ws[U][NPASS];
+            for (int f = 0; f < NC; f++) {
+                if (c0 == 0.f) c0 = cf[f];
+                sgn[f] = cf[f] == 0.f ? 0 : (cf[f] == c0 ? 1 : (cf[f] == -c0 ? -1 : 2));
+                general = general || sgn[f] == 2;
+            }
+            // Wx * (Wy * Wz), then the coefficient: the association of the unstaged path,
+            // so that the deterministic mode's fixed-point values do not depend on staging
+            auto points = [&](auto int_box, auto gen) {
+                constexpr bool IB = decltype(int_box)::value, GN = decltype(gen)::value;
 #pragma unroll
-                for (int u = 0; u < U; u++) {
-                    const float *pj = wt + (jj[u] < 0 ? jj[0] : jj[u]) * WREC;
-                    offs[u] = __float_as_int(pj[P1 + P1 * P1]);
+                for (int e = 0; e < P1; e++)
 #pragma unroll
-                    for (int f = 0; f < NC; f++) cfs[u][f] = jj[u] < 0 ? 0.f : pj[P1 + P1 * P1 + 1 + f];
+                    for (int bb = 0; bb < P1; bb++) {
+                        const float wyz = Wy[bb] * Wz[e];
+                        const int row = o + e * E01 + bb * E0;
 #pragma unroll
-                    for (int k = 0; k < NPASS; k++)
-                        // Wx * (Wy * Wz): the association of the unstaged path, so that the
-                        // deterministic mode's fixed-point values do not depend on staging
-                        ws[u][k] = (lane + 32 * k < G) ? pj[sa[k]] * pj[P1 + syz[k]] : 0.f;
-                }
-                // the box's number type is fixed for the tile: one branch per round
-                auto atomics = [&](auto int_box) {
+                        for (int a = 0; a < P1; a++) {
+                            const float w = Wx[a] * wyz;
+                            if (GN) {
 #pragma unroll
-                    for (int u = 0; u < U; u++)
-#pragma unroll
-                        for (int k = 0; k < NPASS; k++) {
-                            if (lane + 32 * k >= G) break;
-                            const int idx = offs[u] + loff[k];
-#pragma unroll
-                            for (int f = 0; f < NC; f++)
-                                if (cfs[u][f] != 0.f)
-                                    smem_add<FIXED>(tf, tu, f * V + idx, cfs[u][f] * ws[u][k], decltype(int_box)::value);
+                                for (int f = 0; f < NC; f++)
+                                    if (cf[f] != 0.f) smem_add<FIXED>(tf, tu, f * V + row + a, cf[f] * w, IB);
+                            } else {
+                                smem_add_signed<FIXED, IB, NC>(tf, tu, V, row + a, c0 * w, sgn);
+                            }
                         }
-                };
-                if (ia) atomics(std::true_type{});
-                else atomics(std::false_type{});
+                    }
+            };
+            // the box's number type is fixed for the tile, the conversion per warp
+            if (__any_sync(full, general)) {
+                if (ia) points(std::true_type{}, std::true_type{});
+                else points(std::false_type{}, std::true_type{});
+            } else {
+                if (ia) points(std::true_type{}, std::false_type{});
+                else points(std::false_type{}, std::false_type{});
             }
-            __syncwarp();
         }
     } else {
         for (int p = b0 + threadIdx.x; p < b1; p += blockDim.x) {
@@ -378,14 +385,12 @@ static void dep_launch_nf(int nb, int threads, const Geom &g, const ParticlePara
     int cap = tc.start ? (int)((size_t)tc.pbox * nf * esz) : 0;   // the fixed tile box (no staging unsorted)
     cap = std::min(cap, depfix ? kDepSmemFixed : kDepSmemFast);
     cap = (cap + 15) & ~15;
-    constexpr int WREC = (P + 1) + (P + 1) * (P + 1) + 1 + (NF ? NF : kMaxFields);   // as in the kernel
-    const size_t table = (size_t)(threads / 32) * 32 * WREC * sizeof(float);
     if (depfix)
-        k_deposit_tiled<P, NF, true><<<nb, threads, cap + table, st>>>(g, pp.N, pp.quirk4, pp.nd, pp.dchan_charge, X0,
+        k_deposit_tiled<P, NF, true><<<nb, threads, cap, st>>>(g, pp.N, pp.quirk4, pp.nd, pp.dchan_charge, X0,
                                                                        X1, d_step, pflags, q, dep, depfix, cap, tc,
                                                                        pp.int_tile_max);
     else
-        k_deposit_tiled<P, NF, false><<<nb, threads, cap + table, st>>>(g, pp.N, pp.quirk4, pp.nd, pp.dchan_charge, X0,
+        k_deposit_tiled<P, NF, false><<<nb, threads, cap, st>>>(g, pp.N, pp.quirk4, pp.nd, pp.dchan_charge, X0,
                                                                         X1, d_step, pflags, q, dep, depfix, cap, tc,
                                                                         pp.int_tile_max);
 }
@@ -408,8 +413,8 @@ static void dep_launch(const Geom &g, const ParticleParams &pp, const float *X0,
 void init_deposit_attributes()
 {
 #define TILD_DA1(P, NF)                                                                                        \
-    cudaFuncSetAttribute(k_deposit_tiled<P, NF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDepSmemFixed + kDepTableMax); \
-    cudaFuncSetAttribute(k_deposit_tiled<P, NF, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDepSmemFast + kDepTableMax)
+    cudaFuncSetAttribute(k_deposit_tiled<P, NF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDepSmemFixed); \
+    cudaFuncSetAttribute(k_deposit_tiled<P, NF, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDepSmemFast)
 #define TILD_DA(P) TILD_DA1(P, 0); TILD_DA1(P, 1); TILD_DA1(P, 2)
     TILD_DA(0);
     TILD_DA(1);

@@ -178,6 +178,42 @@ def test_autotuned_tiles_are_invisible():
 
 
 @pytest.mark.parametrize("order", [2, 3, 4])
+def test_deposit_tiles_are_invisible(order):
+    """The deposit's own tile size (bricks per CTA) only changes the work split: in
+    deterministic mode the forces and a short trajectory are bit-identical for every size."""
+    spec = synth.small_system(seed=28, order=order, charges=True, n_chains=120, nper=10, L=10.0, grid=(20, 20, 20))
+    outs = []
+    for codes in (8, 16, 32, 64):
+        with make_box(spec, deterministic=1, deposit_codes=codes) as b:
+            assert b.describe()["tiles"]["deposit_codes"] == codes
+            f = b.forces()
+            b.step(5)
+            outs.append((f, b.positions()))
+    for f, x in outs[1:]:
+        assert np.array_equal(outs[0][0], f) and np.array_equal(outs[0][1], x)
+
+
+@pytest.mark.parametrize("qscale", [1.0, 0.5])
+@pytest.mark.parametrize("codes", [8, 32])
+def test_forces_and_energies_match_oracle_deposit_tiles(qscale, codes):
+    """Fast-mode forces and pair energies against the FP64 oracle for small and large
+    deposit tiles, with charges of +-1 (one fixed-point conversion per stencil point serves
+    every density field) and of +-0.5 (a conversion per field)."""
+    spec = synth.small_system(seed=29, order=3, charges=True, n_chains=120, nper=10, L=10.0, grid=(20, 20, 20))
+    spec.charges = (spec.charges * qscale).astype(np.float32)
+    sysm = spec_to_system(spec)
+    fref, _ = oracle.forces(sysm, prec=64)
+    dens, _, _ = oracle.densities(sysm)
+    ref = oracle.pair_energies(sysm, dens)
+    with make_box(spec, deposit_codes=codes) as b:
+        f = b.forces()
+        t = b.thermo()
+    assert force_error(f, fref) <= 1e-5
+    for e, r in zip(t["potentials"], ref):
+        assert abs(e - r) <= 1e-5 * max(abs(r), 1e-12) + 1e-9, (e, r)
+
+
+@pytest.mark.parametrize("order", [2, 3, 4])
 def test_direct_gather_is_invisible(order):
     """Reading every stencil through L1/L2 instead of the tile's staged box changes only
     where the records come from: forces and a short trajectory are bit-identical."""
