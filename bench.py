@@ -36,11 +36,11 @@ import numpy as np  # noqa: E402
 METRIC = "particle-steps/s"
 WORKLOAD = ("c2_coacervate: 2,097,152 particles, 192^3 grid, pmeorder 3, gaussian(all,all) + "
             "smeared charges (lB 1.0, sigma 0.5), harmonic bonds, GJF dt 0.005")
-STAGES = ["deposit", "fft_x_fwd", "fft_y_fwd", "kspace_z", "fft_y_inv", "fft_x_inv", "particles"]
+STAGES = ["deposit", "fft_x_fwd", "fft_y_fwd", "kspace_z", "fft_y_inv", "fft_x_inv", "gather", "integrate"]
 KERNEL_NAMES = {"deposit": "k_deposit", "fft_x_fwd": "k_xfwd", "fft_y_fwd": "k_ypass<false>",
                 "kspace_z": "k_kspace_z", "fft_y_inv": "k_ypass<true>", "fft_x_inv": "k_xinv",
-                "particles": "k_particles"}
-KERNELS_PER_STEP = 8   # deposit, xfwd, yfwd, kspace_z, yinv, xinv, particles, tick
+                "gather": "k_gather_paired", "integrate": "k_integrate"}
+KERNELS_PER_STEP = 9   # deposit, xfwd, yfwd, kspace_z, yinv, xinv, gather, integrate, tick
 
 
 def peaks():
@@ -66,10 +66,13 @@ def algorithmic_bytes(spec, nd=2, nfg=2, maxb=2, charged=True):
         "fft_y_fwd": 2 * nd * hs,
         "kspace_z": nd * hs + 3 * nfg * hs,
         "fft_y_inv": 2 * 3 * nfg * hs,
-        "fft_x_inv": 3 * nfg * hs + nfg * M * 16,
-        # x_t 12, x_{t-1} 12, x_{t+1} 12, noise r/w 24, flags 4, q, ids 4, bonds (nb 1,
-        # partners 4*maxb, types 1*maxb), partner positions assumed cached, records once
-        "particles": N * (12 + 12 + 12 + 24 + 4 + qb + 4 + 1 + 5 * maxb) + nfg * M * 16,
+        # the force records: paired planes, 12 bytes per point and force group
+        "fft_x_inv": 3 * nfg * hs + nfg * M * 12,
+        # x_t 12, flags 4, q, the grid force written 12, the records read once
+        "gather": N * (12 + 4 + qb + 12) + nfg * M * 12,
+        # x_t 12, x_{t-1} 12, x_{t+1} 12, noise r/w 24, flags 4, ids 4, the grid force 12,
+        # bonds (row 4, partners 4*maxb, types 1*maxb), partner positions assumed cached
+        "integrate": N * (12 + 12 + 12 + 24 + 4 + 4 + 12 + 4 + 5 * maxb),
     }
 
 

@@ -994,6 +994,31 @@ void Box::initDevice()
     ready = true;
 }
 
+// Bricks per tile from the density: about one particle per thread of a 192-thread CTA.
+int Box::densityCodes() const
+{
+    const double perCode = 16.0 * std::min(4, geom.nz) * (double)nstot / (double)geom.M;   // particles per brick of 4^3 cells (4x4x1 in 2-D)
+    int codes = 8;
+    while (codes < 64 && perCode * codes * 2.0 <= 192.0) codes *= 2;
+    return codes;
+}
+
+// Bytes of the force records: planar, or paired with the ghost layers of any tiles the
+// autotuner tries (half, the same and twice the density's bricks).
+size_t Box::recordBytes() const
+{
+    const int nfg = std::max(1, (int)fgroups.size()), codes = densityCodes();
+    size_t b = sizeof(float4) * (size_t)nfg * geom.M;
+    for (int c : {codes / 2, codes, codes * 2}) {
+        const TileCfg t = tileGeometry(c, false);
+        if (!t.paired) continue;
+        int gl, gh[3];
+        pairedGhosts(t, &gl, gh);
+        b = std::max(b, rec_layout_bytes(geom, nfg, gl, gh));
+    }
+    return b;
+}
+
 int64_t Box::deviceBytesEstimate() const
 {
     if (!hostPrepared) fail(TILD_ERR_STATE, "the box has not been prepared");
@@ -1006,9 +1031,9 @@ int64_t Box::deviceBytesEstimate() const
     const int64_t bonds = nBondEntries > 0 ? 2 * (4 * (N + 1) + 5 * nBondEntries) : 0;   // CSR + its sort copy
     const int64_t nk = (int64_t)sort_key_count(geom);
     const int64_t angles = nAnglesTot > 0 ? 2 * (1 + 13 * (int64_t)MAXANGLES) : 0;   // arrays and sort copies
-    const int64_t grid = (deterministic ? 16 : 8) * npair * M + 8 * nd * hs + 24 * nfg * hs + 16 * nfg * M +
+    const int64_t grid = (deterministic ? 16 : 8) * npair * M + 8 * nd * hs + 24 * nfg * hs + (int64_t)recordBytes() +
                          4 * std::max<int64_t>(1, (int64_t)potentials.size()) * hs + 8 * nk;
-    return N * (perParticle + angles) + bonds + grid + (int64_t(4) << 20);   // + small arrays, alignment, graphs
+    return N * (perParticle + angles + 12) + bonds + grid + nk + (int64_t(4) << 20);   // + grid forces, tile lists, small arrays, alignment, graphs
 }
 
 void Box::buildPlan()
@@ -1196,7 +1221,6 @@ void Box::allocDevice()
     else dDep = dalloc<float2>((size_t)npair * g.M);
     dH = dalloc<float2>((size_t)nd * g.hstride);
     dHg = dalloc<float2>((size_t)3 * nfg * g.hstride);
-    dRec = dalloc<float4>((size_t)nfg * g.M);
     dTw = dalloc<float2>((size_t)g.nx + g.ny + g.nz);
     build_fft_line(g.nx, lx, dTw);
     build_fft_line(g.ny, ly, dTw + g.nx);
@@ -1223,12 +1247,15 @@ void Box::allocDevice()
     const uint32_t nk = sort_key_count(g);
     sortKeys = nk;
     {   // tile geometry: about one particle per thread (the density decides the bricks)
-        const double perCode = 16.0 * std::min(4, g.nz) * (double)N / (double)g.M;   // particles per brick of 4^3 cells (4x4x1 in 2-D)
-        int codes = 8;
-        while (codes < 64 && perCode * codes * 2.0 <= 192.0) codes *= 2;
+        const int codes = densityCodes();
         tiles = tileGeometry(codes, directGather);
         dtiles = tileGeometry(depositCodes ? depositCodes : codes, true);
+        attachTileList(tiles);
+        attachTileList(dtiles);
+        recBytes = recordBytes();
+        dRec = reinterpret_cast<float4 *>(dalloc<unsigned char>(recBytes));
     }
+    dFgrid = dalloc<float>(3 * N);
     sortW.key = dalloc<uint32_t>(N);
     sortW.rank = dalloc<int>(N);
     sortW.newpos = dalloc<int>(N);
@@ -1425,15 +1452,19 @@ void Box::enqueueStep(bool energy, bool integrate, float *fout_dev)
         if (nfg > 0) {
             ck(launch_ypass(g, ly, 3 * nfg, 1, dHg, st), "fft y inverse");
             mark(STAGE_YINV);
-            ck(launch_xinv(g, lx, nfg, dHg, dRec, st), "fft x inverse");
+            ck(launch_xinv(g, lx, nfg, dHg, dRec, recLayout(), st), "fft x inverse");
             mark(STAGE_XINV);
         }
     }
-    ck(launch_particles(g, ppHost, dPp, dX[0], dX[1], dNoise, dFlags, dQ, dBrow, dPartner, dBtype,
-                        AngleArrays{dNa, dAtype, dAng}, dRec, dOrig, dRng,
-                        dStep, fout_dev, integrate ? 1 : 0, tileCfg(), recordMap(), dErr, st),
-       "particles");
-    mark(STAGE_PARTICLES);
+    const RecLayout rl = recLayout();
+    ck(launch_gather(g, ppHost, dPp, dX[0], dX[1], dFlags, dQ, dRec, rl, dStep, dFgrid, tileCfg(), recordMap(),
+                     rl.paired ? &pmapA : nullptr, rl.paired ? &pmapB : nullptr, dErr, st),
+       "gather");
+    mark(STAGE_GATHER);
+    ck(launch_integrate(g, ppHost, dPp, dX[0], dX[1], dNoise, dFlags, dQ, dBrow, dPartner, dBtype,
+                        AngleArrays{dNa, dAtype, dAng}, dFgrid, rl, dOrig, dRng, dStep, fout_dev, integrate ? 1 : 0, st),
+       "integrate");
+    mark(STAGE_INTEGRATE);
     if (integrate) ck(launch_tick(dStep, st), "tick");
     if (energy) {
         ck(launch_bond_energy(g, ppHost, dPp, dX[0], dX[1], dStep, dBrow, dPartner, dBtype, AngleArrays{dNa, dAtype, dAng},
@@ -1985,13 +2016,92 @@ TileCfg Box::tileGeometry(int codes, bool direct) const
     t.pbox = (((ex | 1) * ey) | 1) * ez;
     t.direct = direct ? 1 : 0;
     t.margin = margin;
-    if (g.nz > 1 && !direct) {   // TMA box: odd x and y edges keep the dense pitches odd
+    const int nfg = (int)fgroups.size();
+    if (g.nz > 1 && !direct && nfg >= 1 && nfg <= 2) {   // paired records: an even x edge
+        t.te[0] = (ex + 1) & ~1;
+        t.te[1] = ey;
+        t.te[2] = ez;
+        t.paired = paired_box_fits(t.te, nfg) ? 1 : 0;
+        if (t.paired) t.pbox = t.te[0] * t.te[1] * t.te[2];
+    }
+    if (g.nz > 1 && !direct && !t.paired) {   // planar TMA box: odd x and y edges keep the dense pitches odd
         t.te[0] = ex | 1;
         t.te[1] = ey | 1;
         t.te[2] = ez;
         t.pbox = std::max(t.pbox, t.te[0] * t.te[1] * t.te[2]);
     }
     return t;
+}
+
+// The tiles of t.codes bricks whose first cell lies inside the grid, for launches over
+// those alone: the Morton code space of the sort is a power-of-two cube of bricks, so the
+// tiles past the grid's edge (more than half of them on a 192^3 grid) hold no particle.
+void Box::attachTileList(TileCfg &t)
+{
+    auto it = tileLists.find(t.codes);
+    if (it == tileLists.end()) {
+        auto compact3 = [](uint32_t v) {
+            v &= 0x09249249u;
+            v = (v | (v >> 2)) & 0x030C30C3u;
+            v = (v | (v >> 4)) & 0x0300F00Fu;
+            v = (v | (v >> 8)) & 0x030000FFu;
+            v = (v | (v >> 16)) & 0x000003FFu;
+            return (int)v;
+        };
+        std::vector<uint32_t> h;
+        const uint32_t ntile = (sortKeys + (uint32_t)t.codes - 1) / (uint32_t)t.codes;
+        for (uint32_t k = 0; k < ntile; k++) {
+            const uint32_t k0 = k * (uint32_t)t.codes;
+            if (4 * compact3(k0) < geom.nx && 4 * compact3(k0 >> 1) < geom.ny && 4 * compact3(k0 >> 2) < geom.nz)
+                h.push_back(k);
+        }
+        uint32_t *d = dalloc<uint32_t>(std::max<size_t>(1, h.size()));
+        ck(cudaMemcpy(d, h.data(), sizeof(uint32_t) * h.size(), cudaMemcpyHostToDevice), "tile list");
+        it = tileLists.emplace(t.codes, std::make_pair(d, (int)h.size())).first;
+    }
+    t.list = it->second.first;
+    t.nlist = it->second.second;
+}
+
+// Ghost layers of the paired records for the tiles t: a tile's box starts gl = P/2 + margin
+// points below its first cell and spans te[] points, so the last tile along an axis reaches
+// gh[] points past the grid.
+void Box::pairedGhosts(const TileCfg &t, int *gl, int *gh) const
+{
+    *gl = pmeorder / 2 + t.margin;
+    int bits = 0;
+    while ((1 << bits) < t.codes) bits++;
+    const int cb[3] = {4 << ((bits + 2) / 3), 4 << ((bits + 1) / 3), 4 << (bits / 3)};
+    const int n[3] = {geom.nx, geom.ny, geom.nz};
+    for (int j = 0; j < 3; j++) {
+        const int c0max = cb[j] * ((n[j] - 1) / cb[j]);
+        gh[j] = std::max(0, c0max - *gl + t.te[j] - n[j]);
+    }
+}
+
+// The records' layout for the current tiles: paired (with their TMA maps) when the tiles
+// use the tile gather, else planar.  Tiles whose maps cannot be built fall back to the
+// planar gather with cp.async staging.
+RecLayout Box::recLayout()
+{
+    RecLayout rl{};
+    if (!tiles.paired) return rl;
+    int gl, gh[3];
+    pairedGhosts(tiles, &gl, gh);
+    if (rec_layout_bytes(geom, (int)fgroups.size(), gl, gh) <= recBytes) {
+        rl = make_rec_layout(geom, (int)fgroups.size(), gl, gh, dRec);
+        if (!pmapOk || std::memcmp(pmapTe, tiles.te, sizeof(pmapTe)) != 0 || pmapGl != rl.gl ||
+            std::memcmp(pmapGh, rl.gh, sizeof(pmapGh)) != 0) {
+            pmapOk = build_paired_maps(&pmapA, &pmapB, rl, tiles.te);
+            std::memcpy(pmapTe, tiles.te, sizeof(pmapTe));
+            std::memcpy(pmapGh, rl.gh, sizeof(pmapGh));
+            pmapGl = rl.gl;
+        }
+        if (pmapOk) return rl;
+    }
+    tiles.paired = 0;
+    tiles.te[0] = tiles.te[1] = tiles.te[2] = 0;
+    return RecLayout{};
 }
 
 // Tile autotuner (option "autotune"): times the force evaluation (deposit, transforms,
@@ -2012,6 +2122,7 @@ void Box::autotuneTiles()
     ck(cudaEventCreate(&e1), "event");
     float best = 1e30f;
     TileCfg pick = tiles;
+    for (TileCfg &t : cands) attachTileList(t);
     for (const TileCfg &t : cands) {
         tiles = t;
         enqueueStep(false, false, dF);   // warm-up
@@ -2034,6 +2145,7 @@ void Box::autotuneTiles()
         TileCfg dpick = dtiles;
         for (int c = tiles.codes; c <= std::min(64, 8 * tiles.codes); c *= 2) {
             dtiles = tileGeometry(c, true);
+            attachTileList(dtiles);
             enqueueStep(false, false, dF);   // warm-up
             ck(cudaEventRecord(e0, stream), "event");
             for (int r = 0; r < 3; r++) enqueueStep(false, false, dF);
@@ -2057,7 +2169,7 @@ void Box::autotuneTiles()
 // change); NULL where none can be built, and the particle pass stages with cp.async.
 const CUtensorMap *Box::recordMap()
 {
-    if (tiles.te[0] <= 0 || !dRec) return nullptr;
+    if (tiles.te[0] <= 0 || tiles.paired || !dRec) return nullptr;
     if (!recMapOk || std::memcmp(recMapTe, tiles.te, sizeof(recMapTe)) != 0) {
         recMapOk = build_record_map(&recMap, dRec, geom, std::max(1, (int)fgroups.size()), tiles.te);
         std::memcpy(recMapTe, tiles.te, sizeof(recMapTe));
@@ -2171,9 +2283,29 @@ void Box::getGridForce(const std::string &group, float *gf)
     }
     std::vector<float4> h((size_t)M);
     ck(cudaSetDevice(device), "cudaSetDevice");
-    ck(cudaMemcpyAsync(h.data(), dRec + (size_t)k * M, sizeof(float4) * M, cudaMemcpyDeviceToHost, stream),
-       "read grid force");
-    ck(cudaStreamSynchronize(stream), "read grid force");
+    const RecLayout rl = recLayout();
+    if (rl.paired) {   // group k's (x, y, z) out of the padded planes
+        std::vector<float4> hA((size_t)rl.pM);
+        std::vector<float2> hB(rl.nfg == 2 ? (size_t)rl.pM : 0);
+        ck(cudaMemcpyAsync(hA.data(), rl.A, sizeof(float4) * rl.pM, cudaMemcpyDeviceToHost, stream), "read grid force");
+        if (rl.nfg == 2)
+            ck(cudaMemcpyAsync(hB.data(), rl.B, sizeof(float2) * rl.pM, cudaMemcpyDeviceToHost, stream), "read grid force");
+        ck(cudaStreamSynchronize(stream), "read grid force");
+        for (int z = 0; z < geom.nz; z++)
+            for (int y = 0; y < geom.ny; y++)
+                for (int x = 0; x < geom.nx; x++) {
+                    const size_t i = ((size_t)(z + rl.gl) * rl.py + (y + rl.gl)) * rl.px + x + rl.gl;
+                    const size_t m = ((size_t)z * geom.ny + y) * geom.nx + x;
+                    const float4 a = hA[i];
+                    if (rl.nfg == 1) h[m] = a;
+                    else if (k == 0) h[m] = make_float4(a.x, a.y, hB[i].x, 0.f);
+                    else h[m] = make_float4(a.z, a.w, hB[i].y, 0.f);
+                }
+    } else {
+        ck(cudaMemcpyAsync(h.data(), dRec + (size_t)k * M, sizeof(float4) * M, cudaMemcpyDeviceToHost, stream),
+           "read grid force");
+        ck(cudaStreamSynchronize(stream), "read grid force");
+    }
     const double gvf = (double)((1.0f * geom.dxf[0]) * geom.dxf[1] * geom.dxf[2]);
     const double scale = gvf / gvol;
     for (long long m = 0; m < M; m++) {

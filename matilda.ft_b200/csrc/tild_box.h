@@ -6,6 +6,7 @@
 #pragma once
 #include <cstdint>
 #include <deque>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -248,6 +249,11 @@ private:
     CUtensorMap recMap;                          // TMA descriptor of dRec for the tiles' box
     int recMapTe[3] = {0, 0, 0};
     bool recMapOk = false;
+    CUtensorMap pmapA, pmapB;                    // TMA descriptors of the paired record planes
+    int pmapTe[3] = {0, 0, 0}, pmapGl = -1, pmapGh[3] = {0, 0, 0};
+    bool pmapOk = false;
+    float *dFgrid = nullptr;                     // [3N] grid force of each particle (the gather's output)
+    size_t recBytes = 0;                         // bytes of dRec: planar or paired records
     uint8_t *dBtype = nullptr;
     uint8_t *dNa = nullptr, *dAtype = nullptr;   // angles (NULL when the box has none)
     int *dAng = nullptr;
@@ -278,6 +284,12 @@ private:
     int depositCodes = 0;           // option "deposit_codes": fixed deposit tile bricks (0: chosen)
     TileCfg tileCfg() const;
     TileCfg depTileCfg() const;
+    void pairedGhosts(const TileCfg &t, int *gl, int *gh) const;   // ghost layers the tiles' boxes reach
+    int densityCodes() const;       // bricks per tile from the density
+    std::map<int, std::pair<uint32_t *, int>> tileLists;   // bricks per tile -> the tiles meeting the grid
+    void attachTileList(TileCfg &t);  // t.list: the tiles of t.codes bricks that meet the grid (built once)
+    size_t recordBytes() const;     // bytes of the force records (planar or paired)
+    RecLayout recLayout();          // the records' layout for the current tiles (maps built)
     TileCfg tileGeometry(int codes, bool direct) const;
     bool autotune = false;          // option "autotune": time tile sizes at endBox
     bool directGather = false;      // option "direct_gather": particle pass reads L1/L2, no box
@@ -312,7 +324,8 @@ private:
     float *hostBuffer(size_t bytes);
     void releaseFrames();
     // per-kernel event timing (option "stage_timing")
-    enum { STAGE_DEPOSIT, STAGE_XFWD, STAGE_YFWD, STAGE_KSPACE, STAGE_YINV, STAGE_XINV, STAGE_PARTICLES, STAGE_COUNT };
+    enum { STAGE_DEPOSIT, STAGE_XFWD, STAGE_YFWD, STAGE_KSPACE, STAGE_YINV, STAGE_XINV, STAGE_GATHER, STAGE_INTEGRATE,
+           STAGE_COUNT };
     bool timing = false;
     std::vector<std::pair<int, cudaEvent_t>> marks;
     void mark(int stage);

@@ -11,7 +11,9 @@
 //   dep[npair][M]  float2  deposit target: field 2i in .x, 2i+1 in .y
 //   H[D][Nz][Ny][hp]  float2  density half spectra (kx in [0, Nx/2])
 //   Hg[3F][Nz][Ny][hp] float2 gradient half spectra
-//   rec[F][M]      float4  grid force of each force group (x, y, z, 0)
+//   rec[F][M]      float4  grid force of each force group (x, y, z, 0) ("planar"), or for
+//                          one or two force groups the "paired" planes of RecLayout
+//   fgrid[N*3]     float   grid force of each particle (sum over its force groups)
 #pragma once
 #include <cstdint>
 #include <cuda.h>            // CUtensorMap (a host-built TMA descriptor; no driver library linked)
@@ -147,6 +149,8 @@ struct ParticleParams {
 // grid points are staged in shared memory.  start == nullptr: fixed windows of slots.
 struct TileCfg {
     const uint32_t *start;
+    const uint32_t *list;   // the tiles that meet the grid (CTA b takes tile list[b]); NULL: every tile
+    int nlist;
     int nkeys;
     int codes;
     int threads;
@@ -155,7 +159,32 @@ struct TileCfg {
     int margin;   // particle pass: drift margin of the fixed box, cells per side
     int direct;   // particle pass: 1 = read every stencil through L1/L2 (no staged box)
     int te[3];    // particle pass: edges of the TMA box of force records (0: stage with cp.async)
+    int paired;   // particle pass: 1 = the tile gather over the paired records (RecLayout)
 };
+
+// Force records in the "paired" layout of the tile gather (one or two force groups, 3-D
+// boxes): plane A holds float4 (g0.x, g0.y, g1.x, g1.y) -- (x, y, z, 0) for one group --
+// and plane B float2 (g0.z, g1.z), both over a padded grid of px x py x pz points that
+// carries `gl` periodic ghost layers below and gh[] above every axis, so that no tile's
+// box wraps: grid point (x, y, z) sits at ((z + gl) * py + (y + gl)) * px + x + gl, and a
+// ghost holds the value of the point it wraps to.
+struct RecLayout {
+    int paired;
+    int nfg;
+    int gl;
+    int gh[3];
+    int px, py, pz;
+    long long pM;         // px * py * pz
+    float4 *A;
+    float2 *B;            // nfg == 2 only
+};
+// layout for tiles whose boxes reach gl points below and gh[] above the grid
+RecLayout make_rec_layout(const Geom &g, int nfg, int gl, const int *gh, void *base);
+size_t rec_layout_bytes(const Geom &g, int nfg, int gl, const int *gh);
+
+// TMA descriptors of the paired planes for boxes of te[] points (te[0] even): false where
+// they cannot be built (the planar path is used then).
+bool build_paired_maps(CUtensorMap *mapA, CUtensorMap *mapB, const RecLayout &rl, const int *te);
 
 // TMA descriptor of the force records rec[F][nz][ny][nx] (float4) for boxes of te[] points:
 // false where it cannot be built (the particle pass then stages with cp.async).
@@ -196,15 +225,27 @@ cudaError_t launch_to_pairs(const float *rho, float2 *out, long long M, cudaStre
 cudaError_t launch_structure_factor(const Geom &g, const FftLine &lx, const FftLine &ly, const FftLine &lz,
                                    const double *twopi_over_L, const float2 *rho_pair, float2 *Hs, int nbins,
                                    double dk, double *bins, cudaStream_t st);
+// x inverse pass: the records of every force group, planar into rec, or into the paired
+// planes of rl when rl.paired
 cudaError_t launch_xinv(const Geom &g, const FftLine &lx, int nfg, const float2 *Hg, float4 *rec,
-                        cudaStream_t st);
-cudaError_t launch_particles(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd,
-                             float *X0, float *X1, float *noise, const uint32_t *pflags,
-                             const float *q, const int *brow, const int *partner,
-                             const uint8_t *btype, AngleArrays aa, const float4 *rec, const int *orig_id,
-                             void *rng_states, const long long *d_step, float *fout,
-                             int integrate, const TileCfg &tc, const CUtensorMap *rec_map, int *err,
+                        const RecLayout &rl, cudaStream_t st);
+// The particle pass as two kernels.  launch_gather: the grid gather of every particle's
+// force groups into fgrid[3N] (the tile gather over the paired records when rl.paired,
+// else the planar gather over rec[F][M]).  launch_integrate: bonds, angles and walls plus
+// fgrid, fout[3N] on request, and the GJF/EM update, one thread per particle (which also
+// gathers, from the paired records, the particles the tile gather left to it).
+cudaError_t launch_gather(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd, const float *X0,
+                          const float *X1, const uint32_t *pflags, const float *q, const float4 *rec,
+                          const RecLayout &rl, const long long *d_step, float *fgrid, const TileCfg &tc,
+                          const CUtensorMap *rec_map, const CUtensorMap *pmapA, const CUtensorMap *pmapB, int *err,
+                          cudaStream_t st);
+cudaError_t launch_integrate(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd, float *X0, float *X1,
+                             float *noise, const uint32_t *pflags, const float *q, const int *brow, const int *partner,
+                             const uint8_t *btype, AngleArrays aa, const float *fgrid, const RecLayout &rl,
+                             const int *orig_id, void *rng_states, const long long *d_step, float *fout, int integrate,
                              cudaStream_t st);
+// whether the paired tile gather can stage a box of te[] points for nfg force groups
+bool paired_box_fits(const int *te, int nfg);
 void init_particle_attributes();
 cudaError_t launch_tick(long long *d_step, cudaStream_t st);
 

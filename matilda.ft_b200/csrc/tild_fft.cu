@@ -626,7 +626,7 @@ __global__ void __launch_bounds__(256) k_sk_z(Geom g, FftLine lz, const float2 *
 // takes L lines of every field: all rows are staged at once, every pair is transformed
 // in one pass over npair*L lines, and the records are written from the transform.
 __global__ void __launch_bounds__(256) k_xinv(Geom g, FftLine lx, int nfg, const float2 *__restrict__ Hg,
-                                              float4 *__restrict__ rec, int L)
+                                              float4 *__restrict__ rec, RecLayout rl, int L)
 {
     extern __shared__ __align__(16) float2 sm[];
     const int n = g.nx, nf = 3 * nfg, npair = (nf + 1) / 2, nxh = g.nxh, hp = g.hp;
@@ -674,6 +674,37 @@ __global__ void __launch_bounds__(256) k_xinv(Geom g, FftLine lx, int nfg, const
         const float2 v = R[((k >> 1) * L + l) * n + x];
         return (k & 1) ? v.y : v.x;
     };
+    if (rl.paired) {
+        // plane A (g0.x, g0.y, g1.x, g1.y) or (x, y, z, 0), plane B (g0.z, g1.z), at the
+        // point and at every ghost of it: the padded coordinates c' in [-gl, n + gh) with
+        // c' = c mod n along each axis
+        const FastDiv dny = make_fastdiv_dev(g.ny);
+        for (int e = threadIdx.x; e < lv * n; e += blockDim.x) {
+            const int l = (int)fdiv((unsigned)e, dn), x = e - l * n;
+            const int line = (int)line0 + l, z = (int)fdiv((unsigned)line, dny), y = line - z * g.ny;
+            float4 a;
+            float2 b = make_float2(0.f, 0.f);
+            if (nfg == 2) {
+                a = make_float4(comp(0, l, x), comp(1, l, x), comp(3, l, x), comp(4, l, x));
+                b = make_float2(comp(2, l, x), comp(5, l, x));
+            } else {
+                a = make_float4(comp(0, l, x), comp(1, l, x), comp(2, l, x), 0.f);
+            }
+            const int gl = rl.gl;
+            // the lowest copy: c itself unless c sits within gl of the top (then c - n,
+            // or lower still on a grid of fewer than gl points)
+            auto low = [gl](int c, int m) { return c + gl < m ? c : c - m * ((c + gl) / m); };
+            for (int zz = low(z, g.nz); zz < g.nz + rl.gh[2]; zz += g.nz)
+                for (int yy = low(y, g.ny); yy < g.ny + rl.gh[1]; yy += g.ny) {
+                    const long long rb = ((long long)(zz + gl) * rl.py + (yy + gl)) * rl.px + gl;
+                    for (int xx = low(x, n); xx < n + rl.gh[0]; xx += n) {
+                        rl.A[rb + xx] = a;
+                        if (nfg == 2) rl.B[rb + xx] = b;
+                    }
+                }
+        }
+        return;
+    }
     for (int f = 0; f < nfg; f++) {
         float4 *rf = rec + f * g.M + line0 * n;
         for (int e = threadIdx.x; e < lv * n; e += blockDim.x) {
@@ -799,15 +830,17 @@ cudaError_t launch_kspace_z(const Geom &g, const FftLine &lz, const KSpace &ks, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_xinv(const Geom &g, const FftLine &lx, int nfg, const float2 *Hg, float4 *rec, cudaStream_t st)
+cudaError_t launch_xinv(const Geom &g, const FftLine &lx, int nfg, const float2 *Hg, float4 *rec, const RecLayout &rl,
+                        cudaStream_t st)
 {
+    if (rl.paired && (rl.nfg != nfg || nfg < 1 || nfg > 2)) return cudaErrorInvalidValue;
     const int nf = 3 * nfg, npair = (nf + 1) / 2;
     int L = (4096 + npair * g.nx - 1) / (npair * g.nx);   // about 4k complex points per block
     L = L < 1 ? 1 : (L > 16 ? 16 : L);
     const long long nlines = (long long)g.ny * g.nz;
     const size_t bsz = (size_t)npair * L * g.nx, stsz = (size_t)nf * L * g.hp;
     const size_t smx = (((bsz + 1) & ~(size_t)1) + std::max(bsz, stsz) + g.nx) * sizeof(float2);
-    k_xinv<<<(unsigned)((nlines + L - 1) / L), 256, smx, st>>>(g, lx, nfg, Hg, rec, L);
+    k_xinv<<<(unsigned)((nlines + L - 1) / L), 256, smx, st>>>(g, lx, nfg, Hg, rec, rl, L);
     return cudaGetLastError();
 }
 

@@ -400,7 +400,7 @@ static void dep_launch(const Geom &g, const ParticleParams &pp, const float *X0,
                        const long long *d_step, const uint32_t *pflags, const float *q, float2 *dep,
                        unsigned long long *depfix, const TileCfg &tc, cudaStream_t st)
 {
-    const int nb = tc.start ? (tc.nkeys + tc.codes - 1) / tc.codes : (pp.N + kDepPB - 1) / kDepPB;
+    const int nb = tc.start ? tile_ctas(tc) : (pp.N + kDepPB - 1) / kDepPB;
     const int threads = tc.start ? tc.threads : 256;
     if (pp.nd == 1)
         dep_launch_nf<P, 1>(nb, threads, g, pp, X0, X1, d_step, pflags, q, dep, depfix, tc, st);

@@ -242,12 +242,6 @@ __device__ __forceinline__ void wall_terms(const ParticleParams &pp, uint32_t fl
     }
 }
 
-__device__ __forceinline__ void cp_async4(void *smem_dst, const void *gsrc)
-{
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
-}
-
 __device__ __forceinline__ void cp_async16p(void *smem_dst, const void *gsrc)
 {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
@@ -303,7 +297,8 @@ __device__ __forceinline__ void gather_global(const Geom &g, const float4 *__res
 {
     // a true modulo past one box length: a position outside [0, L) still reads the grid
     auto wrap = [](int v, int n) { return wrapi(v, n); };
-    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+    float2 a01 = make_float2(0.f, 0.f);
+    float a2 = 0.f;
 #pragma unroll(UNROLL ? P + 1 : 1)
     for (int e = 0; e <= P; e++) {
         const float wz = sel<P>(Wz, e);
@@ -316,15 +311,22 @@ __device__ __forceinline__ void gather_global(const Geom &g, const float4 *__res
             for (int a = 0; a <= P; a++) {
                 const float w = Wx[a] * wyz;
                 const float4 r = __ldg(ry + wrap(gs[0] + a, g.nx));
-                a0 = __fmaf_rn(r.x, w, a0);
-                a1 = __fmaf_rn(r.y, w, a1);
+                a01 = __ffma2_rn(make_float2(r.x, r.y), make_float2(w, w), a01);
                 a2 = __fmaf_rn(r.z, w, a2);
             }
         }
     }
-    acc[0] = a0;
-    acc[1] = a1;
+    acc[0] = a01.x;
+    acc[1] = a01.y;
     acc[2] = a2;
+}
+
+// Force of one group added to a particle's grid force, in group order: q-weighted for the
+// 'charges' group (device_utils.cu:412-461 multiplies by the charge).
+__device__ __forceinline__ void add_group(float *fg, const float *a, bool qw, float qp)
+{
+#pragma unroll
+    for (int j = 0; j < 3; j++) fg[j] = qw ? __fmaf_rn(a[j], qp, fg[j]) : fg[j] + a[j];
 }
 
 constexpr int kPartOut = 32;   // particles per pass gathered from global memory by helpers
@@ -332,39 +334,32 @@ constexpr int kPartOut = 32;   // particles per pass gathered from global memory
 // (a tile with more particles takes more than one pass)
 constexpr int kPartThreadsMax = 448;
 
-// Particle pass over one Morton tile of particles (or a window of slots), one particle
-// per thread and pass: bonds, then per force group the gather (device_utils.cu:358-461),
-// then GJF/EM.  Position, flags, stencil weights and the force stay in registers across
-// the force groups.
+// Planar gather (device_utils.cu:358-461): every particle's grid force, the sum over its
+// force groups in group order, into fgrid[3p].  One particle per thread and pass, over one
+// Morton tile of particles (or a window of slots); the records are planar, rec[F][M].
 //
-// Sorted tiles stage a fixed box per force group in shared memory with cp.async: the grid
-// points of the tile's block of bricks (where its particles were at the last sort), widened
-// by the stencil and by `tc.margin` cells for the drift since.  A particle whose stencil
-// has drifted out of the box is gathered from global memory, before the staging wait, by a
+// Sorted tiles stage a fixed box per force group in shared memory: the grid points of the
+// tile's block of bricks (where its particles were at the last sort), widened by the
+// stencil and by `tc.margin` cells for the drift since.  A particle whose stencil has
+// drifted out of the box is gathered from global memory, before the staging wait, by a
 // helper thread (thread o for the pass's o-th such particle); its owner adds the result in
 // group order like any other, so the sums do not depend on which path served them.
-// EXTRA: the box has angles or walls (compiled out of the common instantiation, whose
-// schedule the unused terms would otherwise disturb)
 // TMA: sorted tiles stage their boxes with one TMA load (the host selects this instantiation
 // when it holds a descriptor for the tiles' box); else with per-thread cp.async copies.
-template <int P, bool EXTRA, bool TMA>
-__global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const ParticleParams *__restrict__ ppd, int N,
-                                                      float *__restrict__ X0, float *__restrict__ X1,
-                                                      float *__restrict__ noise, const uint32_t *__restrict__ pflags,
-                                                      const float *__restrict__ q, const int *__restrict__ brow,
-                                                      const int *__restrict__ partner,
-                                                      const uint8_t *__restrict__ btype, AngleArrays aa,
-                                                      const float4 *__restrict__ rec, const int *__restrict__ orig_id,
-                                                      curandState *__restrict__ rng,
-                                                      const long long *__restrict__ d_step, float *__restrict__ fout,
-                                                      int integrate_flag, TileCfg tc, int box_cap,
+// This kernel serves 2-D boxes, more than two force groups, unsorted particles and the
+// direct gathers; the paired tile gather below serves the rest.
+template <int P, bool TMA>
+__global__ void __launch_bounds__(kPartThreadsMax, 2) k_gather_planar(Geom g, const ParticleParams *__restrict__ ppd, int N,
+                                                      const float *__restrict__ X0, const float *__restrict__ X1,
+                                                      const uint32_t *__restrict__ pflags,
+                                                      const float *__restrict__ q, const float4 *__restrict__ rec,
+                                                      const long long *__restrict__ d_step, float *__restrict__ fgrid,
+                                                      TileCfg tc, int box_cap,
                                                       const __grid_constant__ CUtensorMap rmap, int *__restrict__ err)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     // the box starts on a 128-byte boundary of the shared window (a TMA destination)
     float4 *box = reinterpret_cast<float4 *>(smraw + ((128u - (smem_u32(smraw) & 127u)) & 127u));
-    // per-thread integrator operands (x_{t-1}[3], previous noise[3], particle id), planes of blockDim
-    float *iop = reinterpret_cast<float *>(box + box_cap);
     __shared__ TileShared ts;
     __shared__ float Ao[kPartOut][kMaxFGroups][3];
     __shared__ int outP[kPartOut];
@@ -374,14 +369,13 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
     const ParticleParams &pp = *ppd;
     const long long step = *d_step;
     const float *__restrict__ Xc = (step & 1) ? X1 : X0;   // x_t
-    float *__restrict__ Xn = (step & 1) ? X0 : X1;         // x_{t-1} in, x_{t+1} out
     const int nn[3] = {g.nx, g.ny, g.nz};
     int r0, r1;
     tile_range(tc, N, kPartWindow, r0, r1);
     // the tile's fixed box: stencil origins lo[j] .. lo[j] + span[j]
     int lo[3] = {0, 0, 0}, span[3] = {-1, -1, -1}, E[3] = {0, 0, 0};
     bool staged = false;
-    if (tc.start) {
+    if (tc.start && !tc.direct) {
         tile_box<P>(tc, nn, lo, span, E);
         staged = E[0] <= kMaxBoxEdge && E[1] <= kMaxBoxEdge && E[2] <= kMaxBoxEdge &&
                  (long long)((((E[0] | 1) * E[1]) | 1)) * E[2] <= box_cap;
@@ -448,20 +442,6 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
             x[1] = Xc[3 * p + 1];
             x[2] = Xc[3 * p + 2];
             fl = pflags[p];
-            // operands of the integrator go to shared memory now (their latency is then
-            // hidden behind the gathers instead of stalling the integration at the end);
-            // those of the bonds are brought into L2
-            if (integrate_flag) {
-                const unsigned T = blockDim.x;
-                cp_async4(iop + threadIdx.x, Xn + 3 * p);
-                cp_async4(iop + T + threadIdx.x, Xn + 3 * p + 1);
-                cp_async4(iop + 2 * T + threadIdx.x, Xn + 3 * p + 2);
-                cp_async4(iop + 3 * T + threadIdx.x, noise + 3 * p);
-                cp_async4(iop + 4 * T + threadIdx.x, noise + 3 * p + 1);
-                cp_async4(iop + 5 * T + threadIdx.x, noise + 3 * p + 2);
-                cp_async4(iop + 6 * T + threadIdx.x, orig_id + p);
-            }
-            if (brow) asm volatile("prefetch.global.L2 [%0];" ::"l"(brow + p));
             if (q) asm volatile("prefetch.global.L2 [%0];" ::"l"(q + p));
         }
         const unsigned fm = (fl >> 8) & 0xffu;
@@ -510,15 +490,6 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
             for (int h = 0; h < pp.nfg; h++)
                 if ((flh >> (8 + h)) & 1u) gather_global<P, false>(g, rec + (long long)h * g.M, hs, Hx, Hy, Hz, Ao[threadIdx.x][h]);
         }
-        // 4. bonds
-        float f[3] = {0.f, 0.f, 0.f};
-        if (act) {
-            bond_force(g, pp, p, x, Xc, brow, partner, btype, f);
-            if (EXTRA) {
-                if (aa.na) angle_force(g, pp, p, Xc, aa, f);
-                if (pp.nwall) wall_terms(pp, fl, x, f, nullptr);   // potentials' own forces, before the gathers
-            }
-        }
         const int base = d[2] * E01 + d[1] * E0 + d[0];
         const float qp = (act && q) ? q[p] : 0.f;
         float Wx[P + 1], Wy[P + 1], Wz[P + 1];
@@ -527,7 +498,7 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
             stencil_fast<P>(x[1], g, 1, pp.quirk4, Wy);
             stencil_fast_z<P>(x[2], g, pp.quirk4, Wz);
         }
-        // 4b. deal the box gathers of the warp over its lanes by bank group.  A float4
+        // 4. deal the box gathers of the warp over its lanes by bank group.  A float4
         // record gather of a quarter warp takes one shared-memory wavefront only when its
         // eight lanes start at eight distinct 16-byte bank groups (record offset mod 8);
         // particles of a warp start at random offsets.  So the warp orders its particles
@@ -567,6 +538,7 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
             }
         }
         // 5. gather each force group in group order
+        float fgv[3] = {0.f, 0.f, 0.f};
         bool first = true;
         for (; fg < pp.nfg; fg++) {
             if (!((fmall >> fg) & 1u)) continue;
@@ -618,34 +590,12 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
             } else {
                 gather_global<P, true>(g, rf, gs, Wx, Wy, Wz, a);
             }
-            if ((pp.fg_qweighted >> fg) & 1u) {
-                f[0] = __fmaf_rn(a[0], qp, f[0]);
-                f[1] = __fmaf_rn(a[1], qp, f[1]);
-                f[2] = __fmaf_rn(a[2], qp, f[2]);
-            } else {
-                f[0] += a[0];
-                f[1] += a[1];
-                f[2] += a[2];
-            }
+            add_group(fgv, a, (pp.fg_qweighted >> fg) & 1u, qp);
         }
-        // 6. integrate
         if (act) {
-            if (fout) {
-                fout[3 * p] = f[0];
-                fout[3 * p + 1] = f[1];
-                fout[3 * p + 2] = f[2];
-            }
-            if (integrate_flag) {
-                const float xr[3] = {Xc[3 * p], Xc[3 * p + 1], Xc[3 * p + 2]};
-                // this thread's operands; wait_all also covers copies not yet committed to a
-                // group (tiles that stage no box)
-                asm volatile("cp.async.wait_all;\n" ::: "memory");
-                const unsigned T = blockDim.x;
-                const float xold[3] = {iop[threadIdx.x], iop[T + threadIdx.x], iop[2 * T + threadIdx.x]};
-                const float nold[3] = {iop[3 * T + threadIdx.x], iop[4 * T + threadIdx.x], iop[5 * T + threadIdx.x]};
-                const int oid = __float_as_int(iop[6 * T + threadIdx.x]);
-                integrate(g, pp, p, fl, xr, f, Xn, noise, xold, nold, oid, rng, step);
-            }
+            fgrid[3 * p] = fgv[0];
+            fgrid[3 * p + 1] = fgv[1];
+            fgrid[3 * p + 2] = fgv[2];
         }
         asm volatile("cp.async.wait_all;\n" ::: "memory");   // no copy outlives the pass
         __syncthreads();   // the box, nout and the helpers' results are reused by the next pass
@@ -654,6 +604,293 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_particles(Geom g, const 
 
 #undef TILD_STAGE
 #undef TILD_STAGE_WAIT
+
+// ---- tile gather over the paired records (RecLayout) ----
+// Gather of one particle's stencil from the paired planes in global memory (the helpers'
+// path for particles that drifted out of their tile's box), in the order and with the
+// arithmetic of the box gather: a0 = (g0.x, g0.y), a1 = (g1.x, g1.y), a2 = (g0.z, g1.z);
+// for one force group a0 = (x, y) and a1.x = z.
+template <int P, int NFG>
+__device__ __forceinline__ void gather_paired_global(const Geom &g, const RecLayout &rl, const int *gs,
+                                                     const float *Wx, const float *Wy, const float *Wz,
+                                                     float2 &a0, float2 &a1, float2 &a2)
+{
+    a0 = a1 = a2 = make_float2(0.f, 0.f);
+#pragma unroll 1
+    for (int e = 0; e <= P; e++) {
+        const float wz = sel<P>(Wz, e);
+        const long long rz = (long long)rl.py * (wrapi(gs[2] + e, g.nz) + rl.gl);
+#pragma unroll
+        for (int b = 0; b <= P; b++) {
+            const long long ry = ((long long)rl.px) * (rz + wrapi(gs[1] + b, g.ny) + rl.gl) + rl.gl;
+            const float wyz = Wy[b] * wz;
+#pragma unroll
+            for (int a = 0; a <= P; a++) {
+                const float w = Wx[a] * wyz;
+                const long long m = ry + wrapi(gs[0] + a, g.nx);
+                const float4 r = __ldg(rl.A + m);
+                a0 = __ffma2_rn(make_float2(r.x, r.y), make_float2(w, w), a0);
+                if (NFG == 2) {
+                    a1 = __ffma2_rn(make_float2(r.z, r.w), make_float2(w, w), a1);
+                    const float2 s = __ldg(rl.B + m);
+                    a2 = __ffma2_rn(s, make_float2(w, w), a2);
+                } else {
+                    a1.x = __fmaf_rn(r.z, w, a1.x);
+                }
+            }
+        }
+    }
+}
+
+// Mark of a particle whose stencil left its tile's box, written over fgrid[3p] by the tile
+// gather: a NaN bit pattern that no arithmetic produces (the GPU's NaNs are 0x7fffffff),
+// so that the integrator pass, which gathers such particles from global memory, tells
+// them apart from any force.
+constexpr unsigned kGatherLater = 0x7fa11e57u;
+
+// The tile gather: every particle's grid force into fgrid[3p], for boxes of one or two
+// force groups over the paired records.  One CTA per Morton tile, one particle per thread
+// and pass.  The tile's box (its bricks widened by the stencil and one cell of drift per
+// side) arrives by TMA loads of plane A and plane B, issued first, so that they fly while
+// the particles' positions and stencils are read and computed; the ghost layers of the
+// planes hold the periodic images, so a box never wraps.  Each warp deals its box gathers
+// over its lanes by bank position (below), gathers both force groups in one pass (three
+// paired FMAs per stencil point: (g0.x, g0.y), (g1.x, g1.y), (g0.z, g1.z)), and returns
+// the sums to the particles' own lanes.  A particle that drifted out of the box gets the
+// mark kGatherLater instead: its gather from global memory, a chain of dependent loads,
+// is left to the integrator pass, where many more warps hide it.  Sums per group are
+// formed in the order of the planar gather, so both kernels give the same bits.
+template <int P, int NFG>
+__global__ void __launch_bounds__(kPartThreadsMax, 2) k_gather_paired(Geom g, const ParticleParams *__restrict__ ppd, int N,
+                                                      const float *__restrict__ X0, const float *__restrict__ X1,
+                                                      const uint32_t *__restrict__ pflags,
+                                                      const float *__restrict__ q, RecLayout rl,
+                                                      const long long *__restrict__ d_step, float *__restrict__ fgrid,
+                                                      TileCfg tc, const __grid_constant__ CUtensorMap mapA,
+                                                      const __grid_constant__ CUtensorMap mapB, int *__restrict__ err)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int te0 = tc.te[0], te1 = tc.te[1], te2 = tc.te[2];
+    const int te01 = te0 * te1, V = te01 * te2;
+    unsigned char *al = smraw + ((128u - (smem_u32(smraw) & 127u)) & 127u);
+    float4 *boxA = reinterpret_cast<float4 *>(al);
+    float2 *boxB = reinterpret_cast<float2 *>(al + (((size_t)V * 16 + 127) & ~(size_t)127));
+    __shared__ int deal_src[kPartThreadsMax];
+    __shared__ __align__(8) unsigned long long bar;
+    const ParticleParams &pp = *ppd;
+    const long long step = *d_step;
+    const float *__restrict__ Xc = (step & 1) ? X1 : X0;
+    const int nn[3] = {g.nx, g.ny, g.nz};
+    int r0, r1;
+    tile_range(tc, N, kPartWindow, r0, r1);
+    if (r1 <= r0) return;   // an empty tile (Morton codes beyond the grid among them)
+    int lo[3], span[3], E[3];
+    tile_box<P>(tc, nn, lo, span, E);
+    // 1. the box: one TMA load per plane, coordinates in the padded grid (lo + gl >= 0)
+    if (threadIdx.x == 0) {
+        mbar_init(&bar);
+        const unsigned bytes = (unsigned)V * (NFG == 2 ? 24u : 16u);
+        asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n"
+                     ::"r"(smem_u32(&bar)), "r"(bytes) : "memory");
+        const int cx = lo[0] + rl.gl, cy = lo[1] + rl.gl, cz = lo[2] + rl.gl;
+        asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                     " [%0], [%1, {%2, %3, %4, %5}], [%6];\n"
+                     ::"r"(smem_u32(boxA)), "l"(&mapA), "r"(0), "r"(cx), "r"(cy), "r"(cz), "r"(smem_u32(&bar))
+                     : "memory");
+        if (NFG == 2)
+            asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                         " [%0], [%1, {%2, %3, %4}], [%5];\n"
+                         ::"r"(smem_u32(boxB)), "l"(&mapB), "r"(2 * cx), "r"(cy), "r"(cz), "r"(smem_u32(&bar))
+                         : "memory");
+    }
+    __syncthreads();   // the barrier is initialised before anyone waits on it
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    bool waited = false;
+    for (int c0 = r0; c0 < r1; c0 += blockDim.x) {
+        const int p = c0 + threadIdx.x;
+        const bool act = p < r1;
+        float x[3] = {0.f, 0.f, 0.f};
+        uint32_t fl = 0u;
+        float qp = 0.f;
+        if (act) {
+            x[0] = Xc[3 * p];
+            x[1] = Xc[3 * p + 1];
+            x[2] = Xc[3 * p + 2];
+            fl = pflags[p];
+            if (q) qp = q[p];
+        }
+        const unsigned fm = (fl >> 8) & ((1u << NFG) - 1u);
+        float Wx[P + 1], Wy[P + 1], Wz[P + 1];
+        int d[3] = {0, 0, 0};
+        bool inbox = false;
+        if (fm) {
+            const int gs[3] = {stencil_fast<P>(x[0], g, 0, pp.quirk4, Wx), stencil_fast<P>(x[1], g, 1, pp.quirk4, Wy),
+                               stencil_fast<P>(x[2], g, 2, pp.quirk4, Wz)};
+#pragma unroll
+            for (int j = 0; j < 3; j++) d[j] = wrapi(gs[j] - lo[j], nn[j]);
+            inbox = d[0] <= span[0] && d[1] <= span[1] && d[2] <= span[2];
+        } else {
+#pragma unroll
+            for (int i = 0; i <= P; i++) Wx[i] = Wy[i] = Wz[i] = 0.f;
+        }
+        const int base = d[2] * te01 + d[1] * te0 + d[0];
+        // 2. deal the box gathers of the warp over its lanes by bank group.  A float4 load
+        // of a quarter warp takes one shared-memory wavefront when its eight lanes start at
+        // distinct 16-byte bank groups (record offset mod 8); every stencil point adds the
+        // same offset to all lanes, so the starts decide.  The warp orders its particles by
+        // offset mod 8 (class 8: nothing to gather from the box) and lane 8q + a takes the
+        // particle at position 4a + q of the order, so that the eight lanes of a quarter
+        // warp get positions four apart, spread over the bank groups.  The lane gathers with
+        // the dealt particle's stencil (shuffled in) and returns the sums to the particle's
+        // own lane.
+        const int r = inbox ? (base & 7) : 8;
+        int below = 0;
+#pragma unroll
+        for (int v = 0; v < 8; v++) {
+            const unsigned bl = __ballot_sync(full, r == v);
+            below += v < r ? __popc(bl) : 0;
+        }
+        const int j = below + __popc(__match_any_sync(full, r) & ((1u << lane) - 1u));
+        const int tp = ((j & 3) << 3) | (j >> 2);
+        deal_src[(threadIdx.x & ~31) + tp] = lane;
+        __syncwarp();
+        const int src = deal_src[threadIdx.x];
+        __syncwarp();
+        const int bsrc = __shfl_sync(full, base, src);
+        const bool gsrc = __shfl_sync(full, inbox ? 1 : 0, src) != 0;
+#pragma unroll
+        for (int i = 0; i <= P; i++) {
+            Wx[i] = __shfl_sync(full, Wx[i], src);
+            Wy[i] = __shfl_sync(full, Wy[i], src);
+            Wz[i] = __shfl_sync(full, Wz[i], src);
+        }
+        // 3. the box has landed (bounded wait: a copy that never completes is recorded)
+        if (!waited) {
+            if (!mbar_wait(&bar, 0u)) {
+                if (lane == 0) atomicAdd(err, 1);
+                mbar_wait(&bar, 0u);
+            }
+            waited = true;
+        }
+        // 4. the dealt particle's gather: both groups in one pass
+        float2 a0 = make_float2(0.f, 0.f), a1 = make_float2(0.f, 0.f), a2 = make_float2(0.f, 0.f);
+        if (gsrc) {
+#pragma unroll
+            for (int e = 0; e <= P; e++) {
+#pragma unroll
+                for (int b = 0; b <= P; b++) {
+                    const float wyz = Wy[b] * Wz[e];
+                    const int row = bsrc + e * te01 + b * te0;
+#pragma unroll
+                    for (int aa = 0; aa <= P; aa++) {
+                        const float w = Wx[aa] * wyz;
+                        const float4 rA = boxA[row + aa];
+                        a0 = __ffma2_rn(make_float2(rA.x, rA.y), make_float2(w, w), a0);
+                        if (NFG == 2) {
+                            a1 = __ffma2_rn(make_float2(rA.z, rA.w), make_float2(w, w), a1);
+                            const float2 rB = boxB[row + aa];
+                            a2 = __ffma2_rn(rB, make_float2(w, w), a2);
+                        } else {
+                            a1.x = __fmaf_rn(rA.z, w, a1.x);
+                        }
+                    }
+                }
+            }
+        }
+        // values back to the owning lanes: group 0 (x, y, z), then group 1 (x, y, z)
+        float v[6];
+        v[0] = __shfl_sync(full, a0.x, tp);
+        v[1] = __shfl_sync(full, a0.y, tp);
+        if (NFG == 2) {
+            v[2] = __shfl_sync(full, a2.x, tp);
+            v[3] = __shfl_sync(full, a1.x, tp);
+            v[4] = __shfl_sync(full, a1.y, tp);
+            v[5] = __shfl_sync(full, a2.y, tp);
+        } else {
+            v[2] = __shfl_sync(full, a1.x, tp);
+        }
+        if (act) {
+            float fgv[3] = {0.f, 0.f, 0.f};
+            if (fm && !inbox) {
+                fgv[0] = __uint_as_float(kGatherLater);
+            } else {
+                if (fm & 1u) add_group(fgv, v, pp.fg_qweighted & 1u, qp);
+                if (NFG == 2 && (fm & 2u)) add_group(fgv, v + 3, (pp.fg_qweighted >> 1) & 1u, qp);
+            }
+            fgrid[3 * p] = fgv[0];
+            fgrid[3 * p + 1] = fgv[1];
+            fgrid[3 * p + 2] = fgv[2];
+        }
+    }
+}
+
+// ---- bonds, angles, walls and the integrator (one thread per particle) ----
+// f = (bonds, then angles, then walls: the order of d_bonds, d_angles and the wall
+// potential's CalcForces, PS_Box.cu:240-278) + the grid force fgrid[3p]; fout[3p] = f on
+// request; then GJF (ps_integratorGJF.cu:102-163) or EM (ps_integratorEM.cu:39-82) reads
+// x_t from Xc and replaces x_{t-1} in Xn by x_{t+1}.
+// A particle the tile gather marked (kGatherLater) is gathered here from the paired
+// records in global memory, with the arithmetic and order of the tile gather.
+template <int P, bool EXTRA>
+__global__ void __launch_bounds__(256) k_integrate(Geom g, const ParticleParams *__restrict__ ppd, int N,
+                                                   float *__restrict__ X0, float *__restrict__ X1,
+                                                   float *__restrict__ noise, const uint32_t *__restrict__ pflags,
+                                                   const float *__restrict__ q,
+                                                   const int *__restrict__ brow, const int *__restrict__ partner,
+                                                   const uint8_t *__restrict__ btype, AngleArrays aa,
+                                                   const float *__restrict__ fgrid, RecLayout rl,
+                                                   const int *__restrict__ orig_id,
+                                                   curandState *__restrict__ rng, const long long *__restrict__ d_step,
+                                                   float *__restrict__ fout, int integrate_flag)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    const ParticleParams &pp = *ppd;
+    const long long step = *d_step;
+    const float *__restrict__ Xc = (step & 1) ? X1 : X0;
+    float *__restrict__ Xn = (step & 1) ? X0 : X1;
+    const float x[3] = {Xc[3 * p], Xc[3 * p + 1], Xc[3 * p + 2]};
+    const uint32_t fl = pflags[p];
+    float f[3] = {0.f, 0.f, 0.f};
+    bond_force(g, pp, p, x, Xc, brow, partner, btype, f);
+    if (EXTRA) {
+        if (aa.na) angle_force(g, pp, p, Xc, aa, f);
+        if (pp.nwall) wall_terms(pp, fl, x, f, nullptr);
+    }
+    float fgv[3] = {fgrid[3 * p], fgrid[3 * p + 1], fgrid[3 * p + 2]};
+    if (rl.paired && __float_as_uint(fgv[0]) == kGatherLater) {
+        float Wx[P + 1], Wy[P + 1], Wz[P + 1];
+        const int gs[3] = {stencil_fast<P>(x[0], g, 0, pp.quirk4, Wx), stencil_fast<P>(x[1], g, 1, pp.quirk4, Wy),
+                           stencil_fast<P>(x[2], g, 2, pp.quirk4, Wz)};
+        float2 h0, h1, h2;
+        const float qp = q ? q[p] : 0.f;
+        const unsigned fm = (fl >> 8) & 3u;
+        fgv[0] = fgv[1] = fgv[2] = 0.f;
+        if (rl.nfg == 2) {
+            gather_paired_global<P, 2>(g, rl, gs, Wx, Wy, Wz, h0, h1, h2);
+            const float v[6] = {h0.x, h0.y, h2.x, h1.x, h1.y, h2.y};
+            if (fm & 1u) add_group(fgv, v, pp.fg_qweighted & 1u, qp);
+            if (fm & 2u) add_group(fgv, v + 3, (pp.fg_qweighted >> 1) & 1u, qp);
+        } else {
+            gather_paired_global<P, 1>(g, rl, gs, Wx, Wy, Wz, h0, h1, h2);
+            const float v[3] = {h0.x, h0.y, h1.x};
+            if (fm & 1u) add_group(fgv, v, pp.fg_qweighted & 1u, qp);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 3; j++) f[j] += fgv[j];
+    if (fout) {
+        fout[3 * p] = f[0];
+        fout[3 * p + 1] = f[1];
+        fout[3 * p + 2] = f[2];
+    }
+    if (integrate_flag) {
+        const float xold[3] = {Xn[3 * p], Xn[3 * p + 1], Xn[3 * p + 2]};
+        const float nold[3] = {noise[3 * p], noise[3 * p + 1], noise[3 * p + 2]};
+        integrate(g, pp, p, fl, x, f, Xn, noise, xold, nold, orig_id[p], rng, step);
+    }
+}
 
 __global__ void k_tick(long long *d_step) { *d_step += 1; }
 
@@ -783,48 +1020,62 @@ __global__ void k_reduce_partials(const double *partials, int nblocks, int ncols
 }
 
 
-constexpr size_t kPartSmemMax = 128 + kPartBox * sizeof(float4) + kPartThreadsMax * 7 * sizeof(float);
+constexpr size_t kPartSmemMax = 128 + kPartBox * sizeof(float4);
+constexpr size_t kPairSmemMax = 200 * 1024;   // a paired box of up to 8,500 points
+
+// shared memory of the paired tile gather for boxes of te[] points
+static size_t paired_smem(const int *te, int nfg)
+{
+    const size_t V = (size_t)te[0] * te[1] * te[2];
+    return 128 + ((V * 16 + 127) & ~(size_t)127) + (nfg == 2 ? V * 8 : 0);
+}
 
 template <int P>
-static void part_launch(const Geom &g, const ParticleParams *ppd, int N, float *X0, float *X1, float *noise,
-                        const uint32_t *pflags, const float *q, const int *brow, const int *partner,
-                        const uint8_t *btype, AngleArrays aa, const float4 *rec, const int *orig_id, void *rng,
-                        const long long *d_step, float *fout, int integrate, const TileCfg &tc0, bool walls,
-                        const CUtensorMap *rec_map, int *err, cudaStream_t st)
+static cudaError_t gather_launch(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd, const float *X0,
+                                 const float *X1, const uint32_t *pflags, const float *q, const float4 *rec,
+                                 const RecLayout &rl, const long long *d_step, float *fgrid, const TileCfg &tc0,
+                                 const CUtensorMap *rec_map, const CUtensorMap *pmapA, const CUtensorMap *pmapB,
+                                 int *err, cudaStream_t st)
 {
+    const int N = pp.N;
     TileCfg tc = tc0;
+    const int nbk = tc.start ? tile_ctas(tc) : (N + kPartWindow - 1) / kPartWindow;
+    const int threads = tc.start ? std::min(tc.threads, kPartThreadsMax) : 256;
+    if (rl.paired) {   // the host lays the records out in pairs only for sorted tiles it holds maps for
+        if (!tc.start || !tc.paired || !pmapA || (rl.nfg == 2 && !pmapB) || g.nz < 2) return cudaErrorInvalidValue;
+        const size_t smem = paired_smem(tc.te, rl.nfg);
+        if (smem > kPairSmemMax) return cudaErrorInvalidValue;
+        if (rl.nfg == 2)
+            k_gather_paired<P, 2><<<nbk, threads, smem, st>>>(g, ppd, N, X0, X1, pflags, q, rl, d_step, fgrid, tc,
+                                                              *pmapA, *pmapB, err);
+        else
+            k_gather_paired<P, 1><<<nbk, threads, smem, st>>>(g, ppd, N, X0, X1, pflags, q, rl, d_step, fgrid, tc,
+                                                              *pmapA, *pmapA, err);
+        return cudaGetLastError();
+    }
     CUtensorMap none;
     std::memset(&none, 0, sizeof(none));
     if (!rec_map || tc.direct) tc.te[0] = tc.te[1] = tc.te[2] = 0;   // no TMA descriptor: cp.async staging
     const CUtensorMap &rm = rec_map ? *rec_map : none;
-    const int nbk = tc.start ? (tc.nkeys + tc.codes - 1) / tc.codes : (N + kPartWindow - 1) / kPartWindow;
-    const int threads = tc.start ? std::min(tc.threads, kPartThreadsMax) : 256;
     const int cap = (tc.start && !tc.direct) ? std::min(tc.pbox, kPartBox) : 0;
-    // the box first (moved up to a 128-byte boundary), then the integrator operands
-    const size_t smem = 128 + (size_t)cap * sizeof(float4) + (size_t)threads * 7 * sizeof(float);
-    const bool extra = aa.na != nullptr || walls;
+    const size_t smem = 128 + (size_t)cap * sizeof(float4);
     // TMA staging needs the descriptor and the whole fixed box inside the shared-memory box
     const bool tma = tc.start && tc.te[0] > 0 && (long long)tc.te[0] * tc.te[1] * tc.te[2] <= cap;
-    curandState *rs = reinterpret_cast<curandState *>(rng);
-#define TILD_PK(EX, TM) \
-    k_particles<P, EX, TM><<<nbk, threads, smem, st>>>(g, ppd, N, X0, X1, noise, pflags, q, brow, partner, btype, aa, rec, \
-                                                     orig_id, rs, d_step, fout, integrate, tc, cap, rm, err)
-    if (extra) {
-        if (tma) TILD_PK(true, true);
-        else TILD_PK(true, false);
-    } else {
-        if (tma) TILD_PK(false, true);
-        else TILD_PK(false, false);
-    }
-#undef TILD_PK
+    if (tma)
+        k_gather_planar<P, true><<<nbk, threads, smem, st>>>(g, ppd, N, X0, X1, pflags, q, rec, d_step, fgrid, tc, cap,
+                                                             rm, err);
+    else
+        k_gather_planar<P, false><<<nbk, threads, smem, st>>>(g, ppd, N, X0, X1, pflags, q, rec, d_step, fgrid, tc,
+                                                              cap, rm, err);
+    return cudaGetLastError();
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no driver library link).
-bool build_record_map(CUtensorMap *map, const float4 *rec, const Geom &g, int nfg, const int *te)
+typedef CUresult (*EncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiled tensor_map_encoder()
 {
-    typedef CUresult (*EncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                    const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
     static EncodeTiled fn = nullptr;
     if (!fn) {
         void *p = nullptr;
@@ -832,10 +1083,17 @@ bool build_record_map(CUtensorMap *map, const float4 *rec, const Geom &g, int nf
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &qr) != cudaSuccess ||
             qr != cudaDriverEntryPointSuccess || !p) {
             cudaGetLastError();
-            return false;
+            return nullptr;
         }
         fn = reinterpret_cast<EncodeTiled>(p);
     }
+    return fn;
+}
+
+bool build_record_map(CUtensorMap *map, const float4 *rec, const Geom &g, int nfg, const int *te)
+{
+    EncodeTiled fn = tensor_map_encoder();
+    if (!fn) return false;
     if (te[0] <= 0 || te[0] > 256 || te[1] > 256 || te[2] > 256 || g.nz < 2) return false;
     // float4 records as 4 floats: (component, x, y, z, group); a box is one group's te[] points
     const cuuint64_t dims[5] = {4, (cuuint64_t)g.nx, (cuuint64_t)g.ny, (cuuint64_t)g.nz, (cuuint64_t)nfg};
@@ -848,13 +1106,65 @@ bool build_record_map(CUtensorMap *map, const float4 *rec, const Geom &g, int nf
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+size_t rec_layout_bytes(const Geom &g, int nfg, int gl, const int *gh)
+{
+    const long long px = ((long long)g.nx + gl + gh[0] + 1) & ~1ll, py = (long long)g.ny + gl + gh[1],
+                    pz = (long long)g.nz + gl + gh[2];
+    const size_t pM = (size_t)(px * py * pz);
+    return ((pM * 16 + 255) & ~(size_t)255) + (nfg == 2 ? pM * 8 : 0);
+}
+
+RecLayout make_rec_layout(const Geom &g, int nfg, int gl, const int *gh, void *base)
+{
+    RecLayout r{};
+    r.paired = 1;
+    r.nfg = nfg;
+    r.gl = gl;
+    for (int j = 0; j < 3; j++) r.gh[j] = gh[j];
+    r.px = (g.nx + gl + gh[0] + 1) & ~1;   // even: plane B's rows of 2 px floats stay 16-byte multiples
+    r.gh[0] = r.px - g.nx - gl;
+    r.py = g.ny + gl + gh[1];
+    r.pz = g.nz + gl + gh[2];
+    r.pM = (long long)r.px * r.py * r.pz;
+    r.A = reinterpret_cast<float4 *>(base);
+    r.B = nfg == 2 ? reinterpret_cast<float2 *>(reinterpret_cast<char *>(base) + (((size_t)r.pM * 16 + 255) & ~(size_t)255))
+                   : nullptr;
+    return r;
+}
+
+// Plane A as a 4-D tensor of floats (component, x, y, z), boxes (4, te0, te1, te2); plane B
+// as rows of 2 px floats (x, y, z), boxes (2 te0, te1, te2), which needs te0 even so that
+// a box row is a multiple of 16 bytes (its x coordinate, 2 (lo + gl) with lo + gl a
+// multiple of 4, is always aligned).
+bool build_paired_maps(CUtensorMap *mapA, CUtensorMap *mapB, const RecLayout &rl, const int *te)
+{
+    EncodeTiled fn = tensor_map_encoder();
+    if (!fn || !rl.paired) return false;
+    if (te[0] <= 0 || (te[0] & 1) || 2 * te[0] > 256 || te[1] <= 0 || te[1] > 256 || te[2] <= 0 || te[2] > 256)
+        return false;
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    const cuuint64_t dA[4] = {4, (cuuint64_t)rl.px, (cuuint64_t)rl.py, (cuuint64_t)rl.pz};
+    const cuuint64_t sA[3] = {16, 16ull * rl.px, 16ull * rl.px * rl.py};
+    const cuuint32_t bA[4] = {4, (cuuint32_t)te[0], (cuuint32_t)te[1], (cuuint32_t)te[2]};
+    if (fn(mapA, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, rl.A, dA, sA, bA, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    if (rl.nfg != 2) return true;
+    const cuuint64_t dB[3] = {2ull * rl.px, (cuuint64_t)rl.py, (cuuint64_t)rl.pz};
+    const cuuint64_t sB[2] = {8ull * rl.px, 8ull * rl.px * rl.py};
+    const cuuint32_t bB[3] = {(cuuint32_t)(2 * te[0]), (cuuint32_t)te[1], (cuuint32_t)te[2]};
+    return fn(mapB, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, rl.B, dB, sB, bB, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+           CUDA_SUCCESS;
+}
+
 void init_particle_attributes()
 {
 #define TILD_PA(P)                                                                                        \
-    cudaFuncSetAttribute(k_particles<P, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax); \
-    cudaFuncSetAttribute(k_particles<P, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);  \
-    cudaFuncSetAttribute(k_particles<P, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);  \
-    cudaFuncSetAttribute(k_particles<P, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax)
+    cudaFuncSetAttribute(k_gather_planar<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax); \
+    cudaFuncSetAttribute(k_gather_planar<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);  \
+    cudaFuncSetAttribute(k_gather_paired<P, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmemMax);     \
+    cudaFuncSetAttribute(k_gather_paired<P, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmemMax)
     TILD_PA(0);
     TILD_PA(1);
     TILD_PA(2);
@@ -863,15 +1173,18 @@ void init_particle_attributes()
 #undef TILD_PA
 }
 
-cudaError_t launch_particles(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd, float *X0,
-                             float *X1, float *noise, const uint32_t *pflags, const float *q, const int *brow,
-                             const int *partner, const uint8_t *btype, AngleArrays aa, const float4 *rec,
-                             const int *orig_id, void *rng_states, const long long *d_step, float *fout, int integrate,
-                             const TileCfg &tc, const CUtensorMap *rec_map, int *err, cudaStream_t st)
+bool paired_box_fits(const int *te, int nfg) { return paired_smem(te, nfg) <= kPairSmemMax; }
+
+cudaError_t launch_gather(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd, const float *X0,
+                          const float *X1, const uint32_t *pflags, const float *q, const float4 *rec,
+                          const RecLayout &rl, const long long *d_step, float *fgrid, const TileCfg &tc,
+                          const CUtensorMap *rec_map, const CUtensorMap *pmapA, const CUtensorMap *pmapB, int *err,
+                          cudaStream_t st)
 {
     if (pp.N == 0) return cudaSuccess;
-#define TILD_PL(P) part_launch<P>(g, ppd, pp.N, X0, X1, noise, pflags, q, brow, partner, btype, aa, rec, orig_id, \
-                                  rng_states, d_step, fout, integrate, tc, pp.nwall > 0, rec_map, err, st)
+    if (pp.nfg == 0) return cudaMemsetAsync(fgrid, 0, sizeof(float) * 3 * (size_t)pp.N, st);
+    cudaError_t e = cudaSuccess;
+#define TILD_PL(P) e = gather_launch<P>(g, pp, ppd, X0, X1, pflags, q, rec, rl, d_step, fgrid, tc, rec_map, pmapA, pmapB, err, st)
     switch (pp.order) {
         case 0: TILD_PL(0); break;
         case 1: TILD_PL(1); break;
@@ -880,6 +1193,44 @@ cudaError_t launch_particles(const Geom &g, const ParticleParams &pp, const Part
         default: TILD_PL(4); break;
     }
 #undef TILD_PL
+    return e;
+}
+
+template <int P>
+static void integrate_launch(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd, float *X0, float *X1,
+                             float *noise, const uint32_t *pflags, const float *q, const int *brow, const int *partner,
+                             const uint8_t *btype, AngleArrays aa, const float *fgrid, const RecLayout &rl,
+                             const int *orig_id, curandState *rs, const long long *d_step, float *fout, int integrate,
+                             cudaStream_t st)
+{
+    const bool extra = aa.na != nullptr || pp.nwall > 0;
+    const int nb = (pp.N + 255) / 256;
+    if (extra)
+        k_integrate<P, true><<<nb, 256, 0, st>>>(g, ppd, pp.N, X0, X1, noise, pflags, q, brow, partner, btype, aa, fgrid,
+                                                 rl, orig_id, rs, d_step, fout, integrate);
+    else
+        k_integrate<P, false><<<nb, 256, 0, st>>>(g, ppd, pp.N, X0, X1, noise, pflags, q, brow, partner, btype, aa,
+                                                  fgrid, rl, orig_id, rs, d_step, fout, integrate);
+}
+
+cudaError_t launch_integrate(const Geom &g, const ParticleParams &pp, const ParticleParams *ppd, float *X0, float *X1,
+                             float *noise, const uint32_t *pflags, const float *q, const int *brow, const int *partner,
+                             const uint8_t *btype, AngleArrays aa, const float *fgrid, const RecLayout &rl,
+                             const int *orig_id, void *rng_states, const long long *d_step, float *fout, int integrate,
+                             cudaStream_t st)
+{
+    if (pp.N == 0) return cudaSuccess;
+    curandState *rs = reinterpret_cast<curandState *>(rng_states);
+#define TILD_IL(P) integrate_launch<P>(g, pp, ppd, X0, X1, noise, pflags, q, brow, partner, btype, aa, fgrid, rl, orig_id, \
+                                       rs, d_step, fout, integrate, st)
+    switch (pp.order) {
+        case 0: TILD_IL(0); break;
+        case 1: TILD_IL(1); break;
+        case 2: TILD_IL(2); break;
+        case 3: TILD_IL(3); break;
+        default: TILD_IL(4); break;
+    }
+#undef TILD_IL
     return cudaGetLastError();
 }
 

@@ -176,11 +176,17 @@ __device__ __forceinline__ int stencil_origin_z(float z, const Geom &g)
     return g.nz == 1 ? 0 : stencil_origin<P>(z, g, 2);
 }
 
+// the CTA's tile: entry blockIdx.x of the list of tiles that meet the grid, when there is one
+__device__ __forceinline__ uint32_t tile_id(const TileCfg &tc) { return tc.list ? tc.list[blockIdx.x] : blockIdx.x; }
+
+// number of CTAs of a launch over the tiles (host)
+inline int tile_ctas(const TileCfg &tc) { return tc.list ? tc.nlist : (tc.nkeys + tc.codes - 1) / tc.codes; }
+
 // [b0, b1) of the CTA: a tile of sorted particles, or a fixed window of slots
 __device__ __forceinline__ void tile_range(const TileCfg &tc, int N, int window, int &b0, int &b1)
 {
     if (tc.start) {
-        const int k0 = blockIdx.x * tc.codes;
+        const int k0 = (int)tile_id(tc) * tc.codes;
         b0 = (int)tc.start[k0];
         b1 = (k0 + tc.codes < tc.nkeys) ? (int)tc.start[k0 + tc.codes] : N;
     } else {
@@ -208,7 +214,7 @@ __device__ __forceinline__ void tile_box(const TileCfg &tc, const int *nn, int *
 {
     int bits = 0;
     while ((1 << bits) < tc.codes) bits++;
-    const uint32_t k0 = (uint32_t)blockIdx.x * (uint32_t)tc.codes;
+    const uint32_t k0 = tile_id(tc) * (uint32_t)tc.codes;
     const int nbr[3] = {1 << ((bits + 2) / 3), 1 << ((bits + 1) / 3), 1 << (bits / 3)};
 #pragma unroll
     for (int j = 0; j < 3; j++) {
