@@ -578,6 +578,7 @@ def run_ours(args):
             "config": bench_config(spec, world),
             "rng": "philox",
             "tiles": {"bricks_per_cta": tiles["codes"], "threads": tiles["threads"], "gather": tiles["gather"],
+                      "deposit_bricks_per_cta": tiles["deposit_codes"], "deposit_threads": tiles["deposit_threads"],
                       "autotuned": not args.no_autotune},
             "step_algorithmic_gb": step_bytes / 1e9,
             "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved, "peak": peak,

@@ -186,6 +186,10 @@ void Box::setOption(const std::string &key, int64_t v)
         if (v != 0 && (v < 8 || v > 64 || (v & (v - 1)))) fail(TILD_ERR_ARG, "deposit_codes must be 0 or a power of two in [8, 64]");
         depositCodes = (int)v;
     }
+    else if (key == "deposit_threads") {
+        if (v != 0 && (v < 64 || v > 512 || v % 32)) fail(TILD_ERR_ARG, "deposit_threads must be 0 or a multiple of 32 in [64, 512]");
+        depositThreads = (int)v;
+    }
     else if (key == "sort_interval") {
         if (v < 0) fail(TILD_ERR_ARG, "sort_interval must be >= 0");
         sortInterval = (int)v;
@@ -2113,6 +2117,21 @@ RecLayout Box::recLayout()
 void Box::autotuneTiles()
 {
     if (!sortedTiles) return;
+    // the best of two timings of five force evaluations, after one to warm up
+    auto timeForces = [&](cudaEvent_t a, cudaEvent_t b) {
+        enqueueStep(false, false, dF);
+        float best = 1e30f;
+        for (int rep = 0; rep < 2; rep++) {
+            ck(cudaEventRecord(a, stream), "event");
+            for (int r = 0; r < 5; r++) enqueueStep(false, false, dF);
+            ck(cudaEventRecord(b, stream), "event");
+            ck(cudaEventSynchronize(b), "autotune");
+            float ms = 0.f;
+            ck(cudaEventElapsedTime(&ms, a, b), "event");
+            best = std::min(best, ms / 5.f);
+        }
+        return best;
+    };
     std::vector<TileCfg> cands;
     for (int c : {tiles.codes / 2, tiles.codes, tiles.codes * 2})
         if (c >= 1 && c <= 64)
@@ -2125,34 +2144,33 @@ void Box::autotuneTiles()
     for (TileCfg &t : cands) attachTileList(t);
     for (const TileCfg &t : cands) {
         tiles = t;
-        enqueueStep(false, false, dF);   // warm-up
-        ck(cudaEventRecord(e0, stream), "event");
-        for (int r = 0; r < 3; r++) enqueueStep(false, false, dF);
-        ck(cudaEventRecord(e1, stream), "event");
-        ck(cudaEventSynchronize(e1), "autotune");
-        float ms = 0.f;
-        ck(cudaEventElapsedTime(&ms, e0, e1), "event");
+        const float ms = timeForces(e0, e1);
         if (ms < best) {
             best = ms;
             pick = t;
         }
     }
     tiles = pick;
-    // the deposit's tiles: the same, twice, four and eight times the bricks (a larger tile
-    // zeroes and flushes fewer halo points per particle, but sums in FP32 once its particle
-    // count leaves the int32 range of the fixed-point box)
-    if (!depositCodes) {
+    // the deposit's tiles: the same, twice and four times the bricks (a larger tile zeroes
+    // and flushes fewer halo points per particle, but sums in FP32 once its particle count
+    // leaves the int32 range of the fixed-point box), each with one thread per particle and
+    // with CTAs of 64, 128 and 256 threads (smaller CTAs, more of them per SM)
+    if (!depositCodes || !depositThreads) {
         TileCfg dpick = dtiles;
-        for (int c = tiles.codes; c <= std::min(64, 8 * tiles.codes); c *= 2) {
-            dtiles = tileGeometry(c, true);
+        std::vector<TileCfg> dc;
+        for (int c = tiles.codes; c <= std::min(64, 4 * tiles.codes); c *= 2) {
+            if (depositCodes && c != depositCodes) continue;
+            for (int thr : {0, 64, 128, 256}) {
+                if (depositThreads && thr != depositThreads) continue;
+                TileCfg t = tileGeometry(c, true);
+                if (thr) t.threads = thr;
+                dc.push_back(t);
+            }
+        }
+        for (TileCfg &t : dc) {
+            dtiles = t;
             attachTileList(dtiles);
-            enqueueStep(false, false, dF);   // warm-up
-            ck(cudaEventRecord(e0, stream), "event");
-            for (int r = 0; r < 3; r++) enqueueStep(false, false, dF);
-            ck(cudaEventRecord(e1, stream), "event");
-            ck(cudaEventSynchronize(e1), "autotune");
-            float ms = 0.f;
-            ck(cudaEventElapsedTime(&ms, e0, e1), "event");
+            const float ms = timeForces(e0, e1);
             if (ms < best) {
                 best = ms;
                 dpick = dtiles;
@@ -2162,7 +2180,7 @@ void Box::autotuneTiles()
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    tunedMs = best / 3.f;
+    tunedMs = best;
 }
 
 // TMA descriptor of the force records for the current tiles' box (rebuilt when the tiles
@@ -2200,6 +2218,7 @@ TileCfg Box::tileCfg() const
 TileCfg Box::depTileCfg() const
 {
     TileCfg t = dtiles;
+    if (depositThreads) t.threads = depositThreads;
     t.start = sortedTiles ? sortW.start : nullptr;
     return t;
 }
@@ -2528,7 +2547,8 @@ std::string Box::describe() const
       << ", \"nBonds\": " << nBondsTot << ", \"nAngles\": " << nAnglesTot << ", \"MAXANGLES\": " << MAXANGLES
       << ", \"datFileName\": " << q(datFileName) << ", \"tiles\": {\"codes\": " << tiles.codes
       << ", \"threads\": " << tiles.threads << ", \"gather\": \"" << (tiles.direct ? "direct" : "staged")
-      << "\", \"deposit_codes\": " << dtiles.codes << ", \"autotuned\": " << (autotune ? "true" : "false")
+      << "\", \"deposit_codes\": " << dtiles.codes << ", \"deposit_threads\": " << depTileCfg().threads
+      << ", \"autotuned\": " << (autotune ? "true" : "false")
       << ", \"tuned_ms\": " << tunedMs << "}, \"trajFreq\": " << trajFreq
       << ", \"trajFileName\": " << q(trajFileName) << ", \"fieldFreq\": " << fieldFreq
       << ", \"logScaleFields\": " << (logSpaceFields ? logScaleFields : 0.f) << ", \"gsdFreq\": " << gsdFreq

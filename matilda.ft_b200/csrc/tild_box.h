@@ -282,6 +282,7 @@ private:
     TileCfg dtiles{};               // the deposit's tiles (its own brick count: a larger tile
                                     // zeroes and flushes fewer halo points per particle)
     int depositCodes = 0;           // option "deposit_codes": fixed deposit tile bricks (0: chosen)
+    int depositThreads = 0;         // option "deposit_threads": deposit CTA size (0: one thread per particle)
     TileCfg tileCfg() const;
     TileCfg depTileCfg() const;
     void pairedGhosts(const TileCfg &t, int *gl, int *gh) const;   // ghost layers the tiles' boxes reach

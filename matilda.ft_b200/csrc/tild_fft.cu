@@ -691,17 +691,24 @@ __global__ void __launch_bounds__(256) k_xinv(Geom g, FftLine lx, int nfg, const
                 a = make_float4(comp(0, l, x), comp(1, l, x), comp(2, l, x), 0.f);
             }
             const int gl = rl.gl;
-            // the lowest copy: c itself unless c sits within gl of the top (then c - n,
-            // or lower still on a grid of fewer than gl points)
-            auto low = [gl](int c, int m) { return c + gl < m ? c : c - m * ((c + gl) / m); };
-            for (int zz = low(z, g.nz); zz < g.nz + rl.gh[2]; zz += g.nz)
-                for (int yy = low(y, g.ny); yy < g.ny + rl.gh[1]; yy += g.ny) {
-                    const long long rb = ((long long)(zz + gl) * rl.py + (yy + gl)) * rl.px + gl;
-                    for (int xx = low(x, n); xx < n + rl.gh[0]; xx += n) {
-                        rl.A[rb + xx] = a;
-                        if (nfg == 2) rl.B[rb + xx] = b;
+            const long long r0 = ((long long)(z + gl) * rl.py + (y + gl)) * rl.px + gl + x;
+            rl.A[r0] = a;
+            if (nfg == 2) rl.B[r0] = b;
+            // ghosts: only points within gl of the top or gh of the bottom of an axis have any
+            if (x < rl.gh[0] || x >= n - gl || y < rl.gh[1] || y >= g.ny - gl || z < rl.gh[2] || z >= g.nz - gl) {
+                // the lowest copy: c itself unless c sits within gl of the top (then c - n,
+                // or lower still on a grid of fewer than gl points)
+                auto low = [gl](int c, int m) { return c + gl < m ? c : c - m * ((c + gl) / m); };
+                for (int zz = low(z, g.nz); zz < g.nz + rl.gh[2]; zz += g.nz)
+                    for (int yy = low(y, g.ny); yy < g.ny + rl.gh[1]; yy += g.ny) {
+                        const long long rb = ((long long)(zz + gl) * rl.py + (yy + gl)) * rl.px + gl;
+                        for (int xx = low(x, n); xx < n + rl.gh[0]; xx += n) {
+                            if (zz == z && yy == y && xx == x) continue;
+                            rl.A[rb + xx] = a;
+                            if (nfg == 2) rl.B[rb + xx] = b;
+                        }
                     }
-                }
+            }
         }
         return;
     }

@@ -833,7 +833,7 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_gather_paired(Geom g, co
 // A particle the tile gather marked (kGatherLater) is gathered here from the paired
 // records in global memory, with the arithmetic and order of the tile gather.
 template <int P, bool EXTRA>
-__global__ void __launch_bounds__(256) k_integrate(Geom g, const ParticleParams *__restrict__ ppd, int N,
+__global__ void __launch_bounds__(256, 4) k_integrate(Geom g, const ParticleParams *__restrict__ ppd, int N,
                                                    float *__restrict__ X0, float *__restrict__ X1,
                                                    float *__restrict__ noise, const uint32_t *__restrict__ pflags,
                                                    const float *__restrict__ q,
