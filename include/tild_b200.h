@@ -284,6 +284,38 @@ int tild_pool_release(tild_pool *pool, int64_t job_id);
  * cancelled. */
 int tild_pool_stats(tild_pool *pool, int64_t *out, int32_t nout);
 
+/* ---- Batch: replicas stepped together, one launch per step stage --------------------
+ * No counterpart in the reference, which runs one box per process (main.cu:63-76) and
+ * steps it alone (PS_Box::doTimeStep, PS_Box.cu:73-207).  A batch holds boxes whose
+ * endBox has been processed and that share the kernels' compile-time settings: 3-D, the
+ * same pmeorder, one or two density fields and force groups in each, the same
+ * deterministic mode and sort_interval, no ramped potential, and the tile gather (sorted
+ * tiles with TMA boxes).  Sizes, grids, potentials' amplitudes, tiles, integrators and
+ * seeds may differ.  Each step runs every stage of the TILD step (zeroing the deposit
+ * targets, the deposit, the five transform passes, the grid gather, the integrator pass,
+ * the step counters) as ONE kernel launch over the work of all replicas -- their
+ * geometries, FFT plans, tile lists and TMA descriptors in a device table -- and the ten
+ * launches of a step are captured once in a CUDA graph; each replica's spatial re-sort
+ * runs every sort_interval steps as a branch of one more graph.  A step is bit-identical to
+ * tild_box_step on each replica in deterministic mode.  The boxes stay the caller's: read
+ * them with tild_box_get_positions, tild_box_thermo and the like; destroy the batch before
+ * its boxes (tild_box_destroy refuses a box that belongs to a batch). */
+typedef struct tild_batch tild_batch;
+
+int tild_batch_create(int device, tild_batch **out);
+int tild_batch_destroy(tild_batch *batch);
+/* Adds a box: TILD_ERR_STATE before its endBox or when it belongs to a batch already,
+ * TILD_ERR_UNSUPPORTED (with the reason) when it does not share the batch's settings. */
+int tild_batch_add(tild_batch *batch, tild_box *box);
+int tild_batch_size(tild_batch *batch, int32_t *n);
+/* Splits the replicas into `streams` (1..8) groups of about equal work, each stepped by
+ * its own graph on its own stream: one launch per stage per group, the groups' stages
+ * overlapping on the GPU.  1 (the default) is one launch per stage for the whole batch. */
+int tild_batch_set_streams(tild_batch *batch, int32_t streams);
+/* nsteps steps of every replica (doTimeStep without I/O, like tild_box_step); returns when
+ * they are done. */
+int tild_batch_step(tild_batch *batch, int64_t nsteps);
+
 #ifdef __cplusplus
 }
 #endif

@@ -7,6 +7,7 @@
 #include <string>
 
 #include "tild_b200.h"
+#include "tild_batch.h"
 #include "tild_box.h"
 #include "tild_pool.h"
 
@@ -16,6 +17,10 @@ struct tild_box {
 
 struct tild_pool {
     tild::Pool *impl;
+};
+
+struct tild_batch {
+    tild::Batch *impl;
 };
 
 namespace {
@@ -68,6 +73,7 @@ int tild_box_create(int device, tild_box **out)
 int tild_box_destroy(tild_box *box)
 {
     if (!box) return TILD_OK;
+    if (box->impl && box->impl->inBatch) return fail(TILD_ERR_STATE, "the box belongs to a batch: destroy the batch first");
     delete box->impl;
     delete box;
     return TILD_OK;
@@ -440,6 +446,52 @@ int tild_pool_stats(tild_pool *pool, int64_t *out, int32_t nout)
         pool->impl->stats(v);
         for (int32_t i = 0; i < nout && i < (int32_t)v.size(); i++) out[i] = v[i];
     });
+}
+
+// ---- batch ----
+int tild_batch_create(int device, tild_batch **out)
+{
+    if (!out) return fail(TILD_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+        return fail(TILD_ERR_ARG, "Device " + std::to_string(device) + " not found");
+    return guarded([&] { *out = new tild_batch{new tild::Batch(device)}; });
+}
+
+int tild_batch_destroy(tild_batch *batch)
+{
+    if (!batch) return TILD_OK;
+    delete batch->impl;
+    delete batch;
+    return TILD_OK;
+}
+
+int tild_batch_add(tild_batch *batch, tild_box *box)
+{
+    if (!batch || !batch->impl) return fail(TILD_ERR_ARG, "batch is NULL");
+    if (!box || !box->impl) return fail(TILD_ERR_ARG, "box is NULL or was handed to a pool");
+    return guarded([&] { batch->impl->add(box->impl); });
+}
+
+int tild_batch_size(tild_batch *batch, int32_t *n)
+{
+    if (!batch || !batch->impl || !n) return fail(TILD_ERR_ARG, "batch or n is NULL");
+    *n = batch->impl->size();
+    return TILD_OK;
+}
+
+int tild_batch_set_streams(tild_batch *batch, int32_t streams)
+{
+    if (!batch || !batch->impl) return fail(TILD_ERR_ARG, "batch is NULL");
+    return guarded([&] { batch->impl->setStreams(streams); });
+}
+
+int tild_batch_step(tild_batch *batch, int64_t nsteps)
+{
+    if (!batch || !batch->impl) return fail(TILD_ERR_ARG, "batch is NULL");
+    if (nsteps < 0) return fail(TILD_ERR_ARG, "nsteps must be >= 0");
+    return guarded([&] { batch->impl->step(nsteps); });
 }
 
 }  // extern "C"

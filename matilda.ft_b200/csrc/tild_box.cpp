@@ -2089,7 +2089,7 @@ void Box::pairedGhosts(const TileCfg &t, int *gl, int *gh) const
 RecLayout Box::recLayout()
 {
     RecLayout rl{};
-    if (!tiles.paired) return rl;
+    if (!tiles.paired || !sortedTiles) return rl;   // unsorted particles: windows of slots, planar gather
     int gl, gh[3];
     pairedGhosts(tiles, &gl, gh);
     if (rec_layout_bytes(geom, (int)fgroups.size(), gl, gh) <= recBytes) {

@@ -17,6 +17,8 @@
 
 namespace tild {
 
+class Batch;
+
 struct BoxError {
     int code;
     std::string msg;
@@ -131,8 +133,10 @@ public:
     int64_t deviceBytes() const { return devBytes; }
     int logColumns() const { return 2 + (nAnglesTot > 0 ? 1 : 0) + (int)potentials.size(); }
     bool echo = false;
+    Batch *inBatch = nullptr;       // the batch this box belongs to (tild_batch.h), if any
 
 private:
+    friend class Batch;
     // parse helpers
     void parseWords(std::vector<std::string> &w, size_t &i);
     void addPotential(std::vector<std::string> &w, size_t &i);

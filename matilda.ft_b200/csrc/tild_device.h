@@ -196,6 +196,62 @@ struct AngleArrays {        // angles in slot order (all NULL: the box has none)
 };
 
 // -------------------------------------------------------------------------------------
+// Batched replicas: one launch per step stage over the work of several boxes.  Each box's
+// step state is one entry of a device table; CTA b of a stage belongs to the replica r
+// with pre[r] <= b < pre[r + 1] and works on that replica's block b - pre[r].
+// -------------------------------------------------------------------------------------
+struct BatchRep {
+    CUtensorMap mapA, mapB;     // TMA descriptors of the paired record planes (64-byte aligned)
+    Geom g;
+    FftLine lx, ly, lz;
+    TileCfg tiles, dtiles;      // particle-pass and deposit tiles (start and list set)
+    RecLayout rl;
+    AngleArrays aa;
+    const ParticleParams *ppd;
+    const KSpace *ks;
+    const float *uk;
+    int N, quirk4, nd, nfg, int_tile_max, dep_cap, Lx, Lxi, txz, ks_npots;
+    unsigned dq;
+    float *X0, *X1, *noise;
+    const uint32_t *flags;
+    const float *q;
+    const int *brow, *partner;
+    const uint8_t *btype;
+    const int *orig;
+    void *rng;
+    float2 *dep;
+    unsigned long long *depfix;
+    float2 *H, *Hg;
+    float4 *rec;
+    float *fgrid;
+    long long *d_step;
+    int *err;
+};
+
+enum BatchStage { BS_DEPOSIT, BS_XFWD, BS_YFWD, BS_KSPACE, BS_YINV, BS_XINV, BS_GATHER, BS_INTEGRATE, BS_COUNT };
+
+struct BatchLaunch {        // one stage's launch over all replicas
+    const int *pre;         // device: exclusive prefix of the replicas' CTA counts, R + 1 entries
+    int blocks, threads;
+    size_t smem;
+};
+
+cudaError_t launch_batch_tick(const BatchRep *reps, int R, cudaStream_t st);
+// per-file pieces of the above (tild_grid.cu, tild_fft.cu, tild_particles.cu)
+void zero_batch_shape(const BatchRep &r, int deterministic, int *blocks);
+cudaError_t launch_zero_batch(const BatchRep *reps, int R, const BatchLaunch &bl, int deterministic, cudaStream_t st);
+void deposit_batch_shape(const BatchRep &r, int deterministic, int *blocks, int *threads, size_t *smem, int *cap);
+cudaError_t launch_deposit_batch(const BatchRep *reps, int R, const BatchLaunch &bl, int order, int nd,
+                                 int deterministic, cudaStream_t st);
+int fft_batch_lines(int stage, const Geom &g, int nfg);   // lines per block of the x passes
+void fft_batch_shape(int stage, const BatchRep &r, int *blocks, int *threads, size_t *smem);
+cudaError_t launch_fft_batch(int stage, const BatchRep *reps, int R, const BatchLaunch &bl, int deterministic, int txz,
+                             cudaStream_t st);
+void particles_batch_shape(int stage, const BatchRep &r, int *blocks, int *threads, size_t *smem);
+cudaError_t launch_particles_batch(int stage, const BatchRep *reps, int R, const BatchLaunch &bl, int order, int nfg,
+                                   int extra, cudaStream_t st);
+
+// -------------------------------------------------------------------------------------
 // Launchers (tild_grid.cu, tild_fft.cu, tild_particles.cu, tild_sort.cu).  All run on `st`;
 // none synchronises.
 void build_fft_line(int n, FftLine &pl, float2 *dev_tw_dst);

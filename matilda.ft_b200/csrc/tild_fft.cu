@@ -301,16 +301,16 @@ __device__ __forceinline__ void tile_load_async(float2 *dst, int dpitch, const f
 // FFT A(k) = (Z(k) + conj Z(n-k))/2 and B(k) = (Z(k) - conj Z(n-k))/(2i), k in [0, n/2].
 // -------------------------------------------------------------------------------------
 template <bool FIXED>
-__global__ void __launch_bounds__(256) k_xfwd(Geom g, FftLine lx, int nd, const float2 *__restrict__ dep,
-                                              const unsigned long long *__restrict__ depfix,
-                                              double fscale, float2 *__restrict__ H, int L)
+__device__ __forceinline__ void xfwd_body(const Geom &g, const FftLine &lx, int nd, const float2 *__restrict__ dep,
+                                          const unsigned long long *__restrict__ depfix, double fscale,
+                                          float2 *__restrict__ H, int L, unsigned vbx, unsigned vby)
 {
     extern __shared__ __align__(16) float2 sm[];
     const int n = g.nx;
     float2 *A = sm, *B = sm + L * n, *tw = sm + 2 * L * n;
-    const int pair = blockIdx.y;
+    const int pair = vby;
     const long long nlines = (long long)g.ny * g.nz;
-    const long long line0 = (long long)blockIdx.x * L;
+    const long long line0 = (long long)vbx * L;
     for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = lx.tw[t];
     const int lv = (int)min((long long)L, nlines - line0);   // lines present in this block
     if (!FIXED && (n % 2) == 0) {
@@ -350,16 +350,36 @@ __global__ void __launch_bounds__(256) k_xfwd(Geom g, FftLine lx, int nd, const 
             H[(2 * pair + 1) * g.hstride + o] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
     }
 }
+template <bool FIXED>
+__global__ void __launch_bounds__(256) k_xfwd(Geom g, FftLine lx, int nd, const float2 *__restrict__ dep,
+                                              const unsigned long long *__restrict__ depfix,
+                                              double fscale, float2 *__restrict__ H, int L)
+{
+    xfwd_body<FIXED>(g, lx, nd, dep, depfix, fscale, H, L, blockIdx.x, blockIdx.y);
+}
+
+// the x forward pass over several replicas: CTA b of replica r takes (b % gx, b / gx) of
+// the replica's grid (gx line blocks, one row per field pair)
+template <bool FIXED>
+__global__ void __launch_bounds__(256) k_xfwd_batch(const BatchRep *__restrict__ reps, const int *__restrict__ pre, int R)
+{
+    const int r = batch_replica(pre, R, blockIdx.x);
+    const BatchRep &b = reps[r];
+    const unsigned lb = blockIdx.x - pre[r];
+    const unsigned gx = (unsigned)(((long long)b.g.ny * b.g.nz + b.Lx - 1) / b.Lx);
+    xfwd_body<FIXED>(b.g, b.lx, b.nd, b.dep, b.depfix, FIXED ? 1.0 / kFixScale : 1.0, b.H, b.Lx, lb % gx, lb / gx);
+}
 
 // y-axis pass over TX half-spectrum columns of one z plane of field blockIdx.z.
 template <bool INV, int TX>
-__global__ void __launch_bounds__(256) k_ypass(Geom g, FftLine ly, float2 *__restrict__ H)
+__device__ __forceinline__ void ypass_body(const Geom &g, const FftLine &ly, float2 *__restrict__ H, unsigned vbx,
+                                           unsigned vby, unsigned vbz)
 {
     extern __shared__ __align__(16) float2 sm[];
     const int ny = g.ny;
     float2 *A = sm, *B = sm + ny * TX, *tw = sm + 2 * ny * TX;
-    const int kx0 = blockIdx.x * TX;
-    const long long base = (long long)blockIdx.z * g.hstride + (long long)blockIdx.y * ny * g.hp + kx0;
+    const int kx0 = vbx * TX;
+    const long long base = (long long)vbz * g.hstride + (long long)vby * ny * g.hp + kx0;
     for (int t = threadIdx.x; t < ny; t += blockDim.x) tw[t] = ly.tw[t];
     tile_load_async(A, TX, H + base, g.hp, ny, TX, g.nxh - kx0);
     cp_async_wait_all();
@@ -369,6 +389,23 @@ __global__ void __launch_bounds__(256) k_ypass(Geom g, FftLine ly, float2 *__res
         const int y = e / TX, c = e - y * TX;
         if (kx0 + c < g.nxh) H[base + (long long)y * g.hp + c] = R[e];
     }
+}
+template <bool INV, int TX>
+__global__ void __launch_bounds__(256) k_ypass(Geom g, FftLine ly, float2 *__restrict__ H)
+{
+    ypass_body<INV, TX>(g, ly, H, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// the y pass over several replicas: CTA b of replica r takes (x, z plane, field) of the
+// replica's grid of ceil(nxh / TX) x nz x fields (density fields forward, 3F inverse)
+template <bool INV, int TX>
+__global__ void __launch_bounds__(256) k_ypass_batch(const BatchRep *__restrict__ reps, const int *__restrict__ pre, int R)
+{
+    const int r = batch_replica(pre, R, blockIdx.x);
+    const BatchRep &b = reps[r];
+    const unsigned lb = blockIdx.x - pre[r];
+    const unsigned gx = (unsigned)((b.g.nxh + TX - 1) / TX), gy = (unsigned)b.g.nz;
+    ypass_body<INV, TX>(b.g, b.ly, INV ? b.Hg : b.H, lb % gx, (lb / gx) % gy, lb / (gx * gy));
 }
 
 // û(k) of each potential kind, FP64 (ps_potentialGaussian.cu:38-46,
@@ -450,9 +487,10 @@ __device__ __forceinline__ size_t kspace_uk_offset_dev(int nz, int nsets, int tx
 // Fused z pass: forward z FFT of every density field, k-space combine, gradient and
 // inverse z FFT of each gradient field; FP64 energies on request.
 template <int TX>
-__global__ void __launch_bounds__(256) k_kspace_z(Geom g, FftLine lz, const KSpace *__restrict__ ksp, const float2 *__restrict__ H,
-                                                  const float *__restrict__ uk, float2 *__restrict__ Hg,
-                                                  double *__restrict__ epart, int energy, int forces)
+__device__ __forceinline__ void kspace_body(const Geom &g, const FftLine &lz, const KSpace *__restrict__ ksp,
+                                            const float2 *__restrict__ H, const float *__restrict__ uk,
+                                            float2 *__restrict__ Hg, double *__restrict__ epart, int energy, int forces,
+                                            unsigned vbx, unsigned vby, unsigned vgx)
 {
     extern __shared__ __align__(16) float2 sm[];
     const KSpace &ks = *ksp;
@@ -463,7 +501,7 @@ __global__ void __launch_bounds__(256) k_kspace_z(Geom g, FftLine lz, const KSpa
     const int nsets = ndb > 2 * ks.nfg ? ndb : 2 * ks.nfg;
     float2 *Rho = sm, *S = sm + nsets * nz * TX, *tw = sm + 2 * nsets * nz * TX;
     double *red = reinterpret_cast<double *>(tw + nz);
-    const int kx0 = blockIdx.x * TX, y = blockIdx.y;
+    const int kx0 = vbx * TX, y = vby;
     for (int t = threadIdx.x; t < nz; t += blockDim.x) tw[t] = lz.tw[t];
     for (int d = 0; d < nd; d++)
         tile_load_async(Rho + d * TX, nd * TX, H + d * g.hstride + (long long)y * g.hp + kx0, (long long)g.ny * g.hp,
@@ -518,7 +556,7 @@ __global__ void __launch_bounds__(256) k_kspace_z(Geom g, FftLine lz, const KSpa
             vir[5] += sv * kyv * kzv;
         }
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-        const long long blin = (long long)blockIdx.y * gridDim.x + blockIdx.x;
+        const long long blin = (long long)vby * vgx + vbx;
         const int ncol = ks.neterms + 6;
         for (int t = 0; t < ncol; t++) {
             double v = t < ks.neterms ? acc[t] : sel<5>(vir, t - ks.neterms);
@@ -585,6 +623,24 @@ __global__ void __launch_bounds__(256) k_kspace_z(Geom g, FftLine lz, const KSpa
         }
     }
 }
+template <int TX>
+__global__ void __launch_bounds__(256) k_kspace_z(Geom g, FftLine lz, const KSpace *__restrict__ ksp, const float2 *__restrict__ H,
+                                                  const float *__restrict__ uk, float2 *__restrict__ Hg,
+                                                  double *__restrict__ epart, int energy, int forces)
+{
+    kspace_body<TX>(g, lz, ksp, H, uk, Hg, epart, energy, forces, blockIdx.x, blockIdx.y, gridDim.x);
+}
+
+// the k-space z pass over several replicas (forces only: no energy partials)
+template <int TX>
+__global__ void __launch_bounds__(256) k_kspace_batch(const BatchRep *__restrict__ reps, const int *__restrict__ pre, int R)
+{
+    const int r = batch_replica(pre, R, blockIdx.x);
+    const BatchRep &b = reps[r];
+    const unsigned lb = blockIdx.x - pre[r];
+    const unsigned gx = (unsigned)((b.g.nxh + TX - 1) / TX);
+    kspace_body<TX>(b.g, b.lz, b.ks, b.H, b.uk, b.Hg, nullptr, 0, 1, lb % gx, lb / gx, gx);
+}
 
 // Structure factor pass (after the x and y forward passes of one field): z FFT of a
 // column block, then |rho^(k)|^2 * scale binned by |k| in FP64 over the full grid (the
@@ -625,8 +681,8 @@ __global__ void __launch_bounds__(256) k_sk_z(Geom g, FftLine lz, const float2 *
 // imaginary -> field 2t+1; then float4 records (x, y, z, 0) per force group.  A block
 // takes L lines of every field: all rows are staged at once, every pair is transformed
 // in one pass over npair*L lines, and the records are written from the transform.
-__global__ void __launch_bounds__(256) k_xinv(Geom g, FftLine lx, int nfg, const float2 *__restrict__ Hg,
-                                              float4 *__restrict__ rec, RecLayout rl, int L)
+__device__ __forceinline__ void xinv_body(const Geom &g, const FftLine &lx, int nfg, const float2 *__restrict__ Hg,
+                                          float4 *__restrict__ rec, const RecLayout &rl, int L, unsigned vbx)
 {
     extern __shared__ __align__(16) float2 sm[];
     const int n = g.nx, nf = 3 * nfg, npair = (nf + 1) / 2, nxh = g.nxh, hp = g.hp;
@@ -635,7 +691,7 @@ __global__ void __launch_bounds__(256) k_xinv(Geom g, FftLine lx, int nfg, const
     // St receives 16-byte cp.async copies: start it on an even complex offset
     float2 *A = sm, *St = sm + ((bsz + 1) & ~1), *tw = St + (stsz > bsz ? stsz : bsz);
     const long long nlines = (long long)g.ny * g.nz;
-    const long long line0 = (long long)blockIdx.x * L;
+    const long long line0 = (long long)vbx * L;
     const int lv = (int)min((long long)L, nlines - line0);
     const FastDiv dn = make_fastdiv_dev(n), dL = make_fastdiv_dev(L);
     for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = lx.tw[t];
@@ -720,6 +776,19 @@ __global__ void __launch_bounds__(256) k_xinv(Geom g, FftLine lx, int nfg, const
         }
     }
 }
+__global__ void __launch_bounds__(256) k_xinv(Geom g, FftLine lx, int nfg, const float2 *__restrict__ Hg,
+                                              float4 *__restrict__ rec, RecLayout rl, int L)
+{
+    xinv_body(g, lx, nfg, Hg, rec, rl, L, blockIdx.x);
+}
+
+// the x inverse pass over several replicas
+__global__ void __launch_bounds__(256) k_xinv_batch(const BatchRep *__restrict__ reps, const int *__restrict__ pre, int R)
+{
+    const int r = batch_replica(pre, R, blockIdx.x);
+    const BatchRep &b = reps[r];
+    xinv_body(b.g, b.lx, b.nfg, b.Hg, b.rec, b.rl, b.Lxi, blockIdx.x - pre[r]);
+}
 
 
 // ---- plans and launchers ----
@@ -737,6 +806,13 @@ void init_fft_attributes()
     set_max_smem(k_kspace_z<2>, kKspaceSmemMax);
     set_max_smem(k_sk_z<kTXz>, 200 * 1024);
     set_max_smem(k_xinv, 200 * 1024);
+    set_max_smem(k_xfwd_batch<true>, 200 * 1024);
+    set_max_smem(k_xfwd_batch<false>, 200 * 1024);
+    set_max_smem(k_ypass_batch<false, kTXy>, 200 * 1024);
+    set_max_smem(k_ypass_batch<true, kTXy>, 200 * 1024);
+    set_max_smem(k_kspace_batch<4>, kKspaceSmemMax);
+    set_max_smem(k_kspace_batch<2>, kKspaceSmemMax);
+    set_max_smem(k_xinv_batch, 200 * 1024);
 }
 
 void build_fft_line(int n, FftLine &pl, float2 *dev_tw_dst)
@@ -837,17 +913,81 @@ cudaError_t launch_kspace_z(const Geom &g, const FftLine &lz, const KSpace &ks, 
     return cudaGetLastError();
 }
 
+// lines per block of the x inverse pass (about 4k complex points) and its shared memory
+static int xinv_lines(const Geom &g, int nfg)
+{
+    const int npair = (3 * nfg + 1) / 2;
+    const int L = (4096 + npair * g.nx - 1) / (npair * g.nx);
+    return L < 1 ? 1 : (L > 16 ? 16 : L);
+}
+
+static size_t xinv_smem(const Geom &g, int nfg, int L)
+{
+    const int nf = 3 * nfg, npair = (nf + 1) / 2;
+    const size_t bsz = (size_t)npair * L * g.nx, stsz = (size_t)nf * L * g.hp;
+    return (((bsz + 1) & ~(size_t)1) + std::max(bsz, stsz) + g.nx) * sizeof(float2);
+}
+
 cudaError_t launch_xinv(const Geom &g, const FftLine &lx, int nfg, const float2 *Hg, float4 *rec, const RecLayout &rl,
                         cudaStream_t st)
 {
     if (rl.paired && (rl.nfg != nfg || nfg < 1 || nfg > 2)) return cudaErrorInvalidValue;
-    const int nf = 3 * nfg, npair = (nf + 1) / 2;
-    int L = (4096 + npair * g.nx - 1) / (npair * g.nx);   // about 4k complex points per block
-    L = L < 1 ? 1 : (L > 16 ? 16 : L);
+    const int L = xinv_lines(g, nfg);
     const long long nlines = (long long)g.ny * g.nz;
-    const size_t bsz = (size_t)npair * L * g.nx, stsz = (size_t)nf * L * g.hp;
-    const size_t smx = (((bsz + 1) & ~(size_t)1) + std::max(bsz, stsz) + g.nx) * sizeof(float2);
-    k_xinv<<<(unsigned)((nlines + L - 1) / L), 256, smx, st>>>(g, lx, nfg, Hg, rec, rl, L);
+    k_xinv<<<(unsigned)((nlines + L - 1) / L), 256, xinv_smem(g, nfg, L), st>>>(g, lx, nfg, Hg, rec, rl, L);
+    return cudaGetLastError();
+}
+
+// ---- batched replicas: shapes and launches of the transform stages ----
+int fft_batch_lines(int stage, const Geom &g, int nfg)
+{
+    return stage == BS_XFWD ? lines_per_block(g.nx) : xinv_lines(g, nfg);
+}
+
+void fft_batch_shape(int stage, const BatchRep &r, int *blocks, int *threads, size_t *smem)
+{
+    const Geom &g = r.g;
+    const long long nlines = (long long)g.ny * g.nz;
+    *threads = 256;
+    switch (stage) {
+        case BS_XFWD:
+            *blocks = (int)((nlines + r.Lx - 1) / r.Lx) * ((r.nd + 1) / 2);
+            *smem = (size_t)(2 * r.Lx * g.nx + g.nx) * sizeof(float2);
+            break;
+        case BS_YFWD:
+        case BS_YINV:
+            *blocks = ((g.nxh + kTXy - 1) / kTXy) * g.nz * (stage == BS_YFWD ? r.nd : 3 * r.nfg);
+            *smem = (size_t)(2 * g.ny * kTXy + g.ny) * sizeof(float2);
+            break;
+        case BS_KSPACE:
+            *blocks = ((g.nxh + r.txz - 1) / r.txz) * g.ny;
+            *smem = kspace_smem(g, r.nd, r.nfg, r.ks_npots, r.txz);
+            break;
+        default:   // BS_XINV
+            *blocks = (int)((nlines + r.Lxi - 1) / r.Lxi);
+            *smem = xinv_smem(g, r.nfg, r.Lxi);
+            break;
+    }
+}
+
+cudaError_t launch_fft_batch(int stage, const BatchRep *reps, int R, const BatchLaunch &bl, int deterministic, int txz,
+                             cudaStream_t st)
+{
+    switch (stage) {
+        case BS_XFWD:
+            if (deterministic) k_xfwd_batch<true><<<bl.blocks, 256, bl.smem, st>>>(reps, bl.pre, R);
+            else k_xfwd_batch<false><<<bl.blocks, 256, bl.smem, st>>>(reps, bl.pre, R);
+            break;
+        case BS_YFWD: k_ypass_batch<false, kTXy><<<bl.blocks, 256, bl.smem, st>>>(reps, bl.pre, R); break;
+        case BS_YINV: k_ypass_batch<true, kTXy><<<bl.blocks, 256, bl.smem, st>>>(reps, bl.pre, R); break;
+        case BS_KSPACE:
+            if (txz == 4) k_kspace_batch<4><<<bl.blocks, 256, bl.smem, st>>>(reps, bl.pre, R);
+            else if (txz == 2) k_kspace_batch<2><<<bl.blocks, 256, bl.smem, st>>>(reps, bl.pre, R);
+            else return cudaErrorInvalidValue;
+            break;
+        case BS_XINV: k_xinv_batch<<<bl.blocks, 256, bl.smem, st>>>(reps, bl.pre, R); break;
+        default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 

@@ -174,13 +174,13 @@ __device__ __forceinline__ void global_add(float2 *dep, unsigned long long *depf
 // converted to fixed point once per point).  Each touched point is flushed once.
 // NF: number of density fields when 1 or 2 (unrolled), 0 = any.
 template <int P, int NF, bool FIXED>
-__global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4, int nd, unsigned dq,
-                                                       const float *__restrict__ X0, const float *__restrict__ X1,
-                                                       const long long *__restrict__ d_step,
-                                                       const uint32_t *__restrict__ pflags,
-                                                       const float *__restrict__ q, float2 *__restrict__ dep,
-                                                       unsigned long long *__restrict__ depfix, int cap_bytes,
-                                                       TileCfg tc, int int_tile_max)
+__device__ __forceinline__ void deposit_body(const Geom &g, int N, int quirk4, int nd, unsigned dq,
+                                             const float *__restrict__ X0, const float *__restrict__ X1,
+                                             const long long *__restrict__ d_step,
+                                             const uint32_t *__restrict__ pflags,
+                                             const float *__restrict__ q, float2 *__restrict__ dep,
+                                             unsigned long long *__restrict__ depfix, int cap_bytes,
+                                             const TileCfg &tc, int int_tile_max, unsigned bx)
 {
     constexpr int P1 = P + 1;
     constexpr int NC = NF ? NF : kMaxFields;
@@ -188,13 +188,13 @@ __global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4
     __shared__ TileShared ts;
     const float *__restrict__ X = (*d_step & 1) ? X1 : X0;
     int b0, b1;
-    tile_range(tc, N, kDepPB, b0, b1);
+    tile_range(tc, N, kDepPB, b0, b1, bx);
     if (b1 <= b0) return;
     const int nn[3] = {g.nx, g.ny, g.nz};
     // sorted tiles: the fixed box of the tile's bricks plus the drift margin; particles
     // whose stencil left it deposit with global atomics (windows of unsorted slots: all)
     int lo[3] = {0, 0, 0}, span[3] = {-1, -1, -1}, E[3] = {0, 0, 0};
-    if (tc.start) tile_box<P>(tc, nn, lo, span, E);
+    if (tc.start) tile_box<P>(tc, nn, lo, span, E, bx);
     const int nfields = NF ? NF : nd;
     const size_t esz = FIXED ? sizeof(unsigned long long) : sizeof(float);
     const long long Vl = (long long)E[0] * E[1] * E[2];
@@ -374,17 +374,45 @@ __global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4
     });
 }
 
+template <int P, int NF, bool FIXED>
+__global__ void __launch_bounds__(512) k_deposit_tiled(Geom g, int N, int quirk4, int nd, unsigned dq,
+                                                       const float *__restrict__ X0, const float *__restrict__ X1,
+                                                       const long long *__restrict__ d_step,
+                                                       const uint32_t *__restrict__ pflags,
+                                                       const float *__restrict__ q, float2 *__restrict__ dep,
+                                                       unsigned long long *__restrict__ depfix, int cap_bytes,
+                                                       TileCfg tc, int int_tile_max)
+{
+    deposit_body<P, NF, FIXED>(g, N, quirk4, nd, dq, X0, X1, d_step, pflags, q, dep, depfix, cap_bytes, tc,
+                               int_tile_max, blockIdx.x);
+}
+
+// the deposit over several replicas (one launch; see BatchRep)
+template <int P, int NF, bool FIXED>
+__global__ void __launch_bounds__(512) k_deposit_batch(const BatchRep *__restrict__ reps, const int *__restrict__ pre,
+                                                       int R)
+{
+    const int r = batch_replica(pre, R, blockIdx.x);
+    const BatchRep &b = reps[r];
+    deposit_body<P, NF, FIXED>(b.g, b.N, b.quirk4, b.nd, b.dq, b.X0, b.X1, b.d_step, b.flags, b.q, b.dep, b.depfix,
+                               b.dep_cap, b.dtiles, b.int_tile_max, blockIdx.x - pre[r]);
+}
+
+// the deposit's box capacity in bytes (the host's estimate for sorted tiles, capped)
+static int deposit_cap(const TileCfg &tc, int nf, bool fixed)
+{
+    int cap = tc.start ? (int)((size_t)tc.pbox * nf * (fixed ? 8 : 4)) : 0;
+    cap = std::min(cap, fixed ? kDepSmemFixed : kDepSmemFast);
+    return (cap + 15) & ~15;
+}
+
 template <int P, int NF>
 static void dep_launch_nf(int nb, int threads, const Geom &g, const ParticleParams &pp, const float *X0,
                           const float *X1, const long long *d_step, const uint32_t *pflags, const float *q,
                           float2 *dep, unsigned long long *depfix, const TileCfg &tc, cudaStream_t st)
 {
-    // box capacity: the host's estimate for sorted tiles, else the fixed maximum
-    const int nf = NF ? NF : pp.nd;
-    const size_t esz = depfix ? 8 : 4;
-    int cap = tc.start ? (int)((size_t)tc.pbox * nf * esz) : 0;   // the fixed tile box (no staging unsorted)
-    cap = std::min(cap, depfix ? kDepSmemFixed : kDepSmemFast);
-    cap = (cap + 15) & ~15;
+    // box capacity: the host's estimate for sorted tiles (no staging unsorted), capped
+    const int cap = deposit_cap(tc, NF ? NF : pp.nd, depfix != nullptr);
     if (depfix)
         k_deposit_tiled<P, NF, true><<<nb, threads, cap, st>>>(g, pp.N, pp.quirk4, pp.nd, pp.dchan_charge, X0,
                                                                        X1, d_step, pflags, q, dep, depfix, cap, tc,
@@ -410,11 +438,70 @@ static void dep_launch(const Geom &g, const ParticleParams &pp, const float *X0,
         dep_launch_nf<P, 0>(nb, threads, g, pp, X0, X1, d_step, pflags, q, dep, depfix, tc, st);
 }
 
+// zero every replica's deposit target: 8-byte words (float2 pairs, or 64-bit fixed point
+// in deterministic mode), 2048 per CTA
+__global__ void k_zero_batch(const BatchRep *__restrict__ reps, const int *__restrict__ pre, int R, int fixed)
+{
+    const int r = batch_replica(pre, R, blockIdx.x);
+    const BatchRep &b = reps[r];
+    const long long words = (long long)(fixed ? 2 : 1) * ((b.nd + 1) / 2) * b.g.M;
+    unsigned long long *p = fixed ? b.depfix : reinterpret_cast<unsigned long long *>(b.dep);
+    const long long i0 = (long long)(blockIdx.x - pre[r]) * 2048 + threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const long long i = i0 + k * 256;
+        if (i < words) p[i] = 0ull;
+    }
+}
+
+void zero_batch_shape(const BatchRep &r, int deterministic, int *blocks)
+{
+    const long long words = (long long)(deterministic ? 2 : 1) * ((r.nd + 1) / 2) * r.g.M;
+    *blocks = (int)((words + 2047) / 2048);
+}
+
+cudaError_t launch_zero_batch(const BatchRep *reps, int R, const BatchLaunch &bl, int deterministic, cudaStream_t st)
+{
+    k_zero_batch<<<bl.blocks, 256, 0, st>>>(reps, bl.pre, R, deterministic);
+    return cudaGetLastError();
+}
+
+void deposit_batch_shape(const BatchRep &r, int deterministic, int *blocks, int *threads, size_t *smem, int *cap)
+{
+    *cap = deposit_cap(r.dtiles, r.nd, deterministic != 0);
+    *blocks = tile_ctas(r.dtiles);
+    *threads = r.dtiles.threads;
+    *smem = (size_t)*cap;
+}
+
+cudaError_t launch_deposit_batch(const BatchRep *reps, int R, const BatchLaunch &bl, int order, int nd,
+                                 int deterministic, cudaStream_t st)
+{
+#define TILD_DB(P, NF)                                                                                      \
+    do {                                                                                                    \
+        if (deterministic) k_deposit_batch<P, NF, true><<<bl.blocks, bl.threads, bl.smem, st>>>(reps, bl.pre, R); \
+        else k_deposit_batch<P, NF, false><<<bl.blocks, bl.threads, bl.smem, st>>>(reps, bl.pre, R);         \
+    } while (0)
+#define TILD_DBP(P) do { if (nd == 1) TILD_DB(P, 1); else TILD_DB(P, 2); } while (0)
+    switch (order) {
+        case 0: TILD_DBP(0); break;
+        case 1: TILD_DBP(1); break;
+        case 2: TILD_DBP(2); break;
+        case 3: TILD_DBP(3); break;
+        default: TILD_DBP(4); break;
+    }
+#undef TILD_DBP
+#undef TILD_DB
+    return cudaGetLastError();
+}
+
 void init_deposit_attributes()
 {
 #define TILD_DA1(P, NF)                                                                                        \
     cudaFuncSetAttribute(k_deposit_tiled<P, NF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDepSmemFixed); \
-    cudaFuncSetAttribute(k_deposit_tiled<P, NF, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDepSmemFast)
+    cudaFuncSetAttribute(k_deposit_tiled<P, NF, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDepSmemFast); \
+    cudaFuncSetAttribute(k_deposit_batch<P, NF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDepSmemFixed);  \
+    cudaFuncSetAttribute(k_deposit_batch<P, NF, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDepSmemFast)
 #define TILD_DA(P) TILD_DA1(P, 0); TILD_DA1(P, 1); TILD_DA1(P, 2)
     TILD_DA(0);
     TILD_DA(1);

@@ -661,13 +661,13 @@ constexpr unsigned kGatherLater = 0x7fa11e57u;
 // is left to the integrator pass, where many more warps hide it.  Sums per group are
 // formed in the order of the planar gather, so both kernels give the same bits.
 template <int P, int NFG>
-__global__ void __launch_bounds__(kPartThreadsMax, 2) k_gather_paired(Geom g, const ParticleParams *__restrict__ ppd, int N,
-                                                      const float *__restrict__ X0, const float *__restrict__ X1,
-                                                      const uint32_t *__restrict__ pflags,
-                                                      const float *__restrict__ q, RecLayout rl,
-                                                      const long long *__restrict__ d_step, float *__restrict__ fgrid,
-                                                      TileCfg tc, const __grid_constant__ CUtensorMap mapA,
-                                                      const __grid_constant__ CUtensorMap mapB, int *__restrict__ err)
+__device__ __forceinline__ void gather_paired_body(const Geom &g, const ParticleParams *__restrict__ ppd, int N,
+                                                   const float *__restrict__ X0, const float *__restrict__ X1,
+                                                   const uint32_t *__restrict__ pflags, const float *__restrict__ q,
+                                                   const RecLayout &rl, const long long *__restrict__ d_step,
+                                                   float *__restrict__ fgrid, const TileCfg &tc,
+                                                   const CUtensorMap *mapA, const CUtensorMap *mapB,
+                                                   int *__restrict__ err, unsigned bx, bool maps_in_global)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int te0 = tc.te[0], te1 = tc.te[1], te2 = tc.te[2];
@@ -682,25 +682,29 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_gather_paired(Geom g, co
     const float *__restrict__ Xc = (step & 1) ? X1 : X0;
     const int nn[3] = {g.nx, g.ny, g.nz};
     int r0, r1;
-    tile_range(tc, N, kPartWindow, r0, r1);
-    if (r1 <= r0) return;   // an empty tile (Morton codes beyond the grid among them)
+    tile_range(tc, N, kPartWindow, r0, r1, bx);
+    if (r1 <= r0) return;   // an empty tile
     int lo[3], span[3], E[3];
-    tile_box<P>(tc, nn, lo, span, E);
+    tile_box<P>(tc, nn, lo, span, E, bx);
     // 1. the box: one TMA load per plane, coordinates in the padded grid (lo + gl >= 0)
     if (threadIdx.x == 0) {
         mbar_init(&bar);
+        if (maps_in_global) {   // descriptors in a device table: acquire them for the tensor-map proxy
+            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(mapA) : "memory");
+            if (NFG == 2) asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(mapB) : "memory");
+        }
         const unsigned bytes = (unsigned)V * (NFG == 2 ? 24u : 16u);
         asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n"
                      ::"r"(smem_u32(&bar)), "r"(bytes) : "memory");
         const int cx = lo[0] + rl.gl, cy = lo[1] + rl.gl, cz = lo[2] + rl.gl;
         asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
                      " [%0], [%1, {%2, %3, %4, %5}], [%6];\n"
-                     ::"r"(smem_u32(boxA)), "l"(&mapA), "r"(0), "r"(cx), "r"(cy), "r"(cz), "r"(smem_u32(&bar))
+                     ::"r"(smem_u32(boxA)), "l"(mapA), "r"(0), "r"(cx), "r"(cy), "r"(cz), "r"(smem_u32(&bar))
                      : "memory");
         if (NFG == 2)
             asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
                          " [%0], [%1, {%2, %3, %4}], [%5];\n"
-                         ::"r"(smem_u32(boxB)), "l"(&mapB), "r"(2 * cx), "r"(cy), "r"(cz), "r"(smem_u32(&bar))
+                         ::"r"(smem_u32(boxB)), "l"(mapB), "r"(2 * cx), "r"(cy), "r"(cz), "r"(smem_u32(&bar))
                          : "memory");
     }
     __syncthreads();   // the barrier is initialised before anyone waits on it
@@ -825,6 +829,30 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_gather_paired(Geom g, co
     }
 }
 
+template <int P, int NFG>
+__global__ void __launch_bounds__(kPartThreadsMax, 2) k_gather_paired(Geom g, const ParticleParams *__restrict__ ppd, int N,
+                                                      const float *__restrict__ X0, const float *__restrict__ X1,
+                                                      const uint32_t *__restrict__ pflags,
+                                                      const float *__restrict__ q, RecLayout rl,
+                                                      const long long *__restrict__ d_step, float *__restrict__ fgrid,
+                                                      TileCfg tc, const __grid_constant__ CUtensorMap mapA,
+                                                      const __grid_constant__ CUtensorMap mapB, int *__restrict__ err)
+{
+    gather_paired_body<P, NFG>(g, ppd, N, X0, X1, pflags, q, rl, d_step, fgrid, tc, &mapA, &mapB, err, blockIdx.x,
+                               false);
+}
+
+// the tile gather over several replicas; each replica's TMA descriptors live in the table
+template <int P, int NFG>
+__global__ void __launch_bounds__(kPartThreadsMax, 2) k_gather_batch(const BatchRep *__restrict__ reps,
+                                                                     const int *__restrict__ pre, int R)
+{
+    const int r = batch_replica(pre, R, blockIdx.x);
+    const BatchRep &b = reps[r];
+    gather_paired_body<P, NFG>(b.g, b.ppd, b.N, b.X0, b.X1, b.flags, b.q, b.rl, b.d_step, b.fgrid, b.tiles, &b.mapA,
+                               &b.mapB, b.err, blockIdx.x - pre[r], true);
+}
+
 // ---- bonds, angles, walls and the integrator (one thread per particle) ----
 // f = (bonds, then angles, then walls: the order of d_bonds, d_angles and the wall
 // potential's CalcForces, PS_Box.cu:240-278) + the grid force fgrid[3p]; fout[3p] = f on
@@ -833,18 +861,17 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_gather_paired(Geom g, co
 // A particle the tile gather marked (kGatherLater) is gathered here from the paired
 // records in global memory, with the arithmetic and order of the tile gather.
 template <int P, bool EXTRA>
-__global__ void __launch_bounds__(256, 4) k_integrate(Geom g, const ParticleParams *__restrict__ ppd, int N,
-                                                   float *__restrict__ X0, float *__restrict__ X1,
-                                                   float *__restrict__ noise, const uint32_t *__restrict__ pflags,
-                                                   const float *__restrict__ q,
-                                                   const int *__restrict__ brow, const int *__restrict__ partner,
-                                                   const uint8_t *__restrict__ btype, AngleArrays aa,
-                                                   const float *__restrict__ fgrid, RecLayout rl,
-                                                   const int *__restrict__ orig_id,
-                                                   curandState *__restrict__ rng, const long long *__restrict__ d_step,
-                                                   float *__restrict__ fout, int integrate_flag)
+__device__ __forceinline__ void integrate_body(const Geom &g, const ParticleParams *__restrict__ ppd, int N,
+                                               float *__restrict__ X0, float *__restrict__ X1,
+                                               float *__restrict__ noise, const uint32_t *__restrict__ pflags,
+                                               const float *__restrict__ q, const int *__restrict__ brow,
+                                               const int *__restrict__ partner, const uint8_t *__restrict__ btype,
+                                               const AngleArrays &aa, const float *__restrict__ fgrid,
+                                               const RecLayout &rl, const int *__restrict__ orig_id,
+                                               curandState *__restrict__ rng, const long long *__restrict__ d_step,
+                                               float *__restrict__ fout, int integrate_flag, unsigned bx)
 {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int p = (int)bx * blockDim.x + threadIdx.x;
     if (p >= N) return;
     const ParticleParams &pp = *ppd;
     const long long step = *d_step;
@@ -890,6 +917,41 @@ __global__ void __launch_bounds__(256, 4) k_integrate(Geom g, const ParticlePara
         const float nold[3] = {noise[3 * p], noise[3 * p + 1], noise[3 * p + 2]};
         integrate(g, pp, p, fl, x, f, Xn, noise, xold, nold, orig_id[p], rng, step);
     }
+}
+
+template <int P, bool EXTRA>
+__global__ void __launch_bounds__(256, 4) k_integrate(Geom g, const ParticleParams *__restrict__ ppd, int N,
+                                                   float *__restrict__ X0, float *__restrict__ X1,
+                                                   float *__restrict__ noise, const uint32_t *__restrict__ pflags,
+                                                   const float *__restrict__ q,
+                                                   const int *__restrict__ brow, const int *__restrict__ partner,
+                                                   const uint8_t *__restrict__ btype, AngleArrays aa,
+                                                   const float *__restrict__ fgrid, RecLayout rl,
+                                                   const int *__restrict__ orig_id,
+                                                   curandState *__restrict__ rng, const long long *__restrict__ d_step,
+                                                   float *__restrict__ fout, int integrate_flag)
+{
+    integrate_body<P, EXTRA>(g, ppd, N, X0, X1, noise, pflags, q, brow, partner, btype, aa, fgrid, rl, orig_id, rng,
+                             d_step, fout, integrate_flag, blockIdx.x);
+}
+
+// the integrator pass over several replicas
+template <int P, bool EXTRA>
+__global__ void __launch_bounds__(256, 4) k_integrate_batch(const BatchRep *__restrict__ reps, const int *__restrict__ pre,
+                                                         int R)
+{
+    const int r = batch_replica(pre, R, blockIdx.x);
+    const BatchRep &b = reps[r];
+    integrate_body<P, EXTRA>(b.g, b.ppd, b.N, b.X0, b.X1, b.noise, b.flags, b.q, b.brow, b.partner, b.btype, b.aa,
+                             b.fgrid, b.rl, b.orig, reinterpret_cast<curandState *>(b.rng), b.d_step, nullptr, 1,
+                             blockIdx.x - pre[r]);
+}
+
+// every replica's step counter, one thread each
+__global__ void k_tick_batch(const BatchRep *__restrict__ reps, int R)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < R) *reps[r].d_step += 1;
 }
 
 __global__ void k_tick(long long *d_step) { *d_step += 1; }
@@ -1164,7 +1226,9 @@ void init_particle_attributes()
     cudaFuncSetAttribute(k_gather_planar<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax); \
     cudaFuncSetAttribute(k_gather_planar<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmemMax);  \
     cudaFuncSetAttribute(k_gather_paired<P, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmemMax);     \
-    cudaFuncSetAttribute(k_gather_paired<P, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmemMax)
+    cudaFuncSetAttribute(k_gather_paired<P, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmemMax);     \
+    cudaFuncSetAttribute(k_gather_batch<P, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmemMax);      \
+    cudaFuncSetAttribute(k_gather_batch<P, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmemMax)
     TILD_PA(0);
     TILD_PA(1);
     TILD_PA(2);
@@ -1231,6 +1295,49 @@ cudaError_t launch_integrate(const Geom &g, const ParticleParams &pp, const Part
         default: TILD_IL(4); break;
     }
 #undef TILD_IL
+    return cudaGetLastError();
+}
+
+void particles_batch_shape(int stage, const BatchRep &r, int *blocks, int *threads, size_t *smem)
+{
+    if (stage == BS_GATHER) {
+        *blocks = tile_ctas(r.tiles);
+        *threads = std::min(r.tiles.threads, kPartThreadsMax);
+        *smem = paired_smem(r.tiles.te, r.nfg);
+    } else {   // BS_INTEGRATE
+        *blocks = (r.N + 255) / 256;
+        *threads = 256;
+        *smem = 0;
+    }
+}
+
+cudaError_t launch_particles_batch(int stage, const BatchRep *reps, int R, const BatchLaunch &bl, int order, int nfg,
+                                   int extra, cudaStream_t st)
+{
+#define TILD_GB(P)                                                                                              \
+    do {                                                                                                        \
+        if (stage == BS_GATHER) {                                                                               \
+            if (nfg == 2) k_gather_batch<P, 2><<<bl.blocks, bl.threads, bl.smem, st>>>(reps, bl.pre, R);        \
+            else k_gather_batch<P, 1><<<bl.blocks, bl.threads, bl.smem, st>>>(reps, bl.pre, R);                 \
+        } else {                                                                                                \
+            if (extra) k_integrate_batch<P, true><<<bl.blocks, 256, 0, st>>>(reps, bl.pre, R);                  \
+            else k_integrate_batch<P, false><<<bl.blocks, 256, 0, st>>>(reps, bl.pre, R);                       \
+        }                                                                                                       \
+    } while (0)
+    switch (order) {
+        case 0: TILD_GB(0); break;
+        case 1: TILD_GB(1); break;
+        case 2: TILD_GB(2); break;
+        case 3: TILD_GB(3); break;
+        default: TILD_GB(4); break;
+    }
+#undef TILD_GB
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_tick(const BatchRep *reps, int R, cudaStream_t st)
+{
+    k_tick_batch<<<(R + 127) / 128, 128, 0, st>>>(reps, R);
     return cudaGetLastError();
 }
 

@@ -111,6 +111,19 @@ __device__ __forceinline__ int stencil_fast(float x, const Geom &g, int j, int q
     return g0 - P / 2;
 }
 
+// Batched launches: CTA b of a launch over several replicas belongs to replica r with
+// pre[r] <= b < pre[r + 1] (pre: the exclusive prefix of the replicas' CTA counts).
+__device__ __forceinline__ int batch_replica(const int *__restrict__ pre, int R, int b)
+{
+    int lo = 0, hi = R;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (pre[mid] <= b) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
 // -------------------------------------------------------------------------------------
 // Tiles of spatially sorted particles.  A CTA takes the particles of `codes` (a power of
 // two >= 8) consecutive brick Morton codes -- contiguous slots after the sort, an aligned
@@ -176,23 +189,29 @@ __device__ __forceinline__ int stencil_origin_z(float z, const Geom &g)
     return g.nz == 1 ? 0 : stencil_origin<P>(z, g, 2);
 }
 
-// the CTA's tile: entry blockIdx.x of the list of tiles that meet the grid, when there is one
-__device__ __forceinline__ uint32_t tile_id(const TileCfg &tc) { return tc.list ? tc.list[blockIdx.x] : blockIdx.x; }
+// the CTA's tile: entry bx (the CTA's index among the launch's tiles) of the list of tiles
+// that meet the grid, when there is one
+__device__ __forceinline__ uint32_t tile_id(const TileCfg &tc, unsigned bx) { return tc.list ? tc.list[bx] : bx; }
+__device__ __forceinline__ uint32_t tile_id(const TileCfg &tc) { return tile_id(tc, blockIdx.x); }
 
 // number of CTAs of a launch over the tiles (host)
 inline int tile_ctas(const TileCfg &tc) { return tc.list ? tc.nlist : (tc.nkeys + tc.codes - 1) / tc.codes; }
 
-// [b0, b1) of the CTA: a tile of sorted particles, or a fixed window of slots
-__device__ __forceinline__ void tile_range(const TileCfg &tc, int N, int window, int &b0, int &b1)
+// [b0, b1) of CTA bx: a tile of sorted particles, or a fixed window of slots
+__device__ __forceinline__ void tile_range(const TileCfg &tc, int N, int window, int &b0, int &b1, unsigned bx)
 {
     if (tc.start) {
-        const int k0 = (int)tile_id(tc) * tc.codes;
+        const int k0 = (int)tile_id(tc, bx) * tc.codes;
         b0 = (int)tc.start[k0];
         b1 = (k0 + tc.codes < tc.nkeys) ? (int)tc.start[k0 + tc.codes] : N;
     } else {
-        b0 = blockIdx.x * window;
+        b0 = (int)bx * window;
         b1 = min(N, b0 + window);
     }
+}
+__device__ __forceinline__ void tile_range(const TileCfg &tc, int N, int window, int &b0, int &b1)
+{
+    tile_range(tc, N, window, b0, b1, blockIdx.x);
 }
 
 // every third bit -> 10-bit value (inverse of the sort's brick-key interleave)
@@ -210,11 +229,11 @@ __device__ __forceinline__ int compact3(uint32_t v)
 // were at the last sort) widened by tc.margin cells per side, as stencil origins
 // lo[j] .. lo[j] + span[j]; E[j] = span[j] + P + 1 grid points per axis.
 template <int P>
-__device__ __forceinline__ void tile_box(const TileCfg &tc, const int *nn, int *lo, int *span, int *E)
+__device__ __forceinline__ void tile_box(const TileCfg &tc, const int *nn, int *lo, int *span, int *E, unsigned bx)
 {
     int bits = 0;
     while ((1 << bits) < tc.codes) bits++;
-    const uint32_t k0 = tile_id(tc) * (uint32_t)tc.codes;
+    const uint32_t k0 = tile_id(tc, bx) * (uint32_t)tc.codes;
     const int nbr[3] = {1 << ((bits + 2) / 3), 1 << ((bits + 1) / 3), 1 << (bits / 3)};
 #pragma unroll
     for (int j = 0; j < 3; j++) {
@@ -224,6 +243,11 @@ __device__ __forceinline__ void tile_box(const TileCfg &tc, const int *nn, int *
         span[j] = c1 - c0 + (P % 2 == 0 ? 1 : 0) + 2 * tc.margin;
         E[j] = span[j] + P + 1;
     }
+}
+template <int P>
+__device__ __forceinline__ void tile_box(const TileCfg &tc, const int *nn, int *lo, int *span, int *E)
+{
+    tile_box<P>(tc, nn, lo, span, E, blockIdx.x);
 }
 
 // Fill the per-axis index tables of a box with edges E (all threads; E[d] <= kMaxBoxEdge).

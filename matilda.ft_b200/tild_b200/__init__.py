@@ -76,6 +76,12 @@ _SIGS = {
     "tild_pool_cancel": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
     "tild_pool_set_budget": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
     "tild_pool_stats": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32], ctypes.c_int),
+    "tild_batch_create": ([ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    "tild_batch_destroy": ([ctypes.c_void_p], ctypes.c_int),
+    "tild_batch_add": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "tild_batch_size": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
+    "tild_batch_step": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
+    "tild_batch_set_streams": ([ctypes.c_void_p, ctypes.c_int32], ctypes.c_int),
 }
 
 
@@ -134,7 +140,7 @@ class Box:
 
     def close(self):
         if getattr(self, "_h", None):
-            lib().tild_box_destroy(self._h)
+            _check(lib().tild_box_destroy(self._h))   # refused while the box belongs to a batch
             self._h = None
 
     def __del__(self):
@@ -289,6 +295,52 @@ def run_script_file(path: str, device: int = 0):
 
 
 JOB_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
+
+
+class Batch:
+    """Replicas stepped together (tild_batch_*): every stage of a step is one kernel launch
+    over all replicas, and a step's launches are one CUDA graph.  The boxes stay the
+    caller's (read them as usual); close the batch before closing its boxes."""
+
+    def __init__(self, device=0, streams=1):
+        h = ctypes.c_void_p()
+        _check(lib().tild_batch_create(int(device), ctypes.byref(h)))
+        self._h = h
+        self._boxes = []
+        if streams != 1:
+            _check(lib().tild_batch_set_streams(self._h, int(streams)))
+
+    def add(self, box: "Box"):
+        """Add a box whose endBox has been processed."""
+        _check(lib().tild_batch_add(self._h, box._h))
+        self._boxes.append(box)
+
+    def step(self, n: int):
+        """n steps of every replica."""
+        _check(lib().tild_batch_step(self._h, int(n)))
+
+    def __len__(self):
+        n = ctypes.c_int32()
+        _check(lib().tild_batch_size(self._h, ctypes.byref(n)))
+        return n.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().tild_batch_destroy(self._h)
+            self._h = None
+            self._boxes = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 class Pool:

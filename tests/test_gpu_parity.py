@@ -250,6 +250,21 @@ def test_blown_up_positions_are_reported_as_err_device():
         assert np.allclose(again["potentials"], ok["potentials"], rtol=1e-6)
 
 
+def test_spatial_sort_is_invisible_tile_gather():
+    """The same for a box of two force groups, whose sorted steps take the tile gather over
+    paired records and whose unsorted ones (sort_interval 0) the planar gather."""
+    spec = synth.small_system(seed=19, order=3, n_free=30)
+    outs = []
+    for interval in (0, 3, 1):
+        with make_box(spec, deterministic=1, sort_interval=interval) as b:
+            f = b.forces()
+            b.step(10)
+            outs.append((f, b.positions(), b.forces()))
+    for o in outs[1:]:
+        for a, b2 in zip(outs[0], o):
+            assert np.array_equal(a, b2)
+
+
 def test_spatial_sort_is_invisible():
     """Re-sorting the particle arrays changes only memory order: in deterministic mode the
     trajectory is bit-identical with no sort, a sort every 3 steps and every step."""
