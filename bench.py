@@ -602,7 +602,12 @@ def run_ours(args):
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic, "algorithmic_bytes": ab[dom],
                          "kernel_ms": {k: v * 1e3 for k, v in stage_s.items()},
-                         "step_algorithmic_gbs": step_bytes / (ms / args.steps * 1e-3) / 1e9},
+                         # every kernel of the step: algorithmic bytes / CUDA-event time, of peak
+                         "kernels": {KERNEL_NAMES[k]: {"ms": v * 1e3, "algorithmic_mb": ab[k] / 1e6,
+                                                       "gbs": ab[k] / v / 1e9, "frac": ab[k] / v / 1e9 / peak}
+                                     for k, v in stage_s.items() if v > 0},
+                         "step_algorithmic_gbs": step_bytes / (ms / args.steps * 1e-3) / 1e9,
+                         "step_frac": step_bytes / (ms / args.steps * 1e-3) / 1e9 / peak},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": METRIC, "steps_per_job": S,
                     "h2d_bytes_per_step": spec.N * 12 / S, "d2h_bytes_per_step": spec.N * 12 / S},

@@ -147,8 +147,8 @@ __device__ __forceinline__ void smem_add_signed(float *tf, unsigned long long *t
 #pragma unroll
         for (int f = 0; f < NC; f++)
             if (sgn[f]) atomicAdd(tu + f * V + i, (unsigned long long)(sgn[f] > 0 ? k : -k));
-    } else if (IB) {
-        const int k = __float2int_rn(v * kTileFix);
+    } else if (IB) {   // v carries the scale kTileFix already (see the caller)
+        const int k = __float2int_rn(v);
 #pragma unroll
         for (int f = 0; f < NC; f++)
             if (sgn[f]) atomicAdd(reinterpret_cast<int *>(tf) + f * V + i, sgn[f] > 0 ? k : -k);
@@ -211,10 +211,10 @@ __device__ __forceinline__ void deposit_body(const Geom &g, int N, int quirk4, i
         }
         __syncthreads();
         tile_tables(ts, g.nx, g.ny, g.nz, E);
-        for (int v = threadIdx.x; v < V * nfields; v += blockDim.x) {
-            if (FIXED) tu[v] = 0ull;
-            else tf[v] = 0.f;
-        }
+        // 16-byte stores (the box and its capacity are multiples of 16 bytes)
+        const int n16 = (int)(((long long)V * nfields * (long long)esz + 15) / 16);
+        uint4 *z4 = reinterpret_cast<uint4 *>(smraw);
+        for (int v = threadIdx.x; v < n16; v += blockDim.x) z4[v] = make_uint4(0u, 0u, 0u, 0u);
     }
     __syncthreads();
     const unsigned full = 0xffffffffu;
@@ -281,6 +281,9 @@ __device__ __forceinline__ void deposit_body(const Geom &g, int N, int quirk4, i
                 sgn[f] = cf[f] == 0.f ? 0 : (cf[f] == c0 ? 1 : (cf[f] == -c0 ? -1 : 2));
                 general = general || sgn[f] == 2;
             }
+            // in an int32 box the conversion's scale 2^24 rides on the coefficient: an exact
+            // power-of-two scaling, so c0 2^24 w rounds to the same value as (c0 w) 2^24
+            const float c0v = (!FIXED && ia) ? c0 * kTileFix : c0;
             // Wx * (Wy * Wz), then the coefficient: the association of the unstaged path,
             // so that the deterministic mode's fixed-point values do not depend on staging
             auto points = [&](auto int_box, auto gen) {
@@ -299,7 +302,7 @@ __device__ __forceinline__ void deposit_body(const Geom &g, int N, int quirk4, i
                                 for (int f = 0; f < NC; f++)
                                     if (cf[f] != 0.f) smem_add<FIXED>(tf, tu, f * V + row + a, cf[f] * w, IB);
                             } else {
-                                smem_add_signed<FIXED, IB, NC>(tf, tu, V, row + a, c0 * w, sgn);
+                                smem_add_signed<FIXED, IB, NC>(tf, tu, V, row + a, c0v * w, sgn);
                             }
                         }
                     }
