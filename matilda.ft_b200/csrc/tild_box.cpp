@@ -186,6 +186,10 @@ void Box::setOption(const std::string &key, int64_t v)
         if (v != 0 && (v < 8 || v > 64 || (v & (v - 1)))) fail(TILD_ERR_ARG, "deposit_codes must be 0 or a power of two in [8, 64]");
         depositCodes = (int)v;
     }
+    else if (key == "tile_codes") {
+        if (v != 0 && (v < 1 || v > 64 || (v & (v - 1)))) fail(TILD_ERR_ARG, "tile_codes must be 0 or a power of two in [1, 64]");
+        tileCodes = (int)v;
+    }
     else if (key == "deposit_threads") {
         if (v != 0 && (v < 64 || v > 512 || v % 32)) fail(TILD_ERR_ARG, "deposit_threads must be 0 or a multiple of 32 in [64, 512]");
         depositThreads = (int)v;
@@ -1001,6 +1005,7 @@ void Box::initDevice()
 // Bricks per tile from the density: about one particle per thread of a 192-thread CTA.
 int Box::densityCodes() const
 {
+    if (tileCodes) return tileCodes;
     const double perCode = 16.0 * std::min(4, geom.nz) * (double)nstot / (double)geom.M;   // particles per brick of 4^3 cells (4x4x1 in 2-D)
     int codes = 8;
     while (codes < 64 && perCode * codes * 2.0 <= 192.0) codes *= 2;
@@ -2021,8 +2026,11 @@ TileCfg Box::tileGeometry(int codes, bool direct) const
     t.direct = direct ? 1 : 0;
     t.margin = margin;
     const int nfg = (int)fgroups.size();
-    if (g.nz > 1 && !direct && nfg >= 1 && nfg <= 2) {   // paired records: an even x edge
+    if (g.nz > 1 && !direct && nfg >= 1 && nfg <= 2) {
+        // paired records: an x edge of 2 (mod 4), even for plane B's rows and such that the
+        // 8-lane gather's quarter warps start at eight distinct bank groups
         t.te[0] = (ex + 1) & ~1;
+        if (t.te[0] % 4 == 0) t.te[0] += 2;
         t.te[1] = ey;
         t.te[2] = ez;
         t.paired = paired_box_fits(t.te, nfg) ? 1 : 0;

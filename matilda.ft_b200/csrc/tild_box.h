@@ -287,6 +287,7 @@ private:
                                     // zeroes and flushes fewer halo points per particle)
     int depositCodes = 0;           // option "deposit_codes": fixed deposit tile bricks (0: chosen)
     int depositThreads = 0;         // option "deposit_threads": deposit CTA size (0: one thread per particle)
+    int tileCodes = 0;              // option "tile_codes": fixed particle-pass tile bricks (0: from the density)
     TileCfg tileCfg() const;
     TileCfg depTileCfg() const;
     void pairedGhosts(const TileCfg &t, int *gl, int *gh) const;   // ghost layers the tiles' boxes reach

@@ -284,6 +284,54 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *mb, unsigned phase
     return false;
 }
 
+// The cubic stencil (P = 3) is summed in the order of the 8-lane tile gather on every path,
+// so that every path gives the same bits: lane k of a particle's eight (column a = k & 3,
+// rows b = 2 (k >> 2) + i) chains its eight points over the planes e, then i, with one FMA
+// each, w = Wx[a] (Wy[b] Wz[e]); the eight lane sums then add as the tree
+// ((s0 + s1) + (s2 + s3)) + ((s4 + s5) + (s6 + s7)).  fetch(a, b, e, r) gives the NC
+// components r[] of one stencil point; out[] receives the NC sums.
+template <int NC, typename Fetch>
+__device__ __forceinline__ void sum8_cubic(const float *Wx, const float *Wy, const float *Wz, Fetch fetch, float *out)
+{
+    float lo[NC], hi[NC], cur[NC];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        float sk[NC];
+#pragma unroll
+        for (int c = 0; c < NC; c++) sk[c] = 0.f;
+        const int a = k & 3, bh = k >> 2;
+#pragma unroll
+        for (int e = 0; e < 4; e++)
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+                const int b = 2 * bh + i;
+                const float w = Wx[a] * (Wy[b] * Wz[e]);
+                float r[NC];
+                fetch(a, b, e, r);
+#pragma unroll
+                for (int c = 0; c < NC; c++) sk[c] = __fmaf_rn(r[c], w, sk[c]);
+            }
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+            if ((k & 1) == 0) cur[c] = sk[c];
+            else cur[c] = cur[c] + sk[c];             // s0 + s1, s2 + s3, ...
+        }
+        if (k == 1 || k == 5) {
+#pragma unroll
+            for (int c = 0; c < NC; c++) lo[c] = cur[c];
+        } else if (k == 3 || k == 7) {
+#pragma unroll
+            for (int c = 0; c < NC; c++) cur[c] = lo[c] + cur[c];   // (s0 + s1) + (s2 + s3), ...
+            if (k == 3) {
+#pragma unroll
+                for (int c = 0; c < NC; c++) hi[c] = cur[c];
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < NC; c++) out[c] = hi[c] + cur[c];
+}
+
 constexpr int kPartBox = 4096;     // float4 records staged per force group (64 KB)
 constexpr int kPartWindow = 256;   // slots per CTA when the particles are not sorted
 
@@ -297,28 +345,38 @@ __device__ __forceinline__ void gather_global(const Geom &g, const float4 *__res
 {
     // a true modulo past one box length: a position outside [0, L) still reads the grid
     auto wrap = [](int v, int n) { return wrapi(v, n); };
-    float2 a01 = make_float2(0.f, 0.f);
-    float a2 = 0.f;
+    if constexpr (P == 3) {
+        sum8_cubic<3>(Wx, Wy, Wz, [&](int a, int b, int e, float *r) {
+            const float4 v = __ldg(rf + (long long)g.nx * ((long long)g.ny * wrap(gs[2] + e, g.nz) + wrap(gs[1] + b, g.ny)) +
+                                   wrap(gs[0] + a, g.nx));
+            r[0] = v.x;
+            r[1] = v.y;
+            r[2] = v.z;
+        }, acc);
+    } else {
+        float2 a01 = make_float2(0.f, 0.f);
+        float a2 = 0.f;
 #pragma unroll(UNROLL ? P + 1 : 1)
-    for (int e = 0; e <= P; e++) {
-        const float wz = sel<P>(Wz, e);
-        const float4 *rz = rf + (long long)g.nx * g.ny * wrap(gs[2] + e, g.nz);
+        for (int e = 0; e <= P; e++) {
+            const float wz = sel<P>(Wz, e);
+            const float4 *rz = rf + (long long)g.nx * g.ny * wrap(gs[2] + e, g.nz);
 #pragma unroll
-        for (int b = 0; b <= P; b++) {
-            const float4 *ry = rz + (long long)g.nx * wrap(gs[1] + b, g.ny);
-            const float wyz = Wy[b] * wz;
+            for (int b = 0; b <= P; b++) {
+                const float4 *ry = rz + (long long)g.nx * wrap(gs[1] + b, g.ny);
+                const float wyz = Wy[b] * wz;
 #pragma unroll
-            for (int a = 0; a <= P; a++) {
-                const float w = Wx[a] * wyz;
-                const float4 r = __ldg(ry + wrap(gs[0] + a, g.nx));
-                a01 = __ffma2_rn(make_float2(r.x, r.y), make_float2(w, w), a01);
-                a2 = __fmaf_rn(r.z, w, a2);
+                for (int a = 0; a <= P; a++) {
+                    const float w = Wx[a] * wyz;
+                    const float4 r = __ldg(ry + wrap(gs[0] + a, g.nx));
+                    a01 = __ffma2_rn(make_float2(r.x, r.y), make_float2(w, w), a01);
+                    a2 = __fmaf_rn(r.z, w, a2);
+                }
             }
         }
+        acc[0] = a01.x;
+        acc[1] = a01.y;
+        acc[2] = a2;
     }
-    acc[0] = a01.x;
-    acc[1] = a01.y;
-    acc[2] = a2;
 }
 
 // Force of one group added to a particle's grid force, in group order: q-weighted for the
@@ -556,7 +614,17 @@ __global__ void __launch_bounds__(kPartThreadsMax, 2) k_gather_planar(Geom g, co
             first = false;
             float2 a01 = make_float2(0.f, 0.f);
             float a2 = 0.f;
-            if ((flsrc >> (8 + fg)) & 1u) {   // the box gather of the particle dealt to this lane
+            if (P == 3 && ((flsrc >> (8 + fg)) & 1u)) {
+                float sv[3];
+                sum8_cubic<3>(Wx, Wy, Wz, [&](int a, int b, int e, float *r) {
+                    const float4 v = box[bsrc + e * E01 + b * E0 + a];
+                    r[0] = v.x;
+                    r[1] = v.y;
+                    r[2] = v.z;
+                }, sv);
+                a01 = make_float2(sv[0], sv[1]);
+                a2 = sv[2];
+            } else if ((flsrc >> (8 + fg)) & 1u) {   // the box gather of the particle dealt to this lane
 #pragma unroll
                 for (int e = 0; e <= P; e++) {
 #pragma unroll
@@ -616,26 +684,60 @@ __device__ __forceinline__ void gather_paired_global(const Geom &g, const RecLay
                                                      float2 &a0, float2 &a1, float2 &a2)
 {
     a0 = a1 = a2 = make_float2(0.f, 0.f);
+    if constexpr (P == 3) {
+        auto pt = [&](int a, int b, int e) {
+            return ((long long)rl.py * (wrapi(gs[2] + e, g.nz) + rl.gl) + wrapi(gs[1] + b, g.ny) + rl.gl) * rl.px + rl.gl +
+                   wrapi(gs[0] + a, g.nx);
+        };
+        if (NFG == 2) {
+            float v[6];
+            sum8_cubic<6>(Wx, Wy, Wz, [&](int a, int b, int e, float *r) {
+                const long long m = pt(a, b, e);
+                const float4 q4 = __ldg(rl.A + m);
+                const float2 q2 = __ldg(rl.B + m);
+                r[0] = q4.x;
+                r[1] = q4.y;
+                r[2] = q4.z;
+                r[3] = q4.w;
+                r[4] = q2.x;
+                r[5] = q2.y;
+            }, v);
+            a0 = make_float2(v[0], v[1]);
+            a1 = make_float2(v[2], v[3]);
+            a2 = make_float2(v[4], v[5]);
+        } else {
+            float v[3];
+            sum8_cubic<3>(Wx, Wy, Wz, [&](int a, int b, int e, float *r) {
+                const float4 q4 = __ldg(rl.A + pt(a, b, e));
+                r[0] = q4.x;
+                r[1] = q4.y;
+                r[2] = q4.z;
+            }, v);
+            a0 = make_float2(v[0], v[1]);
+            a1.x = v[2];
+        }
+    } else {
 #pragma unroll 1
-    for (int e = 0; e <= P; e++) {
-        const float wz = sel<P>(Wz, e);
-        const long long rz = (long long)rl.py * (wrapi(gs[2] + e, g.nz) + rl.gl);
+        for (int e = 0; e <= P; e++) {
+            const float wz = sel<P>(Wz, e);
+            const long long rz = (long long)rl.py * (wrapi(gs[2] + e, g.nz) + rl.gl);
 #pragma unroll
-        for (int b = 0; b <= P; b++) {
-            const long long ry = ((long long)rl.px) * (rz + wrapi(gs[1] + b, g.ny) + rl.gl) + rl.gl;
-            const float wyz = Wy[b] * wz;
+            for (int b = 0; b <= P; b++) {
+                const long long ry = ((long long)rl.px) * (rz + wrapi(gs[1] + b, g.ny) + rl.gl) + rl.gl;
+                const float wyz = Wy[b] * wz;
 #pragma unroll
-            for (int a = 0; a <= P; a++) {
-                const float w = Wx[a] * wyz;
-                const long long m = ry + wrapi(gs[0] + a, g.nx);
-                const float4 r = __ldg(rl.A + m);
-                a0 = __ffma2_rn(make_float2(r.x, r.y), make_float2(w, w), a0);
-                if (NFG == 2) {
-                    a1 = __ffma2_rn(make_float2(r.z, r.w), make_float2(w, w), a1);
-                    const float2 s = __ldg(rl.B + m);
-                    a2 = __ffma2_rn(s, make_float2(w, w), a2);
-                } else {
-                    a1.x = __fmaf_rn(r.z, w, a1.x);
+                for (int a = 0; a <= P; a++) {
+                    const float w = Wx[a] * wyz;
+                    const long long m = ry + wrapi(gs[0] + a, g.nx);
+                    const float4 r = __ldg(rl.A + m);
+                    a0 = __ffma2_rn(make_float2(r.x, r.y), make_float2(w, w), a0);
+                    if (NFG == 2) {
+                        a1 = __ffma2_rn(make_float2(r.z, r.w), make_float2(w, w), a1);
+                        const float2 s = __ldg(rl.B + m);
+                        a2 = __ffma2_rn(s, make_float2(w, w), a2);
+                    } else {
+                        a1.x = __fmaf_rn(r.z, w, a1.x);
+                    }
                 }
             }
         }
@@ -739,80 +841,188 @@ __device__ __forceinline__ void gather_paired_body(const Geom &g, const Particle
             for (int i = 0; i <= P; i++) Wx[i] = Wy[i] = Wz[i] = 0.f;
         }
         const int base = d[2] * te01 + d[1] * te0 + d[0];
-        // 2. deal the box gathers of the warp over its lanes by bank group.  A float4 load
-        // of a quarter warp takes one shared-memory wavefront when its eight lanes start at
-        // distinct 16-byte bank groups (record offset mod 8); every stencil point adds the
-        // same offset to all lanes, so the starts decide.  The warp orders its particles by
-        // offset mod 8 (class 8: nothing to gather from the box) and lane 8q + a takes the
-        // particle at position 4a + q of the order, so that the eight lanes of a quarter
-        // warp get positions four apart, spread over the bank groups.  The lane gathers with
-        // the dealt particle's stencil (shuffled in) and returns the sums to the particle's
-        // own lane.
-        const int r = inbox ? (base & 7) : 8;
-        int below = 0;
+        float v[6];
+        if constexpr (P == 3) {
+            // 2. eight lanes per particle: lane k = 8 q' + k' of quarter q' takes column a = k' & 3
+            // and rows b = 2 (k' >> 2) + i of every plane of the stencil.  With a box row pitch
+            // te0 = 2 (mod 4), the eight starting records of a quarter warp are a + 2 (k' >> 2)
+            // te0 = 0..7 (mod 8) after the particle's own offset: eight distinct 16-byte bank
+            // groups, whatever the particle, so plane A's float4 loads take one wavefront per
+            // quarter.  A half warp holds two particles; their plane-B float2 loads cover eight
+            // consecutive 8-byte bank pairs each, so the warp orders its in-box particles by
+            // offset mod 16 and pairs position j with j + ceil(m / 2), about 8 apart.  The lane
+            // sums add by a fixed tree (the order of sum8_cubic) and the result goes back to the
+            // particle's own lane.
+            const int r16 = inbox ? (base & 15) : 16;
+            int below = 0;
 #pragma unroll
-        for (int v = 0; v < 8; v++) {
-            const unsigned bl = __ballot_sync(full, r == v);
-            below += v < r ? __popc(bl) : 0;
-        }
-        const int j = below + __popc(__match_any_sync(full, r) & ((1u << lane) - 1u));
-        const int tp = ((j & 3) << 3) | (j >> 2);
-        deal_src[(threadIdx.x & ~31) + tp] = lane;
-        __syncwarp();
-        const int src = deal_src[threadIdx.x];
-        __syncwarp();
-        const int bsrc = __shfl_sync(full, base, src);
-        const bool gsrc = __shfl_sync(full, inbox ? 1 : 0, src) != 0;
-#pragma unroll
-        for (int i = 0; i <= P; i++) {
-            Wx[i] = __shfl_sync(full, Wx[i], src);
-            Wy[i] = __shfl_sync(full, Wy[i], src);
-            Wz[i] = __shfl_sync(full, Wz[i], src);
-        }
-        // 3. the box has landed (bounded wait: a copy that never completes is recorded)
-        if (!waited) {
-            if (!mbar_wait(&bar, 0u)) {
-                if (lane == 0) atomicAdd(err, 1);
-                mbar_wait(&bar, 0u);
+            for (int c = 0; c < 16; c++) {
+                const unsigned bl = __ballot_sync(full, r16 == c);
+                below += c < r16 ? __popc(bl) : 0;
             }
-            waited = true;
-        }
-        // 4. the dealt particle's gather: both groups in one pass
-        float2 a0 = make_float2(0.f, 0.f), a1 = make_float2(0.f, 0.f), a2 = make_float2(0.f, 0.f);
-        if (gsrc) {
+            const int j = below + __popc(__match_any_sync(full, r16) & ((1u << lane) - 1u));
+            const int m = __popc(__ballot_sync(full, inbox));
+            const int hm = (m + 1) >> 1;
+            int myround = -1, myq = 0;
+            if (inbox) {
+                const int jj = j < hm ? j : j - hm;
+                myround = jj >> 1;
+                myq = 2 * (jj & 1) + (j < hm ? 0 : 1);
+                deal_src[(threadIdx.x & ~31) + myround * 4 + myq] = lane;
+            }
+            __syncwarp();
+            // 3. the box has landed (bounded wait: a copy that never completes is recorded)
+            if (!waited) {
+                if (!mbar_wait(&bar, 0u)) {
+                    if (lane == 0) atomicAdd(err, 1);
+                    mbar_wait(&bar, 0u);
+                }
+                waited = true;
+            }
+            const int qd = lane >> 3, ca = lane & 3, bh = (lane >> 2) & 1;
+            const int rounds = (hm + 1) >> 1;
+            float2 res0 = make_float2(0.f, 0.f), res1 = res0, res2 = res0;
+            for (int rd = 0; rd < rounds; rd++) {
+                // the particle of this quarter in this round, if any
+                const int jj = 2 * rd + (qd >> 1);
+                const bool filled = (qd & 1) == 0 ? jj < hm : jj < m - hm;
+                const int src = filled ? deal_src[(threadIdx.x & ~31) + rd * 4 + qd] : lane;
+                // the dealt particle's position and box offset; its weights are recomputed
+                // here (the same bits as its own lane's), which takes fewer shuffles -- and
+                // shuffles share the shared-memory pipe with the gathers
+                const int bs = __shfl_sync(full, base, src);
+                const float px = __shfl_sync(full, x[0], src), py = __shfl_sync(full, x[1], src),
+                            pz = __shfl_sync(full, x[2], src);
+                float wx[4], wy[4], wz[4];
+                stencil_fast<3>(px, g, 0, pp.quirk4, wx);
+                stencil_fast<3>(py, g, 1, pp.quirk4, wy);
+                stencil_fast<3>(pz, g, 2, pp.quirk4, wz);
+                const float wa = sel<3>(wx, ca), wy0 = sel<3>(wy, 2 * bh), wy1 = sel<3>(wy, 2 * bh + 1);
+                float2 s0 = make_float2(0.f, 0.f), s1 = s0, s2 = s0;
+                if (filled) {
+                    const int col = bs + ca + 2 * bh * te0;
 #pragma unroll
-            for (int e = 0; e <= P; e++) {
+                    for (int e = 0; e < 4; e++)
 #pragma unroll
-                for (int b = 0; b <= P; b++) {
-                    const float wyz = Wy[b] * Wz[e];
-                    const int row = bsrc + e * te01 + b * te0;
+                        for (int i = 0; i < 2; i++) {
+                            const float w = wa * ((i ? wy1 : wy0) * wz[e]);
+                            const int row = col + e * te01 + i * te0;
+                            const float4 rA = boxA[row];
+                            s0 = __ffma2_rn(make_float2(rA.x, rA.y), make_float2(w, w), s0);
+                            if (NFG == 2) {
+                                s1 = __ffma2_rn(make_float2(rA.z, rA.w), make_float2(w, w), s1);
+                                s2 = __ffma2_rn(boxB[row], make_float2(w, w), s2);
+                            } else {
+                                s1.x = __fmaf_rn(rA.z, w, s1.x);
+                            }
+                        }
+                }
+                // ((s0 + s1) + (s2 + s3)) + ((s4 + s5) + (s6 + s7)) over the quarter's lanes
 #pragma unroll
-                    for (int aa = 0; aa <= P; aa++) {
-                        const float w = Wx[aa] * wyz;
-                        const float4 rA = boxA[row + aa];
-                        a0 = __ffma2_rn(make_float2(rA.x, rA.y), make_float2(w, w), a0);
-                        if (NFG == 2) {
-                            a1 = __ffma2_rn(make_float2(rA.z, rA.w), make_float2(w, w), a1);
-                            const float2 rB = boxB[row + aa];
-                            a2 = __ffma2_rn(rB, make_float2(w, w), a2);
-                        } else {
-                            a1.x = __fmaf_rn(rA.z, w, a1.x);
+                for (int o = 1; o < 8; o <<= 1) {
+                    s0 = __fadd2_rn(s0, make_float2(__shfl_xor_sync(full, s0.x, o), __shfl_xor_sync(full, s0.y, o)));
+                    s1 = __fadd2_rn(s1, make_float2(__shfl_xor_sync(full, s1.x, o), __shfl_xor_sync(full, s1.y, o)));
+                    if (NFG == 2)
+                        s2 = __fadd2_rn(s2, make_float2(__shfl_xor_sync(full, s2.x, o), __shfl_xor_sync(full, s2.y, o)));
+                }
+                // the particle's own lane takes the sums of its quarter
+                const int from = 8 * myq;
+                const float2 t0 = make_float2(__shfl_sync(full, s0.x, from), __shfl_sync(full, s0.y, from));
+                const float2 t1 = make_float2(__shfl_sync(full, s1.x, from), __shfl_sync(full, s1.y, from));
+                float2 t2 = make_float2(0.f, 0.f);
+                if (NFG == 2) t2 = make_float2(__shfl_sync(full, s2.x, from), __shfl_sync(full, s2.y, from));
+                if (myround == rd) {
+                    res0 = t0;
+                    res1 = t1;
+                    res2 = t2;
+                }
+            }
+            __syncwarp();   // deal_src is rewritten by the next pass
+            v[0] = res0.x;
+            v[1] = res0.y;
+            if (NFG == 2) {
+                v[2] = res2.x;
+                v[3] = res1.x;
+                v[4] = res1.y;
+                v[5] = res2.y;
+            } else {
+                v[2] = res1.x;
+            }
+        } else {
+            // 2. deal the box gathers of the warp over its lanes by bank group.  A float4 load
+            // of a quarter warp takes one shared-memory wavefront when its eight lanes start at
+            // distinct 16-byte bank groups (record offset mod 8); every stencil point adds the
+            // same offset to all lanes, so the starts decide.  The warp orders its particles by
+            // offset mod 8 (class 8: nothing to gather from the box) and lane 8q + a takes the
+            // particle at position 4a + q of the order, so that the eight lanes of a quarter
+            // warp get positions four apart, spread over the bank groups.  The lane gathers with
+            // the dealt particle's stencil (shuffled in) and returns the sums to the particle's
+            // own lane.
+            const int r = inbox ? (base & 7) : 8;
+            int below = 0;
+#pragma unroll
+            for (int c = 0; c < 8; c++) {
+                const unsigned bl = __ballot_sync(full, r == c);
+                below += c < r ? __popc(bl) : 0;
+            }
+            const int j = below + __popc(__match_any_sync(full, r) & ((1u << lane) - 1u));
+            const int tp = ((j & 3) << 3) | (j >> 2);
+            deal_src[(threadIdx.x & ~31) + tp] = lane;
+            __syncwarp();
+            const int src = deal_src[threadIdx.x];
+            __syncwarp();
+            const int bsrc = __shfl_sync(full, base, src);
+            const bool gsrc = __shfl_sync(full, inbox ? 1 : 0, src) != 0;
+#pragma unroll
+            for (int i = 0; i <= P; i++) {
+                Wx[i] = __shfl_sync(full, Wx[i], src);
+                Wy[i] = __shfl_sync(full, Wy[i], src);
+                Wz[i] = __shfl_sync(full, Wz[i], src);
+            }
+            // 3. the box has landed (bounded wait: a copy that never completes is recorded)
+            if (!waited) {
+                if (!mbar_wait(&bar, 0u)) {
+                    if (lane == 0) atomicAdd(err, 1);
+                    mbar_wait(&bar, 0u);
+                }
+                waited = true;
+            }
+            // 4. the dealt particle's gather: both groups in one pass
+            float2 a0 = make_float2(0.f, 0.f), a1 = make_float2(0.f, 0.f), a2 = make_float2(0.f, 0.f);
+            if (gsrc) {
+#pragma unroll
+                for (int e = 0; e <= P; e++) {
+#pragma unroll
+                    for (int b = 0; b <= P; b++) {
+                        const float wyz = Wy[b] * Wz[e];
+                        const int row = bsrc + e * te01 + b * te0;
+#pragma unroll
+                        for (int aa = 0; aa <= P; aa++) {
+                            const float w = Wx[aa] * wyz;
+                            const float4 rA = boxA[row + aa];
+                            a0 = __ffma2_rn(make_float2(rA.x, rA.y), make_float2(w, w), a0);
+                            if (NFG == 2) {
+                                a1 = __ffma2_rn(make_float2(rA.z, rA.w), make_float2(w, w), a1);
+                                const float2 rB = boxB[row + aa];
+                                a2 = __ffma2_rn(rB, make_float2(w, w), a2);
+                            } else {
+                                a1.x = __fmaf_rn(rA.z, w, a1.x);
+                            }
                         }
                     }
                 }
             }
-        }
-        // values back to the owning lanes: group 0 (x, y, z), then group 1 (x, y, z)
-        float v[6];
-        v[0] = __shfl_sync(full, a0.x, tp);
-        v[1] = __shfl_sync(full, a0.y, tp);
-        if (NFG == 2) {
-            v[2] = __shfl_sync(full, a2.x, tp);
-            v[3] = __shfl_sync(full, a1.x, tp);
-            v[4] = __shfl_sync(full, a1.y, tp);
-            v[5] = __shfl_sync(full, a2.y, tp);
-        } else {
-            v[2] = __shfl_sync(full, a1.x, tp);
+            // values back to the owning lanes: group 0 (x, y, z), then group 1 (x, y, z)
+                v[0] = __shfl_sync(full, a0.x, tp);
+            v[1] = __shfl_sync(full, a0.y, tp);
+            if (NFG == 2) {
+                v[2] = __shfl_sync(full, a2.x, tp);
+                v[3] = __shfl_sync(full, a1.x, tp);
+                v[4] = __shfl_sync(full, a1.y, tp);
+                v[5] = __shfl_sync(full, a2.y, tp);
+            } else {
+                v[2] = __shfl_sync(full, a1.x, tp);
+            }
         }
         if (act) {
             float fgv[3] = {0.f, 0.f, 0.f};
