@@ -505,7 +505,9 @@ def run_ours(args):
     torch.cuda.set_device(local)
     spec = make_spec(args.scale)
     stream = torch.cuda.Stream(device=local)
-    box = tild_b200.box_from_spec(spec, device=local, options={"write_files": 0, "autotune": 0 if args.no_autotune else 1})
+    opts = {"write_files": 0, "autotune": 0 if args.no_autotune else 1}
+    opts.update(json.loads(args.box_options))
+    box = tild_b200.box_from_spec(spec, device=local, options=opts)
     box.set_stream(stream.cuda_stream)
     box.command("endBox")
     info = box.info()
@@ -642,6 +644,9 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched (C3) and served (C5) runs")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the density rule's tiles (profiling: fewer launches before the steps)")
+    ap.add_argument("--box-options", default="{}",
+                    help="JSON of box options, e.g. fixed tiles for profiling: "
+                         '\'{"tile_codes": 4, "deposit_codes": 8, "deposit_threads": 128}\'')
     ap.add_argument("--c3-replicas", type=int, default=64)
     ap.add_argument("--c3-steps", type=int, default=2000)
     ap.add_argument("--c5-jobs", type=int, default=24, help="served jobs (the stated stream has 2,000)")
