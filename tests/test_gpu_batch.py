@@ -116,3 +116,41 @@ def test_batch_c3_like_replicas_run():
         x = b.positions()
         assert np.isfinite(x).all() and (x >= 0).all() and (x <= s.L[:3]).all()
         b.close()
+
+
+ANGLES = [dict(style="harmonic", k=3.0, theta=120.0), dict(style="wlc", k=2.0)]
+
+
+@pytest.mark.parametrize("kind", ["one_force_group", "angles", "curand_noise", "em"])
+def test_batch_other_kernel_settings_match_alone(kind):
+    """The batch's other instantiations: one density field and force group (a homopolymer
+    with one Gaussian), replicas with angles (the integrator pass's extra terms), the
+    cuRAND-compatible noise (per-particle generator states) and the EM integrator; each
+    replica bit-identical in deterministic mode to its run alone."""
+    opts = {"deterministic": 1}
+    if kind == "one_force_group":
+        pots = [dict(kind="gaussian", I="all", J="all", A=3.0, sigma=0.7)]
+        specs = [synth.small_system(seed=50 + k, n_chains=70 + 30 * k, nper=8, L=8.0 + k, grid=(16 + 2 * k,) * 3,
+                                    pots=pots) for k in range(3)]
+    elif kind == "angles":
+        specs = [synth.small_system(seed=60 + k, n_chains=60 + 20 * k, nper=10, L=8.0, grid=(16, 16, 18),
+                                    angle_params=ANGLES) for k in range(2)]
+    elif kind == "curand_noise":
+        specs = replicas()
+        opts["rng"] = 1
+    else:
+        specs = [synth.small_system(seed=70 + k, n_chains=80, nper=8, L=8.0, grid=(16, 16, 16), integrator="EM")
+                 for k in range(2)]
+    alone = []
+    for s in specs:
+        with make(s, **opts) as b:
+            b.step(12)
+            alone.append(b.positions())
+    boxes = [make(s, **opts) for s in specs]
+    with tild_b200.Batch() as batch:
+        for b in boxes:
+            batch.add(b)
+        batch.step(12)
+    for b, x in zip(boxes, alone):
+        assert np.array_equal(b.positions(), x)
+        b.close()
