@@ -120,8 +120,8 @@ int tild_box_set_angles(tild_box *box, int64_t nangles, const int64_t *triples, 
  *   "sort_interval"  steps between spatial re-sorts of the particle arrays (0 = never)
  *   "autotune"       1 = at endBox, time the force evaluation with particle tiles of
  *                    half, the same and twice the bricks per CTA, each with a staged and a
- *                    direct gather, then the deposit's tiles (the same, twice and four
- *                    times the bricks; one thread per particle or CTAs of 64, 128, 256),
+ *                    direct gather, then the deposit's tiles (the same, twice, four and
+ *                    eight times the bricks; one thread per particle or CTAs of 64, 128, 256),
  *                    and keep the fastest (default 0)
  *   "direct_gather"  1 = the particle gather reads each stencil through L1/L2 instead of
  *                    staging its tile's box in shared memory (default 0; same bits)

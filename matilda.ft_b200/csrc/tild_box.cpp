@@ -2159,14 +2159,14 @@ void Box::autotuneTiles()
         }
     }
     tiles = pick;
-    // the deposit's tiles: the same, twice and four times the bricks (a larger tile zeroes
-    // and flushes fewer halo points per particle, but sums in FP32 once its particle count
-    // leaves the int32 range of the fixed-point box), each with one thread per particle and
-    // with CTAs of 64, 128 and 256 threads (smaller CTAs, more of them per SM)
+    // the deposit's tiles: the same, twice, four and eight times the bricks (a larger tile
+    // zeroes and flushes fewer halo points per particle, but its fixed-point scale drops,
+    // and past four times the count bound it sums in FP32), each with one thread per
+    // particle and with CTAs of 64, 128 and 256 threads (smaller CTAs, more of them per SM)
     if (!depositCodes || !depositThreads) {
         TileCfg dpick = dtiles;
         std::vector<TileCfg> dc;
-        for (int c = tiles.codes; c <= std::min(64, 4 * tiles.codes); c *= 2) {
+        for (int c = tiles.codes; c <= std::min(64, 8 * tiles.codes); c *= 2) {
             if (depositCodes && c != depositCodes) continue;
             for (int thr : {0, 64, 128, 256}) {
                 if (depositThreads && thr != depositThreads) continue;

@@ -121,17 +121,19 @@ __device__ __forceinline__ float field_coef(uint32_t dm, unsigned dq, int f, flo
 }
 
 // Shared-memory accumulation of one contribution.  Deterministic mode: 64-bit fixed
-// point (kFixScale), exact and order-independent.  Fast mode: 32-bit fixed point
-// (kTileFix per unit, integer shared atomics, about 1.2x the speed of FP32 ones) in tiles
-// whose particle count keeps every sum inside int32 (`ia`), else FP32 atomics.  A
-// contribution is rounded once to 2^-24 (3e-8 absolute), below the FP32 rounding of a
-// running sum of order one.
-constexpr float kTileFix = 16777216.f;   // 2^24 per unit weight
+// point (kFixScale), exact and order-independent.  Fast mode: 32-bit fixed point (integer
+// shared atomics, about twice the speed of FP32 ones) in tiles whose particle count keeps
+// every sum inside int32 (`ia`), else FP32 atomics.  The scale is 2^24 per unit weight for
+// tiles within the count bound int_tile_max (a contribution rounded once to 3e-8, below the
+// FP32 rounding of a running sum of order one), 2^23 or 2^22 for tiles of up to two or four
+// times as many particles (1.2e-7 at most), so that large deposit tiles stay in integers.
+constexpr int kTileFixLog2 = 24;
+constexpr int kTileFixSteps = 2;   // the scale may drop to 2^22
 template <bool FIXED>
-__device__ __forceinline__ void smem_add(float *tf, unsigned long long *tu, int i, float v, bool ia)
+__device__ __forceinline__ void smem_add(float *tf, unsigned long long *tu, int i, float v, bool ia, float tfix)
 {
     if (FIXED) atomicAdd(tu + i, (unsigned long long)__double2ll_rn((double)v * kFixScale));
-    else if (ia) atomicAdd(reinterpret_cast<int *>(tf) + i, __float2int_rn(v * kTileFix));
+    else if (ia) atomicAdd(reinterpret_cast<int *>(tf) + i, __float2int_rn(v * tfix));
     else atomicAdd(tf + i, v);
 }
 
@@ -147,7 +149,7 @@ __device__ __forceinline__ void smem_add_signed(float *tf, unsigned long long *t
 #pragma unroll
         for (int f = 0; f < NC; f++)
             if (sgn[f]) atomicAdd(tu + f * V + i, (unsigned long long)(sgn[f] > 0 ? k : -k));
-    } else if (IB) {   // v carries the scale kTileFix already (see the caller)
+    } else if (IB) {   // v carries the tile's fixed-point scale already (see the caller)
         const int k = __float2int_rn(v);
 #pragma unroll
         for (int f = 0; f < NC; f++)
@@ -201,7 +203,13 @@ __device__ __forceinline__ void deposit_body(const Geom &g, int N, int quirk4, i
     const bool staged = tc.start && E[0] <= kMaxBoxEdge && E[1] <= kMaxBoxEdge && E[2] <= kMaxBoxEdge &&
                         Vl * nfields * (long long)esz <= cap_bytes;
     const int V = staged ? (int)Vl : 0, E0 = E[0], E01 = E[0] * E[1];
-    const bool ia = !FIXED && staged && (b1 - b0) <= int_tile_max;   // int32 fixed-point box
+    // int32 fixed-point box: the scale 2^(24 - k) with the least k <= 2 whose count bound
+    // int_tile_max 2^k covers the tile (powers of two: exact scalings)
+    int ksh = 0;
+    while (ksh < kTileFixSteps && (long long)(b1 - b0) > ((long long)int_tile_max << ksh)) ksh++;
+    const bool ia = !FIXED && staged && (long long)(b1 - b0) <= ((long long)int_tile_max << ksh);
+    const float tfix = __int_as_float((127 + kTileFixLog2 - ksh) << 23);      // 2^(24 - k)
+    const float tinv = __int_as_float((127 - kTileFixLog2 + ksh) << 23);      // 2^-(24 - k)
     float *tf = reinterpret_cast<float *>(smraw);
     unsigned long long *tu = reinterpret_cast<unsigned long long *>(smraw);
     if (staged) {
@@ -281,9 +289,9 @@ __device__ __forceinline__ void deposit_body(const Geom &g, int N, int quirk4, i
                 sgn[f] = cf[f] == 0.f ? 0 : (cf[f] == c0 ? 1 : (cf[f] == -c0 ? -1 : 2));
                 general = general || sgn[f] == 2;
             }
-            // in an int32 box the conversion's scale 2^24 rides on the coefficient: an exact
-            // power-of-two scaling, so c0 2^24 w rounds to the same value as (c0 w) 2^24
-            const float c0v = (!FIXED && ia) ? c0 * kTileFix : c0;
+            // in an int32 box the conversion's scale rides on the coefficient: an exact
+            // power-of-two scaling, so c0 2^s w rounds to the same value as (c0 w) 2^s
+            const float c0v = (!FIXED && ia) ? c0 * tfix : c0;
             // Wx * (Wy * Wz), then the coefficient: the association of the unstaged path,
             // so that the deterministic mode's fixed-point values do not depend on staging
             auto points = [&](auto int_box, auto gen) {
@@ -300,7 +308,7 @@ __device__ __forceinline__ void deposit_body(const Geom &g, int N, int quirk4, i
                             if (GN) {
 #pragma unroll
                                 for (int f = 0; f < NC; f++)
-                                    if (cf[f] != 0.f) smem_add<FIXED>(tf, tu, f * V + row + a, cf[f] * w, IB);
+                                    if (cf[f] != 0.f) smem_add<FIXED>(tf, tu, f * V + row + a, cf[f] * w, IB, tfix);
                             } else {
                                 smem_add_signed<FIXED, IB, NC>(tf, tu, V, row + a, c0v * w, sgn);
                             }
@@ -366,8 +374,8 @@ __device__ __forceinline__ void deposit_body(const Geom &g, int N, int quirk4, i
                 float a0 = tf[(2 * t) * V + v];
                 float a1 = (2 * t + 1 < nfields) ? tf[(2 * t + 1) * V + v] : 0.f;
                 if (ia) {
-                    a0 = (float)__float_as_int(a0) * (1.f / kTileFix);
-                    a1 = (float)__float_as_int(a1) * (1.f / kTileFix);
+                    a0 = (float)__float_as_int(a0) * tinv;
+                    a1 = (float)__float_as_int(a1) * tinv;
                 }
                 if (a0 != 0.f && a1 != 0.f) atomicAdd(dep + t * g.M + m, make_float2(a0, a1));
                 else if (a0 != 0.f) atomicAdd(&dep[t * g.M + m].x, a0);

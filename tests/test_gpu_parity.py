@@ -213,6 +213,26 @@ def test_forces_and_energies_match_oracle_deposit_tiles(qscale, codes):
         assert abs(e - r) <= 1e-5 * max(abs(r), 1e-12) + 1e-9, (e, r)
 
 
+@pytest.mark.parametrize("n_chains", [120, 300])
+def test_large_deposit_tiles_match_oracle(n_chains):
+    """Deposit tiles of 64 bricks on a dense coacervate-like system: their particle counts
+    exceed the int32 box's count bound at 2^24 per unit weight, so the box sums at 2^23 or
+    2^22 (or in FP32 beyond); forces and energies against the FP64 oracle stay within 1e-5."""
+    pots = [dict(kind="gaussian", I="all", J="all", A=2.0, sigma=0.7), dict(kind="charges", lB=1.0, sigma=0.5)]
+    spec = synth.small_system(seed=31, order=3, charges=True, n_chains=n_chains, nper=10, L=10.0, grid=(20, 20, 20),
+                              pots=pots)
+    sysm = spec_to_system(spec)
+    fref, _ = oracle.forces(sysm, prec=64)
+    dens, _, _ = oracle.densities(sysm)
+    ref = oracle.pair_energies(sysm, dens)
+    with make_box(spec, deposit_codes=64) as b:
+        f = b.forces()
+        t = b.thermo()
+    assert force_error(f, fref) <= 1e-5
+    for e, r in zip(t["potentials"], ref):
+        assert abs(e - r) <= 1e-5 * max(abs(r), 1e-12) + 1e-9, (e, r)
+
+
 @pytest.mark.parametrize("order", [2, 3, 4])
 def test_direct_gather_is_invisible(order):
     """Reading every stencil through L1/L2 instead of the tile's staged box changes only

@@ -20,19 +20,29 @@ from tild_b200 import synth
 pytestmark = pytest.mark.gpu
 
 
-def test_c2_forces_and_energies_match_the_fp64_oracle():
+@pytest.fixture(scope="module")
+def c2_reference():
     spec = synth.config_c2()
     assert spec.N == 2097152 and list(spec.grid) == [192, 192, 192]
     sysm = spec_to_system(spec)
     fref, inter = oracle.forces(sysm, prec=64)
-    with tild_b200.box_from_spec(spec, options={"write_files": 0}) as b:
+    return spec, sysm, fref, inter
+
+
+# the density rule's deposit tiles (8 bricks: int32 boxes at 2^24 per unit weight), and the
+# 32-brick tiles the autotuner picks on this workload (about 600 particles each: 2^23)
+@pytest.mark.parametrize("deposit_codes", [0, 32])
+def test_c2_forces_and_energies_match_the_fp64_oracle(c2_reference, deposit_codes):
+    spec, sysm, fref, inter = c2_reference
+    with tild_b200.box_from_spec(spec, options={"write_files": 0, "deposit_codes": deposit_codes}) as b:
         b.command("endBox")
         f = b.forces()
         th = b.thermo()
     mag = np.linalg.norm(fref, axis=1)
     den = np.maximum(mag, np.sqrt(np.mean(mag ** 2)))
     err = np.linalg.norm(f - fref, axis=1) / den
-    print("c2 force error percentiles 50/99/99.9/max:", np.percentile(err, [50, 99, 99.9]), err.max())
+    print("c2 (deposit_codes %d) force error percentiles 50/99/99.9/max:" % deposit_codes,
+          np.percentile(err, [50, 99, 99.9]), err.max())
     assert err.max() <= 1e-5
     pe = oracle.pair_energies(sysm, inter["dens"])
     assert len(th["potentials"]) == 2
