@@ -14,6 +14,9 @@ with CUDA events on the box's stream, max over ranks.  The per-step working set
 is needed between steps.
 e2e: the same metric through the C ABI for one job of S steps: positions uploaded from
 pinned host memory, S steps, positions read back; copies inside the timed region.
+batched: C3, 64 uneven diblock replicas stepped as one batch (every stage of a step one
+kernel launch over all replicas), beside the same jobs one after another and in the job
+pool.  served: C5, a Poisson job stream through the job pool, with p50/p99 latency.
 --impl reference: MATILDA.FT's own CUDA build (the unmodified sources compiled into
 oracle/_ref by oracle/ref_harness/Makefile) on the same workload, GPU and metric, rank 0
 only, plus its plain per-job form on samples of the batched and served job lists; when
