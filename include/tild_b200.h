@@ -120,9 +120,10 @@ int tild_box_set_angles(tild_box *box, int64_t nangles, const int64_t *triples, 
  *   "sort_interval"  steps between spatial re-sorts of the particle arrays (0 = never)
  *   "autotune"       1 = at endBox, time the force evaluation with particle tiles of
  *                    half, the same and twice the bricks per CTA, each with a staged and a
- *                    direct gather, then the deposit's tiles (the same, twice, four and
- *                    eight times the bricks; one thread per particle or CTAs of 64, 128, 256),
- *                    and keep the fastest (default 0)
+ *                    direct gather (staged cubic ones also with 64 more threads), then
+ *                    the deposit's tiles (the same, twice, four and eight times the
+ *                    bricks; one thread per particle or CTAs of 64, 128, 256), and keep
+ *                    the fastest (default 0)
  *   "direct_gather"  1 = the particle gather reads each stencil through L1/L2 instead of
  *                    staging its tile's box in shared memory (default 0; same bits)
  *   "tile_codes"     fixed bricks per particle tile, a power of two <= 64 (0 = from the
@@ -130,6 +131,8 @@ int tild_box_set_angles(tild_box *box, int64_t nangles, const int64_t *triples, 
  *   "deposit_codes"  fixed bricks per deposit tile, a power of two in [8, 64] (0 = chosen)
  *   "deposit_threads" fixed deposit CTA size, a multiple of 32 in [64, 512] (0 = one
  *                    thread per particle of a typical tile)
+ *   "gather_threads" fixed CTA size of the particle gather, a multiple of 32 in [64, 448]
+ *                    (0 = about one thread per particle of a typical tile; same bits)
  * Must precede endBox except "write_files", "echo", "stage_timing" and "sort_interval". */
 int tild_box_set_option(tild_box *box, const char *key, int64_t value);
 

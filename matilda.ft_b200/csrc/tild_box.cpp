@@ -194,6 +194,10 @@ void Box::setOption(const std::string &key, int64_t v)
         if (v != 0 && (v < 64 || v > 512 || v % 32)) fail(TILD_ERR_ARG, "deposit_threads must be 0 or a multiple of 32 in [64, 512]");
         depositThreads = (int)v;
     }
+    else if (key == "gather_threads") {
+        if (v != 0 && (v < 64 || v > 448 || v % 32)) fail(TILD_ERR_ARG, "gather_threads must be 0 or a multiple of 32 in [64, 448]");
+        gatherThreads = (int)v;
+    }
     else if (key == "sort_interval") {
         if (v < 0) fail(TILD_ERR_ARG, "sort_interval must be >= 0");
         sortInterval = (int)v;
@@ -2140,10 +2144,19 @@ void Box::autotuneTiles()
         }
         return best;
     };
+    // particle tiles of half, the same and twice the bricks, staged and direct; staged ones
+    // also with 64 more threads (the cubic tile gather spreads a tile's particles over all
+    // its warps: shorter chains of gathers per warp, fewer CTAs per SM)
     std::vector<TileCfg> cands;
     for (int c : {tiles.codes / 2, tiles.codes, tiles.codes * 2})
         if (c >= 1 && c <= 64)
-            for (bool direct : {false, true}) cands.push_back(tileGeometry(c, direct));
+            for (bool direct : {false, true}) {
+                cands.push_back(tileGeometry(c, direct));
+                if (!direct && pmeorder == 3 && !gatherThreads && cands.back().threads + 64 <= 448) {
+                    cands.push_back(cands.back());
+                    cands.back().threads += 64;
+                }
+            }
     cudaEvent_t e0, e1;
     ck(cudaEventCreate(&e0), "event");
     ck(cudaEventCreate(&e1), "event");
@@ -2219,6 +2232,7 @@ void Box::checkDeviceErrors()
 TileCfg Box::tileCfg() const
 {
     TileCfg t = tiles;
+    if (gatherThreads) t.threads = gatherThreads;
     t.start = sortedTiles ? sortW.start : nullptr;
     return t;
 }
@@ -2554,7 +2568,7 @@ std::string Box::describe() const
       << ", \"doCharges\": " << (doCharges ? "true" : "false") << ", \"MAXBONDS\": " << MAXBONDS
       << ", \"nBonds\": " << nBondsTot << ", \"nAngles\": " << nAnglesTot << ", \"MAXANGLES\": " << MAXANGLES
       << ", \"datFileName\": " << q(datFileName) << ", \"tiles\": {\"codes\": " << tiles.codes
-      << ", \"threads\": " << tiles.threads << ", \"gather\": \"" << (tiles.direct ? "direct" : "staged")
+      << ", \"threads\": " << (gatherThreads ? gatherThreads : tiles.threads) << ", \"gather\": \"" << (tiles.direct ? "direct" : "staged")
       << "\", \"deposit_codes\": " << dtiles.codes << ", \"deposit_threads\": " << depTileCfg().threads
       << ", \"autotuned\": " << (autotune ? "true" : "false")
       << ", \"tuned_ms\": " << tunedMs << "}, \"trajFreq\": " << trajFreq

@@ -288,6 +288,7 @@ private:
     int depositCodes = 0;           // option "deposit_codes": fixed deposit tile bricks (0: chosen)
     int depositThreads = 0;         // option "deposit_threads": deposit CTA size (0: one thread per particle)
     int tileCodes = 0;              // option "tile_codes": fixed particle-pass tile bricks (0: from the density)
+    int gatherThreads = 0;          // option "gather_threads": tile-gather CTA size (0: about one thread per particle)
     TileCfg tileCfg() const;
     TileCfg depTileCfg() const;
     void pairedGhosts(const TileCfg &t, int *gl, int *gh) const;   // ghost layers the tiles' boxes reach

@@ -814,8 +814,16 @@ __device__ __forceinline__ void gather_paired_body(const Geom &g, const Particle
     const int lane = threadIdx.x & 31;
     bool waited = false;
     for (int c0 = r0; c0 < r1; c0 += blockDim.x) {
-        const int p = c0 + threadIdx.x;
-        const bool act = p < r1;
+        int p = c0 + threadIdx.x;
+        bool act = p < r1;
+        if constexpr (P == 3) {
+            // the pass's particles spread evenly over the warps, k consecutive ones each, so
+            // that no warp holds more rounds of box gathers than it must
+            const int cnt = min(r1 - c0, (int)blockDim.x), nw = (int)(blockDim.x >> 5);
+            const int k = (cnt + nw - 1) / nw;
+            p = c0 + (int)(threadIdx.x >> 5) * k + lane;
+            act = lane < k && p < c0 + cnt;
+        }
         float x[3] = {0.f, 0.f, 0.f};
         uint32_t fl = 0u;
         float qp = 0.f;

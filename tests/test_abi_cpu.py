@@ -157,6 +157,21 @@ def test_bond_errors():
     assert "MAXBONDS" in str(e.value)
 
 
+@pytest.mark.parametrize("key,good,bad", [
+    ("tile_codes", 8, 3), ("deposit_codes", 16, 4), ("deposit_threads", 128, 48), ("gather_threads", 160, 512),
+])
+def test_tile_options_checked(key, good, bad):
+    """Tile and CTA-size options take their documented ranges (0 = chosen) and refuse the
+    rest with TILD_ERR_ARG before any GPU work."""
+    b = tild_b200.Box(0)
+    b.set_option(key, good)
+    b.set_option(key, 0)
+    with pytest.raises(tild_b200.TildError) as e:
+        b.set_option(key, bad)
+    assert e.value.code == 1 and key in str(e.value)
+    b.close()
+
+
 def test_synth_data_round_trip(tmp_path):
     """The synthetic writer's file parses back to the same arrays through the library."""
     s = synth.config_c2(scale=1e-3)

@@ -285,6 +285,26 @@ def test_spatial_sort_is_invisible_tile_gather():
             assert np.array_equal(a, b2)
 
 
+@pytest.mark.parametrize("order", [2, 3])
+def test_gather_threads_are_invisible(order):
+    """The tile gather's CTA size (option gather_threads) decides how a tile's particles
+    are spread over warps and passes, not what a particle's sum is: forces and a trajectory
+    with re-sorts are bit-identical from 64 to 448 threads (tiles of 1 and 4 bricks on a
+    scaled coacervate, so that passes hold both full and ragged warps)."""
+    spec = synth.config_c2(scale=0.03)
+    spec.order = order
+    for codes in (1, 4):
+        outs = []
+        for thr in (0, 64, 160, 448):
+            with make_box(spec, deterministic=1, tile_codes=codes, gather_threads=thr) as b:
+                f = b.forces()
+                b.step(12)
+                outs.append((f, b.positions(), b.forces()))
+        for o in outs[1:]:
+            for a, b2 in zip(outs[0], o):
+                assert np.array_equal(a, b2)
+
+
 def test_spatial_sort_is_invisible():
     """Re-sorting the particle arrays changes only memory order: in deterministic mode the
     trajectory is bit-identical with no sort, a sort every 3 steps and every step."""
