@@ -680,30 +680,41 @@ __global__ void __launch_bounds__(256) k_sk_z(Geom g, FftLine lz, const float2 *
 // completion of both half spectra), one complex inverse FFT, real -> field 2t,
 // imaginary -> field 2t+1; then float4 records (x, y, z, 0) per force group.  A block
 // takes L lines of every field: all rows are staged at once, every pair is transformed
-// in one pass over npair*L lines, and the records are written from the transform.
+// in one pass over npair*L lines, and the records are written from the transform.  The
+// transform's lines are interleaved (element x of line j at x*ls + j, ls = npair*L made
+// odd): each radix stage then reads and writes consecutive lines of one element in
+// consecutive lanes, and the record writes, which step along x, read rows ls apart --
+// distinct bank pairs for every half warp, where lines stored one after another put the
+// first stages' outputs R complex values apart (a 16-way conflict at R = 8).
+__host__ __device__ inline int xinv_pitch(int nf, int L)
+{
+    const int lines = ((nf + 1) / 2) * L;
+    return lines | 1;
+}
+
 __device__ __forceinline__ void xinv_body(const Geom &g, const FftLine &lx, int nfg, const float2 *__restrict__ Hg,
                                           float4 *__restrict__ rec, const RecLayout &rl, int L, unsigned vbx)
 {
     extern __shared__ __align__(16) float2 sm[];
     const int n = g.nx, nf = 3 * nfg, npair = (nf + 1) / 2, nxh = g.nxh, hp = g.hp;
-    const int lines = npair * L;
-    const int stsz = nf * L * hp, bsz = lines * n;
+    const int lines = npair * L, ls = xinv_pitch(nf, L);
+    const int stsz = nf * L * hp, bsz = n * ls;
     // St receives 16-byte cp.async copies: start it on an even complex offset
     float2 *A = sm, *St = sm + ((bsz + 1) & ~1), *tw = St + (stsz > bsz ? stsz : bsz);
     const long long nlines = (long long)g.ny * g.nz;
     const long long line0 = (long long)vbx * L;
     const int lv = (int)min((long long)L, nlines - line0);
-    const FastDiv dn = make_fastdiv_dev(n), dL = make_fastdiv_dev(L);
+    const FastDiv dn = make_fastdiv_dev(n), dL = make_fastdiv_dev(L), dlines = make_fastdiv_dev(lines);
     for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = lx.tw[t];
     // consecutive lines are consecutive rows of pitch hp: stage every field's rows
     for (int f = 0; f < nf; f++)
         tile_load_async(St + f * L * hp, hp, Hg + f * g.hstride + line0 * hp, hp, lv, hp, nxh);
     cp_async_wait_all();
     __syncthreads();
-    // line (pr, l) of A holds pair pr of line l
-    for (int e = threadIdx.x; e < bsz; e += blockDim.x) {
-        const int ln = (int)fdiv((unsigned)e, dn), x = e - ln * n;
-        const int pr = (int)fdiv((unsigned)ln, dL), l = ln - pr * L;
+    // transform line j = pr * L + l holds pair pr of line l; element x of it sits at x*ls + j
+    for (int e = threadIdx.x; e < n * lines; e += blockDim.x) {
+        const int x = (int)fdiv((unsigned)e, dlines), j = e - x * lines;
+        const int pr = (int)fdiv((unsigned)j, dL), l = j - pr * L;
         const int f1 = 2 * pr, f2 = 2 * pr + 1;
         float2 v = make_float2(0.f, 0.f);
         if (l < lv) {
@@ -721,13 +732,13 @@ __device__ __forceinline__ void xinv_body(const Geom &g, const FftLine &lx, int 
             }
             v = make_float2(g1.x - g2.y, g1.y + g2.x);
         }
-        A[e] = v;
+        A[x * ls + j] = v;
     }
     __syncthreads();
-    const float2 *R = fft_lines<true>(A, St, lines, n, 1, lx, tw, false, dL);
+    const float2 *R = fft_lines<true>(A, St, lines, 1, ls, lx, tw, true, dlines);
     // field k is component k % 2 of pair k / 2
     auto comp = [&](int k, int l, int x) {
-        const float2 v = R[((k >> 1) * L + l) * n + x];
+        const float2 v = R[x * ls + (k >> 1) * L + l];
         return (k & 1) ? v.y : v.x;
     };
     if (rl.paired) {
@@ -913,18 +924,19 @@ cudaError_t launch_kspace_z(const Geom &g, const FftLine &lz, const KSpace &ks, 
     return cudaGetLastError();
 }
 
-// lines per block of the x inverse pass (about 4k complex points) and its shared memory
+// lines per block of the x inverse pass (at most 4k complex points: three blocks per SM
+// on a 192-point line) and its shared memory
 static int xinv_lines(const Geom &g, int nfg)
 {
     const int npair = (3 * nfg + 1) / 2;
-    const int L = (4096 + npair * g.nx - 1) / (npair * g.nx);
+    const int L = 4096 / (npair * g.nx);
     return L < 1 ? 1 : (L > 16 ? 16 : L);
 }
 
 static size_t xinv_smem(const Geom &g, int nfg, int L)
 {
-    const int nf = 3 * nfg, npair = (nf + 1) / 2;
-    const size_t bsz = (size_t)npair * L * g.nx, stsz = (size_t)nf * L * g.hp;
+    const int nf = 3 * nfg;
+    const size_t bsz = (size_t)g.nx * xinv_pitch(nf, L), stsz = (size_t)nf * L * g.hp;
     return (((bsz + 1) & ~(size_t)1) + std::max(bsz, stsz) + g.nx) * sizeof(float2);
 }
 
