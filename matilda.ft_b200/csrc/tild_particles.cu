@@ -925,20 +925,44 @@ __device__ __forceinline__ void gather_paired_body(const Geom &g, const Particle
                             }
                         }
                 }
-                // ((s0 + s1) + (s2 + s3)) + ((s4 + s5) + (s6 + s7)) over the quarter's lanes
-#pragma unroll
-                for (int o = 1; o < 8; o <<= 1) {
-                    s0 = __fadd2_rn(s0, make_float2(__shfl_xor_sync(full, s0.x, o), __shfl_xor_sync(full, s0.y, o)));
-                    s1 = __fadd2_rn(s1, make_float2(__shfl_xor_sync(full, s1.x, o), __shfl_xor_sync(full, s1.y, o)));
-                    if (NFG == 2)
-                        s2 = __fadd2_rn(s2, make_float2(__shfl_xor_sync(full, s2.x, o), __shfl_xor_sync(full, s2.y, o)));
-                }
-                // the particle's own lane takes the sums of its quarter
+                // ((s0 + s1) + (s2 + s3)) + ((s4 + s5) + (s6 + s7)) over the quarter's lanes, as a
+                // reduce-scatter: at each level a lane keeps part of its values, adds its
+                // partner's partial sums of that part (a + b = b + a: every node of the tree
+                // gives the same bits in either lane) and passes on the rest, so each level
+                // shuffles only the values it halves; the sums end spread over the quarter
                 const int from = 8 * myq;
-                const float2 t0 = make_float2(__shfl_sync(full, s0.x, from), __shfl_sync(full, s0.y, from));
-                const float2 t1 = make_float2(__shfl_sync(full, s1.x, from), __shfl_sync(full, s1.y, from));
-                float2 t2 = make_float2(0.f, 0.f);
-                if (NFG == 2) t2 = make_float2(__shfl_sync(full, s2.x, from), __shfl_sync(full, s2.y, from));
+                const bool b0 = lane & 1, b1 = (lane >> 1) & 1, b2 = (lane >> 2) & 1;
+                float2 t0, t1, t2 = make_float2(0.f, 0.f);
+                if (NFG == 2) {
+                    // values s0.x s0.y s1.x | s1.y s2.x s2.y: lane bit 0 picks a half, bit 1 two
+                    // of its three or the third, bit 2 one of those two
+                    const float a[6] = {s0.x, s0.y, s1.x, s1.y, s2.x, s2.y};
+                    float k3[3];
+#pragma unroll
+                    for (int j = 0; j < 3; j++)
+                        k3[j] = __fadd_rn(b0 ? a[j + 3] : a[j], __shfl_xor_sync(full, b0 ? a[j] : a[j + 3], 1));
+                    const float r1 = __shfl_xor_sync(full, b1 ? k3[0] : k3[2], 2);
+                    const float r2 = __shfl_xor_sync(full, k3[1], 2);
+                    const float c0 = __fadd_rn(b1 ? k3[2] : k3[0], r1), c1 = __fadd_rn(k3[1], r2);
+                    const float fin = __fadd_rn(b1 ? c0 : (b2 ? c1 : c0),
+                                                __shfl_xor_sync(full, b1 ? c0 : (b2 ? c0 : c1), 4));
+                    // the particle's own lane takes the sums of its quarter: s0.x at quarter
+                    // lane 0, s0.y 4, s1.x 2, s1.y 1, s2.x 5, s2.y 3
+                    t0 = make_float2(__shfl_sync(full, fin, from), __shfl_sync(full, fin, from + 4));
+                    t1 = make_float2(__shfl_sync(full, fin, from + 2), __shfl_sync(full, fin, from + 1));
+                    t2 = make_float2(__shfl_sync(full, fin, from + 5), __shfl_sync(full, fin, from + 3));
+                } else {
+                    // values s0.x s0.y | s1.x: bit 0 picks the pair or the single value, bit 1
+                    // one of the pair
+                    const float k0 = __fadd_rn(b0 ? s1.x : s0.x, __shfl_xor_sync(full, b0 ? s0.x : s1.x, 1));
+                    const float k1 = __fadd_rn(s0.y, __shfl_xor_sync(full, s0.y, 1));
+                    const float m = __fadd_rn(b0 ? k0 : (b1 ? k1 : k0),
+                                              __shfl_xor_sync(full, b0 ? k0 : (b1 ? k0 : k1), 2));
+                    const float fin = __fadd_rn(m, __shfl_xor_sync(full, m, 4));
+                    // s0.x at quarter lane 0, s0.y 2, s1.x 1
+                    t0 = make_float2(__shfl_sync(full, fin, from), __shfl_sync(full, fin, from + 2));
+                    t1 = make_float2(__shfl_sync(full, fin, from + 1), 0.f);
+                }
                 if (myround == rd) {
                     res0 = t0;
                     res1 = t1;
