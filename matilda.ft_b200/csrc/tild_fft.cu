@@ -712,8 +712,9 @@ __device__ __forceinline__ void xinv_body(const Geom &g, const FftLine &lx, int 
     cp_async_wait_all();
     __syncthreads();
     // transform line j = pr * L + l holds pair pr of line l; element x of it sits at x*ls + j
+    // (lanes step along x: contiguous reads of the staged rows, writes ls apart)
     for (int e = threadIdx.x; e < n * lines; e += blockDim.x) {
-        const int x = (int)fdiv((unsigned)e, dlines), j = e - x * lines;
+        const int j = (int)fdiv((unsigned)e, dn), x = e - j * n;
         const int pr = (int)fdiv((unsigned)j, dL), l = j - pr * L;
         const int f1 = 2 * pr, f2 = 2 * pr + 1;
         float2 v = make_float2(0.f, 0.f);
