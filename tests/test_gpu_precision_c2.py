@@ -30,11 +30,13 @@ def c2_reference():
 
 
 # the density rule's deposit tiles (8 bricks: int32 boxes at 2^24 per unit weight), and the
-# 32-brick tiles the autotuner picks on this workload (about 600 particles each: 2^23)
-@pytest.mark.parametrize("deposit_codes", [0, 32])
-def test_c2_forces_and_energies_match_the_fp64_oracle(c2_reference, deposit_codes):
+# 32- and 64-brick tiles the autotuner picks on this workload (about 600 and 1,200 particles
+# each: 2^23 and 2^22, FP32 for the rare tile past four times the count bound)
+@pytest.mark.parametrize("deposit_codes,deposit_threads", [(0, 0), (32, 0), (64, 512)])
+def test_c2_forces_and_energies_match_the_fp64_oracle(c2_reference, deposit_codes, deposit_threads):
     spec, sysm, fref, inter = c2_reference
-    with tild_b200.box_from_spec(spec, options={"write_files": 0, "deposit_codes": deposit_codes}) as b:
+    opts = {"write_files": 0, "deposit_codes": deposit_codes, "deposit_threads": deposit_threads}
+    with tild_b200.box_from_spec(spec, options=opts) as b:
         b.command("endBox")
         f = b.forces()
         th = b.thermo()
