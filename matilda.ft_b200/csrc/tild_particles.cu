@@ -771,14 +771,22 @@ __device__ __forceinline__ void gather_paired_body(const Geom &g, const Particle
                                                    const CUtensorMap *mapA, const CUtensorMap *mapB,
                                                    int *__restrict__ err, unsigned bx, bool maps_in_global)
 {
-    extern __shared__ __align__(16) unsigned char smraw[];
+    // All of the CTA's shared memory is dynamic (paired_smem): plane A's box, plane B's, the
+    // dealing table (a lane index per thread) and the barrier, with no static variables, so
+    // that the window starts 128-byte aligned for the TMA boxes and no alignment slack is
+    // spent (an 8-brick tile's box then fits four CTAs per SM).  Should the window ever
+    // start unaligned, the CTA loads no box and leaves its particles to the integrator
+    // pass's global gather: slower, the same forces.
+    extern __shared__ __align__(128) unsigned char smbox[];
     const int te0 = tc.te[0], te1 = tc.te[1], te2 = tc.te[2];
     const int te01 = te0 * te1, V = te01 * te2;
-    unsigned char *al = smraw + ((128u - (smem_u32(smraw) & 127u)) & 127u);
-    float4 *boxA = reinterpret_cast<float4 *>(al);
-    float2 *boxB = reinterpret_cast<float2 *>(al + (((size_t)V * 16 + 127) & ~(size_t)127));
-    __shared__ int deal_src[kPartThreadsMax];
-    __shared__ __align__(8) unsigned long long bar;
+    const size_t offB = ((size_t)V * 16 + 127) & ~(size_t)127;
+    const size_t offD = offB + (NFG == 2 ? (((size_t)V * 8 + 15) & ~(size_t)15) : 0);
+    float4 *boxA = reinterpret_cast<float4 *>(smbox);
+    float2 *boxB = reinterpret_cast<float2 *>(smbox + offB);
+    unsigned char *deal_src = smbox + offD;
+    unsigned long long &bar = *reinterpret_cast<unsigned long long *>(smbox + offD + kPartThreadsMax);
+    const bool aligned = (smem_u32(smbox) & 127u) == 0u;
     const ParticleParams &pp = *ppd;
     const long long step = *d_step;
     const float *__restrict__ Xc = (step & 1) ? X1 : X0;
@@ -789,7 +797,7 @@ __device__ __forceinline__ void gather_paired_body(const Geom &g, const Particle
     int lo[3], span[3], E[3];
     tile_box<P>(tc, nn, lo, span, E, bx);
     // 1. the box: one TMA load per plane, coordinates in the padded grid (lo + gl >= 0)
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && aligned) {
         mbar_init(&bar);
         if (maps_in_global) {   // descriptors in a device table: acquire them for the tensor-map proxy
             asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(mapA) : "memory");
@@ -843,7 +851,7 @@ __device__ __forceinline__ void gather_paired_body(const Geom &g, const Particle
                                stencil_fast<P>(x[2], g, 2, pp.quirk4, Wz)};
 #pragma unroll
             for (int j = 0; j < 3; j++) d[j] = wrapi(gs[j] - lo[j], nn[j]);
-            inbox = d[0] <= span[0] && d[1] <= span[1] && d[2] <= span[2];
+            inbox = aligned && d[0] <= span[0] && d[1] <= span[1] && d[2] <= span[2];
         } else {
 #pragma unroll
             for (int i = 0; i <= P; i++) Wx[i] = Wy[i] = Wz[i] = 0.f;
@@ -880,7 +888,7 @@ __device__ __forceinline__ void gather_paired_body(const Geom &g, const Particle
             }
             __syncwarp();
             // 3. the box has landed (bounded wait: a copy that never completes is recorded)
-            if (!waited) {
+            if (!waited && aligned) {
                 if (!mbar_wait(&bar, 0u)) {
                     if (lane == 0) atomicAdd(err, 1);
                     mbar_wait(&bar, 0u);
@@ -1012,7 +1020,7 @@ __device__ __forceinline__ void gather_paired_body(const Geom &g, const Particle
                 Wz[i] = __shfl_sync(full, Wz[i], src);
             }
             // 3. the box has landed (bounded wait: a copy that never completes is recorded)
-            if (!waited) {
+            if (!waited && aligned) {
                 if (!mbar_wait(&bar, 0u)) {
                     if (lane == 0) atomicAdd(err, 1);
                     mbar_wait(&bar, 0u);
@@ -1071,8 +1079,11 @@ __device__ __forceinline__ void gather_paired_body(const Geom &g, const Particle
     }
 }
 
+// 64 registers: an 8-brick tile's box (57 KB) then fits four CTAs of 256 threads per SM,
+// and the boxes in flight, not the registers, set the gather's pace (C2: 0.222 ->
+// 0.200 ms; 56 registers: 0.207)
 template <int P, int NFG>
-__global__ void __launch_bounds__(kPartThreadsMax, 2) k_gather_paired(Geom g, const ParticleParams *__restrict__ ppd, int N,
+__global__ void __maxnreg__(64) k_gather_paired(Geom g, const ParticleParams *__restrict__ ppd, int N,
                                                       const float *__restrict__ X0, const float *__restrict__ X1,
                                                       const uint32_t *__restrict__ pflags,
                                                       const float *__restrict__ q, RecLayout rl,
@@ -1331,11 +1342,12 @@ __global__ void k_reduce_partials(const double *partials, int nblocks, int ncols
 constexpr size_t kPartSmemMax = 128 + kPartBox * sizeof(float4);
 constexpr size_t kPairSmemMax = 200 * 1024;   // a paired box of up to 8,500 points
 
-// shared memory of the paired tile gather for boxes of te[] points
+// shared memory of the paired tile gather for boxes of te[] points: the planes' boxes, the
+// dealing table and the barrier (the layout of gather_paired_body)
 static size_t paired_smem(const int *te, int nfg)
 {
     const size_t V = (size_t)te[0] * te[1] * te[2];
-    return 128 + ((V * 16 + 127) & ~(size_t)127) + (nfg == 2 ? V * 8 : 0);
+    return ((V * 16 + 127) & ~(size_t)127) + (nfg == 2 ? ((V * 8 + 15) & ~(size_t)15) : 0) + kPartThreadsMax + 8;
 }
 
 template <int P>
